@@ -1,0 +1,327 @@
+/*
+ * tilespgemm_b200.h -- C ABI of the B200 (sm_100a) tiled SpGEMM library.
+ *
+ * Two layers are exported by libtilespgemm_b200.so:
+ *
+ *  1. Drop-in entry points with the exact signatures, struct layouts and
+ *     ownership rules of the TileSpGEMM reference (for-the-juan/RW-SpGEMM).
+ *     Each declaration names the reference function it replaces (file:line).
+ *     All of them take HOST buffers, run the work on the current CUDA device
+ *     and return host arrays that the caller frees (matrix_destroy / free).
+ *
+ *  2. A handle API (tsg_*) over device-resident tiled matrices.  Every pointer
+ *     inside tsg_tiled is a DEVICE pointer owned by the library; status codes
+ *     are returned instead of printing.  Batching, serving and the benchmarks
+ *     are built on this layer.
+ *
+ * Tile format (16x16 tiles, identical to the reference's SMatrix):
+ *   tile_ptr[tilem+1]       tiles of each tile row (row-major tile order)
+ *   tile_columnidx[T]       tile column of each tile, ascending within a row
+ *   tile_rowidx[T]          tile row of each tile
+ *   tile_nnz[T+1]           exclusive scan of nonzeros per tile (value offsets)
+ *   tile_csr_Ptr[16T]       per-tile, per-row offset (uint8) of the row's first
+ *                           nonzero; rows past the matrix edge hold the tile nnz
+ *   tile_csr_Col[nnz]       in-tile column byte; (row<<4)|col for a row-major
+ *                           "A" operand, plain col for B and C
+ *   tile_csr_Value[nnz]     FP64 values, row-major inside the tile
+ *   mask[16T]               per-row 16-bit mask, bit (15-col) set per nonzero
+ *   csc_tile_ptr/rowidx     column-major tile view (B operand)
+ */
+#ifndef TILESPGEMM_B200_H
+#define TILESPGEMM_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TSG_BLOCK_SIZE 16
+
+/* ------------------------------------------------------------------------ */
+/* Layer 1: drop-in surface of the reference                                */
+/* ------------------------------------------------------------------------ */
+
+/* Matrix container; field order and types identical to src/common.h:113-135
+ * (MAT_VAL_TYPE = double, MAT_PTR_TYPE = int) so that callers compiled
+ * against the reference header link unchanged. */
+#ifndef SMATRIX
+#define SMATRIX
+typedef struct
+{
+    int m;
+    int n;
+    int nnz;
+    int isSymmetric;
+    double *value;
+    int *columnindex;
+    int *rowpointer;
+    int tilem;
+    int tilen;
+    int *tile_ptr;
+    int *tile_columnidx;
+    int *tile_rowidx;
+    int *tile_nnz;
+    int numtile;
+    double *tile_csr_Value;
+    unsigned char *tile_csr_Col;
+    unsigned char *tile_csr_Ptr;
+    unsigned short *mask;
+    int *csc_tile_ptr;
+    int *csc_tile_rowidx;
+} SMatrix;
+#endif
+
+/* CSR -> row-major tiles with packed (row<<4)|col bytes.
+ * Replaces csr2tile_row_major, src/csr2tile.h:196-259.
+ * Reads m, n, nnz, rowpointer, columnindex, value; mallocs and fills tilem,
+ * tilen, numtile, tile_ptr, tile_columnidx, tile_rowidx, tile_nnz,
+ * tile_csr_Ptr, tile_csr_Col, tile_csr_Value, mask.  Rows must be sorted by
+ * strictly increasing column; any input error is printed and aborts the
+ * process (the reference function returns void and has no error path). */
+void csr2tile_row_major(SMatrix *matrix);
+
+/* CSR -> tiles stored in column-major tile order with in-tile CSR and plain
+ * column bytes, plus the row-major tile_ptr/tile_columnidx used by step 1.
+ * Replaces csr2tile_col_major, src/csr2tile.h:261-478. */
+void csr2tile_col_major(SMatrix *matrix);
+
+/* Tiled SpGEMM C = A*B.  A from csr2tile_row_major, B from
+ * csr2tile_col_major.  Replaces tilespgemm, src/tilespgemm-cuda.h:2610-2624.
+ * The intersection bitmaps and densities are accepted for ABI compatibility
+ * and not needed by this implementation.  Runs the product REPEAT (5) times,
+ * reports the minimum time of the reference's window (C allocation through
+ * the numeric step), and fills matrixC's host tile arrays (tile_ptr,
+ * tile_columnidx, tile_rowidx, tile_nnz, tile_csr_Ptr, tile_csr_Col,
+ * tile_csr_Value, mask, numtile, nnz, m, n, tilem, tilen). */
+void tilespgemm(SMatrix *matrixA,
+                SMatrix *matrixB,
+                SMatrix *matrixC,
+                unsigned int *blk_intersec_bitmask_A,
+                unsigned int *blk_intersec_bitmask_B,
+                int blk_intersec_bitmask_len,
+                double densityA,
+                double densityB,
+                unsigned long long int nnzCub,
+                unsigned long long int *nnzC_computed,
+                double *compression_rate,
+                double *time_tile,
+                double *gflops_tile,
+                char *filename,
+                double *time_step1, double *time_step2, double *time_step3, double *time_malloc);
+
+/* Tiles -> CSR with ascending columns; zeros are kept.
+ * Replaces tile2csr, src/tile2csr.h:71-137. */
+void tile2csr(SMatrix *matrix);
+
+/* Frees the tile arrays (and only those), src/csr2tile.h:481-492. */
+void matrix_destroy(SMatrix *matrix);
+
+/* Reordering types, src/reorder.h:26-77 (field order kept). */
+typedef struct
+{
+    int n;
+    int *old_id; /* new id -> original id */
+    int *new_id; /* original id -> new id */
+} AxisPermutation;
+
+typedef struct
+{
+    int enabled;
+    int n;
+    AxisPermutation row_perm;
+    AxisPermutation inner_perm;
+    AxisPermutation col_perm;
+    long long input_tiles_A_before;
+    long long input_tiles_A_after;
+    long long input_tiles_B_before;
+    long long input_tiles_B_after;
+    long long estimated_c_tiles_before;
+    long long estimated_c_tiles_after;
+    double reorder_time_ms;
+    double signature_time_ms;
+    double tile_profile_time_ms;
+    double affinity_time_ms;
+    double sort_time_ms;
+    double local_refine_time_ms;
+    double proxy_time_ms;
+    double permute_time_ms;
+    double risk_input_tile_ratio;
+    double risk_c_tile_ratio;
+    int local_refine_window;
+    int proxy_sample_rows;
+    int guard_degraded_to_identity;
+    int structural_conservative;
+    int shared_symmetric_csr;
+    char mode[64];
+    char risk_reason[128];
+} ReorderInfo;
+
+typedef enum
+{
+    REORDER_PROBLEM_AA = 0,
+    REORDER_PROBLEM_AAT = 1,
+    REORDER_PROBLEM_AB = 2
+} ReorderProblemKind;
+
+void reorder_info_init(ReorderInfo *info);
+void reorder_info_destroy(ReorderInfo *info);
+
+/* Identity plan; replaces build_original_reorder_plan,
+ * src/external_reorder.h:173-202.  Returns 0 or a negative code. */
+int build_original_reorder_plan(ReorderProblemKind kind,
+                                const SMatrix *matrixA,
+                                const SMatrix *matrixB,
+                                ReorderInfo *info);
+
+/* Named ordering computed on the GPU ("original", "rcm", "degree", "gray",
+ * "random"); replaces build_external_reorder_plan,
+ * src/external_reorder.h:204-321, which ran reorder_algorithm/<algo>/order_gen
+ * in a child process.  The matrix paths are accepted and unused (the order is
+ * computed from matrixA / matrixB in memory); ordergen_ms receives the GPU
+ * ordering time.  AA/AAT apply A's order to all three axes; AB uses A's order
+ * for rows and inner axis and B's order for the column axis.  Returns 0, or
+ * -42 for an algorithm this library does not provide (the reference's
+ * missing-dependency exit code). */
+int build_external_reorder_plan(ReorderProblemKind kind,
+                                const char *algorithm,
+                                const char *matrix_path_A,
+                                const char *matrix_path_B,
+                                const SMatrix *matrixA,
+                                const SMatrix *matrixB,
+                                ReorderInfo *info,
+                                double *ordergen_ms);
+
+/* output = P_row * input * P_col^T in CSR with sorted rows (GPU).
+ * Replaces apply_bipermutation_csr, src/reorder.h:2429-2504. */
+int apply_bipermutation_csr(const SMatrix *input,
+                            const AxisPermutation *row_perm,
+                            const AxisPermutation *col_perm,
+                            SMatrix *output);
+
+/* Un-permutes rows and columns of a CSR matrix in place, rows re-sorted
+ * (GPU).  Replaces restore_bipermutation_csr, src/reorder.h:2506-2551. */
+int restore_bipermutation_csr(SMatrix *matrix,
+                              const AxisPermutation *row_perm,
+                              const AxisPermutation *col_perm);
+
+/* ------------------------------------------------------------------------ */
+/* Layer 2: handle API over device-resident tiled matrices                  */
+/* ------------------------------------------------------------------------ */
+
+typedef enum
+{
+    TSG_OK = 0,
+    TSG_ERR_INVALID = -1,     /* bad argument                          */
+    TSG_ERR_CUDA = -2,        /* CUDA runtime error                    */
+    TSG_ERR_OOM = -3,         /* device allocation failed              */
+    TSG_ERR_INPUT = -4,       /* malformed CSR (range, order, ptr)     */
+    TSG_ERR_OVERFLOW = -5,    /* result exceeds 32-bit offsets / cap   */
+    TSG_ERR_UNSUPPORTED = -6, /* feature not provided                  */
+    TSG_ERR_TIMEOUT = -7,     /* a bounded device wait gave up         */
+    TSG_ERR_REJECTED = -8     /* admission refused (memory cap)        */
+} tsg_status;
+
+/* Flags for tsg_csr_to_tiled. */
+#define TSG_TILED_PACKED_COL 1 /* A operand: Col bytes are (row<<4)|col    */
+#define TSG_TILED_CSC_VIEW 2   /* B operand: build the column-major view   */
+
+typedef struct tsg_context tsg_context;
+
+/* Device-resident tiled matrix.  Tile data is stored in row-major tile order;
+ * the optional column view lists, per tile column, the tile rows
+ * (csc_tile_rowidx) and the row-major tile index (csc_tile_pos) of each tile.
+ * All pointers are device pointers owned by the library. */
+typedef struct
+{
+    int m, n, nnz;
+    int tilem, tilen, numtile;
+    int col_packed;
+    int *tile_ptr;
+    int *tile_columnidx;
+    int *tile_rowidx;
+    int *tile_nnz;
+    unsigned char *tile_csr_Ptr;
+    unsigned char *tile_csr_Col;
+    double *tile_csr_Value;
+    unsigned short *mask;
+    int *csc_tile_ptr;
+    int *csc_tile_rowidx;
+    int *csc_tile_pos;
+    void *_alloc; /* internal: single backing allocation */
+} tsg_tiled;
+
+/* Per-product statistics filled by tsg_spgemm. */
+typedef struct
+{
+    long long numtile_C;
+    long long nnz_C;
+    long long nnzCub;     /* scalar products, sum over A nonzeros of |B row| */
+    long long tile_pairs; /* matched (A tile, B tile) pairs                   */
+    double ms_step1, ms_step2, ms_step3, ms_total;
+    int bins[4];          /* C tiles by nnz: <=32, <=224, <256, ==256         */
+} tsg_spgemm_info;
+
+const char *tsg_status_string(int status);
+/* Message describing the last failure on the calling thread. */
+const char *tsg_last_error(void);
+
+int tsg_context_create(int device, tsg_context **ctx);
+int tsg_context_destroy(tsg_context *ctx);
+/* Use an existing cudaStream_t (passed as void*) for all work; NULL = own. */
+int tsg_context_set_stream(tsg_context *ctx, void *cuda_stream);
+/* Number of this library's kernels launched on the context so far. */
+long long tsg_context_launches(tsg_context *ctx);
+/* Record per-step CUDA-event timings into tsg_spgemm_info. */
+int tsg_context_set_timing(tsg_context *ctx, int enabled);
+
+/* GPU CSR -> tiles.  d_rowptr/d_colidx/d_val are device pointers; rows must
+ * be sorted by strictly increasing column.  flags: TSG_TILED_* above. */
+int tsg_csr_to_tiled(tsg_context *ctx, int m, int n, int nnz,
+                     const int *d_rowptr, const int *d_colidx, const double *d_val,
+                     int flags, tsg_tiled *out);
+
+/* Upload a host tiled matrix produced by csr2tile_row_major (role A) or
+ * csr2tile_col_major (role B: column-major data, identity csc_tile_pos). */
+int tsg_tiled_upload_rowmajor(tsg_context *ctx, const SMatrix *host, tsg_tiled *out);
+int tsg_tiled_upload_colmajor(tsg_context *ctx, const SMatrix *host, tsg_tiled *out);
+
+int tsg_tiled_free(tsg_context *ctx, tsg_tiled *mat);
+
+/* C = A*B on the device.  A needs col_packed tiles (row role), B needs the
+ * column view.  C is allocated by the library (row-major, plain Col bytes,
+ * masks set, no column view). */
+int tsg_spgemm(tsg_context *ctx, const tsg_tiled *A, const tsg_tiled *B,
+               tsg_tiled *C, tsg_spgemm_info *info);
+
+/* Tiles -> CSR into caller-provided device buffers: d_rowptr[m+1],
+ * d_colidx[nnz], d_val[nnz]. */
+int tsg_tiled_to_csr(tsg_context *ctx, const tsg_tiled *C,
+                     int *d_rowptr, int *d_colidx, double *d_val);
+
+/* Copy a device tiled matrix into host arrays of an SMatrix (malloc'd,
+ * caller frees).  colmajor != 0 writes B's reference layout (column-major
+ * tile data, plain Col bytes, csc_tile_ptr/csc_tile_rowidx). */
+int tsg_tiled_download(tsg_context *ctx, const tsg_tiled *src, int colmajor, SMatrix *dst);
+
+/* End to end with HOST buffers: CSR A (m x k) times CSR B (k x n) -> CSR C.
+ * Copies inputs to the device, converts, multiplies, converts back and copies
+ * the result to freshly malloc'd host arrays (*c_rowptr, *c_colidx, *c_val;
+ * caller frees).  B may alias A. */
+int tsg_spgemm_csr_host(tsg_context *ctx,
+                        int m, int k, int n,
+                        int nnzA, const int *a_rowptr, const int *a_colidx, const double *a_val,
+                        int nnzB, const int *b_rowptr, const int *b_colidx, const double *b_val,
+                        int *nnzC, int **c_rowptr, int **c_colidx, double **c_val,
+                        tsg_spgemm_info *info);
+
+/* Scalar product count nnzCub = sum over A nonzeros (i,k) of nnz(B row k),
+ * computed on the device from device CSR arrays. */
+int tsg_count_products(tsg_context *ctx, int nnzA, const int *d_a_colidx,
+                       const int *d_b_rowptr, long long *nnzCub);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TILESPGEMM_B200_H */

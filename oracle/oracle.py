@@ -1,0 +1,286 @@
+"""ctypes binding of the CPU oracle -- TEST INFRASTRUCTURE ONLY.
+
+Loads oracle/libtsg_oracle.so (the plain-C restatement) and, when present,
+oracle/_ref/libtsgref.so (the reference's own CPU code compiled from its
+sources).  Used by tests/, the smoke check and bench.py's CPU-baseline leg as
+the checker; the product never imports it.
+"""
+from __future__ import annotations
+
+import ctypes
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ORACLE_SO = HERE / "libtsg_oracle.so"
+REF_SO = HERE / "_ref" / "libtsgref.so"
+
+_ip = ctypes.POINTER(ctypes.c_int)
+_dp = ctypes.POINTER(ctypes.c_double)
+_u8p = ctypes.POINTER(ctypes.c_ubyte)
+_u16p = ctypes.POINTER(ctypes.c_ushort)
+
+
+class OMatrix(ctypes.Structure):
+    _fields_ = [
+        ("m", ctypes.c_int), ("n", ctypes.c_int), ("nnz", ctypes.c_int), ("isSymmetric", ctypes.c_int),
+        ("value", _dp), ("columnindex", _ip), ("rowpointer", _ip),
+        ("tilem", ctypes.c_int), ("tilen", ctypes.c_int),
+        ("tile_ptr", _ip), ("tile_columnidx", _ip), ("tile_rowidx", _ip),
+        ("tile_nnz", _ip), ("numtile", ctypes.c_int),
+        ("tile_csr_Value", _dp), ("tile_csr_Col", _u8p), ("tile_csr_Ptr", _u8p),
+        ("mask", _u16p), ("csc_tile_ptr", _ip), ("csc_tile_rowidx", _ip),
+    ]
+
+
+_libc = ctypes.CDLL(None)
+_libc.free.argtypes = [ctypes.c_void_p]
+_o = None
+_r = None
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+
+
+def olib():
+    global _o
+    if _o is None:
+        if not ORACLE_SO.exists():
+            build()
+        _o = ctypes.CDLL(str(ORACLE_SO))
+        vp = ctypes.c_void_p
+        _o.tsgo_count_products.restype = ctypes.c_longlong
+        _o.tsgo_count_products.argtypes = [ctypes.c_int, vp, vp]
+        _o.tsgo_gustavson_symbolic.restype = ctypes.c_longlong
+        _o.tsgo_gustavson_symbolic.argtypes = [ctypes.c_int, ctypes.c_int, vp, vp, vp, vp, vp, ctypes.c_int]
+        _o.tsgo_gustavson_numeric.argtypes = [ctypes.c_int, ctypes.c_int, vp, vp, vp, vp, vp, vp, vp, vp, vp,
+                                              ctypes.c_int]
+        _o.tsgo_order_degree.argtypes = [ctypes.c_int, vp, vp]
+        _o.tsgo_order_random.argtypes = [ctypes.c_int, ctypes.c_ulonglong, vp]
+        _o.tsgo_order_rcm.argtypes = [ctypes.c_int, vp, vp, vp]
+        _o.tsgo_order_gray.argtypes = [ctypes.c_int, ctypes.c_int, vp, vp, vp]
+        _o.tsgo_apply_bipermutation.argtypes = [ctypes.c_int, vp, vp, vp, vp, vp, vp, vp, vp]
+        _o.tsgo_random_key.restype = ctypes.c_ulonglong
+        _o.tsgo_random_key.argtypes = [ctypes.c_ulonglong, ctypes.c_ulonglong]
+    return _o
+
+
+def ref_available() -> bool:
+    return REF_SO.exists()
+
+
+def rlib():
+    global _r
+    if _r is None:
+        if not REF_SO.exists():
+            raise FileNotFoundError(f"{REF_SO} not built (reference tree absent when oracle/Makefile ran)")
+        _r = ctypes.CDLL(str(REF_SO))
+        vp = ctypes.c_void_p
+        _r.ref_spgemm_spa_rowptr.restype = ctypes.c_int
+        _r.ref_spgemm_spa_rowptr.argtypes = [ctypes.c_int] * 3 + [vp, vp] + [ctypes.c_int] * 3 + [vp, vp, vp]
+        _r.ref_spgemm_spa_cols.argtypes = [ctypes.c_int] * 3 + [vp, vp] + [ctypes.c_int] * 3 + [vp, vp, vp, vp]
+        _r.ref_omp_max_threads.restype = ctypes.c_int
+    return _r
+
+
+def _arr(ptr, count, dtype, free=False):
+    if count <= 0 or not ptr:
+        out = np.zeros(0, dtype=dtype)
+    else:
+        addr = ctypes.cast(ptr, ctypes.c_void_p).value
+        buf = (ctypes.c_char * (count * np.dtype(dtype).itemsize)).from_address(addr)
+        out = np.frombuffer(buf, dtype=dtype).copy()
+    if free and ptr:
+        _libc.free(ctypes.cast(ptr, ctypes.c_void_p))
+    return out
+
+
+class _CSRHold:
+    def __init__(self, mat):
+        m, n, rp, ci, v = mat
+        self.rp = np.ascontiguousarray(rp, dtype=np.int32)
+        self.ci = np.ascontiguousarray(ci, dtype=np.int32)
+        self.v = np.ascontiguousarray(v, dtype=np.float64)
+        self.om = OMatrix()
+        self.om.m, self.om.n, self.om.nnz = int(m), int(n), int(self.ci.size)
+        self.om.rowpointer = self.rp.ctypes.data_as(_ip)
+        self.om.columnindex = self.ci.ctypes.data_as(_ip)
+        self.om.value = self.v.ctypes.data_as(_dp)
+
+
+def _tiles(om: OMatrix, colmajor=False, free=True, rowidx=True):
+    T, nnz = om.numtile, om.nnz
+    d = dict(m=om.m, n=om.n, nnz=nnz, tilem=om.tilem, tilen=om.tilen, numtile=T)
+    d["tile_ptr"] = _arr(om.tile_ptr, om.tilem + 1, np.int32, free)
+    d["tile_columnidx"] = _arr(om.tile_columnidx, T, np.int32, free)
+    d["tile_rowidx"] = _arr(om.tile_rowidx, T, np.int32, free) if rowidx else None
+    d["tile_nnz"] = _arr(om.tile_nnz, T + 1, np.int32, free)
+    d["tile_csr_Ptr"] = _arr(om.tile_csr_Ptr, 16 * T, np.uint8, free)
+    d["tile_csr_Col"] = _arr(om.tile_csr_Col, nnz, np.uint8, free)
+    d["tile_csr_Value"] = _arr(om.tile_csr_Value, nnz, np.float64, free)
+    d["mask"] = _arr(om.mask, 16 * T, np.uint16, free) if om.mask else None
+    if colmajor:
+        d["csc_tile_ptr"] = _arr(om.csc_tile_ptr, om.tilen + 1, np.int32, free)
+        d["csc_tile_rowidx"] = _arr(om.csc_tile_rowidx, T, np.int32, free)
+    return d
+
+
+def _om_from_tiles(d):
+    hold = {k: np.ascontiguousarray(v) for k, v in d.items() if isinstance(v, np.ndarray)}
+    om = OMatrix()
+    for k in ("m", "n", "nnz", "tilem", "tilen", "numtile"):
+        setattr(om, k, int(d[k]))
+    types = dict(tile_ptr=_ip, tile_columnidx=_ip, tile_rowidx=_ip, tile_nnz=_ip, tile_csr_Ptr=_u8p,
+                 tile_csr_Col=_u8p, tile_csr_Value=_dp, mask=_u16p, csc_tile_ptr=_ip, csc_tile_rowidx=_ip)
+    for k, t in types.items():
+        if k in hold:
+            setattr(om, k, hold[k].ctypes.data_as(t))
+    return om, hold
+
+
+# --- oracle restatement -----------------------------------------------------
+def csr2tile_row_major(mat):
+    h = _CSRHold(mat)
+    olib().tsgo_csr2tile_row_major(ctypes.byref(h.om))
+    return _tiles(h.om)
+
+
+def csr2tile_col_major(mat):
+    h = _CSRHold(mat)
+    olib().tsgo_csr2tile_col_major(ctypes.byref(h.om))
+    return _tiles(h.om, colmajor=True)
+
+
+def spgemm_tiled(tA, tB):
+    omA, hA = _om_from_tiles(tA)
+    omB, hB = _om_from_tiles(tB)
+    omC = OMatrix()
+    olib().tsgo_spgemm_tiled(ctypes.byref(omA), ctypes.byref(omB), ctypes.byref(omC))
+    return _tiles(omC)
+
+
+def tile2csr(tiles):
+    om, hold = _om_from_tiles(tiles)
+    olib().tsgo_tile2csr(ctypes.byref(om))
+    rp = _arr(om.rowpointer, om.m + 1, np.int32, True)
+    ci = _arr(om.columnindex, om.nnz, np.int32, True)
+    v = _arr(om.value, om.nnz, np.float64, True)
+    return rp, ci, v
+
+
+def count_products(matA, matB):
+    _, _, _, ciA, _ = matA
+    _, _, rpB, _, _ = matB
+    ciA = np.ascontiguousarray(ciA, dtype=np.int32)
+    rpB = np.ascontiguousarray(rpB, dtype=np.int32)
+    return olib().tsgo_count_products(int(ciA.size), ciA.ctypes.data, rpB.ctypes.data)
+
+
+def gustavson(matA, matB, nthreads=1):
+    """Element-level CSR SpGEMM: (m, n, rowptr, col, val)."""
+    mA, nA, rpA, ciA, vA = [np.ascontiguousarray(x) if isinstance(x, np.ndarray) else x for x in matA]
+    mB, nB, rpB, ciB, vB = [np.ascontiguousarray(x) if isinstance(x, np.ndarray) else x for x in matB]
+    rpC = np.zeros(mA + 1, dtype=np.int32)
+    nnz = olib().tsgo_gustavson_symbolic(mA, nB, rpA.ctypes.data, ciA.ctypes.data, rpB.ctypes.data,
+                                         ciB.ctypes.data, rpC.ctypes.data, nthreads)
+    if nnz < 0:
+        raise OverflowError("nnz(C) exceeds int32")
+    ciC = np.zeros(max(nnz, 1), dtype=np.int32)
+    vC = np.zeros(max(nnz, 1), dtype=np.float64)
+    olib().tsgo_gustavson_numeric(mA, nB, rpA.ctypes.data, ciA.ctypes.data, vA.ctypes.data, rpB.ctypes.data,
+                                  ciB.ctypes.data, vB.ctypes.data, rpC.ctypes.data, ciC.ctypes.data,
+                                  vC.ctypes.data, nthreads)
+    return mA, nB, rpC, ciC[:nnz], vC[:nnz]
+
+
+def order(kind, mat, seed=1):
+    m, n, rp, ci, _ = mat
+    rp = np.ascontiguousarray(rp, dtype=np.int32)
+    ci = np.ascontiguousarray(ci, dtype=np.int32)
+    out = np.zeros(m, dtype=np.int32)
+    L = olib()
+    if kind == "original":
+        return np.arange(m, dtype=np.int32)
+    if kind == "degree":
+        L.tsgo_order_degree(m, rp.ctypes.data, out.ctypes.data)
+    elif kind == "random":
+        L.tsgo_order_random(m, ctypes.c_ulonglong(seed), out.ctypes.data)
+    elif kind == "rcm":
+        L.tsgo_order_rcm(m, rp.ctypes.data, ci.ctypes.data, out.ctypes.data)
+    elif kind == "gray":
+        L.tsgo_order_gray(m, n, rp.ctypes.data, ci.ctypes.data, out.ctypes.data)
+    else:
+        raise ValueError(kind)
+    return out
+
+
+def apply_bipermutation(mat, row_old, col_new):
+    m, n, rp, ci, v = mat
+    rp = np.ascontiguousarray(rp, dtype=np.int32)
+    ci = np.ascontiguousarray(ci, dtype=np.int32)
+    v = np.ascontiguousarray(v, dtype=np.float64)
+    row_old = np.ascontiguousarray(row_old, dtype=np.int32)
+    col_new = np.ascontiguousarray(col_new, dtype=np.int32)
+    orp = np.zeros(m + 1, dtype=np.int32)
+    oci = np.zeros(max(ci.size, 1), dtype=np.int32)
+    ov = np.zeros(max(ci.size, 1), dtype=np.float64)
+    olib().tsgo_apply_bipermutation(m, rp.ctypes.data, ci.ctypes.data, v.ctypes.data, row_old.ctypes.data,
+                                    col_new.ctypes.data, orp.ctypes.data, oci.ctypes.data, ov.ctypes.data)
+    return m, n, orp, oci[:ci.size], ov[:ci.size]
+
+
+# --- the reference's own CPU code (compiled from its sources) ----------------
+def ref_csr2tile_row_major(mat):
+    h = _CSRHold(mat)
+    rlib().ref_csr2tile_row_major(ctypes.byref(h.om))
+    return _tiles(h.om)
+
+
+def ref_csr2tile_col_major(mat):
+    h = _CSRHold(mat)
+    rlib().ref_csr2tile_col_major(ctypes.byref(h.om))
+    return _tiles(h.om, colmajor=True)
+
+
+def ref_spgemm_cpu(tA, tB):
+    """Reference spgemm_cpu (src/spgemm-cpu.h:369); C has tile_ptr, tile_columnidx,
+    tile_nnz, tile_csr_Ptr/Col/Value, numtile, nnz (no mask, no rowidx)."""
+    omA, hA = _om_from_tiles(tA)
+    omB, hB = _om_from_tiles(tB)
+    omC = OMatrix()
+    omC.m, omC.n, omC.tilem, omC.tilen = tA["m"], tB["n"], tA["tilem"], tB["tilen"]
+    rlib().ref_spgemm_cpu(ctypes.byref(omA), ctypes.byref(omB), ctypes.byref(omC))
+    omC.tilem = tA["tilem"]
+    omC.tilen = tB["tilen"]
+    omC.m, omC.n = tA["m"], tB["n"]
+    return _tiles(omC, rowidx=False)
+
+
+def ref_tile2csr(tiles):
+    om, hold = _om_from_tiles(tiles)
+    rlib().ref_tile2csr(ctypes.byref(om))
+    rp = _arr(om.rowpointer, om.m + 1, np.int32, True)
+    ci = _arr(om.columnindex, om.nnz, np.int32, True)
+    v = _arr(om.value, om.nnz, np.float64, True)
+    return rp, ci, v
+
+
+def ref_spgemm_spa(matA, matB):
+    """Reference spgemm_spa (src/spgemm_serialref_spa_new.h:7): rowptr, cols."""
+    mA, nA, rpA, ciA, _ = matA
+    mB, nB, rpB, ciB, _ = matB
+    rpA = np.ascontiguousarray(rpA, dtype=np.int32)
+    ciA = np.ascontiguousarray(ciA, dtype=np.int32)
+    rpB = np.ascontiguousarray(rpB, dtype=np.int32)
+    ciB = np.ascontiguousarray(ciB, dtype=np.int32)
+    rpC = np.zeros(mA + 2, dtype=np.int32)
+    R = rlib()
+    nnz = R.ref_spgemm_spa_rowptr(mA, nA, int(ciA.size), rpA.ctypes.data, ciA.ctypes.data, mB, nB, int(ciB.size),
+                                  rpB.ctypes.data, ciB.ctypes.data, rpC.ctypes.data)
+    ciC = np.zeros(max(nnz, 1), dtype=np.int32)
+    R.ref_spgemm_spa_cols(mA, nA, int(ciA.size), rpA.ctypes.data, ciA.ctypes.data, mB, nB, int(ciB.size),
+                          rpB.ctypes.data, ciB.ctypes.data, rpC.ctypes.data, ciC.ctypes.data)
+    return rpC[:mA + 1], ciC[:nnz]

@@ -1,0 +1,389 @@
+"""B200 (sm_100a) tiled SpGEMM -- Python host side over the C ABI.
+
+The compute path is libtilespgemm_b200.so (hand-written CUDA for sm_100a,
+built in-tree by ``make -C rw-spgemm_b200``); this module only binds it with
+ctypes.  Nothing here computes: if the library is missing, every call raises.
+
+Two surfaces mirror the C ABI (include/tilespgemm_b200.h):
+
+* the reference's drop-in functions on host arrays -- ``csr2tile_row_major``,
+  ``csr2tile_col_major``, ``tilespgemm``, ``tile2csr`` (same names, same
+  argument meaning, same outputs as for-the-juan/RW-SpGEMM's src/csr2tile.h,
+  src/tilespgemm-cuda.h and src/tile2csr.h);
+* the device-resident handle API -- ``Context``, ``csr_to_tiled``,
+  ``spgemm``, ``tiled_to_csr``, ``spgemm_csr_host``.
+
+The package directory is named ``rw-spgemm_b200``; load it with
+``importlib`` (see ``load_package`` in tests/conftest.py or bench.py).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+import numpy as np
+
+_HERE = Path(__file__).resolve().parent
+LIB_PATH = _HERE / "lib" / "libtilespgemm_b200.so"
+
+TSG_TILED_PACKED_COL = 1
+TSG_TILED_CSC_VIEW = 2
+
+_c_int_p = ctypes.POINTER(ctypes.c_int)
+_c_dbl_p = ctypes.POINTER(ctypes.c_double)
+_c_u8_p = ctypes.POINTER(ctypes.c_ubyte)
+_c_u16_p = ctypes.POINTER(ctypes.c_ushort)
+
+
+class SMatrix(ctypes.Structure):
+    """Reference matrix container (src/common.h:113-135), host pointers."""
+    _fields_ = [
+        ("m", ctypes.c_int), ("n", ctypes.c_int), ("nnz", ctypes.c_int), ("isSymmetric", ctypes.c_int),
+        ("value", _c_dbl_p), ("columnindex", _c_int_p), ("rowpointer", _c_int_p),
+        ("tilem", ctypes.c_int), ("tilen", ctypes.c_int),
+        ("tile_ptr", _c_int_p), ("tile_columnidx", _c_int_p), ("tile_rowidx", _c_int_p),
+        ("tile_nnz", _c_int_p), ("numtile", ctypes.c_int),
+        ("tile_csr_Value", _c_dbl_p), ("tile_csr_Col", _c_u8_p), ("tile_csr_Ptr", _c_u8_p),
+        ("mask", _c_u16_p), ("csc_tile_ptr", _c_int_p), ("csc_tile_rowidx", _c_int_p),
+    ]
+
+
+class TsgTiled(ctypes.Structure):
+    """Device-resident tiled matrix (tsg_tiled), device pointers."""
+    _fields_ = [
+        ("m", ctypes.c_int), ("n", ctypes.c_int), ("nnz", ctypes.c_int),
+        ("tilem", ctypes.c_int), ("tilen", ctypes.c_int), ("numtile", ctypes.c_int),
+        ("col_packed", ctypes.c_int),
+        ("tile_ptr", ctypes.c_void_p), ("tile_columnidx", ctypes.c_void_p), ("tile_rowidx", ctypes.c_void_p),
+        ("tile_nnz", ctypes.c_void_p), ("tile_csr_Ptr", ctypes.c_void_p), ("tile_csr_Col", ctypes.c_void_p),
+        ("tile_csr_Value", ctypes.c_void_p), ("mask", ctypes.c_void_p),
+        ("csc_tile_ptr", ctypes.c_void_p), ("csc_tile_rowidx", ctypes.c_void_p), ("csc_tile_pos", ctypes.c_void_p),
+        ("_alloc", ctypes.c_void_p),
+    ]
+
+
+class TsgInfo(ctypes.Structure):
+    _fields_ = [
+        ("numtile_C", ctypes.c_longlong), ("nnz_C", ctypes.c_longlong), ("nnzCub", ctypes.c_longlong),
+        ("tile_pairs", ctypes.c_longlong),
+        ("ms_step1", ctypes.c_double), ("ms_step2", ctypes.c_double), ("ms_step3", ctypes.c_double),
+        ("ms_total", ctypes.c_double), ("bins", ctypes.c_int * 4),
+    ]
+
+    def as_dict(self):
+        d = {f: getattr(self, f) for f, _ in self._fields_ if f != "bins"}
+        d["bins"] = list(self.bins)
+        return d
+
+
+class TsgError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__(f"tilespgemm_b200 status {status}: {message}")
+        self.status = status
+
+
+_lib = None
+_libc = ctypes.CDLL(None)
+_libc.free.argtypes = [ctypes.c_void_p]
+
+
+def lib():
+    """The loaded C library; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `make -C rw-spgemm_b200` "
+                               "(the CUDA library is required; there is no fallback)")
+        _lib = ctypes.CDLL(str(LIB_PATH))
+        _declare(_lib)
+    return _lib
+
+
+def _declare(L):
+    vp, ip = ctypes.c_void_p, ctypes.c_int
+    L.tsg_status_string.restype = ctypes.c_char_p
+    L.tsg_last_error.restype = ctypes.c_char_p
+    L.tsg_context_create.argtypes = [ip, ctypes.POINTER(vp)]
+    L.tsg_context_destroy.argtypes = [vp]
+    L.tsg_context_set_stream.argtypes = [vp, vp]
+    L.tsg_context_set_timing.argtypes = [vp, ip]
+    L.tsg_context_launches.argtypes = [vp]
+    L.tsg_context_launches.restype = ctypes.c_longlong
+    L.tsg_csr_to_tiled.argtypes = [vp, ip, ip, ip, vp, vp, vp, ip, ctypes.POINTER(TsgTiled)]
+    L.tsg_tiled_free.argtypes = [vp, ctypes.POINTER(TsgTiled)]
+    L.tsg_spgemm.argtypes = [vp, ctypes.POINTER(TsgTiled), ctypes.POINTER(TsgTiled), ctypes.POINTER(TsgTiled),
+                             ctypes.POINTER(TsgInfo)]
+    L.tsg_tiled_to_csr.argtypes = [vp, ctypes.POINTER(TsgTiled), vp, vp, vp]
+    L.tsg_tiled_download.argtypes = [vp, ctypes.POINTER(TsgTiled), ip, ctypes.POINTER(SMatrix)]
+    L.tsg_tiled_upload_rowmajor.argtypes = [vp, ctypes.POINTER(SMatrix), ctypes.POINTER(TsgTiled)]
+    L.tsg_tiled_upload_colmajor.argtypes = [vp, ctypes.POINTER(SMatrix), ctypes.POINTER(TsgTiled)]
+    L.tsg_count_products.argtypes = [vp, ip, vp, vp, ctypes.POINTER(ctypes.c_longlong)]
+    L.tsg_spgemm_csr_host.argtypes = [vp, ip, ip, ip,
+                                      ip, vp, vp, vp, ip, vp, vp, vp,
+                                      ctypes.POINTER(ip), ctypes.POINTER(vp), ctypes.POINTER(vp),
+                                      ctypes.POINTER(vp), ctypes.POINTER(TsgInfo)]
+    for name in ("csr2tile_row_major", "csr2tile_col_major", "tile2csr", "matrix_destroy"):
+        getattr(L, name).argtypes = [ctypes.POINTER(SMatrix)]
+        getattr(L, name).restype = None
+    L.tilespgemm.argtypes = [ctypes.POINTER(SMatrix)] * 3 + [
+        vp, vp, ip, ctypes.c_double, ctypes.c_double, ctypes.c_ulonglong, ctypes.POINTER(ctypes.c_ulonglong),
+        _c_dbl_p, _c_dbl_p, _c_dbl_p, ctypes.c_char_p, _c_dbl_p, _c_dbl_p, _c_dbl_p, _c_dbl_p]
+    L.tilespgemm.restype = None
+
+
+def check(status):
+    if status != 0:
+        L = lib()
+        raise TsgError(status, f"{L.tsg_status_string(status).decode()}: {L.tsg_last_error().decode()}")
+
+
+# ---------------------------------------------------------------------------
+# host array helpers
+# ---------------------------------------------------------------------------
+def _np_from(ptr, count, dtype, free=False):
+    if count == 0 or not ptr:
+        out = np.zeros(0, dtype=dtype)
+    else:
+        addr = ctypes.cast(ptr, ctypes.c_void_p).value
+        buf = (ctypes.c_char * (count * np.dtype(dtype).itemsize)).from_address(addr)
+        out = np.frombuffer(buf, dtype=dtype).copy()
+    if free and ptr:
+        _libc.free(ctypes.cast(ptr, ctypes.c_void_p))
+    return out
+
+
+TILE_FIELDS = ("tile_ptr", "tile_columnidx", "tile_rowidx", "tile_nnz", "tile_csr_Ptr", "tile_csr_Col",
+               "tile_csr_Value", "mask", "csc_tile_ptr", "csc_tile_rowidx")
+
+
+def smatrix_tiles_to_numpy(sm: SMatrix, free=True, colmajor=False) -> dict:
+    T, nnz = sm.numtile, sm.nnz
+    d = dict(m=sm.m, n=sm.n, nnz=nnz, tilem=sm.tilem, tilen=sm.tilen, numtile=T)
+    d["tile_ptr"] = _np_from(sm.tile_ptr, sm.tilem + 1, np.int32, free)
+    d["tile_columnidx"] = _np_from(sm.tile_columnidx, T, np.int32, free)
+    d["tile_rowidx"] = _np_from(sm.tile_rowidx, T, np.int32, free)
+    d["tile_nnz"] = _np_from(sm.tile_nnz, T + 1, np.int32, free)
+    d["tile_csr_Ptr"] = _np_from(sm.tile_csr_Ptr, 16 * T, np.uint8, free)
+    d["tile_csr_Col"] = _np_from(sm.tile_csr_Col, nnz, np.uint8, free)
+    d["tile_csr_Value"] = _np_from(sm.tile_csr_Value, nnz, np.float64, free)
+    d["mask"] = _np_from(sm.mask, 16 * T, np.uint16, free)
+    if colmajor:
+        d["csc_tile_ptr"] = _np_from(sm.csc_tile_ptr, sm.tilen + 1, np.int32, free)
+        d["csc_tile_rowidx"] = _np_from(sm.csc_tile_rowidx, T, np.int32, free)
+    for f in TILE_FIELDS:
+        setattr(sm, f, None)
+    return d
+
+
+class HostCSR:
+    """Keeps numpy CSR arrays alive behind an SMatrix."""
+
+    def __init__(self, mat):
+        m, n, rp, ci, v = mat
+        self.rp = np.ascontiguousarray(rp, dtype=np.int32)
+        self.ci = np.ascontiguousarray(ci, dtype=np.int32)
+        self.v = np.ascontiguousarray(v, dtype=np.float64)
+        self.sm = SMatrix()
+        self.sm.m, self.sm.n, self.sm.nnz = int(m), int(n), int(self.ci.size)
+        self.sm.rowpointer = self.rp.ctypes.data_as(_c_int_p)
+        self.sm.columnindex = self.ci.ctypes.data_as(_c_int_p)
+        self.sm.value = self.v.ctypes.data_as(_c_dbl_p)
+
+
+def smatrix_from_tiles(d: dict):
+    """SMatrix over numpy tile arrays (kept alive by the returned holder)."""
+    hold = {k: np.ascontiguousarray(v) for k, v in d.items() if isinstance(v, np.ndarray)}
+    sm = SMatrix()
+    for k in ("m", "n", "nnz", "tilem", "tilen", "numtile"):
+        setattr(sm, k, int(d[k]))
+    types = dict(tile_ptr=_c_int_p, tile_columnidx=_c_int_p, tile_rowidx=_c_int_p, tile_nnz=_c_int_p,
+                 tile_csr_Ptr=_c_u8_p, tile_csr_Col=_c_u8_p, tile_csr_Value=_c_dbl_p, mask=_c_u16_p,
+                 csc_tile_ptr=_c_int_p, csc_tile_rowidx=_c_int_p)
+    for k, t in types.items():
+        if k in hold:
+            setattr(sm, k, hold[k].ctypes.data_as(t))
+    return sm, hold
+
+
+# ---------------------------------------------------------------------------
+# drop-in functions on host arrays
+# ---------------------------------------------------------------------------
+def csr2tile_row_major(mat) -> dict:
+    """src/csr2tile.h:196 on the GPU; returns the tile arrays as numpy."""
+    h = HostCSR(mat)
+    lib().csr2tile_row_major(ctypes.byref(h.sm))
+    return smatrix_tiles_to_numpy(h.sm)
+
+
+def csr2tile_col_major(mat) -> dict:
+    """src/csr2tile.h:261 on the GPU; returns the tile arrays as numpy."""
+    h = HostCSR(mat)
+    lib().csr2tile_col_major(ctypes.byref(h.sm))
+    return smatrix_tiles_to_numpy(h.sm, colmajor=True)
+
+
+def tile2csr(tiles: dict):
+    """src/tile2csr.h:71 on the GPU; returns (rowptr, colidx, val)."""
+    sm, hold = smatrix_from_tiles(tiles)
+    lib().tile2csr(ctypes.byref(sm))
+    rp = _np_from(sm.rowpointer, sm.m + 1, np.int32, True)
+    ci = _np_from(sm.columnindex, sm.nnz, np.int32, True)
+    v = _np_from(sm.value, sm.nnz, np.float64, True)
+    return rp, ci, v
+
+
+def tilespgemm(tilesA: dict, tilesB: dict, nnzCub: int = 0) -> tuple[dict, dict]:
+    """src/tilespgemm-cuda.h:2610 on host tiles (A row-major, B column-major).
+    Returns (C tiles, timings)."""
+    smA, holdA = smatrix_from_tiles(tilesA)
+    smB, holdB = smatrix_from_tiles(tilesB)
+    smC = SMatrix()
+    nnzC = ctypes.c_ulonglong(0)
+    dbl = [ctypes.c_double(0.0) for _ in range(7)]
+    lib().tilespgemm(ctypes.byref(smA), ctypes.byref(smB), ctypes.byref(smC), None, None, 0, 0.0, 0.0,
+                     ctypes.c_ulonglong(nnzCub), ctypes.byref(nnzC), *[ctypes.byref(x) for x in dbl[:3]],
+                     b"", *[ctypes.byref(x) for x in dbl[3:]])
+    C = smatrix_tiles_to_numpy(smC)
+    t = dict(nnzC=nnzC.value, compression_rate=dbl[0].value, time_ms=dbl[1].value, gflops=dbl[2].value,
+             step1_ms=dbl[3].value, step2_ms=dbl[4].value, step3_ms=dbl[5].value, malloc_ms=dbl[6].value)
+    return C, t
+
+
+# ---------------------------------------------------------------------------
+# handle API (device-resident)
+# ---------------------------------------------------------------------------
+class Context:
+    """tsg_context on one device; uses torch's current stream when given."""
+
+    def __init__(self, device: int = 0, stream=None, timing: bool = False):
+        self.handle = ctypes.c_void_p()
+        check(lib().tsg_context_create(device, ctypes.byref(self.handle)))
+        if stream is not None:
+            self.set_stream(stream)
+        if timing:
+            self.set_timing(True)
+
+    def set_stream(self, stream_ptr: int):
+        check(lib().tsg_context_set_stream(self.handle, ctypes.c_void_p(int(stream_ptr))))
+
+    def set_timing(self, on: bool):
+        check(lib().tsg_context_set_timing(self.handle, 1 if on else 0))
+
+    def launches(self) -> int:
+        return int(lib().tsg_context_launches(self.handle))
+
+    def close(self):
+        if self.handle:
+            lib().tsg_context_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Tiled:
+    """Owner of a device tsg_tiled."""
+
+    def __init__(self, ctx: Context):
+        self.ctx = ctx
+        self.s = TsgTiled()
+
+    @property
+    def numtile(self):
+        return self.s.numtile
+
+    @property
+    def nnz(self):
+        return self.s.nnz
+
+    def download(self, colmajor: bool = False) -> dict:
+        sm = SMatrix()
+        check(lib().tsg_tiled_download(self.ctx.handle, ctypes.byref(self.s), 1 if colmajor else 0,
+                                       ctypes.byref(sm)))
+        return smatrix_tiles_to_numpy(sm, colmajor=colmajor)
+
+    def free(self):
+        if self.ctx is not None and self.ctx.handle:
+            lib().tsg_tiled_free(self.ctx.handle, ctypes.byref(self.s))
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def csr_to_tiled(ctx: Context, m: int, n: int, rowptr, colidx, val, flags: int) -> Tiled:
+    """GPU CSR -> tiles from device tensors (torch int32/int32/float64)."""
+    t = Tiled(ctx)
+    check(lib().tsg_csr_to_tiled(ctx.handle, int(m), int(n), int(colidx.numel()), ctypes.c_void_p(rowptr.data_ptr()),
+                                 ctypes.c_void_p(colidx.data_ptr()), ctypes.c_void_p(val.data_ptr()), int(flags),
+                                 ctypes.byref(t.s)))
+    return t
+
+
+def upload_rowmajor(ctx: Context, tiles: dict) -> Tiled:
+    sm, hold = smatrix_from_tiles(tiles)
+    t = Tiled(ctx)
+    check(lib().tsg_tiled_upload_rowmajor(ctx.handle, ctypes.byref(sm), ctypes.byref(t.s)))
+    t._hold = hold
+    return t
+
+
+def upload_colmajor(ctx: Context, tiles: dict) -> Tiled:
+    sm, hold = smatrix_from_tiles(tiles)
+    t = Tiled(ctx)
+    check(lib().tsg_tiled_upload_colmajor(ctx.handle, ctypes.byref(sm), ctypes.byref(t.s)))
+    t._hold = hold
+    return t
+
+
+def spgemm(ctx: Context, A: Tiled, B: Tiled) -> tuple[Tiled, dict]:
+    C = Tiled(ctx)
+    info = TsgInfo()
+    check(lib().tsg_spgemm(ctx.handle, ctypes.byref(A.s), ctypes.byref(B.s), ctypes.byref(C.s), ctypes.byref(info)))
+    return C, info.as_dict()
+
+
+def tiled_to_csr(ctx: Context, C: Tiled):
+    """Device CSR (torch tensors) of a tiled matrix."""
+    import torch
+    dev = torch.device("cuda", torch.cuda.current_device())
+    rp = torch.empty(C.s.m + 1, dtype=torch.int32, device=dev)
+    ci = torch.empty(max(C.s.nnz, 1), dtype=torch.int32, device=dev)
+    v = torch.empty(max(C.s.nnz, 1), dtype=torch.float64, device=dev)
+    check(lib().tsg_tiled_to_csr(ctx.handle, ctypes.byref(C.s), ctypes.c_void_p(rp.data_ptr()),
+                                 ctypes.c_void_p(ci.data_ptr()), ctypes.c_void_p(v.data_ptr())))
+    return rp, ci[:C.s.nnz], v[:C.s.nnz]
+
+
+def count_products(ctx: Context, a_colidx, b_rowptr) -> int:
+    out = ctypes.c_longlong(0)
+    check(lib().tsg_count_products(ctx.handle, int(a_colidx.numel()), ctypes.c_void_p(a_colidx.data_ptr()),
+                                   ctypes.c_void_p(b_rowptr.data_ptr()), ctypes.byref(out)))
+    return out.value
+
+
+def spgemm_csr_host(ctx: Context, matA, matB=None):
+    """End to end through the C ABI with host buffers: CSR A * CSR B -> CSR C
+    (numpy).  matB=None computes A*A."""
+    hA = HostCSR(matA)
+    hB = hA if matB is None else HostCSR(matB)
+    nnzC = ctypes.c_int(0)
+    prp, pci, pv = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
+    info = TsgInfo()
+    m, k = hA.sm.m, hA.sm.n
+    n = hB.sm.n
+    check(lib().tsg_spgemm_csr_host(
+        ctx.handle, m, k, n,
+        hA.sm.nnz, hA.rp.ctypes.data, hA.ci.ctypes.data, hA.v.ctypes.data,
+        hB.sm.nnz, hB.rp.ctypes.data, hB.ci.ctypes.data, hB.v.ctypes.data,
+        ctypes.byref(nnzC), ctypes.byref(prp), ctypes.byref(pci), ctypes.byref(pv), ctypes.byref(info)))
+    rp = _np_from(prp, m + 1, np.int32, True)
+    ci = _np_from(pci, nnzC.value, np.int32, True)
+    v = _np_from(pv, nnzC.value, np.float64, True)
+    return (m, n, rp, ci, v), info.as_dict()

@@ -1,0 +1,394 @@
+// GPU format conversion: CSR -> 16x16 tiles, the column view of B, the
+// column-major (reference B layout) gather, and tiles -> CSR.
+//
+// CSR -> tiles restates src/csr2tile.h:6-259 (row-major, packed (row<<4)|col
+// bytes) and :261-478 (column-major B, plain bytes) of the reference, and
+// tiles -> CSR restates src/tile2csr.h:8-137.  Rows must be sorted by
+// strictly increasing column (checked by tsg_check_csr): the tile columns of
+// one tile row are then the merge of 16 sorted lists, which a half-warp walks
+// with one lane per row, so every tile row is converted in one pass with no
+// scratch memory and the output comes out already sorted.
+#include <limits.h>
+
+#include "tsg_internal.h"
+
+#define HW_MASK(tid) (0xFFFFu << ((tid) & 16))
+
+// ---------------------------------------------------------------------------
+// Pass 1: number of non-empty tiles in each tile row (half-warp per row).
+// ---------------------------------------------------------------------------
+__global__ void k_tile_count(int m, int tilem, const int *__restrict__ rowptr,
+                             const int *__restrict__ col, int *__restrict__ tile_cnt)
+{
+    const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int tr = (int)(gid >> 4);
+    const int lane = threadIdx.x & 15;
+    const unsigned hmask = HW_MASK(threadIdx.x);
+    if (tr >= tilem)
+        return;
+    const int r = tr * TSG_BS + lane;
+    int p = 0, e = 0;
+    if (r < m)
+    {
+        p = rowptr[r];
+        e = rowptr[r + 1];
+    }
+    int cur = p < e ? (col[p] >> 4) : INT_MAX;
+    int cnt = 0;
+    while (true)
+    {
+        const int jm = __reduce_min_sync(hmask, cur);
+        if (jm == INT_MAX)
+            break;
+        cnt++;
+        if (cur == jm)
+        {
+            do
+            {
+                ++p;
+            } while (p < e && (col[p] >> 4) == jm);
+            cur = p < e ? (col[p] >> 4) : INT_MAX;
+        }
+    }
+    if (lane == 0)
+        tile_cnt[tr] = cnt;
+}
+
+// ---------------------------------------------------------------------------
+// Pass 2: tile columns, per-row offsets, masks and the in-tile entries.
+// ---------------------------------------------------------------------------
+__global__ void k_tile_fill(int m, int tilem, const int *__restrict__ rowptr,
+                            const int *__restrict__ col, const double *__restrict__ val,
+                            const int *__restrict__ tile_ptr, int packed,
+                            int *__restrict__ tile_columnidx, int *__restrict__ tile_rowidx,
+                            int *__restrict__ tile_nnz, unsigned char *__restrict__ tPtr,
+                            unsigned char *__restrict__ tCol, double *__restrict__ tVal,
+                            unsigned short *__restrict__ tMask)
+{
+    const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int tr = (int)(gid >> 4);
+    const int lane = threadIdx.x & 15;
+    const unsigned hmask = HW_MASK(threadIdx.x);
+    if (tr >= tilem)
+        return;
+    const int r = tr * TSG_BS + lane;
+    int p = 0, e = 0;
+    if (r < m)
+    {
+        p = rowptr[r];
+        e = rowptr[r + 1];
+    }
+    // value offset of the tile row's first tile: the row's first CSR entry
+    int run = __shfl_sync(hmask, p, 0, 16);
+    int t = tile_ptr[tr];
+    int cur = p < e ? (col[p] >> 4) : INT_MAX;
+    while (true)
+    {
+        const int jm = __reduce_min_sync(hmask, cur);
+        if (jm == INT_MAX)
+            break;
+        int c = 0;
+        unsigned mk = 0;
+        if (cur == jm)
+        {
+            int q = p;
+            int cc;
+            while (q < e && ((cc = col[q]) >> 4) == jm)
+            {
+                mk |= 0x8000u >> (cc & 15);
+                q++;
+            }
+            c = q - p;
+        }
+        int incl = c;
+#pragma unroll
+        for (int d = 1; d < 16; d <<= 1)
+        {
+            int o = __shfl_up_sync(hmask, incl, d, 16);
+            if (lane >= d)
+                incl += o;
+        }
+        const int excl = incl - c;
+        const int total = __shfl_sync(hmask, incl, 15, 16);
+        tPtr[(long long)t * TSG_BS + lane] = (unsigned char)excl;
+        tMask[(long long)t * TSG_BS + lane] = (unsigned short)mk;
+        if (lane == 0)
+        {
+            tile_columnidx[t] = jm;
+            tile_rowidx[t] = tr;
+            tile_nnz[t] = run;
+        }
+        const int dst = run + excl;
+        for (int i = 0; i < c; i++)
+        {
+            const int cc = col[p + i] & 15;
+            tCol[dst + i] = (unsigned char)(packed ? ((lane << 4) | cc) : cc);
+            tVal[dst + i] = val[p + i];
+        }
+        p += c;
+        cur = p < e ? (col[p] >> 4) : INT_MAX;
+        run += total;
+        t++;
+    }
+    if (tr == tilem - 1 && lane == 0)
+        tile_nnz[t] = run; // tile_nnz[numtile] = nnz
+}
+
+int tsg_tiled_alloc_arrays(tsg_context *ctx, tsg_tiled *t, int with_csc)
+{
+    const size_t T = (size_t)t->numtile;
+    TSG_TRY(tsg_alloc(ctx, &t->tile_columnidx, T));
+    TSG_TRY(tsg_alloc(ctx, &t->tile_rowidx, T));
+    TSG_TRY(tsg_alloc(ctx, &t->tile_nnz, T + 1));
+    TSG_TRY(tsg_alloc(ctx, &t->tile_csr_Ptr, T * TSG_BS));
+    TSG_TRY(tsg_alloc(ctx, &t->mask, T * TSG_BS));
+    TSG_TRY(tsg_alloc(ctx, &t->tile_csr_Col, (size_t)t->nnz));
+    TSG_TRY(tsg_alloc(ctx, &t->tile_csr_Value, (size_t)t->nnz));
+    if (with_csc)
+    {
+        TSG_TRY(tsg_alloc(ctx, &t->csc_tile_ptr, (size_t)t->tilen + 1));
+        TSG_TRY(tsg_alloc(ctx, &t->csc_tile_rowidx, T));
+        TSG_TRY(tsg_alloc(ctx, &t->csc_tile_pos, T));
+    }
+    return TSG_OK;
+}
+
+extern "C" int tsg_csr_to_tiled(tsg_context *ctx, int m, int n, int nnz, const int *d_rowptr,
+                                const int *d_colidx, const double *d_val, int flags, tsg_tiled *out)
+{
+    if (!ctx || !out)
+        return tsg_set_error(TSG_ERR_INVALID, "null argument");
+    memset(out, 0, sizeof(*out));
+    TSG_TRY(tsg_check_csr(ctx, m, n, nnz, d_rowptr, d_colidx));
+    out->m = m;
+    out->n = n;
+    out->nnz = nnz;
+    out->tilem = (m + TSG_BS - 1) / TSG_BS;
+    out->tilen = (n + TSG_BS - 1) / TSG_BS;
+    out->col_packed = (flags & TSG_TILED_PACKED_COL) ? 1 : 0;
+    const int tilem = out->tilem;
+    TSG_TRY(tsg_alloc(ctx, &out->tile_ptr, (size_t)tilem + 1));
+    long long T = 0;
+    if (tilem > 0)
+    {
+        k_tile_count<<<tsg_blocks((long long)tilem * 16, 256), 256, 0, ctx->stream>>>(
+            m, tilem, d_rowptr, d_colidx, out->tile_ptr);
+        TSG_LAUNCH_CHECK();
+        TSG_TRY(tsg_scan_counts(ctx, out->tile_ptr, out->tile_ptr, tilem, &T));
+    }
+    else
+    {
+        TSG_CUDA(cudaMemsetAsync(out->tile_ptr, 0, sizeof(int), ctx->stream));
+    }
+    out->numtile = (int)T;
+    TSG_TRY(tsg_tiled_alloc_arrays(ctx, out, (flags & TSG_TILED_CSC_VIEW) ? 1 : 0));
+    if (tilem > 0)
+    {
+        k_tile_fill<<<tsg_blocks((long long)tilem * 16, 256), 256, 0, ctx->stream>>>(
+            m, tilem, d_rowptr, d_colidx, d_val, out->tile_ptr, out->col_packed, out->tile_columnidx,
+            out->tile_rowidx, out->tile_nnz, out->tile_csr_Ptr, out->tile_csr_Col, out->tile_csr_Value,
+            out->mask);
+        TSG_LAUNCH_CHECK();
+    }
+    else
+    {
+        TSG_CUDA(cudaMemsetAsync(out->tile_nnz, 0, sizeof(int), ctx->stream));
+    }
+    if (flags & TSG_TILED_CSC_VIEW)
+        TSG_TRY(tsg_build_csc_view(ctx, out));
+    return TSG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Column view: tiles sorted stably by tile column (row order kept inside a
+// column), giving csc_tile_ptr / csc_tile_rowidx / csc_tile_pos.
+// ---------------------------------------------------------------------------
+__global__ void k_csc_keys(int T, const int *__restrict__ tile_col, unsigned int *__restrict__ keys,
+                           int *__restrict__ vals, int *__restrict__ hist)
+{
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < T; t += gridDim.x * blockDim.x)
+    {
+        int j = tile_col[t];
+        keys[t] = (unsigned int)j;
+        vals[t] = t;
+        atomicAdd(&hist[j], 1);
+    }
+}
+
+__global__ void k_csc_rows(int T, const int *__restrict__ pos, const int *__restrict__ tile_row,
+                           int *__restrict__ csc_row)
+{
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < T; q += gridDim.x * blockDim.x)
+        csc_row[q] = tile_row[pos[q]];
+}
+
+static int bits_for(long long v)
+{
+    int b = 1;
+    while (b < 63 && (1LL << b) <= v)
+        b++;
+    return b;
+}
+
+int tsg_build_csc_view(tsg_context *ctx, tsg_tiled *mat)
+{
+    const int T = mat->numtile, tilen = mat->tilen;
+    if (!mat->csc_tile_ptr)
+    {
+        TSG_TRY(tsg_alloc(ctx, &mat->csc_tile_ptr, (size_t)tilen + 1));
+        TSG_TRY(tsg_alloc(ctx, &mat->csc_tile_rowidx, (size_t)T));
+        TSG_TRY(tsg_alloc(ctx, &mat->csc_tile_pos, (size_t)T));
+    }
+    TSG_CUDA(cudaMemsetAsync(mat->csc_tile_ptr, 0, ((size_t)tilen + 1) * sizeof(int), ctx->stream));
+    if (T == 0)
+        return TSG_OK;
+    unsigned int *keys;
+    TSG_TRY(tsg_alloc(ctx, &keys, (size_t)T));
+    unsigned grid = tsg_blocks(T, 256);
+    k_csc_keys<<<grid, 256, 0, ctx->stream>>>(T, mat->tile_columnidx, keys, mat->csc_tile_pos, mat->csc_tile_ptr);
+    TSG_LAUNCH_CHECK();
+    TSG_TRY(tsg_scan_counts(ctx, mat->csc_tile_ptr, mat->csc_tile_ptr, tilen, nullptr));
+    TSG_TRY(tsg_sort_pairs_u32(ctx, keys, mat->csc_tile_pos, T, bits_for(tilen)));
+    k_csc_rows<<<grid, 256, 0, ctx->stream>>>(T, mat->csc_tile_pos, mat->tile_rowidx, mat->csc_tile_rowidx);
+    TSG_LAUNCH_CHECK();
+    tsg_release(ctx, keys);
+    return TSG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Column-major gather (the reference B layout): tile data reordered by the
+// column view, Col bytes unpacked to plain columns.
+// ---------------------------------------------------------------------------
+__global__ void k_cm_counts(int T, const int *__restrict__ pos, const int *__restrict__ tnnz,
+                            int *__restrict__ cnt)
+{
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < T; q += gridDim.x * blockDim.x)
+    {
+        int t = pos ? pos[q] : q;
+        cnt[q] = tnnz[t + 1] - tnnz[t];
+    }
+}
+
+// Half-warp per output tile q.
+__global__ void k_cm_gather(int T, const int *__restrict__ pos, const int *__restrict__ tnnz_src,
+                            const unsigned char *__restrict__ Ptr_src, const unsigned short *__restrict__ mask_src,
+                            const unsigned char *__restrict__ Col_src, const double *__restrict__ Val_src,
+                            const int *__restrict__ tnnz_dst, unsigned char *__restrict__ Ptr_dst,
+                            unsigned short *__restrict__ mask_dst, unsigned char *__restrict__ Col_dst,
+                            double *__restrict__ Val_dst)
+{
+    const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int q = (int)(gid >> 4);
+    const int lane = threadIdx.x & 15;
+    if (q >= T)
+        return;
+    const int t = pos ? pos[q] : q;
+    Ptr_dst[(long long)q * TSG_BS + lane] = Ptr_src[(long long)t * TSG_BS + lane];
+    mask_dst[(long long)q * TSG_BS + lane] = mask_src[(long long)t * TSG_BS + lane];
+    const int s = tnnz_src[t], n = tnnz_src[t + 1] - s, d = tnnz_dst[q];
+    for (int i = lane; i < n; i += 16)
+    {
+        Col_dst[d + i] = Col_src[s + i] & 15;
+        Val_dst[d + i] = Val_src[s + i];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Tiles -> CSR (src/tile2csr.h:8-137).  Half-warp per tile row, lane = row.
+// Row r of a tile spans [Ptr[r], Ptr[r+1]); the last real row of the tile
+// row ends at the tile nnz.
+// ---------------------------------------------------------------------------
+__global__ void k_t2c_rowlen(int m, int tilem, const int *__restrict__ tile_ptr,
+                             const int *__restrict__ tnnz, const unsigned char *__restrict__ Ptr,
+                             int *__restrict__ rowlen)
+{
+    const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int tr = (int)(gid >> 4);
+    const int lane = threadIdx.x & 15;
+    if (tr >= tilem)
+        return;
+    const int rows = tr == tilem - 1 ? m - (tilem - 1) * TSG_BS : TSG_BS;
+    if (lane >= rows)
+        return;
+    int sum = 0;
+    for (int t = tile_ptr[tr]; t < tile_ptr[tr + 1]; t++)
+    {
+        const int s = Ptr[(long long)t * TSG_BS + lane];
+        const int e = lane == rows - 1 ? tnnz[t + 1] - tnnz[t] : Ptr[(long long)t * TSG_BS + lane + 1];
+        sum += e - s;
+    }
+    rowlen[tr * TSG_BS + lane] = sum;
+}
+
+__global__ void k_t2c_fill(int m, int tilem, const int *__restrict__ tile_ptr,
+                           const int *__restrict__ tile_col, const int *__restrict__ tnnz,
+                           const unsigned char *__restrict__ Ptr, const unsigned char *__restrict__ Col,
+                           const double *__restrict__ Val, const int *__restrict__ rowptr,
+                           int *__restrict__ ccol, double *__restrict__ cval)
+{
+    const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int tr = (int)(gid >> 4);
+    const int lane = threadIdx.x & 15;
+    if (tr >= tilem)
+        return;
+    const int rows = tr == tilem - 1 ? m - (tilem - 1) * TSG_BS : TSG_BS;
+    if (lane >= rows)
+        return;
+    int off = rowptr[tr * TSG_BS + lane];
+    for (int t = tile_ptr[tr]; t < tile_ptr[tr + 1]; t++)
+    {
+        const int s = Ptr[(long long)t * TSG_BS + lane];
+        const int e = lane == rows - 1 ? tnnz[t + 1] - tnnz[t] : Ptr[(long long)t * TSG_BS + lane + 1];
+        const int base = tnnz[t];
+        const int cb = tile_col[t] * TSG_BS;
+        for (int q = s; q < e; q++)
+        {
+            ccol[off] = cb + Col[base + q];
+            cval[off] = Val[base + q];
+            off++;
+        }
+    }
+}
+
+extern "C" int tsg_tiled_to_csr(tsg_context *ctx, const tsg_tiled *C, int *d_rowptr, int *d_colidx,
+                                double *d_val)
+{
+    if (!ctx || !C || !d_rowptr)
+        return tsg_set_error(TSG_ERR_INVALID, "null argument");
+    const int m = C->m, tilem = C->tilem;
+    if (m == 0)
+    {
+        TSG_CUDA(cudaMemsetAsync(d_rowptr, 0, sizeof(int), ctx->stream));
+        return TSG_OK;
+    }
+    k_t2c_rowlen<<<tsg_blocks((long long)tilem * 16, 256), 256, 0, ctx->stream>>>(
+        m, tilem, C->tile_ptr, C->tile_nnz, C->tile_csr_Ptr, d_rowptr);
+    TSG_LAUNCH_CHECK();
+    TSG_TRY(tsg_scan_counts(ctx, d_rowptr, d_rowptr, m, nullptr));
+    k_t2c_fill<<<tsg_blocks((long long)tilem * 16, 256), 256, 0, ctx->stream>>>(
+        m, tilem, C->tile_ptr, C->tile_columnidx, C->tile_nnz, C->tile_csr_Ptr, C->tile_csr_Col,
+        C->tile_csr_Value, d_rowptr, d_colidx, d_val);
+    TSG_LAUNCH_CHECK();
+    return TSG_OK;
+}
+
+// Column-major download helper used by tsg_tiled_download (tsg_api.cu).
+int tsg_gather_colmajor(tsg_context *ctx, const tsg_tiled *src, int *tnnz_cm, unsigned char *Ptr_cm,
+                        unsigned short *mask_cm, unsigned char *Col_cm, double *Val_cm)
+{
+    const int T = src->numtile;
+    if (T == 0)
+    {
+        TSG_CUDA(cudaMemsetAsync(tnnz_cm, 0, sizeof(int), ctx->stream));
+        return TSG_OK;
+    }
+    unsigned grid = tsg_blocks(T, 256);
+    k_cm_counts<<<grid, 256, 0, ctx->stream>>>(T, src->csc_tile_pos, src->tile_nnz, tnnz_cm);
+    TSG_LAUNCH_CHECK();
+    TSG_TRY(tsg_scan_counts(ctx, tnnz_cm, tnnz_cm, T, nullptr));
+    k_cm_gather<<<tsg_blocks((long long)T * 16, 256), 256, 0, ctx->stream>>>(
+        T, src->csc_tile_pos, src->tile_nnz, src->tile_csr_Ptr, src->mask, src->tile_csr_Col,
+        src->tile_csr_Value, tnnz_cm, Ptr_cm, mask_cm, Col_cm, Val_cm);
+    TSG_LAUNCH_CHECK();
+    return TSG_OK;
+}

@@ -1,0 +1,106 @@
+// Internal declarations shared by the library's translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string.h>
+
+#include "tilespgemm_b200.h"
+
+#define TSG_BS 16
+
+struct tsg_context
+{
+    int device;
+    int num_sms;
+    cudaStream_t stream;
+    int own_stream;
+    int timing;
+    cudaEvent_t ev[8];
+    long long *h_pinned; // small pinned buffer for scalar read-backs
+    long long launches;  // kernels this library launched on the context
+};
+
+// Records a formatted message as the thread's last error and returns code.
+int tsg_set_error(int code, const char *fmt, ...);
+
+#define TSG_CUDA(call)                                                                      \
+    do                                                                                      \
+    {                                                                                       \
+        cudaError_t _e = (call);                                                            \
+        if (_e != cudaSuccess)                                                              \
+            return tsg_set_error(_e == cudaErrorMemoryAllocation ? TSG_ERR_OOM : TSG_ERR_CUDA, \
+                                 "%s:%d %s: %s", __FILE__, __LINE__, #call,                \
+                                 cudaGetErrorString(_e));                                   \
+    } while (0)
+
+#define TSG_TRY(expr)      \
+    do                     \
+    {                      \
+        int _s = (expr);   \
+        if (_s != TSG_OK)  \
+            return _s;     \
+    } while (0)
+
+#define TSG_LAUNCH_CHECK()     \
+    do                         \
+    {                          \
+        ctx->launches++;       \
+        TSG_CUDA(cudaGetLastError()); \
+    } while (0)
+
+template <typename T>
+static inline int tsg_alloc(tsg_context *ctx, T **p, size_t count)
+{
+    *p = nullptr;
+    if (count == 0)
+        count = 1;
+    cudaError_t e = cudaMallocAsync((void **)p, count * sizeof(T), ctx->stream);
+    if (e != cudaSuccess)
+    {
+        *p = nullptr;
+        return tsg_set_error(TSG_ERR_OOM, "device allocation of %zu bytes failed: %s",
+                             count * sizeof(T), cudaGetErrorString(e));
+    }
+    return TSG_OK;
+}
+
+template <typename T>
+static inline void tsg_release(tsg_context *ctx, T *&p)
+{
+    if (p)
+        cudaFreeAsync((void *)p, ctx->stream);
+    p = nullptr;
+}
+
+static inline unsigned int tsg_blocks(long long work, int per_block)
+{
+    long long b = (work + per_block - 1) / per_block;
+    return (unsigned int)(b < 1 ? 1 : b);
+}
+
+// Exclusive scan of n int32 counts into out[0..n] (out[n] = total).  in and
+// out may alias.  The total is also returned through *total (synchronous
+// read-back) when total != nullptr.
+int tsg_scan_counts(tsg_context *ctx, const int *in, int *out, long long n, long long *total);
+
+// Stable sort of (key, value) pairs by the low end_bit bits of the keys.
+int tsg_sort_pairs_u64(tsg_context *ctx, unsigned long long *keys, int *vals, long long n, int end_bit);
+int tsg_sort_pairs_u32(tsg_context *ctx, unsigned int *keys, int *vals, long long n, int end_bit);
+
+// Validates a device CSR (ptr monotone, rowptr[0]=0, rowptr[m]=nnz, columns
+// in range and strictly increasing per row).
+int tsg_check_csr(tsg_context *ctx, int m, int n, int nnz, const int *rowptr, const int *colidx);
+
+// Column view of a row-major tiled matrix (csc_tile_ptr / rowidx / pos).
+int tsg_build_csc_view(tsg_context *ctx, tsg_tiled *mat);
+
+// Readback helper: copies one long long / int from device to host (syncs).
+int tsg_read_int(tsg_context *ctx, const int *dptr, long long *out);
+
+// Product count over device CSR arrays.
+int tsg_count_products_dev(tsg_context *ctx, int nnzA, const int *a_col, const int *b_rowptr,
+                           long long *out);
+
+int tsg_tiled_alloc_arrays(tsg_context *ctx, tsg_tiled *t, int with_csc);

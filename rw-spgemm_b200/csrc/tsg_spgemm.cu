@@ -1,0 +1,473 @@
+// Tiled SpGEMM C = A*B on 16x16 tiles, FP64, for sm_100a.
+//
+// Restates the three steps of the reference's tilespgemm()
+// (src/tilespgemm-cuda.h:2610-3221):
+//   step 1  tile structure of C        (reference :257-369, :2766-2848)
+//   step 2  per-tile bitmask symbolic   (reference :371-755, :2866-2989)
+//   step 3  numeric                     (reference :1505-2608, :3006-3118)
+// with the same outputs (tile_ptr, sorted tile columns, 16-bit row masks,
+// uint8 row offsets, tile nnz scan, plain column bytes, FP64 values).
+//
+// Design (B200):
+//  * step 1: one warp per A tile row ORs the tile-column lists of the B tile
+//    rows it touches into a shared-memory bitmap restricted to the row's
+//    column window; popcount gives the count, an ordered bit walk emits the
+//    sorted C tile columns.
+//  * step 2/3: one half-warp per C tile.  The A tile row and the B tile
+//    column are intersected 16 elements at a time with lanes holding the
+//    chunks in registers (shuffle binary search + ballot), so matches come
+//    out in ascending k with no scratch memory.  Step 2 multiplies 16x16
+//    boolean tiles: lane r ORs the B mask rows selected by A's row-r mask
+//    (the whole B mask is one 32-byte broadcast load).  Step 3 gives lane r
+//    ownership of C row r: it accumulates a*b for its A row entries against
+//    the selected B rows into a padded shared-memory row, in k-ascending,
+//    A-entry order, with separately rounded multiply and add -- the order and
+//    rounding of the reference's CPU oracle (src/spgemm-cpu.h:330), so
+//    results are deterministic and bit-identical run to run, with no FP64
+//    atomics.  The compressed tile is then written with coalesced stores,
+//    columns recovered from the mask with __fns.
+#include <limits.h>
+
+#include "tsg_internal.h"
+
+#define FULL_MASK 0xffffffffu
+#define HW_MASK(tid) (0xFFFFu << ((tid) & 16))
+
+// ---------------------------------------------------------------------------
+// Step 1
+// ---------------------------------------------------------------------------
+#define S1_WARPS 8
+#define S1_WORDS 1024
+
+template <bool EMIT>
+__global__ void __launch_bounds__(S1_WARPS * 32)
+    k_step1(int tilemA, const int *__restrict__ A_ptr, const int *__restrict__ A_col,
+            const int *__restrict__ B_ptr, const int *__restrict__ B_col, int *__restrict__ C_cnt,
+            const int *__restrict__ C_ptr, int *__restrict__ C_col, int *__restrict__ C_row,
+            unsigned long long *__restrict__ pairs)
+{
+    __shared__ unsigned int s_bm[S1_WARPS][S1_WORDS];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int i = blockIdx.x * S1_WARPS + warp;
+    if (i >= tilemA)
+        return;
+    unsigned int *bm = s_bm[warp];
+    const int a0 = A_ptr[i], a1 = A_ptr[i + 1];
+    int lo = INT_MAX, hi = -1;
+    unsigned long long np = 0;
+    for (int pa = a0 + lane; pa < a1; pa += 32)
+    {
+        const int k = A_col[pa];
+        const int b0 = B_ptr[k], b1 = B_ptr[k + 1];
+        if (b1 > b0)
+        {
+            lo = min(lo, B_col[b0]);
+            hi = max(hi, B_col[b1 - 1]);
+            np += (unsigned long long)(b1 - b0);
+        }
+    }
+    lo = __reduce_min_sync(FULL_MASK, lo);
+    hi = __reduce_max_sync(FULL_MASK, hi);
+    if (!EMIT && pairs)
+    {
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1)
+            np += __shfl_xor_sync(FULL_MASK, np, d);
+        if (lane == 0 && np)
+            atomicAdd(pairs, np);
+    }
+    int out = 0;
+    const int cbase = EMIT ? C_ptr[i] : 0;
+    if (hi >= 0)
+    {
+        for (int c0 = lo & ~31; c0 <= hi; c0 += S1_WORDS * 32)
+        {
+            const int c1 = min(hi + 1, c0 + S1_WORDS * 32);
+            const int nw = (c1 - c0 + 31) >> 5;
+            for (int w = lane; w < nw; w += 32)
+                bm[w] = 0;
+            __syncwarp();
+            for (int pa = a0; pa < a1; pa++)
+            {
+                const int k = A_col[pa];
+                const int b0 = B_ptr[k], b1 = B_ptr[k + 1];
+                for (int pb = b0 + lane; pb < b1; pb += 32)
+                {
+                    const int j = B_col[pb];
+                    if (j >= c0 && j < c1)
+                        atomicOr(&bm[(j - c0) >> 5], 1u << ((j - c0) & 31));
+                }
+            }
+            __syncwarp();
+            for (int wb = 0; wb < nw; wb += 32)
+            {
+                const int w = wb + lane;
+                unsigned bits = w < nw ? bm[w] : 0u;
+                const int cnt = __popc(bits);
+                if (EMIT)
+                {
+                    int incl = cnt;
+#pragma unroll
+                    for (int d = 1; d < 32; d <<= 1)
+                    {
+                        int o = __shfl_up_sync(FULL_MASK, incl, d);
+                        if (lane >= d)
+                            incl += o;
+                    }
+                    int pos = cbase + out + incl - cnt;
+                    while (bits)
+                    {
+                        const int b = __ffs(bits) - 1;
+                        bits &= bits - 1;
+                        C_col[pos] = c0 + (w << 5) + b;
+                        C_row[pos] = i;
+                        pos++;
+                    }
+                    out += __shfl_sync(FULL_MASK, incl, 31);
+                }
+                else
+                {
+                    out += __reduce_add_sync(FULL_MASK, cnt);
+                }
+            }
+            __syncwarp();
+        }
+    }
+    if (!EMIT && lane == 0)
+        C_cnt[i] = out;
+}
+
+// ---------------------------------------------------------------------------
+// Tile-list intersection for one C tile (half-warp).  Calls f(x, posA, posB)
+// for every matched k in ascending order; uniform across the half-warp.
+// ---------------------------------------------------------------------------
+template <typename F>
+__device__ __forceinline__ void intersect_tiles(unsigned hmask, int lane, const int *__restrict__ a_list,
+                                                int abase, int la, const int *__restrict__ b_list,
+                                                const int *__restrict__ b_pos, int bbase, int lb, F f)
+{
+    int ia = 0, ib = 0;
+    while (ia < la && ib < lb)
+    {
+        const int va = ia + lane < la ? a_list[abase + ia + lane] : INT_MAX;
+        const int vb = ib + lane < lb ? b_list[bbase + ib + lane] : INT_MAX;
+        int pos = 0;
+#pragma unroll
+        for (int s = 8; s >= 1; s >>= 1)
+        {
+            const int v = __shfl_sync(hmask, vb, pos + s - 1, 16);
+            if (v < va)
+                pos += s;
+        }
+        const int cand = __shfl_sync(hmask, vb, pos, 16);
+        const bool found = (cand == va) && (va != INT_MAX);
+        unsigned bal = __ballot_sync(hmask, found);
+        bal = (bal >> (threadIdx.x & 16)) & 0xFFFFu;
+        while (bal)
+        {
+            const int x = __ffs(bal) - 1;
+            bal &= bal - 1;
+            const int y = __shfl_sync(hmask, pos, x, 16);
+            const int q = bbase + ib + y;
+            const int posB = b_pos ? b_pos[q] : q;
+            f(abase + ia + x, posB);
+        }
+        const int amax = __shfl_sync(hmask, va, 15, 16);
+        const int bmax = __shfl_sync(hmask, vb, 15, 16);
+        if (amax <= bmax)
+            ia += 16;
+        if (bmax <= amax)
+            ib += 16;
+    }
+}
+
+// Row r of the boolean product: OR of B's mask rows c for every column c set
+// in A's row mask (bit 15-c).  q0/q1 hold B's 16 row masks (rows 2w, 2w+1 in
+// the low / high half of word w).
+__device__ __forceinline__ unsigned bool_row(unsigned ma, uint4 q0, uint4 q1)
+{
+    unsigned r = 0;
+    const unsigned w[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
+#pragma unroll
+    for (int c = 0; c < 16; c++)
+    {
+        const unsigned row = (c & 1) ? (w[c >> 1] >> 16) : (w[c >> 1] & 0xFFFFu);
+        r |= ((ma >> (15 - c)) & 1u) ? row : 0u;
+    }
+    return r;
+}
+
+// ---------------------------------------------------------------------------
+// Step 2: masks, row offsets and nnz of every C tile (half-warp per tile).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+    k_step2(int numC, const int *__restrict__ C_row, const int *__restrict__ C_col,
+            const int *__restrict__ A_ptr, const int *__restrict__ A_col,
+            const unsigned short *__restrict__ A_mask, const int *__restrict__ B_cptr,
+            const int *__restrict__ B_crow, const int *__restrict__ B_cpos,
+            const unsigned short *__restrict__ B_mask, unsigned short *__restrict__ C_mask,
+            unsigned char *__restrict__ C_Ptr, int *__restrict__ C_cnt, int *__restrict__ bins)
+{
+    __shared__ int s_bins[4];
+    if (threadIdx.x < 4)
+        s_bins[threadIdx.x] = 0;
+    __syncthreads();
+    const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = (int)(gid >> 4);
+    const int lane = threadIdx.x & 15;
+    const unsigned hmask = HW_MASK(threadIdx.x);
+    if (t < numC)
+    {
+        const int i = C_row[t], j = C_col[t];
+        const int abase = A_ptr[i], la = A_ptr[i + 1] - abase;
+        const int bbase = B_cptr[j], lb = B_cptr[j + 1] - bbase;
+        unsigned acc = 0;
+        intersect_tiles(hmask, lane, A_col, abase, la, B_crow, B_cpos, bbase, lb, [&](int posA, int posB) {
+            const unsigned ma = A_mask[(long long)posA * TSG_BS + lane];
+            const uint4 *mb = reinterpret_cast<const uint4 *>(B_mask + (long long)posB * TSG_BS);
+            const uint4 q0 = __ldg(mb), q1 = __ldg(mb + 1);
+            acc |= bool_row(ma, q0, q1);
+        });
+        const int cnt = __popc(acc);
+        int incl = cnt;
+#pragma unroll
+        for (int d = 1; d < 16; d <<= 1)
+        {
+            const int o = __shfl_up_sync(hmask, incl, d, 16);
+            if (lane >= d)
+                incl += o;
+        }
+        const int total = __shfl_sync(hmask, incl, 15, 16);
+        C_mask[(long long)t * TSG_BS + lane] = (unsigned short)acc;
+        C_Ptr[(long long)t * TSG_BS + lane] = (unsigned char)(incl - cnt);
+        if (lane == 0)
+        {
+            C_cnt[t] = total;
+            if (total > 0)
+            {
+                const int b = total <= 32 ? 0 : total <= 224 ? 1 : total < 256 ? 2 : 3;
+                atomicAdd(&s_bins[b], 1);
+            }
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < 4 && s_bins[threadIdx.x])
+        atomicAdd(&bins[threadIdx.x], s_bins[threadIdx.x]);
+}
+
+// ---------------------------------------------------------------------------
+// Step 3: numeric (half-warp per C tile, lane r owns C row r).
+// ---------------------------------------------------------------------------
+#define S3_THREADS 256
+#define S3_HW (S3_THREADS / 16)
+#define S3_STRIDE 17
+
+__global__ void __launch_bounds__(S3_THREADS)
+    k_step3(int numC, const int *__restrict__ C_row, const int *__restrict__ C_col,
+            const int *__restrict__ A_ptr, const int *__restrict__ A_col, const int *__restrict__ A_tnnz,
+            const unsigned char *__restrict__ A_Ptr, const unsigned char *__restrict__ A_Colb,
+            const double *__restrict__ A_Val, const int *__restrict__ B_cptr, const int *__restrict__ B_crow,
+            const int *__restrict__ B_cpos, const int *__restrict__ B_tnnz,
+            const unsigned char *__restrict__ B_Ptr, const unsigned char *__restrict__ B_Colb,
+            const double *__restrict__ B_Val, const int *__restrict__ C_tnnz,
+            const unsigned short *__restrict__ C_mask, const unsigned char *__restrict__ C_Ptr,
+            unsigned char *__restrict__ C_Colb, double *__restrict__ C_Val)
+{
+    __shared__ double s_acc[S3_HW][TSG_BS * S3_STRIDE];
+    const int hw = threadIdx.x >> 4;
+    double *acc = s_acc[hw];
+    const int lane = threadIdx.x & 15;
+    const unsigned hmask = HW_MASK(threadIdx.x);
+    for (int q = lane; q < TSG_BS * S3_STRIDE; q += 16)
+        acc[q] = 0.0;
+    __syncwarp(hmask);
+    const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = (int)(gid >> 4);
+    if (t >= numC)
+        return;
+    const int cb = C_tnnz[t], cn = C_tnnz[t + 1] - cb;
+    if (cn == 0)
+        return;
+    const int i = C_row[t], j = C_col[t];
+    const int abase = A_ptr[i], la = A_ptr[i + 1] - abase;
+    const int bbase = B_cptr[j], lb = B_cptr[j + 1] - bbase;
+    double *myrow = acc + lane * S3_STRIDE;
+    intersect_tiles(hmask, lane, A_col, abase, la, B_crow, B_cpos, bbase, lb, [&](int posA, int posB) {
+        const int a0 = A_tnnz[posA], na = A_tnnz[posA + 1] - a0;
+        const int sa = A_Ptr[(long long)posA * TSG_BS + lane];
+        const int ea = lane == TSG_BS - 1 ? na : A_Ptr[(long long)posA * TSG_BS + lane + 1];
+        const int b0 = B_tnnz[posB], nb = B_tnnz[posB + 1] - b0;
+        const unsigned char *bp = B_Ptr + (long long)posB * TSG_BS;
+        for (int x = sa; x < ea; x++)
+        {
+            const int ca = A_Colb[a0 + x] & 15;
+            const double a = A_Val[a0 + x];
+            const int sb = bp[ca];
+            const int eb = ca == TSG_BS - 1 ? nb : bp[ca + 1];
+            for (int y = sb; y < eb; y++)
+            {
+                const int c = B_Colb[b0 + y] & 15;
+                myrow[c] = __dadd_rn(myrow[c], __dmul_rn(a, B_Val[b0 + y]));
+            }
+        }
+    });
+    __syncwarp(hmask);
+    const int excl = C_Ptr[(long long)t * TSG_BS + lane];
+    const unsigned mrev = __brev((unsigned)C_mask[(long long)t * TSG_BS + lane]) >> 16;
+    // every lane runs the same trip count so the shuffles see all 16 lanes
+    for (int pb = 0; pb < cn; pb += 16)
+    {
+        const int p = pb + lane;
+        int r = 0;
+#pragma unroll
+        for (int s = 8; s >= 1; s >>= 1)
+        {
+            const int v = __shfl_sync(hmask, excl, r + s, 16);
+            if (v <= p)
+                r += s;
+        }
+        const unsigned mr = __shfl_sync(hmask, mrev, r, 16);
+        const int rank = p - __shfl_sync(hmask, excl, r, 16);
+        if (p < cn)
+        {
+            const int c = (int)__fns(mr, 0, rank + 1) & 15;
+            double *cell = acc + r * S3_STRIDE + c;
+            C_Colb[cb + p] = (unsigned char)c;
+            C_Val[cb + p] = *cell;
+            *cell = 0.0;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host orchestration.
+// ---------------------------------------------------------------------------
+static int validate_operands(const tsg_tiled *A, const tsg_tiled *B)
+{
+    if (!A || !B)
+        return tsg_set_error(TSG_ERR_INVALID, "null operand");
+    if (A->n != B->m)
+        return tsg_set_error(TSG_ERR_INVALID, "inner dimensions differ (A is %dx%d, B is %dx%d)", A->m,
+                             A->n, B->m, B->n);
+    if (!B->csc_tile_ptr || !B->csc_tile_rowidx)
+        return tsg_set_error(TSG_ERR_INVALID, "B has no column view (build it with TSG_TILED_CSC_VIEW)");
+    if (!A->tile_ptr || !B->tile_ptr)
+        return tsg_set_error(TSG_ERR_INVALID, "operand without tile structure");
+    return TSG_OK;
+}
+
+static float ev_ms(cudaEvent_t a, cudaEvent_t b)
+{
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    return ms;
+}
+
+extern "C" int tsg_spgemm(tsg_context *ctx, const tsg_tiled *A, const tsg_tiled *B, tsg_tiled *C,
+                          tsg_spgemm_info *info)
+{
+    if (!ctx || !C)
+        return tsg_set_error(TSG_ERR_INVALID, "null argument");
+    TSG_TRY(validate_operands(A, B));
+    memset(C, 0, sizeof(*C));
+    C->m = A->m;
+    C->n = B->n;
+    C->tilem = A->tilem;
+    C->tilen = B->tilen;
+    C->col_packed = 0;
+    const int tilem = C->tilem;
+    cudaStream_t st = ctx->stream;
+    const int timing = ctx->timing;
+    if (timing)
+        TSG_CUDA(cudaEventRecord(ctx->ev[0], st));
+
+    // step 1: structure
+    unsigned long long *d_pairs;
+    int *d_bins;
+    TSG_TRY(tsg_alloc(ctx, &d_pairs, 1));
+    TSG_TRY(tsg_alloc(ctx, &d_bins, 4));
+    TSG_CUDA(cudaMemsetAsync(d_pairs, 0, sizeof(unsigned long long), st));
+    TSG_CUDA(cudaMemsetAsync(d_bins, 0, 4 * sizeof(int), st));
+    TSG_TRY(tsg_alloc(ctx, &C->tile_ptr, (size_t)tilem + 1));
+    long long numC = 0;
+    if (tilem > 0)
+    {
+        k_step1<false><<<tsg_blocks(tilem, S1_WARPS), S1_WARPS * 32, 0, st>>>(
+            tilem, A->tile_ptr, A->tile_columnidx, B->tile_ptr, B->tile_columnidx, C->tile_ptr, nullptr,
+            nullptr, nullptr, d_pairs);
+        TSG_LAUNCH_CHECK();
+        TSG_TRY(tsg_scan_counts(ctx, C->tile_ptr, C->tile_ptr, tilem, &numC));
+    }
+    else
+        TSG_CUDA(cudaMemsetAsync(C->tile_ptr, 0, sizeof(int), st));
+    C->numtile = (int)numC;
+    TSG_TRY(tsg_alloc(ctx, &C->tile_columnidx, (size_t)numC));
+    TSG_TRY(tsg_alloc(ctx, &C->tile_rowidx, (size_t)numC));
+    if (numC > 0)
+    {
+        k_step1<true><<<tsg_blocks(tilem, S1_WARPS), S1_WARPS * 32, 0, st>>>(
+            tilem, A->tile_ptr, A->tile_columnidx, B->tile_ptr, B->tile_columnidx, nullptr, C->tile_ptr,
+            C->tile_columnidx, C->tile_rowidx, nullptr);
+        TSG_LAUNCH_CHECK();
+    }
+    if (timing)
+        TSG_CUDA(cudaEventRecord(ctx->ev[1], st));
+
+    // step 2: symbolic
+    TSG_TRY(tsg_alloc(ctx, &C->mask, (size_t)numC * TSG_BS));
+    TSG_TRY(tsg_alloc(ctx, &C->tile_csr_Ptr, (size_t)numC * TSG_BS));
+    TSG_TRY(tsg_alloc(ctx, &C->tile_nnz, (size_t)numC + 1));
+    long long nnzC = 0;
+    if (numC > 0)
+    {
+        k_step2<<<tsg_blocks(numC * 16, 256), 256, 0, st>>>(
+            (int)numC, C->tile_rowidx, C->tile_columnidx, A->tile_ptr, A->tile_columnidx, A->mask,
+            B->csc_tile_ptr, B->csc_tile_rowidx, B->csc_tile_pos, B->mask, C->mask, C->tile_csr_Ptr,
+            C->tile_nnz, d_bins);
+        TSG_LAUNCH_CHECK();
+        TSG_TRY(tsg_scan_counts(ctx, C->tile_nnz, C->tile_nnz, numC, &nnzC));
+    }
+    else
+        TSG_CUDA(cudaMemsetAsync(C->tile_nnz, 0, sizeof(int), st));
+    C->nnz = (int)nnzC;
+    if (timing)
+        TSG_CUDA(cudaEventRecord(ctx->ev[2], st));
+
+    // step 3: numeric
+    TSG_TRY(tsg_alloc(ctx, &C->tile_csr_Col, (size_t)nnzC));
+    TSG_TRY(tsg_alloc(ctx, &C->tile_csr_Value, (size_t)nnzC));
+    if (nnzC > 0)
+    {
+        k_step3<<<tsg_blocks(numC * 16, S3_THREADS), S3_THREADS, 0, st>>>(
+            (int)numC, C->tile_rowidx, C->tile_columnidx, A->tile_ptr, A->tile_columnidx, A->tile_nnz,
+            A->tile_csr_Ptr, A->tile_csr_Col, A->tile_csr_Value, B->csc_tile_ptr, B->csc_tile_rowidx,
+            B->csc_tile_pos, B->tile_nnz, B->tile_csr_Ptr, B->tile_csr_Col, B->tile_csr_Value, C->tile_nnz,
+            C->mask, C->tile_csr_Ptr, C->tile_csr_Col, C->tile_csr_Value);
+        TSG_LAUNCH_CHECK();
+    }
+    if (timing)
+        TSG_CUDA(cudaEventRecord(ctx->ev[3], st));
+
+    if (info)
+    {
+        memset(info, 0, sizeof(*info));
+        info->numtile_C = numC;
+        info->nnz_C = nnzC;
+        long long *h = ctx->h_pinned;
+        TSG_CUDA(cudaMemcpyAsync(h, d_pairs, sizeof(long long), cudaMemcpyDeviceToHost, st));
+        TSG_CUDA(cudaMemcpyAsync(h + 1, d_bins, 4 * sizeof(int), cudaMemcpyDeviceToHost, st));
+        TSG_CUDA(cudaStreamSynchronize(st));
+        info->tile_pairs = h[0];
+        memcpy(info->bins, h + 1, 4 * sizeof(int));
+        if (timing)
+        {
+            info->ms_step1 = ev_ms(ctx->ev[0], ctx->ev[1]);
+            info->ms_step2 = ev_ms(ctx->ev[1], ctx->ev[2]);
+            info->ms_step3 = ev_ms(ctx->ev[2], ctx->ev[3]);
+            info->ms_total = ev_ms(ctx->ev[0], ctx->ev[3]);
+        }
+    }
+    tsg_release(ctx, d_pairs);
+    tsg_release(ctx, d_bins);
+    return TSG_OK;
+}

@@ -1,0 +1,147 @@
+"""Seeded synthetic sparse matrices (CSR, int32 indices, FP64 values, rows
+sorted, no duplicates) standing in for the SuiteSparse inputs of the
+reference's experiments.
+
+Every generator returns ``(m, n, rowptr, colidx, val)`` as numpy arrays.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def _coo_to_csr(m, n, rows, cols, vals):
+    rows = np.asarray(rows, dtype=np.int64)
+    cols = np.asarray(cols, dtype=np.int64)
+    key = rows * n + cols
+    order = np.argsort(key, kind="stable")
+    key = key[order]
+    vals = np.asarray(vals, dtype=np.float64)[order]
+    keep = np.ones(key.size, dtype=bool)
+    keep[1:] = key[1:] != key[:-1]  # duplicates merged: first value kept
+    key = key[keep]
+    vals = vals[keep]
+    r = (key // n).astype(np.int64)
+    c = (key % n).astype(np.int32)
+    rowptr = np.zeros(m + 1, dtype=np.int64)
+    np.add.at(rowptr, r + 1, 1)
+    rowptr = np.cumsum(rowptr).astype(np.int32)
+    return m, n, rowptr, c, vals
+
+
+def laplacian_2d(nx: int, ny: int | None = None):
+    """5-point Laplacian on an nx x ny grid: 4 on the diagonal, -1 off it."""
+    ny = nx if ny is None else ny
+    n = nx * ny
+    idx = np.arange(n, dtype=np.int64)
+    x, y = idx % nx, idx // nx
+    rows, cols, vals = [idx], [idx], [np.full(n, 4.0)]
+    for dx, dy in ((1, 0), (-1, 0), (0, 1), (0, -1)):
+        ok = (x + dx >= 0) & (x + dx < nx) & (y + dy >= 0) & (y + dy < ny)
+        rows.append(idx[ok])
+        cols.append(idx[ok] + dx + dy * nx)
+        vals.append(np.full(int(ok.sum()), -1.0))
+    return _coo_to_csr(n, n, np.concatenate(rows), np.concatenate(cols), np.concatenate(vals))
+
+
+def stencil_27pt_3d(nx: int, seed: int = 0, low: float = 0.5, high: float = 1.5):
+    """27-point stencil on an nx^3 grid, values uniform(low, high)."""
+    n = nx ** 3
+    idx = np.arange(n, dtype=np.int64)
+    x, y, z = idx % nx, (idx // nx) % nx, idx // (nx * nx)
+    rows, cols = [], []
+    for dz in (-1, 0, 1):
+        for dy in (-1, 0, 1):
+            for dx in (-1, 0, 1):
+                ok = ((x + dx >= 0) & (x + dx < nx) & (y + dy >= 0) & (y + dy < nx)
+                      & (z + dz >= 0) & (z + dz < nx))
+                rows.append(idx[ok])
+                cols.append(idx[ok] + dx + dy * nx + dz * nx * nx)
+    rows = np.concatenate(rows)
+    cols = np.concatenate(cols)
+    m, n_, rp, ci, _ = _coo_to_csr(n, n, rows, cols, np.zeros(rows.size))
+    rng = np.random.default_rng(seed)
+    return m, n_, rp, ci, rng.uniform(low, high, ci.size)
+
+
+def rmat(scale: int, edge_factor: int, a=0.57, b=0.19, c=0.19, seed: int = 1,
+         low: float = -1.0, high: float = 1.0):
+    """R-MAT graph: 2^scale vertices, edge_factor * 2^scale edges drawn by
+    per-level quadrant choice with probabilities (a, b, c, 1-a-b-c);
+    duplicates merged; values uniform(low, high)."""
+    n = 1 << scale
+    ne = edge_factor * n
+    rng = np.random.default_rng(seed)
+    rows = np.zeros(ne, dtype=np.int64)
+    cols = np.zeros(ne, dtype=np.int64)
+    ab, abc = a + b, a + b + c
+    for level in range(scale):
+        u = rng.random(ne)
+        bit = 1 << (scale - 1 - level)
+        down = u >= ab            # quadrants c, d
+        right = ((u >= a) & (u < ab)) | (u >= abc)   # quadrants b, d
+        rows += down * bit
+        cols += right * bit
+    m, n_, rp, ci, _ = _coo_to_csr(n, n, rows, cols, np.zeros(ne))
+    return m, n_, rp, ci, rng.uniform(low, high, ci.size)
+
+
+def banded(n: int, half_bandwidth: int, seed: int = 0, low=-1.0, high=1.0):
+    """Full band |i-j| <= half_bandwidth, values uniform(low, high)."""
+    rows, cols = [], []
+    idx = np.arange(n, dtype=np.int64)
+    for d in range(-half_bandwidth, half_bandwidth + 1):
+        ok = (idx + d >= 0) & (idx + d < n)
+        rows.append(idx[ok])
+        cols.append(idx[ok] + d)
+    rows = np.concatenate(rows)
+    cols = np.concatenate(cols)
+    m, n_, rp, ci, _ = _coo_to_csr(n, n, rows, cols, np.zeros(rows.size))
+    rng = np.random.default_rng(seed)
+    return m, n_, rp, ci, rng.uniform(low, high, ci.size)
+
+
+def random_poisson(m: int, n: int | None = None, lam: float = 8.0, seed: int = 0, low=-1.0, high=1.0):
+    """Each row draws Poisson(lam) uniform random columns (duplicates merged)."""
+    n = m if n is None else n
+    rng = np.random.default_rng(seed)
+    per = rng.poisson(lam, m)
+    rows = np.repeat(np.arange(m, dtype=np.int64), per)
+    cols = rng.integers(0, n, rows.size)
+    mm, nn, rp, ci, _ = _coo_to_csr(m, n, rows, cols, np.zeros(rows.size))
+    return mm, nn, rp, ci, rng.uniform(low, high, ci.size)
+
+
+def random_symmetric_permutation(n: int, seed: int = 7):
+    """new -> old permutation (numpy default_rng(seed).permutation)."""
+    return np.random.default_rng(seed).permutation(n).astype(np.int32)
+
+
+def permute_symmetric(mat, order):
+    """P A P^T for a new->old order; rows re-sorted."""
+    m, n, rp, ci, v = mat
+    order = np.asarray(order, dtype=np.int64)
+    new_of_old = np.empty(n, dtype=np.int64)
+    new_of_old[order] = np.arange(n)
+    lens = np.diff(rp)
+    rows_old = np.repeat(np.arange(m), lens)
+    return _coo_to_csr(m, n, new_of_old[rows_old], new_of_old[ci], v)
+
+
+def transpose(mat):
+    m, n, rp, ci, v = mat
+    rows = np.repeat(np.arange(m, dtype=np.int64), np.diff(rp))
+    return _coo_to_csr(n, m, ci, rows, v)
+
+
+def overwrite_values_mod10(mat):
+    """value[i] = i % 10 by CSR position, as the reference CLI does before
+    computing (src/main.cu:191-197)."""
+    m, n, rp, ci, _ = mat
+    return m, n, rp, ci, (np.arange(ci.size) % 10).astype(np.float64)
+
+
+def products(matA, matB) -> int:
+    """nnzCub: sum over A's nonzeros (i, k) of nnz(B row k) (src/main.cu:392-397)."""
+    _, _, _, ci, _ = matA
+    _, _, rpB, _, _ = matB
+    return int(np.diff(rpB.astype(np.int64))[ci].sum())

@@ -1,0 +1,220 @@
+"""GPU parity of the core path against the CPU oracle, through the C ABI.
+
+Bar: tile structure, masks, row offsets, per-tile nnz, column bytes and CSR
+structure are bit-exact; FP64 values must be within relative error 1e-12 per
+entry (REL_TOL below) -- and because the GPU accumulates each output entry in
+the oracle's order with separately rounded multiply and add, the tests also
+assert they are bit-identical.
+"""
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+REL_TOL = 1e-12
+GOLD = Path(__file__).resolve().parent / "golden"
+TILE_KEYS = ["tile_ptr", "tile_columnidx", "tile_rowidx", "tile_nnz", "tile_csr_Ptr", "tile_csr_Col",
+             "tile_csr_Value", "mask"]
+C_KEYS = ["tile_ptr", "tile_columnidx", "tile_rowidx", "tile_nnz", "tile_csr_Ptr", "tile_csr_Col", "mask"]
+
+
+def golden_cases():
+    z = np.load(GOLD / "cases.npz")
+    names = sorted({k.split("/")[0] for k in z.files})
+    return {nm: (z, (int(z[f"{nm}/m"][0]), int(z[f"{nm}/m"][1]), z[f"{nm}/rowptr"], z[f"{nm}/colidx"],
+                     z[f"{nm}/val"])) for nm in names}
+
+
+CASES = golden_cases()
+
+
+def assert_values(got, want):
+    got = np.asarray(got, dtype=np.float64)
+    want = np.asarray(want, dtype=np.float64)
+    assert got.shape == want.shape
+    den = np.maximum(np.abs(want), np.finfo(np.float64).tiny)
+    rel = np.abs(got - want) / den
+    rel[(got == want)] = 0.0
+    assert float(rel.max(initial=0.0)) <= REL_TOL
+    assert np.array_equal(got.view(np.uint64), want.view(np.uint64)), "values not bit-identical to the oracle"
+
+
+def assert_tiles(got, want, keys):
+    for k in keys:
+        if k == "tile_csr_Value":
+            assert_values(got[k], want[k])
+        else:
+            np.testing.assert_array_equal(got[k], want[k], err_msg=k)
+
+
+# ---------------------------------------------------------------------------
+# conversion
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_dropin_csr2tile_matches_reference_fixture(tsg, name):
+    z, mat = CASES[name]
+    A = tsg.csr2tile_row_major(mat)
+    for k in TILE_KEYS:
+        np.testing.assert_array_equal(A[k], z[f"{name}/A/{k}"], err_msg=f"row-major {k}")
+    B = tsg.csr2tile_col_major(mat)
+    for k in TILE_KEYS + ["csc_tile_ptr", "csc_tile_rowidx"]:
+        np.testing.assert_array_equal(B[k], z[f"{name}/B/{k}"], err_msg=f"col-major {k}")
+
+
+def test_conversion_random_and_edges(tsg, gen, oracle):
+    mats = [gen.random_poisson(int(m), int(n), lam, seed=s) for s, (m, n, lam) in
+            enumerate([(1, 1, 1.0), (17, 33, 3.0), (250, 97, 6.0), (512, 512, 12.0), (1000, 40, 30.0)])]
+    mats.append(gen.banded(300, 40, seed=1))              # full 16x16 tiles
+    mats.append((5, 7, np.zeros(6, np.int32), np.zeros(0, np.int32), np.zeros(0)))  # empty
+    mats.append(gen.rmat(10, 8, seed=3))                  # skewed rows
+    for mat in mats:
+        assert_tiles(tsg.csr2tile_row_major(mat), oracle.csr2tile_row_major(mat), TILE_KEYS)
+        B, Bo = tsg.csr2tile_col_major(mat), oracle.csr2tile_col_major(mat)
+        assert_tiles(B, Bo, TILE_KEYS + ["csc_tile_ptr", "csc_tile_rowidx"])
+
+
+# ---------------------------------------------------------------------------
+# SpGEMM
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_dropin_tilespgemm_matches_oracle(tsg, oracle, name):
+    z, mat = CASES[name]
+    if mat[0] != mat[1]:
+        pytest.skip("rectangular")
+    A = {k: z[f"{name}/A/{k}"] for k in TILE_KEYS}
+    B = {k: z[f"{name}/B/{k}"] for k in TILE_KEYS + ["csc_tile_ptr", "csc_tile_rowidx"]}
+    for d in (A, B):
+        d.update(m=mat[0], n=mat[1], nnz=mat[3].size, tilem=(mat[0] + 15) // 16, tilen=(mat[1] + 15) // 16,
+                 numtile=d["tile_columnidx"].size)
+    C, t = tsg.tilespgemm(A, B, nnzCub=oracle.count_products(mat, mat))
+    Co = oracle.spgemm_tiled(A, B)
+    assert_tiles(C, Co, C_KEYS + ["tile_csr_Value"])
+    rp, ci, v = tsg.tile2csr(C)
+    np.testing.assert_array_equal(rp, z[f"{name}/C/rowptr"])
+    np.testing.assert_array_equal(ci, z[f"{name}/C/colidx"])
+    if f"{name}/C/val" in z.files:
+        assert_values(v, z[f"{name}/C/val"])
+
+
+def _handle_product(tsg, ctx, matA, matB):
+    import torch
+    dev = torch.device("cuda", 0)
+
+    def up(mat):
+        m, n, rp, ci, v = mat
+        return (torch.from_numpy(np.ascontiguousarray(rp, np.int32)).to(dev),
+                torch.from_numpy(np.ascontiguousarray(ci, np.int32)).to(dev),
+                torch.from_numpy(np.ascontiguousarray(v, np.float64)).to(dev))
+
+    torch.cuda.synchronize()
+    a = up(matA)
+    b = up(matB)
+    torch.cuda.synchronize()
+    A = tsg.csr_to_tiled(ctx, matA[0], matA[1], *a, tsg.TSG_TILED_PACKED_COL)
+    B = tsg.csr_to_tiled(ctx, matB[0], matB[1], *b, tsg.TSG_TILED_CSC_VIEW)
+    C, info = tsg.spgemm(ctx, A, B)
+    return A, B, C, info
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_handle_spgemm_random_rectangular(tsg, ctx, oracle, gen, seed):
+    rng = np.random.default_rng(100 + seed)
+    m, k, n = (int(x) for x in rng.integers(1, 700, 3))
+    matA = gen.random_poisson(m, k, float(rng.uniform(0.5, 14)), seed=seed)
+    matB = gen.random_poisson(k, n, float(rng.uniform(0.5, 14)), seed=seed + 50)
+    A, B, C, info = _handle_product(tsg, ctx, matA, matB)
+    Co = oracle.spgemm_tiled(oracle.csr2tile_row_major(matA), oracle.csr2tile_col_major(matB))
+    assert_tiles(C.download(), Co, C_KEYS + ["tile_csr_Value"])
+    assert info["numtile_C"] == Co["numtile"] and info["nnz_C"] == Co["nnz"]
+
+
+def test_aat_and_dense_tiles(tsg, ctx, oracle, gen):
+    cases = [(gen.random_poisson(300, 200, 9.0, seed=4), None),
+             (gen.banded(257, 48, seed=5), None),             # full (256) and dense (225-255) C tiles
+             (gen.rmat(11, 16, seed=7), None)]                # hub rows
+    for matA, _ in cases:
+        matB = gen.transpose(matA) if matA[0] != matA[1] else matA
+        for B in ([matB, gen.transpose(matA)] if matA[0] == matA[1] else [matB]):
+            A_, B_, C, info = _handle_product(tsg, ctx, matA, B)
+            Co = oracle.spgemm_tiled(oracle.csr2tile_row_major(matA), oracle.csr2tile_col_major(B))
+            assert_tiles(C.download(), Co, C_KEYS + ["tile_csr_Value"])
+
+
+def test_laplacian_256_known_answers(tsg, ctx, oracle, gen):
+    facts = json.loads((GOLD / "known_answers.json").read_text())["laplacian_256x256"]
+    mat = gen.laplacian_2d(256)
+    A, B, C, info = _handle_product(tsg, ctx, mat, mat)
+    assert info["numtile_C"] == facts["tilesC"] and info["nnz_C"] == facts["nnzC"]
+    Cd = C.download()
+    assert int(np.count_nonzero(np.diff(Cd["tile_nnz"]))) == facts["tilesC_nonempty"]
+    Co = oracle.spgemm_tiled(oracle.csr2tile_row_major(mat), oracle.csr2tile_col_major(mat))
+    assert_tiles(Cd, Co, C_KEYS + ["tile_csr_Value"])
+    rp, ci, v = (x.cpu().numpy() for x in tsg.tiled_to_csr(ctx, C))
+    assert ci[rp[0]:rp[1]].tolist() == facts["row0_cols"]
+    assert v[rp[0]:rp[1]].tolist() == facts["row0_vals"]
+
+
+def test_stencil27_full_size_against_gustavson(tsg, ctx, oracle, gen):
+    """27-point stencil 64^3 (n=262,144): structure and every value against the
+    element-level oracle; the known answers pin the counts."""
+    facts = json.loads((GOLD / "known_answers.json").read_text())["stencil27_64"]
+    mat = gen.stencil_27pt_3d(64, seed=0)
+    A, B, C, info = _handle_product(tsg, ctx, mat, mat)
+    assert A.numtile == facts["tilesA"]
+    assert info["numtile_C"] == facts["tilesC"] and info["nnz_C"] == facts["nnzC"]
+    rp, ci, v = (x.cpu().numpy() for x in tsg.tiled_to_csr(ctx, C))
+    G = oracle.gustavson(mat, mat, nthreads=8)
+    np.testing.assert_array_equal(rp, G[2])
+    np.testing.assert_array_equal(ci, G[3])
+    assert_values(v, G[4])
+
+
+def test_spgemm_is_deterministic(tsg, ctx, gen):
+    mat = gen.rmat(12, 8, seed=2)
+    _, _, C1, _ = _handle_product(tsg, ctx, mat, mat)
+    _, _, C2, _ = _handle_product(tsg, ctx, mat, mat)
+    d1, d2 = C1.download(), C2.download()
+    for k in C_KEYS + ["tile_csr_Value"]:
+        assert np.array_equal(np.asarray(d1[k]).view(np.uint8), np.asarray(d2[k]).view(np.uint8))
+
+
+# ---------------------------------------------------------------------------
+# tile -> CSR and end to end
+# ---------------------------------------------------------------------------
+def test_tile2csr_dropin_matches_oracle(tsg, oracle, gen):
+    for mat in [gen.laplacian_2d(37, 29), gen.random_poisson(200, 300, 7.0, seed=8)]:
+        T = oracle.csr2tile_row_major(mat)
+        T["tile_csr_Col"] = T["tile_csr_Col"] & 15  # plain bytes, as C tiles carry
+        rp, ci, v = tsg.tile2csr(T)
+        np.testing.assert_array_equal(rp, mat[2])
+        np.testing.assert_array_equal(ci, mat[3])
+        assert_values(v, mat[4])
+
+
+def test_end_to_end_host_call(tsg, ctx, oracle, gen):
+    for matA, matB in [(gen.laplacian_2d(100), None),
+                       (gen.random_poisson(333, 444, 5.0, seed=1), gen.random_poisson(444, 222, 5.0, seed=2))]:
+        C, info = tsg.spgemm_csr_host(ctx, matA, matB)
+        G = oracle.gustavson(matA, matA if matB is None else matB)
+        np.testing.assert_array_equal(C[2], G[2])
+        np.testing.assert_array_equal(C[3], G[3])
+        assert_values(C[4], G[4])
+
+
+# ---------------------------------------------------------------------------
+# input errors come back as status codes, never as a device fault
+# ---------------------------------------------------------------------------
+def test_malformed_csr_is_rejected(tsg, ctx):
+    import torch
+    dev = torch.device("cuda", 0)
+    rp = torch.tensor([0, 2, 3], dtype=torch.int32, device=dev)
+    unsorted = torch.tensor([5, 1, 0], dtype=torch.int32, device=dev)
+    out_of_range = torch.tensor([1, 9, 0], dtype=torch.int32, device=dev)
+    v = torch.ones(3, dtype=torch.float64, device=dev)
+    for ci in (unsorted, out_of_range):
+        with pytest.raises(tsg.TsgError) as e:
+            tsg.csr_to_tiled(ctx, 2, 8, rp, ci, v, tsg.TSG_TILED_PACKED_COL)
+        assert e.value.status == -4

@@ -1,0 +1,122 @@
+"""The CPU oracle is pinned before it is trusted: against the golden fixtures
+produced by the reference's own CPU code (tests/golden/), against that code
+live when it is built (oracle/_ref), and for internal consistency (tiled
+oracle == element-level Gustavson, bit for bit)."""
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+GOLD = Path(__file__).resolve().parent / "golden"
+TILE_KEYS = ["tile_ptr", "tile_columnidx", "tile_rowidx", "tile_nnz", "tile_csr_Ptr", "tile_csr_Col",
+             "tile_csr_Value", "mask"]
+
+
+def golden_cases():
+    z = np.load(GOLD / "cases.npz")
+    names = sorted({k.split("/")[0] for k in z.files})
+    out = {}
+    for nm in names:
+        m, n = (int(x) for x in z[f"{nm}/m"])
+        out[nm] = (z, (m, n, z[f"{nm}/rowptr"], z[f"{nm}/colidx"], z[f"{nm}/val"]))
+    return out
+
+
+CASES = golden_cases()
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_oracle_csr2tile_matches_reference_fixtures(oracle, name):
+    z, mat = CASES[name]
+    A = oracle.csr2tile_row_major(mat)
+    for k in TILE_KEYS:
+        np.testing.assert_array_equal(A[k], z[f"{name}/A/{k}"], err_msg=f"row-major {k}")
+    B = oracle.csr2tile_col_major(mat)
+    for k in TILE_KEYS + ["csc_tile_ptr", "csc_tile_rowidx"]:
+        np.testing.assert_array_equal(B[k], z[f"{name}/B/{k}"], err_msg=f"col-major {k}")
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_oracle_spgemm_matches_reference_fixtures(oracle, name):
+    z, mat = CASES[name]
+    if mat[0] != mat[1]:
+        pytest.skip("rectangular: no A*A")
+    A = oracle.csr2tile_row_major(mat)
+    B = oracle.csr2tile_col_major(mat)
+    C = oracle.spgemm_tiled(A, B)
+    rp, ci, v = oracle.tile2csr(C)
+    np.testing.assert_array_equal(rp, z[f"{name}/C/rowptr"])   # reference spgemm_spa structure
+    np.testing.assert_array_equal(ci, z[f"{name}/C/colidx"])
+    if f"{name}/Ct/tile_ptr" in z.files:                          # reference spgemm_cpu, bit for bit
+        for k in ["tile_ptr", "tile_columnidx", "tile_nnz", "tile_csr_Ptr", "tile_csr_Col", "tile_csr_Value"]:
+            np.testing.assert_array_equal(C[k], z[f"{name}/Ct/{k}"], err_msg=k)
+        np.testing.assert_array_equal(v, z[f"{name}/C/val"])
+
+
+def test_oracle_known_answers(oracle, gen):
+    facts = json.loads((GOLD / "known_answers.json").read_text())
+    for name, mat in [("laplacian_64x64", gen.laplacian_2d(64)), ("laplacian_256x256", gen.laplacian_2d(256))]:
+        f = facts[name]
+        A = oracle.csr2tile_row_major(mat)
+        C = oracle.spgemm_tiled(A, oracle.csr2tile_col_major(mat))
+        assert mat[3].size == f["nnzA"] and A["numtile"] == f["tilesA"]
+        assert C["numtile"] == f["tilesC"] and C["nnz"] == f["nnzC"]
+        assert int(np.count_nonzero(np.diff(C["tile_nnz"]))) == f["tilesC_nonempty"]
+        assert oracle.count_products(mat, mat) == f["products"]
+        rp, ci, v = oracle.tile2csr(C)
+        assert ci[rp[0]:rp[1]].tolist() == f["row0_cols"]
+        assert v[rp[0]:rp[1]].tolist() == f["row0_vals"]
+    f = facts["stencil27_64"]
+    mat = gen.stencil_27pt_3d(64, seed=0)
+    assert mat[3].size == f["nnzA"]
+    assert oracle.count_products(mat, mat) == f["products"]
+    G = oracle.gustavson(mat, mat, nthreads=8)
+    assert G[3].size == f["nnzC"]
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_oracle_tiled_equals_gustavson(oracle, gen, seed):
+    rng = np.random.default_rng(seed)
+    m, k, n = (int(x) for x in rng.integers(20, 140, 3))
+    A = gen.random_poisson(m, k, float(rng.uniform(1, 9)), seed=seed)
+    B = gen.random_poisson(k, n, float(rng.uniform(1, 9)), seed=seed + 100)
+    C = oracle.spgemm_tiled(oracle.csr2tile_row_major(A), oracle.csr2tile_col_major(B))
+    rp, ci, v = oracle.tile2csr(C)
+    G = oracle.gustavson(A, B)
+    np.testing.assert_array_equal(rp, G[2])
+    np.testing.assert_array_equal(ci, G[3])
+    np.testing.assert_array_equal(v, G[4])  # same accumulation order, bit for bit
+
+
+def test_oracle_against_live_reference(oracle, gen):
+    if not oracle.ref_available():
+        pytest.skip("reference CPU build absent")
+    for seed in range(3):
+        mat = gen.random_poisson(160, None, 5.0, seed=seed)      # n % 16 == 0
+        A, B = oracle.csr2tile_row_major(mat), oracle.csr2tile_col_major(mat)
+        Ar, Br = oracle.ref_csr2tile_row_major(mat), oracle.ref_csr2tile_col_major(mat)
+        for k in TILE_KEYS:
+            np.testing.assert_array_equal(A[k], Ar[k])
+            np.testing.assert_array_equal(B[k], Br[k])
+        C, Cr = oracle.spgemm_tiled(A, B), oracle.ref_spgemm_cpu(Ar, Br)
+        for k in ["tile_ptr", "tile_columnidx", "tile_nnz", "tile_csr_Ptr", "tile_csr_Col", "tile_csr_Value"]:
+            np.testing.assert_array_equal(C[k], Cr[k])
+
+
+def test_reference_spgemm_cpu_edge_overcount_is_a_reference_bug(oracle, gen):
+    """spgemm_cpu's counting pass (src/spgemm-cpu.h:206,232) bounds B's row by
+    C's tile-column width; with n % 16 != 0 it over-counts tiles in the last
+    tile column while its numeric pass writes nothing there.  The oracle
+    follows the numeric pass (and the reference's GPU masks)."""
+    if not oracle.ref_available():
+        pytest.skip("reference CPU build absent")
+    mat = gen.laplacian_2d(37, 29)
+    Cr = oracle.ref_spgemm_cpu(oracle.ref_csr2tile_row_major(mat), oracle.ref_csr2tile_col_major(mat))
+    C = oracle.spgemm_tiled(oracle.csr2tile_row_major(mat), oracle.csr2tile_col_major(mat))
+    bad = np.nonzero(np.diff(C["tile_nnz"]) != np.diff(Cr["tile_nnz"]))[0]
+    assert bad.size > 0 and set(C["tile_columnidx"][bad].tolist()) == {C["tilen"] - 1}
+    srp, sci = oracle.ref_spgemm_spa(mat, mat)
+    rp, ci, _ = oracle.tile2csr(C)
+    np.testing.assert_array_equal(rp, srp)
+    np.testing.assert_array_equal(ci, sci)
