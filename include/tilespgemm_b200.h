@@ -270,6 +270,19 @@ int tsg_context_create(int device, tsg_context **ctx);
 int tsg_context_destroy(tsg_context *ctx);
 /* Use an existing cudaStream_t (passed as void*) for all work; NULL = own. */
 int tsg_context_set_stream(tsg_context *ctx, void *cuda_stream);
+/* Work schedule of steps 2 and 3 (results are bit-identical either way):
+ * TSG_SCHED_TILES  one half-warp per C tile, intersecting A's tile row with
+ *                  B's tile column (the reference's decomposition);
+ * TSG_SCHED_ROWS   one half-warp per run of seg_tiles C tiles of one tile
+ *                  row, walking A's tile row and B's tile rows (no
+ *                  intersection search), accumulating into acc_cap FP64
+ *                  shared-memory slots.  seg_tiles in {8, 16}; acc_cap in
+ *                  {256, 512, 1024, 2048}. */
+#define TSG_SCHED_TILES 0
+#define TSG_SCHED_ROWS 1
+int tsg_context_set_schedule(tsg_context *ctx, int schedule, int seg_tiles, int acc_cap);
+/* Blocks until all work queued on the context's stream has finished. */
+int tsg_context_synchronize(tsg_context *ctx);
 /* Number of this library's kernels launched on the context so far. */
 long long tsg_context_launches(tsg_context *ctx);
 /* Record per-step CUDA-event timings into tsg_spgemm_info. */
@@ -314,6 +327,34 @@ int tsg_spgemm_csr_host(tsg_context *ctx,
                         int nnzB, const int *b_rowptr, const int *b_colidx, const double *b_val,
                         int *nnzC, int **c_rowptr, int **c_colidx, double **c_val,
                         tsg_spgemm_info *info);
+
+/* GPU orderings of the rows of a CSR matrix, written to d_order as a
+ * new -> old permutation (reorder_algorithm/README.md:6-12 convention):
+ * TSG_ORDER_ORIGINAL identity; TSG_ORDER_RCM reverse Cuthill-McKee on the
+ * symmetrised pattern with (degree, id) tie-break (square only);
+ * TSG_ORDER_DEGREE by (-degree, id); TSG_ORDER_GRAY by (density group,
+ * Gray-decoded column signature, id); TSG_ORDER_RANDOM by
+ * (SplitMix64(seed, id), id).  Replaces the order_gen adapters of
+ * reorder_algorithm/{original,rcm,degree,gray,random}/ (run through
+ * src/external_reorder.h:100-141). */
+#define TSG_ORDER_ORIGINAL 0
+#define TSG_ORDER_RCM 1
+#define TSG_ORDER_DEGREE 2
+#define TSG_ORDER_GRAY 3
+#define TSG_ORDER_RANDOM 4
+int tsg_order(tsg_context *ctx, int kind, int m, int n, int nnz,
+              const int *d_rowptr, const int *d_col, unsigned long long seed, int *d_order);
+/* "original", "rcm", "degree", "gray", "random" -> TSG_ORDER_*, else -1. */
+int tsg_order_from_name(const char *name);
+
+/* Device bipermutation: out = P_row * A * P_col^T with rows sorted by column;
+ * output row r is input row d_row_old[r], column c becomes d_col_new[c].
+ * Output arrays are caller-allocated (m+1, nnz, nnz).  The device form of
+ * apply_bipermutation_csr, src/reorder.h:2429-2504. */
+int tsg_permute_csr(tsg_context *ctx, int m, int n, int nnz,
+                    const int *d_rowptr, const int *d_col, const double *d_val,
+                    const int *d_row_old, const int *d_col_new,
+                    int *d_out_rowptr, int *d_out_col, double *d_out_val);
 
 /* Scalar product count nnzCub = sum over A nonzeros (i,k) of nnz(B row k),
  * computed on the device from device CSR arrays. */

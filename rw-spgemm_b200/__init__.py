@@ -109,6 +109,7 @@ def _declare(L):
     L.tsg_context_set_stream.argtypes = [vp, vp]
     L.tsg_context_set_timing.argtypes = [vp, ip]
     L.tsg_context_launches.argtypes = [vp]
+    L.tsg_context_synchronize.argtypes = [vp]
     L.tsg_context_launches.restype = ctypes.c_longlong
     L.tsg_csr_to_tiled.argtypes = [vp, ip, ip, ip, vp, vp, vp, ip, ctypes.POINTER(TsgTiled)]
     L.tsg_tiled_free.argtypes = [vp, ctypes.POINTER(TsgTiled)]
@@ -254,11 +255,20 @@ def tilespgemm(tilesA: dict, tilesB: dict, nnzCub: int = 0) -> tuple[dict, dict]
 # handle API (device-resident)
 # ---------------------------------------------------------------------------
 class Context:
-    """tsg_context on one device; uses torch's current stream when given."""
+    """tsg_context on one device.  Work goes to ``stream`` (a cudaStream_t as
+    int) when given, else to torch's current stream on that device when torch
+    is importable, so library calls are ordered with the caller's torch work;
+    ``own_stream=True`` keeps the context's private stream."""
 
-    def __init__(self, device: int = 0, stream=None, timing: bool = False):
+    def __init__(self, device: int = 0, stream=None, timing: bool = False, own_stream: bool = False):
         self.handle = ctypes.c_void_p()
         check(lib().tsg_context_create(device, ctypes.byref(self.handle)))
+        if stream is None and not own_stream:
+            try:
+                import torch
+                stream = torch.cuda.current_stream(device).cuda_stream
+            except Exception:
+                stream = None
         if stream is not None:
             self.set_stream(stream)
         if timing:
@@ -269,6 +279,9 @@ class Context:
 
     def set_timing(self, on: bool):
         check(lib().tsg_context_set_timing(self.handle, 1 if on else 0))
+
+    def synchronize(self):
+        check(lib().tsg_context_synchronize(self.handle))
 
     def launches(self) -> int:
         return int(lib().tsg_context_launches(self.handle))
@@ -358,6 +371,7 @@ def tiled_to_csr(ctx: Context, C: Tiled):
     v = torch.empty(max(C.s.nnz, 1), dtype=torch.float64, device=dev)
     check(lib().tsg_tiled_to_csr(ctx.handle, ctypes.byref(C.s), ctypes.c_void_p(rp.data_ptr()),
                                  ctypes.c_void_p(ci.data_ptr()), ctypes.c_void_p(v.data_ptr())))
+    ctx.synchronize()
     return rp, ci[:C.s.nnz], v[:C.s.nnz]
 
 
@@ -387,3 +401,165 @@ def spgemm_csr_host(ctx: Context, matA, matB=None):
     ci = _np_from(pci, nnzC.value, np.int32, True)
     v = _np_from(pv, nnzC.value, np.float64, True)
     return (m, n, rp, ci, v), info.as_dict()
+
+
+# ---------------------------------------------------------------------------
+# orderings and bipermutations
+# ---------------------------------------------------------------------------
+ORDER_KINDS = {"original": 0, "rcm": 1, "degree": 2, "gray": 3, "random": 4}
+
+
+class AxisPermutation(ctypes.Structure):
+    """src/reorder.h:26-31: new -> old (old_id) and old -> new (new_id)."""
+    _fields_ = [("n", ctypes.c_int), ("old_id", _c_int_p), ("new_id", _c_int_p)]
+
+
+class ReorderInfo(ctypes.Structure):
+    """src/reorder.h:33-64 (field order kept)."""
+    _fields_ = [
+        ("enabled", ctypes.c_int), ("n", ctypes.c_int),
+        ("row_perm", AxisPermutation), ("inner_perm", AxisPermutation), ("col_perm", AxisPermutation),
+        ("input_tiles_A_before", ctypes.c_longlong), ("input_tiles_A_after", ctypes.c_longlong),
+        ("input_tiles_B_before", ctypes.c_longlong), ("input_tiles_B_after", ctypes.c_longlong),
+        ("estimated_c_tiles_before", ctypes.c_longlong), ("estimated_c_tiles_after", ctypes.c_longlong),
+        ("reorder_time_ms", ctypes.c_double), ("signature_time_ms", ctypes.c_double),
+        ("tile_profile_time_ms", ctypes.c_double), ("affinity_time_ms", ctypes.c_double),
+        ("sort_time_ms", ctypes.c_double), ("local_refine_time_ms", ctypes.c_double),
+        ("proxy_time_ms", ctypes.c_double), ("permute_time_ms", ctypes.c_double),
+        ("risk_input_tile_ratio", ctypes.c_double), ("risk_c_tile_ratio", ctypes.c_double),
+        ("local_refine_window", ctypes.c_int), ("proxy_sample_rows", ctypes.c_int),
+        ("guard_degraded_to_identity", ctypes.c_int), ("structural_conservative", ctypes.c_int),
+        ("shared_symmetric_csr", ctypes.c_int), ("mode", ctypes.c_char * 64), ("risk_reason", ctypes.c_char * 128),
+    ]
+
+
+def _declare_reorder(L):
+    vp, ip = ctypes.c_void_p, ctypes.c_int
+    L.tsg_order.argtypes = [vp, ip, ip, ip, ip, vp, vp, ctypes.c_ulonglong, vp]
+    L.tsg_order_from_name.argtypes = [ctypes.c_char_p]
+    L.tsg_permute_csr.argtypes = [vp, ip, ip, ip, vp, vp, vp, vp, vp, vp, vp, vp]
+    L.reorder_info_init.argtypes = [ctypes.POINTER(ReorderInfo)]
+    L.reorder_info_init.restype = None
+    L.reorder_info_destroy.argtypes = [ctypes.POINTER(ReorderInfo)]
+    L.reorder_info_destroy.restype = None
+    L.build_original_reorder_plan.argtypes = [ip, ctypes.POINTER(SMatrix), ctypes.POINTER(SMatrix),
+                                              ctypes.POINTER(ReorderInfo)]
+    L.build_external_reorder_plan.argtypes = [ip, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
+                                              ctypes.POINTER(SMatrix), ctypes.POINTER(SMatrix),
+                                              ctypes.POINTER(ReorderInfo), ctypes.POINTER(ctypes.c_double)]
+    L.apply_bipermutation_csr.argtypes = [ctypes.POINTER(SMatrix), ctypes.POINTER(AxisPermutation),
+                                          ctypes.POINTER(AxisPermutation), ctypes.POINTER(SMatrix)]
+    L.restore_bipermutation_csr.argtypes = [ctypes.POINTER(SMatrix), ctypes.POINTER(AxisPermutation),
+                                            ctypes.POINTER(AxisPermutation)]
+
+
+_declare_base = _declare
+
+
+def _declare(L):  # noqa: F811
+    _declare_base(L)
+    _declare_reorder(L)
+
+
+def order(ctx: Context, kind: str, m: int, n: int, rowptr, colidx, seed: int = 1):
+    """GPU ordering (new -> old, torch int32 tensor on the current device)."""
+    import torch
+    out = torch.empty(max(m, 1), dtype=torch.int32, device=rowptr.device)
+    check(lib().tsg_order(ctx.handle, ORDER_KINDS[kind], int(m), int(n), int(colidx.numel()),
+                          ctypes.c_void_p(rowptr.data_ptr()), ctypes.c_void_p(colidx.data_ptr()),
+                          ctypes.c_ulonglong(seed), ctypes.c_void_p(out.data_ptr())))
+    ctx.synchronize()
+    return out[:m]
+
+
+def permute_csr(ctx: Context, m: int, n: int, rowptr, colidx, val, row_old, col_new):
+    """Device bipermutation P_r A P_c^T (torch tensors in and out)."""
+    import torch
+    nnz = int(colidx.numel())
+    orp = torch.empty(m + 1, dtype=torch.int32, device=rowptr.device)
+    oci = torch.empty(max(nnz, 1), dtype=torch.int32, device=rowptr.device)
+    ov = torch.empty(max(nnz, 1), dtype=torch.float64, device=rowptr.device)
+    check(lib().tsg_permute_csr(ctx.handle, int(m), int(n), nnz, *[ctypes.c_void_p(t.data_ptr()) for t in
+                                (rowptr, colidx, val, row_old, col_new, orp, oci, ov)]))
+    ctx.synchronize()
+    return orp, oci[:nnz], ov[:nnz]
+
+
+class _Axis:
+    def __init__(self, old_id):
+        self.old = np.ascontiguousarray(old_id, dtype=np.int32)
+        self.new = np.empty_like(self.old)
+        self.new[self.old] = np.arange(self.old.size, dtype=np.int32)
+        self.s = AxisPermutation(int(self.old.size), self.old.ctypes.data_as(_c_int_p), self.new.ctypes.data_as(_c_int_p))
+
+
+def _csr_from_smatrix(sm: SMatrix, free=True):
+    rp = _np_from(sm.rowpointer, sm.m + 1, np.int32, free)
+    ci = _np_from(sm.columnindex, sm.nnz, np.int32, free)
+    v = _np_from(sm.value, sm.nnz, np.float64, free)
+    return sm.m, sm.n, rp, ci, v
+
+
+def apply_bipermutation_csr(mat, row_old, col_old):
+    """src/reorder.h:2429 on the GPU; permutations given new -> old."""
+    h = HostCSR(mat)
+    r, c = _Axis(row_old), _Axis(col_old)
+    out = SMatrix()
+    st = lib().apply_bipermutation_csr(ctypes.byref(h.sm), ctypes.byref(r.s), ctypes.byref(c.s), ctypes.byref(out))
+    if st != 0:
+        raise TsgError(st, "apply_bipermutation_csr failed")
+    return _csr_from_smatrix(out)
+
+
+def restore_bipermutation_csr(mat, row_old, col_old):
+    """src/reorder.h:2506 on the GPU (the inverse of apply)."""
+    m, n, rp, ci, v = mat
+    sm = SMatrix()
+    sm.m, sm.n, sm.nnz = int(m), int(n), int(len(ci))
+    # the function frees and replaces the CSR arrays: hand it malloc'd copies
+    for field, arr, ctype in (("rowpointer", rp, ctypes.c_int), ("columnindex", ci, ctypes.c_int),
+                              ("value", v, ctypes.c_double)):
+        a = np.ascontiguousarray(arr)
+        nbytes = max(a.nbytes, 1)
+        _libc.malloc.restype = ctypes.c_void_p
+        _libc.malloc.argtypes = [ctypes.c_size_t]
+        p = _libc.malloc(nbytes)
+        ctypes.memmove(p, a.ctypes.data, a.nbytes)
+        setattr(sm, field, ctypes.cast(p, ctypes.POINTER(ctype)))
+    r, c = _Axis(row_old), _Axis(col_old)
+    st = lib().restore_bipermutation_csr(ctypes.byref(sm), ctypes.byref(r.s), ctypes.byref(c.s))
+    if st != 0:
+        raise TsgError(st, "restore_bipermutation_csr failed")
+    return _csr_from_smatrix(sm)
+
+
+REORDER_PROBLEM = {"AA": 0, "AAT": 1, "AB": 2}
+
+
+def build_reorder_plan(kind: str, algorithm: str, matA, matB=None) -> dict:
+    """build_original_reorder_plan / build_external_reorder_plan
+    (src/external_reorder.h:173-321) with the ordering computed on the GPU."""
+    L = lib()
+    hA = HostCSR(matA)
+    hB = HostCSR(matB) if matB is not None else None
+    info = ReorderInfo()
+    L.reorder_info_init(ctypes.byref(info))
+    ms = ctypes.c_double(0.0)
+    pB = ctypes.byref(hB.sm) if hB else None
+    if algorithm == "original":
+        st = L.build_original_reorder_plan(REORDER_PROBLEM[kind], ctypes.byref(hA.sm), pB, ctypes.byref(info))
+    else:
+        st = L.build_external_reorder_plan(REORDER_PROBLEM[kind], algorithm.encode(), b"", b"", ctypes.byref(hA.sm),
+                                           pB, ctypes.byref(info), ctypes.byref(ms))
+    if st != 0:
+        L.reorder_info_destroy(ctypes.byref(info))
+        raise TsgError(st, f"reorder plan '{algorithm}' failed")
+    d = {f: getattr(info, f) for f, _ in ReorderInfo._fields_ if not f.endswith("_perm")}
+    d["mode"] = info.mode.decode()
+    d["risk_reason"] = info.risk_reason.decode()
+    for ax in ("row_perm", "inner_perm", "col_perm"):
+        p = getattr(info, ax)
+        d[ax] = _np_from(p.old_id, p.n, np.int32, False)
+    d["ordergen_ms"] = ms.value
+    L.reorder_info_destroy(ctypes.byref(info))
+    return d

@@ -7,6 +7,7 @@
 
 int tsg_gather_colmajor(tsg_context *ctx, const tsg_tiled *src, int *tnnz_cm, unsigned char *Ptr_cm,
                         unsigned short *mask_cm, unsigned char *Col_cm, double *Val_cm);
+int tsg_colmajor_data_to_rowmajor(tsg_context *ctx, tsg_tiled *mat);
 
 extern "C" const char *tsg_last_error(void);
 
@@ -59,6 +60,9 @@ extern "C" int tsg_context_create(int device, tsg_context **out)
         return tsg_set_error(TSG_ERR_CUDA, "context creation failed: %s", cudaGetErrorString(e));
     }
     ctx->own_stream = 1;
+    ctx->sched = TSG_SCHED_ROWS;
+    ctx->seg_tiles = 8;
+    ctx->acc_cap = 512;
     // keep freed pool memory cached so repeated products do not return pages
     cudaMemPool_t pool;
     if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess)
@@ -104,6 +108,33 @@ extern "C" int tsg_context_set_stream(tsg_context *ctx, void *stream)
         TSG_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
         ctx->own_stream = 1;
     }
+    return TSG_OK;
+}
+
+extern "C" int tsg_context_set_schedule(tsg_context *ctx, int schedule, int seg_tiles, int acc_cap)
+{
+    if (!ctx)
+        return tsg_set_error(TSG_ERR_INVALID, "null context");
+    if (schedule != TSG_SCHED_TILES && schedule != TSG_SCHED_ROWS)
+        return tsg_set_error(TSG_ERR_INVALID, "unknown schedule %d", schedule);
+    if (schedule == TSG_SCHED_ROWS)
+    {
+        const bool ok = (seg_tiles == 8 && (acc_cap == 256 || acc_cap == 512 || acc_cap == 1024)) ||
+                        (seg_tiles == 16 && (acc_cap == 512 || acc_cap == 1024 || acc_cap == 2048));
+        if (!ok)
+            return tsg_set_error(TSG_ERR_INVALID, "unsupported (seg_tiles, acc_cap) = (%d, %d)", seg_tiles, acc_cap);
+        ctx->seg_tiles = seg_tiles;
+        ctx->acc_cap = acc_cap;
+    }
+    ctx->sched = schedule;
+    return TSG_OK;
+}
+
+extern "C" int tsg_context_synchronize(tsg_context *ctx)
+{
+    if (!ctx)
+        return tsg_set_error(TSG_ERR_INVALID, "null context");
+    TSG_CUDA(cudaStreamSynchronize(ctx->stream));
     return TSG_OK;
 }
 
@@ -236,10 +267,9 @@ extern "C" int tsg_tiled_upload_colmajor(tsg_context *ctx, const SMatrix *h, tsg
     out->col_packed = 0;
     TSG_TRY(h2d(ctx, &out->csc_tile_ptr, h->csc_tile_ptr, (size_t)h->tilen + 1));
     TSG_TRY(h2d(ctx, &out->csc_tile_rowidx, h->csc_tile_rowidx, (size_t)h->numtile));
-    // data is stored in column-major order: tile q sits in tile row csc_tile_rowidx[q]
-    TSG_TRY(h2d(ctx, &out->tile_rowidx, h->csc_tile_rowidx, (size_t)h->numtile));
-    out->csc_tile_pos = nullptr; // identity
-    return TSG_OK;
+    TSG_TRY(tsg_alloc(ctx, &out->tile_rowidx, (size_t)h->numtile));
+    // internal layout: row-major tile data plus the column view
+    return tsg_colmajor_data_to_rowmajor(ctx, out);
 }
 
 extern "C" int tsg_tiled_download(tsg_context *ctx, const tsg_tiled *src, int colmajor, SMatrix *dst)
@@ -385,7 +415,7 @@ extern "C" int tsg_spgemm_csr_host(tsg_context *ctx, int m, int k, int n, int nn
 static tsg_context *g_ctx = nullptr;
 static int g_ctx_device = -1;
 
-static tsg_context *dropin_ctx(void)
+tsg_context *tsg_dropin_context(void)
 {
     int dev = 0;
     cudaGetDevice(&dev);
@@ -414,7 +444,7 @@ static void dropin_check(int st, const char *what)
 
 static void dropin_convert(SMatrix *matrix, int colmajor)
 {
-    tsg_context *ctx = dropin_ctx();
+    tsg_context *ctx = tsg_dropin_context();
     int *rp, *ci;
     double *v;
     dropin_check(h2d(ctx, &rp, matrix->rowpointer, (size_t)matrix->m + 1), "upload");
@@ -449,7 +479,7 @@ extern "C" void matrix_destroy(SMatrix *matrix)
 
 extern "C" void tile2csr(SMatrix *matrix)
 {
-    tsg_context *ctx = dropin_ctx();
+    tsg_context *ctx = tsg_dropin_context();
     tsg_tiled t;
     memset(&t, 0, sizeof(t));
     t.m = matrix->m;
@@ -500,7 +530,7 @@ extern "C" void tilespgemm(SMatrix *matrixA, SMatrix *matrixB, SMatrix *matrixC,
     (void)densityA;
     (void)densityB;
     (void)filename;
-    tsg_context *ctx = dropin_ctx();
+    tsg_context *ctx = tsg_dropin_context();
     tsg_tiled A, B, C;
     dropin_check(tsg_tiled_upload_rowmajor(ctx, matrixA, &A), "upload A");
     dropin_check(tsg_tiled_upload_colmajor(ctx, matrixB, &B), "upload B");

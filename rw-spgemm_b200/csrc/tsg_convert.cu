@@ -392,3 +392,125 @@ int tsg_gather_colmajor(tsg_context *ctx, const tsg_tiled *src, int *tnnz_cm, un
     TSG_LAUNCH_CHECK();
     return TSG_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Column-major tile data (the reference's B layout) -> the library's layout:
+// row-major tile data plus the column view (csc_tile_pos[q] = row-major
+// index of column-major tile q).
+// ---------------------------------------------------------------------------
+// warp per tile column: row-major index of every tile of the column
+__global__ void k_cm_rowpos(int tilen, const int *__restrict__ cptr, const int *__restrict__ crow,
+                            const int *__restrict__ tile_ptr, const int *__restrict__ tile_col, int *__restrict__ pos)
+{
+    const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= tilen)
+        return;
+    const int j = (int)w;
+    for (int q = cptr[j] + lane; q < cptr[j + 1]; q += 32)
+    {
+        const int R = crow[q];
+        int lo = tile_ptr[R], n = tile_ptr[R + 1] - lo;
+        while (n > 0)
+        {
+            const int h = n >> 1;
+            if (tile_col[lo + h] < j)
+            {
+                lo += h + 1;
+                n -= h + 1;
+            }
+            else
+                n = h;
+        }
+        pos[q] = lo;
+    }
+}
+
+__global__ void k_cm_rm_counts(int T, const int *__restrict__ pos, const int *__restrict__ tnnz_cm, int *__restrict__ cnt)
+{
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < T; q += gridDim.x * blockDim.x)
+        cnt[pos[q]] = tnnz_cm[q + 1] - tnnz_cm[q];
+}
+
+// half-warp per column-major tile q, scattered to row-major slot pos[q]
+__global__ void k_cm_rm_scatter(int T, const int *__restrict__ pos, const int *__restrict__ tnnz_cm,
+                                const unsigned char *__restrict__ Ptr_cm, const unsigned short *__restrict__ mask_cm,
+                                const unsigned char *__restrict__ Col_cm, const double *__restrict__ Val_cm,
+                                const int *__restrict__ tnnz_rm, unsigned char *__restrict__ Ptr_rm,
+                                unsigned short *__restrict__ mask_rm, unsigned char *__restrict__ Col_rm,
+                                double *__restrict__ Val_rm)
+{
+    const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int q = (int)(gid >> 4);
+    const int lane = threadIdx.x & 15;
+    if (q >= T)
+        return;
+    const int p = pos[q];
+    Ptr_rm[(long long)p * TSG_BS + lane] = Ptr_cm[(long long)q * TSG_BS + lane];
+    mask_rm[(long long)p * TSG_BS + lane] = mask_cm[(long long)q * TSG_BS + lane];
+    const int s = tnnz_cm[q], n = tnnz_cm[q + 1] - s, d = tnnz_rm[p];
+    for (int i = lane; i < n; i += 16)
+    {
+        Col_rm[d + i] = Col_cm[s + i];
+        Val_rm[d + i] = Val_cm[s + i];
+    }
+}
+
+__global__ void k_rowidx_from_ptr(int tilem, const int *__restrict__ tile_ptr, int *__restrict__ rowidx)
+{
+    const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= tilem)
+        return;
+    for (int t = tile_ptr[w] + lane; t < tile_ptr[w + 1]; t += 32)
+        rowidx[t] = (int)w;
+}
+
+// mat holds column-major data (tile_nnz, Ptr, mask, Col, Value in csc order),
+// row-major tile_ptr / tile_columnidx and csc_tile_ptr / csc_tile_rowidx.
+int tsg_colmajor_data_to_rowmajor(tsg_context *ctx, tsg_tiled *mat)
+{
+    const int T = mat->numtile;
+    cudaStream_t st = ctx->stream;
+    TSG_TRY(tsg_alloc(ctx, &mat->csc_tile_pos, (size_t)T));
+    int *tnnz, *rowidx;
+    unsigned char *Ptr, *Col;
+    unsigned short *mask;
+    double *Val;
+    TSG_TRY(tsg_alloc(ctx, &tnnz, (size_t)T + 1));
+    TSG_TRY(tsg_alloc(ctx, &rowidx, (size_t)T));
+    TSG_TRY(tsg_alloc(ctx, &Ptr, (size_t)T * TSG_BS));
+    TSG_TRY(tsg_alloc(ctx, &mask, (size_t)T * TSG_BS));
+    TSG_TRY(tsg_alloc(ctx, &Col, (size_t)mat->nnz));
+    TSG_TRY(tsg_alloc(ctx, &Val, (size_t)mat->nnz));
+    if (T > 0)
+    {
+        k_cm_rowpos<<<tsg_blocks((long long)mat->tilen * 32, 256), 256, 0, st>>>(
+            mat->tilen, mat->csc_tile_ptr, mat->csc_tile_rowidx, mat->tile_ptr, mat->tile_columnidx, mat->csc_tile_pos);
+        TSG_LAUNCH_CHECK();
+        k_cm_rm_counts<<<tsg_blocks(T, 256), 256, 0, st>>>(T, mat->csc_tile_pos, mat->tile_nnz, tnnz);
+        TSG_LAUNCH_CHECK();
+        TSG_TRY(tsg_scan_counts(ctx, tnnz, tnnz, T, nullptr));
+        k_cm_rm_scatter<<<tsg_blocks((long long)T * 16, 256), 256, 0, st>>>(
+            T, mat->csc_tile_pos, mat->tile_nnz, mat->tile_csr_Ptr, mat->mask, mat->tile_csr_Col, mat->tile_csr_Value,
+            tnnz, Ptr, mask, Col, Val);
+        TSG_LAUNCH_CHECK();
+        k_rowidx_from_ptr<<<tsg_blocks((long long)mat->tilem * 32, 256), 256, 0, st>>>(mat->tilem, mat->tile_ptr, rowidx);
+        TSG_LAUNCH_CHECK();
+    }
+    else
+        TSG_CUDA(cudaMemsetAsync(tnnz, 0, sizeof(int), st));
+    tsg_release(ctx, mat->tile_nnz);
+    tsg_release(ctx, mat->tile_rowidx);
+    tsg_release(ctx, mat->tile_csr_Ptr);
+    tsg_release(ctx, mat->mask);
+    tsg_release(ctx, mat->tile_csr_Col);
+    tsg_release(ctx, mat->tile_csr_Value);
+    mat->tile_nnz = tnnz;
+    mat->tile_rowidx = rowidx;
+    mat->tile_csr_Ptr = Ptr;
+    mat->mask = mask;
+    mat->tile_csr_Col = Col;
+    mat->tile_csr_Value = Val;
+    return TSG_OK;
+}

@@ -20,6 +20,9 @@ struct tsg_context
     cudaEvent_t ev[8];
     long long *h_pinned; // small pinned buffer for scalar read-backs
     long long launches;  // kernels this library launched on the context
+    int sched;           // TSG_SCHED_TILES / TSG_SCHED_ROWS for steps 2-3
+    int seg_tiles;       // row schedule: C tiles per work item (8 or 16)
+    int acc_cap;         // row schedule: FP64 accumulator slots per half-warp
 };
 
 // Records a formatted message as the thread's last error and returns code.

@@ -1,0 +1,929 @@
+// GPU orderings, bipermutations and the reference's reorder-plan entry points.
+//
+// Orderings (new -> old permutations, the order-file convention of
+// reorder_algorithm/README.md:6-12):
+//   original  identity                      (src/external_reorder.h:173-202)
+//   degree    sorted by (-degree, id)       (reorder_algorithm/common/order_utils.py:78-81)
+//   random    sorted by (SplitMix64(seed, id), id) -- a seeded GPU shuffle
+//   rcm       reverse Cuthill-McKee on the symmetrised off-diagonal pattern
+//             with the (degree, id) tie-break (the scheme of scipy's RCM used
+//             by order_utils.py:84-104; tie-break of src/reorder.h:1678-1722),
+//             built level by level: the next level is every unvisited
+//             neighbour of the current one, ordered by (position of its
+//             earliest-placed neighbour, degree, id), which is exactly the
+//             order in which sequential Cuthill-McKee appends them
+//   gray      rows sorted by (density group, Gray-decoded 32-segment column
+//             signature, id)
+// Apply / restore restate src/reorder.h:2429-2551: rows gathered new->old,
+// columns mapped old->new, each row re-sorted by column through a stable
+// radix sort of (row, column) keys, like the reference's thrust::sort_by_key.
+#include <stdlib.h>
+#include <sys/time.h>
+
+#include "tsg_internal.h"
+
+
+int tsg_count_c_tiles(tsg_context *ctx, const tsg_tiled *A, const tsg_tiled *B, long long *numC);
+
+extern "C" int tsg_order_from_name(const char *name)
+{
+    if (!name)
+        return -1;
+    if (!strcmp(name, "original"))
+        return TSG_ORDER_ORIGINAL;
+    if (!strcmp(name, "rcm"))
+        return TSG_ORDER_RCM;
+    if (!strcmp(name, "degree"))
+        return TSG_ORDER_DEGREE;
+    if (!strcmp(name, "gray"))
+        return TSG_ORDER_GRAY;
+    if (!strcmp(name, "random"))
+        return TSG_ORDER_RANDOM;
+    return -1;
+}
+
+__device__ __forceinline__ unsigned long long splitmix_key(unsigned long long seed, unsigned long long id)
+{
+    unsigned long long x = seed * 0x9E3779B97F4A7C15ULL + id + 1ULL;
+    x ^= x >> 30;
+    x *= 0xBF58476D1CE4E5B9ULL;
+    x ^= x >> 27;
+    x *= 0x94D049BB133111EBULL;
+    x ^= x >> 31;
+    return x;
+}
+
+__global__ void k_iota(long long n, int *__restrict__ v)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        v[i] = (int)i;
+}
+
+__global__ void k_fill_int(long long n, int v, int *__restrict__ a)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        a[i] = v;
+}
+
+// descending = 1: key = ~degree (sort ascending gives degree descending)
+__global__ void k_degree_keys(int n, const int *__restrict__ rowptr, int descending, unsigned int *__restrict__ keys)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        unsigned d = (unsigned)(rowptr[i + 1] - rowptr[i]);
+        keys[i] = descending ? ~d : d;
+    }
+}
+
+__global__ void k_random_keys(int n, unsigned long long seed, unsigned long long *__restrict__ keys)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        keys[i] = splitmix_key(seed, (unsigned long long)i);
+}
+
+__device__ __forceinline__ unsigned gray_decode32(unsigned g)
+{
+    g ^= g >> 1;
+    g ^= g >> 2;
+    g ^= g >> 4;
+    g ^= g >> 8;
+    g ^= g >> 16;
+    return g;
+}
+
+// warp per row; the 32-segment signature is OR-reduced across the lanes
+__global__ void k_gray_keys(int n, int ncols, long long thr, const int *__restrict__ rowptr,
+                            const int *__restrict__ col, unsigned long long *__restrict__ keys)
+{
+    const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= n)
+        return;
+    const int r = (int)w, s = rowptr[r], e = rowptr[r + 1];
+    unsigned sig = 0;
+    for (int p = s + lane; p < e; p += 32)
+    {
+        long long seg = ncols > 0 ? ((long long)col[p] * 32) / ncols : 0;
+        if (seg > 31)
+            seg = 31;
+        sig |= 1u << (31 - (int)seg);
+    }
+    sig = __reduce_or_sync(0xffffffffu, sig);
+    if (lane == 0)
+        keys[r] = ((unsigned long long)((e - s) > thr ? 1 : 0) << 32) | gray_decode32(sig);
+}
+
+static int bits_needed(unsigned long long v)
+{
+    int b = 1;
+    while (b < 64 && (v >> b))
+        b++;
+    return b;
+}
+
+// ---------------------------------------------------------------------------
+// symmetrised graph for RCM
+// ---------------------------------------------------------------------------
+__global__ void k_offdiag_count(int n, const int *__restrict__ rowptr, const int *__restrict__ col,
+                                int *__restrict__ cnt)
+{
+    const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= n)
+        return;
+    const int r = (int)w, s = rowptr[r], e = rowptr[r + 1];
+    unsigned c = 0;
+    for (int p = s + lane; p < e; p += 32)
+    {
+        const int j = col[p];
+        c += (j != r && j >= 0 && j < n) ? 1u : 0u;
+    }
+    c = __reduce_add_sync(0xffffffffu, c);
+    if (lane == 0)
+        cnt[r] = (int)c;
+}
+
+__global__ void k_sym_edges(int n, const int *__restrict__ rowptr, const int *__restrict__ col,
+                            const int *__restrict__ offs, unsigned long long *__restrict__ keys)
+{
+    const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= n)
+        return;
+    const int r = (int)w, s = rowptr[r], e = rowptr[r + 1];
+    long long base = offs[r];
+    for (int p0 = s; p0 < e; p0 += 32)
+    {
+        const int p = p0 + lane;
+        const int j = p < e ? col[p] : r;
+        const bool ok = p < e && j != r && j >= 0 && j < n;
+        const unsigned bal = __ballot_sync(0xffffffffu, ok);
+        const int off = __popc(bal & ((1u << lane) - 1u));
+        if (ok)
+        {
+            keys[2 * (base + off)] = ((unsigned long long)r << 32) | (unsigned)j;
+            keys[2 * (base + off) + 1] = ((unsigned long long)j << 32) | (unsigned)r;
+        }
+        base += __popc(bal);
+    }
+}
+
+__global__ void k_uniq_flags(long long ne, const unsigned long long *__restrict__ keys, int *__restrict__ rowlen,
+                             int *__restrict__ keep)
+{
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < ne; q += (long long)gridDim.x * blockDim.x)
+    {
+        const bool first = q == 0 || keys[q] != keys[q - 1];
+        keep[q] = first ? 1 : 0;
+        if (first)
+            atomicAdd(&rowlen[(int)(keys[q] >> 32)], 1);
+    }
+}
+
+__global__ void k_uniq_scatter(long long ne, const unsigned long long *__restrict__ keys,
+                               const int *__restrict__ keep_scan, int *__restrict__ adj)
+{
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < ne; q += (long long)gridDim.x * blockDim.x)
+        if (q == 0 || keys[q] != keys[q - 1])
+            adj[keep_scan[q]] = (int)(keys[q] & 0xFFFFFFFFu);
+}
+
+// ---------------------------------------------------------------------------
+// RCM level expansion
+// ---------------------------------------------------------------------------
+// Warp per frontier vertex (positions [lo, hi) of order[]): every unplaced
+// neighbour records the earliest frontier position (parent) and is listed
+// once in next[].  pos[u] = -1 unplaced, -2 listed in this level, >= 0 placed.
+__global__ void k_rcm_expand(int lo, int hi, const int *__restrict__ order, const int *__restrict__ gptr,
+                             const int *__restrict__ adj, int *__restrict__ pos, int *__restrict__ parent,
+                             int *__restrict__ next, int *__restrict__ next_cnt)
+{
+    const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= hi - lo)
+        return;
+    const int p = lo + (int)w;
+    const int v = order[p];
+    for (int q = gptr[v] + lane; q < gptr[v + 1]; q += 32)
+    {
+        const int u = adj[q];
+        if (pos[u] >= 0)
+            continue;
+        atomicMin(&parent[u], p);
+        if (atomicCAS(&pos[u], -1, -2) == -1)
+            next[atomicAdd(next_cnt, 1)] = u;
+    }
+}
+
+__global__ void k_u32_of(int cnt, const int *__restrict__ a, unsigned int *__restrict__ keys)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x)
+        keys[i] = (unsigned)a[i];
+}
+
+__global__ void k_rcm_keys(int cnt, const int *__restrict__ next, const int *__restrict__ parent,
+                           const int *__restrict__ gptr, unsigned long long *__restrict__ keys)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x)
+    {
+        const int u = next[i];
+        keys[i] = ((unsigned long long)(unsigned)parent[u] << 32) | (unsigned)(gptr[u + 1] - gptr[u]);
+    }
+}
+
+__global__ void k_rcm_place(int cnt, int base, const int *__restrict__ next, int *__restrict__ order,
+                            int *__restrict__ pos)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x)
+    {
+        const int u = next[i];
+        order[base + i] = u;
+        pos[u] = base + i;
+    }
+}
+
+__global__ void k_rcm_find_seed(int n, int from, const int *__restrict__ seeds, const int *__restrict__ pos,
+                                int *__restrict__ best)
+{
+    for (int i = from + blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        if (pos[seeds[i]] == -1)
+        {
+            atomicMin(best, i);
+            return;
+        }
+}
+
+__global__ void k_count_isolated(int n, const int *__restrict__ gptr, int *__restrict__ cnt)
+{
+    unsigned c = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        c += gptr[i + 1] == gptr[i] ? 1u : 0u;
+    c = __reduce_add_sync(0xffffffffu, c);
+    if ((threadIdx.x & 31) == 0 && c)
+        atomicAdd(cnt, (int)c);
+}
+
+__global__ void k_reverse(int n, const int *__restrict__ in, int *__restrict__ out)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        out[i] = in[n - 1 - i];
+}
+
+static int rcm_order(tsg_context *ctx, int n, const int *rowptr, const int *col, int *d_order)
+{
+    cudaStream_t st = ctx->stream;
+    const unsigned gw = tsg_blocks((long long)n * 32, 256), g1 = tsg_blocks(n, 256);
+    // symmetrised off-diagonal graph: gptr / adj (sorted, duplicate-free)
+    int *offs, *gptr;
+    TSG_TRY(tsg_alloc(ctx, &offs, (size_t)n + 1));
+    TSG_TRY(tsg_alloc(ctx, &gptr, (size_t)n + 1));
+    k_offdiag_count<<<gw, 256, 0, st>>>(n, rowptr, col, offs);
+    TSG_LAUNCH_CHECK();
+    long long half = 0;
+    TSG_TRY(tsg_scan_counts(ctx, offs, offs, n, &half));
+    const long long ne = 2 * half;
+    unsigned long long *keys;
+    int *idx, *keep, *adj;
+    TSG_TRY(tsg_alloc(ctx, &keys, (size_t)ne));
+    TSG_TRY(tsg_alloc(ctx, &idx, (size_t)ne));
+    TSG_TRY(tsg_alloc(ctx, &keep, (size_t)ne + 1));
+    TSG_CUDA(cudaMemsetAsync(gptr, 0, ((size_t)n + 1) * sizeof(int), st));
+    long long nuniq = 0;
+    if (ne > 0)
+    {
+        k_sym_edges<<<gw, 256, 0, st>>>(n, rowptr, col, offs, keys);
+        TSG_LAUNCH_CHECK();
+        k_iota<<<tsg_blocks(ne, 256), 256, 0, st>>>(ne, idx);
+        TSG_LAUNCH_CHECK();
+        TSG_TRY(tsg_sort_pairs_u64(ctx, keys, idx, ne, 32 + bits_needed((unsigned long long)n)));
+        k_uniq_flags<<<tsg_blocks(ne, 256), 256, 0, st>>>(ne, keys, gptr, keep);
+        TSG_LAUNCH_CHECK();
+        TSG_TRY(tsg_scan_counts(ctx, keep, keep, ne, &nuniq));
+    }
+    TSG_TRY(tsg_alloc(ctx, &adj, (size_t)nuniq));
+    if (ne > 0)
+    {
+        k_uniq_scatter<<<tsg_blocks(ne, 256), 256, 0, st>>>(ne, keys, keep, adj);
+        TSG_LAUNCH_CHECK();
+    }
+    TSG_TRY(tsg_scan_counts(ctx, gptr, gptr, n, nullptr));
+    tsg_release(ctx, keys);
+    tsg_release(ctx, idx);
+    tsg_release(ctx, keep);
+    tsg_release(ctx, offs);
+
+    // seeds in (degree, id) order; isolated vertices are the leading seeds
+    unsigned int *dk;
+    int *seeds, *pos, *parent, *order, *next, *cnt, *best;
+    unsigned long long *lk;
+    unsigned int *ik;
+    TSG_TRY(tsg_alloc(ctx, &dk, (size_t)n));
+    TSG_TRY(tsg_alloc(ctx, &seeds, (size_t)n));
+    TSG_TRY(tsg_alloc(ctx, &pos, (size_t)n));
+    TSG_TRY(tsg_alloc(ctx, &parent, (size_t)n));
+    TSG_TRY(tsg_alloc(ctx, &order, (size_t)n));
+    TSG_TRY(tsg_alloc(ctx, &next, (size_t)n));
+    TSG_TRY(tsg_alloc(ctx, &lk, (size_t)n));
+    TSG_TRY(tsg_alloc(ctx, &ik, (size_t)n));
+    TSG_TRY(tsg_alloc(ctx, &cnt, 1));
+    TSG_TRY(tsg_alloc(ctx, &best, 1));
+    k_degree_keys<<<g1, 256, 0, st>>>(n, gptr, 0, dk);
+    TSG_LAUNCH_CHECK();
+    k_iota<<<g1, 256, 0, st>>>(n, seeds);
+    TSG_LAUNCH_CHECK();
+    TSG_TRY(tsg_sort_pairs_u32(ctx, dk, seeds, n, 32));
+    k_fill_int<<<g1, 256, 0, st>>>(n, -1, pos);
+    TSG_LAUNCH_CHECK();
+    k_fill_int<<<g1, 256, 0, st>>>(n, 0x7fffffff, parent);
+    TSG_LAUNCH_CHECK();
+
+    // isolated vertices lead the (degree, id) seed order and each is its own
+    // component: place them in one step
+    int *h = (int *)ctx->h_pinned;
+    TSG_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int), st));
+    k_count_isolated<<<g1, 256, 0, st>>>(n, gptr, cnt);
+    TSG_LAUNCH_CHECK();
+    TSG_CUDA(cudaMemcpyAsync(h, cnt, sizeof(int), cudaMemcpyDeviceToHost, st));
+    TSG_CUDA(cudaStreamSynchronize(st));
+    const int niso = h[0];
+    if (niso > 0)
+    {
+        k_rcm_place<<<tsg_blocks(niso, 256), 256, 0, st>>>(niso, 0, seeds, order, pos);
+        TSG_LAUNCH_CHECK();
+    }
+    int placed = niso, seed_from = niso;
+    while (placed < n)
+    {
+        TSG_CUDA(cudaMemcpyAsync(best, &n, sizeof(int), cudaMemcpyHostToDevice, st));
+        k_rcm_find_seed<<<g1, 256, 0, st>>>(n, seed_from, seeds, pos, best);
+        TSG_LAUNCH_CHECK();
+        TSG_CUDA(cudaMemcpyAsync(h, best, sizeof(int), cudaMemcpyDeviceToHost, st));
+        TSG_CUDA(cudaStreamSynchronize(st));
+        const int b = h[0];
+        if (b >= n)
+            return tsg_set_error(TSG_ERR_CUDA, "RCM lost track of unplaced vertices");
+        seed_from = b + 1;
+        k_rcm_place<<<1, 32, 0, st>>>(1, placed, seeds + b, order, pos);
+        TSG_LAUNCH_CHECK();
+        int lo = placed, hi = placed + 1;
+        placed++;
+        while (lo < hi)
+        {
+            TSG_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int), st));
+            k_rcm_expand<<<tsg_blocks((long long)(hi - lo) * 32, 256), 256, 0, st>>>(lo, hi, order, gptr, adj, pos,
+                                                                                    parent, next, cnt);
+            TSG_LAUNCH_CHECK();
+            TSG_CUDA(cudaMemcpyAsync(h, cnt, sizeof(int), cudaMemcpyDeviceToHost, st));
+            TSG_CUDA(cudaStreamSynchronize(st));
+            const int c = h[0];
+            if (c == 0)
+                break;
+            const unsigned gc = tsg_blocks(c, 256);
+            // id order first, then a stable sort on (parent position, degree)
+            k_u32_of<<<gc, 256, 0, st>>>(c, next, ik);
+            TSG_LAUNCH_CHECK();
+            TSG_TRY(tsg_sort_pairs_u32(ctx, ik, next, c, bits_needed((unsigned long long)n)));
+            k_rcm_keys<<<gc, 256, 0, st>>>(c, next, parent, gptr, lk);
+            TSG_LAUNCH_CHECK();
+            TSG_TRY(tsg_sort_pairs_u64(ctx, lk, next, c, 64));
+            k_rcm_place<<<gc, 256, 0, st>>>(c, hi, next, order, pos);
+            TSG_LAUNCH_CHECK();
+            lo = hi;
+            hi += c;
+            placed += c;
+        }
+    }
+    k_reverse<<<g1, 256, 0, st>>>(n, order, d_order);
+    TSG_LAUNCH_CHECK();
+    tsg_release(ctx, dk);
+    tsg_release(ctx, seeds);
+    tsg_release(ctx, pos);
+    tsg_release(ctx, parent);
+    tsg_release(ctx, order);
+    tsg_release(ctx, next);
+    tsg_release(ctx, lk);
+    tsg_release(ctx, ik);
+    tsg_release(ctx, cnt);
+    tsg_release(ctx, best);
+    tsg_release(ctx, gptr);
+    tsg_release(ctx, adj);
+    return TSG_OK;
+}
+
+extern "C" int tsg_order(tsg_context *ctx, int kind, int m, int n, int nnz, const int *d_rowptr, const int *d_col,
+                         unsigned long long seed, int *d_order)
+{
+    if (!ctx || !d_order || m < 0)
+        return tsg_set_error(TSG_ERR_INVALID, "bad argument");
+    if (m == 0)
+        return TSG_OK;
+    cudaStream_t st = ctx->stream;
+    const unsigned g1 = tsg_blocks(m, 256);
+    switch (kind)
+    {
+    case TSG_ORDER_ORIGINAL:
+        k_iota<<<g1, 256, 0, st>>>(m, d_order);
+        TSG_LAUNCH_CHECK();
+        return TSG_OK;
+    case TSG_ORDER_DEGREE:
+    {
+        unsigned int *k;
+        TSG_TRY(tsg_alloc(ctx, &k, (size_t)m));
+        k_degree_keys<<<g1, 256, 0, st>>>(m, d_rowptr, 1, k);
+        TSG_LAUNCH_CHECK();
+        k_iota<<<g1, 256, 0, st>>>(m, d_order);
+        TSG_LAUNCH_CHECK();
+        TSG_TRY(tsg_sort_pairs_u32(ctx, k, d_order, m, 32));
+        tsg_release(ctx, k);
+        return TSG_OK;
+    }
+    case TSG_ORDER_RANDOM:
+    {
+        unsigned long long *k;
+        TSG_TRY(tsg_alloc(ctx, &k, (size_t)m));
+        k_random_keys<<<g1, 256, 0, st>>>(m, seed, k);
+        TSG_LAUNCH_CHECK();
+        k_iota<<<g1, 256, 0, st>>>(m, d_order);
+        TSG_LAUNCH_CHECK();
+        TSG_TRY(tsg_sort_pairs_u64(ctx, k, d_order, m, 64));
+        tsg_release(ctx, k);
+        return TSG_OK;
+    }
+    case TSG_ORDER_GRAY:
+    {
+        unsigned long long *k;
+        TSG_TRY(tsg_alloc(ctx, &k, (size_t)m));
+        const long long thr = 2 * (((long long)nnz + m - 1) / m);
+        k_gray_keys<<<tsg_blocks((long long)m * 32, 256), 256, 0, st>>>(m, n, thr, d_rowptr, d_col, k);
+        TSG_LAUNCH_CHECK();
+        k_iota<<<g1, 256, 0, st>>>(m, d_order);
+        TSG_LAUNCH_CHECK();
+        TSG_TRY(tsg_sort_pairs_u64(ctx, k, d_order, m, 33));
+        tsg_release(ctx, k);
+        return TSG_OK;
+    }
+    case TSG_ORDER_RCM:
+        if (m != n)
+            return tsg_set_error(TSG_ERR_INVALID, "RCM needs a square matrix");
+        return rcm_order(ctx, m, d_rowptr, d_col, d_order);
+    default:
+        return tsg_set_error(TSG_ERR_UNSUPPORTED, "unknown ordering %d", kind);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// bipermutation of a device CSR
+// ---------------------------------------------------------------------------
+__global__ void k_perm_rowlen(int m, const int *__restrict__ rowptr, const int *__restrict__ row_old,
+                              int *__restrict__ cnt)
+{
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < m; r += gridDim.x * blockDim.x)
+    {
+        const int o = row_old[r];
+        cnt[r] = rowptr[o + 1] - rowptr[o];
+    }
+}
+
+__global__ void k_perm_emit(int m, const int *__restrict__ rowptr, const int *__restrict__ col,
+                            const int *__restrict__ row_old, const int *__restrict__ col_new,
+                            const int *__restrict__ out_rowptr, unsigned long long *__restrict__ keys,
+                            int *__restrict__ src)
+{
+    const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= m)
+        return;
+    const int r = (int)w, o = row_old[r];
+    const int s = rowptr[o], e = rowptr[o + 1], d = out_rowptr[r];
+    for (int p = s + lane; p < e; p += 32)
+    {
+        keys[d + (p - s)] = ((unsigned long long)r << 32) | (unsigned)col_new[col[p]];
+        src[d + (p - s)] = p;
+    }
+}
+
+__global__ void k_perm_gather(long long nnz, const unsigned long long *__restrict__ keys, const int *__restrict__ src,
+                              const double *__restrict__ val, int *__restrict__ out_col, double *__restrict__ out_val)
+{
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < nnz; q += (long long)gridDim.x * blockDim.x)
+    {
+        out_col[q] = (int)(keys[q] & 0xFFFFFFFFu);
+        out_val[q] = val[src[q]];
+    }
+}
+
+extern "C" int tsg_permute_csr(tsg_context *ctx, int m, int n, int nnz, const int *d_rowptr, const int *d_col,
+                               const double *d_val, const int *d_row_old, const int *d_col_new, int *d_out_rowptr,
+                               int *d_out_col, double *d_out_val)
+{
+    if (!ctx || m < 0 || nnz < 0)
+        return tsg_set_error(TSG_ERR_INVALID, "bad argument");
+    cudaStream_t st = ctx->stream;
+    if (m == 0)
+    {
+        TSG_CUDA(cudaMemsetAsync(d_out_rowptr, 0, sizeof(int), st));
+        return TSG_OK;
+    }
+    k_perm_rowlen<<<tsg_blocks(m, 256), 256, 0, st>>>(m, d_rowptr, d_row_old, d_out_rowptr);
+    TSG_LAUNCH_CHECK();
+    TSG_TRY(tsg_scan_counts(ctx, d_out_rowptr, d_out_rowptr, m, nullptr));
+    if (nnz == 0)
+        return TSG_OK;
+    unsigned long long *keys;
+    int *src;
+    TSG_TRY(tsg_alloc(ctx, &keys, (size_t)nnz));
+    TSG_TRY(tsg_alloc(ctx, &src, (size_t)nnz));
+    k_perm_emit<<<tsg_blocks((long long)m * 32, 256), 256, 0, st>>>(m, d_rowptr, d_col, d_row_old, d_col_new,
+                                                                     d_out_rowptr, keys, src);
+    TSG_LAUNCH_CHECK();
+    TSG_TRY(tsg_sort_pairs_u64(ctx, keys, src, nnz, 32 + bits_needed((unsigned long long)m)));
+    k_perm_gather<<<tsg_blocks(nnz, 256), 256, 0, st>>>(nnz, keys, src, d_val, d_out_col, d_out_val);
+    TSG_LAUNCH_CHECK();
+    tsg_release(ctx, keys);
+    tsg_release(ctx, src);
+    return TSG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Drop-in reorder entry points on host SMatrix CSR.
+// ---------------------------------------------------------------------------
+static void axis_init(AxisPermutation *p)
+{
+    p->n = 0;
+    p->old_id = nullptr;
+    p->new_id = nullptr;
+}
+
+static void axis_destroy(AxisPermutation *p)
+{
+    free(p->old_id);
+    free(p->new_id);
+    axis_init(p);
+}
+
+static int axis_alloc(AxisPermutation *p, int n)
+{
+    axis_destroy(p);
+    p->n = n;
+    p->old_id = (int *)malloc((size_t)(n > 0 ? n : 1) * sizeof(int));
+    p->new_id = (int *)malloc((size_t)(n > 0 ? n : 1) * sizeof(int));
+    return (p->old_id && p->new_id) ? 0 : -1;
+}
+
+static int axis_from_order(AxisPermutation *p, const int *order, int n)
+{
+    if (axis_alloc(p, n) != 0)
+        return -1;
+    for (int i = 0; i < n; i++)
+    {
+        p->old_id[i] = order[i];
+        p->new_id[order[i]] = i;
+    }
+    return 0;
+}
+
+static int axis_copy(AxisPermutation *dst, const AxisPermutation *src)
+{
+    if (axis_alloc(dst, src->n) != 0)
+        return -1;
+    memcpy(dst->old_id, src->old_id, (size_t)src->n * sizeof(int));
+    memcpy(dst->new_id, src->new_id, (size_t)src->n * sizeof(int));
+    return 0;
+}
+
+static void set_text(char *dst, size_t size, const char *src)
+{
+    strncpy(dst, src ? src : "", size - 1);
+    dst[size - 1] = '\0';
+}
+
+extern "C" void reorder_info_init(ReorderInfo *info)
+{
+    memset(info, 0, sizeof(*info));
+    axis_init(&info->row_perm);
+    axis_init(&info->inner_perm);
+    axis_init(&info->col_perm);
+    info->risk_input_tile_ratio = 1.0;
+    info->risk_c_tile_ratio = 1.0;
+    info->proxy_sample_rows = 0;
+    set_text(info->mode, sizeof(info->mode), "unset");
+    set_text(info->risk_reason, sizeof(info->risk_reason), "none");
+}
+
+extern "C" void reorder_info_destroy(ReorderInfo *info)
+{
+    axis_destroy(&info->row_perm);
+    axis_destroy(&info->inner_perm);
+    axis_destroy(&info->col_perm);
+    reorder_info_init(info);
+}
+
+// global context of the drop-in layer (tsg_api.cu)
+tsg_context *tsg_dropin_context(void);
+
+struct DevCSR
+{
+    int m = 0, n = 0, nnz = 0;
+    int *rp = nullptr, *ci = nullptr;
+    double *v = nullptr;
+};
+
+static int upload_csr(tsg_context *ctx, const SMatrix *h, DevCSR *d)
+{
+    d->m = h->m;
+    d->n = h->n;
+    d->nnz = h->nnz;
+    TSG_TRY(tsg_alloc(ctx, &d->rp, (size_t)h->m + 1));
+    TSG_TRY(tsg_alloc(ctx, &d->ci, (size_t)h->nnz));
+    TSG_TRY(tsg_alloc(ctx, &d->v, (size_t)h->nnz));
+    TSG_CUDA(cudaMemcpyAsync(d->rp, h->rowpointer, ((size_t)h->m + 1) * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    if (h->nnz)
+    {
+        TSG_CUDA(cudaMemcpyAsync(d->ci, h->columnindex, (size_t)h->nnz * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+        if (h->value)
+            TSG_CUDA(cudaMemcpyAsync(d->v, h->value, (size_t)h->nnz * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+        else
+            TSG_CUDA(cudaMemsetAsync(d->v, 0, (size_t)h->nnz * sizeof(double), ctx->stream));
+    }
+    return TSG_OK;
+}
+
+static void free_csr(tsg_context *ctx, DevCSR *d)
+{
+    tsg_release(ctx, d->rp);
+    tsg_release(ctx, d->ci);
+    tsg_release(ctx, d->v);
+}
+
+static int permute_dev(tsg_context *ctx, const DevCSR *in, const int *h_row_old, const int *h_col_new, DevCSR *out)
+{
+    int *d_ro, *d_cn;
+    TSG_TRY(tsg_alloc(ctx, &d_ro, (size_t)in->m));
+    TSG_TRY(tsg_alloc(ctx, &d_cn, (size_t)in->n));
+    if (in->m)
+        TSG_CUDA(cudaMemcpyAsync(d_ro, h_row_old, (size_t)in->m * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    if (in->n)
+        TSG_CUDA(cudaMemcpyAsync(d_cn, h_col_new, (size_t)in->n * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    out->m = in->m;
+    out->n = in->n;
+    out->nnz = in->nnz;
+    TSG_TRY(tsg_alloc(ctx, &out->rp, (size_t)in->m + 1));
+    TSG_TRY(tsg_alloc(ctx, &out->ci, (size_t)in->nnz));
+    TSG_TRY(tsg_alloc(ctx, &out->v, (size_t)in->nnz));
+    TSG_TRY(tsg_permute_csr(ctx, in->m, in->n, in->nnz, in->rp, in->ci, in->v, d_ro, d_cn, out->rp, out->ci, out->v));
+    tsg_release(ctx, d_ro);
+    tsg_release(ctx, d_cn);
+    return TSG_OK;
+}
+
+// tiles of A, tiles of B and C tiles of A*B (exact, from the tile structure)
+static int structure_counts(tsg_context *ctx, const DevCSR *A, const DevCSR *B, long long *tA, long long *tB,
+                            long long *tC)
+{
+    tsg_tiled ta, tb;
+    TSG_TRY(tsg_csr_to_tiled(ctx, A->m, A->n, A->nnz, A->rp, A->ci, A->v, 0, &ta));
+    TSG_TRY(tsg_csr_to_tiled(ctx, B->m, B->n, B->nnz, B->rp, B->ci, B->v, 0, &tb));
+    *tA = ta.numtile;
+    *tB = tb.numtile;
+    TSG_TRY(tsg_count_c_tiles(ctx, &ta, &tb, tC));
+    tsg_tiled_free(ctx, &ta);
+    tsg_tiled_free(ctx, &tb);
+    return TSG_OK;
+}
+
+static double safe_ratio(long long after, long long before)
+{
+    return before <= 0 ? 1.0 : (double)after / (double)before;
+}
+
+// before/after tile counts (src/external_reorder.h:148-171, exact instead of sampled)
+static int fill_estimates(tsg_context *ctx, const SMatrix *A, const SMatrix *B, ReorderInfo *info)
+{
+    DevCSR dA, dB, pA, pB;
+    TSG_TRY(upload_csr(ctx, A, &dA));
+    TSG_TRY(upload_csr(ctx, B, &dB));
+    TSG_TRY(structure_counts(ctx, &dA, &dB, &info->input_tiles_A_before, &info->input_tiles_B_before,
+                             &info->estimated_c_tiles_before));
+    TSG_TRY(permute_dev(ctx, &dA, info->row_perm.old_id, info->inner_perm.new_id, &pA));
+    TSG_TRY(permute_dev(ctx, &dB, info->inner_perm.old_id, info->col_perm.new_id, &pB));
+    TSG_TRY(structure_counts(ctx, &pA, &pB, &info->input_tiles_A_after, &info->input_tiles_B_after,
+                             &info->estimated_c_tiles_after));
+    free_csr(ctx, &dA);
+    free_csr(ctx, &dB);
+    free_csr(ctx, &pA);
+    free_csr(ctx, &pB);
+    const double ra = safe_ratio(info->input_tiles_A_after, info->input_tiles_A_before);
+    const double rb = safe_ratio(info->input_tiles_B_after, info->input_tiles_B_before);
+    info->risk_input_tile_ratio = ra > rb ? ra : rb;
+    info->risk_c_tile_ratio = safe_ratio(info->estimated_c_tiles_after, info->estimated_c_tiles_before);
+    TSG_CUDA(cudaStreamSynchronize(ctx->stream));
+    return TSG_OK;
+}
+
+extern "C" int build_original_reorder_plan(ReorderProblemKind kind, const SMatrix *matrixA, const SMatrix *matrixB,
+                                           ReorderInfo *info)
+{
+    if (matrixA == NULL || info == NULL)
+        return -1;
+    if (kind != REORDER_PROBLEM_AA && matrixB == NULL)
+        return -2;
+    reorder_info_destroy(info);
+    const int ncol = kind == REORDER_PROBLEM_AA ? matrixA->n : matrixB->n;
+    if (axis_alloc(&info->row_perm, matrixA->m) || axis_alloc(&info->inner_perm, matrixA->n) ||
+        axis_alloc(&info->col_perm, ncol))
+        return -1;
+    for (int i = 0; i < matrixA->m; i++)
+        info->row_perm.old_id[i] = info->row_perm.new_id[i] = i;
+    for (int i = 0; i < matrixA->n; i++)
+        info->inner_perm.old_id[i] = info->inner_perm.new_id[i] = i;
+    for (int i = 0; i < ncol; i++)
+        info->col_perm.old_id[i] = info->col_perm.new_id[i] = i;
+    info->enabled = 1;
+    info->n = matrixA->n;
+    info->shared_symmetric_csr = (kind == REORDER_PROBLEM_AA);
+    info->guard_degraded_to_identity = 1;
+    info->structural_conservative = 0;
+    set_text(info->mode, sizeof(info->mode), "original");
+    set_text(info->risk_reason, sizeof(info->risk_reason), "original_order");
+    tsg_context *ctx = tsg_dropin_context();
+    if (fill_estimates(ctx, matrixA, kind == REORDER_PROBLEM_AA ? matrixA : matrixB, info) != TSG_OK)
+        return -30;
+    return 0;
+}
+
+static unsigned long long random_seed_from_env(void)
+{
+    const char *s = getenv("TASA_RANDOM_SEED");
+    return s ? strtoull(s, nullptr, 10) : 1ULL;
+}
+
+static int order_host(tsg_context *ctx, int kind, const SMatrix *M, AxisPermutation *perm, double *ms)
+{
+    DevCSR d;
+    TSG_TRY(upload_csr(ctx, M, &d));
+    int *d_order;
+    TSG_TRY(tsg_alloc(ctx, &d_order, (size_t)M->m));
+    TSG_CUDA(cudaStreamSynchronize(ctx->stream));
+    TSG_CUDA(cudaEventRecord(ctx->ev[6], ctx->stream));
+    TSG_TRY(tsg_order(ctx, kind, M->m, M->n, M->nnz, d.rp, d.ci, random_seed_from_env(), d_order));
+    TSG_CUDA(cudaEventRecord(ctx->ev[7], ctx->stream));
+    int *h = (int *)malloc((size_t)(M->m > 0 ? M->m : 1) * sizeof(int));
+    if (!h)
+        return tsg_set_error(TSG_ERR_OOM, "host allocation failed");
+    if (M->m)
+        TSG_CUDA(cudaMemcpyAsync(h, d_order, (size_t)M->m * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    TSG_CUDA(cudaStreamSynchronize(ctx->stream));
+    float e = 0.f;
+    cudaEventElapsedTime(&e, ctx->ev[6], ctx->ev[7]);
+    *ms += e;
+    int st = axis_from_order(perm, h, M->m) == 0 ? TSG_OK : TSG_ERR_OOM;
+    free(h);
+    tsg_release(ctx, d_order);
+    free_csr(ctx, &d);
+    return st;
+}
+
+extern "C" int build_external_reorder_plan(ReorderProblemKind kind, const char *algorithm, const char *matrix_path_A,
+                                           const char *matrix_path_B, const SMatrix *matrixA, const SMatrix *matrixB,
+                                           ReorderInfo *info, double *ordergen_ms)
+{
+    (void)matrix_path_A;
+    (void)matrix_path_B;
+    if (matrixA == NULL || info == NULL || ordergen_ms == NULL)
+        return -1;
+    if (kind != REORDER_PROBLEM_AA && matrixB == NULL)
+        return -2;
+    if (kind != REORDER_PROBLEM_AA && matrixA->n != matrixB->m)
+        return -3;
+    reorder_info_destroy(info);
+    *ordergen_ms = 0.0;
+    const int okind = tsg_order_from_name(algorithm);
+    if (okind < 0)
+    {
+        printf("external reorder missing dependency: %s\n", algorithm ? algorithm : "(null)");
+        return -20;
+    }
+    tsg_context *ctx = tsg_dropin_context();
+    int st = TSG_OK;
+    if (kind == REORDER_PROBLEM_AA)
+    {
+        if (matrixA->m != matrixA->n)
+        {
+            printf("external reorder AA currently requires a square matrix.\n");
+            return -4;
+        }
+        st = order_host(ctx, okind, matrixA, &info->row_perm, ordergen_ms);
+        if (st == TSG_OK && (axis_copy(&info->inner_perm, &info->row_perm) || axis_copy(&info->col_perm, &info->row_perm)))
+            st = TSG_ERR_OOM;
+        info->shared_symmetric_csr = 1;
+    }
+    else if (kind == REORDER_PROBLEM_AAT)
+    {
+        if (matrixA->m != matrixA->n || matrixB->m != matrixB->n || matrixA->m != matrixB->m)
+        {
+            printf("external reorder AAT currently requires square A and A^T with matching dimensions.\n");
+            return -5;
+        }
+        st = order_host(ctx, okind, matrixA, &info->row_perm, ordergen_ms);
+        if (st == TSG_OK && (axis_copy(&info->inner_perm, &info->row_perm) || axis_copy(&info->col_perm, &info->row_perm)))
+            st = TSG_ERR_OOM;
+        info->shared_symmetric_csr = 0;
+    }
+    else if (kind == REORDER_PROBLEM_AB)
+    {
+        if (matrixA->m != matrixA->n)
+        {
+            printf("external reorder AB currently requires square A so row and inner axes can share A's order.\n");
+            return -6;
+        }
+        if (matrixB->m != matrixB->n)
+        {
+            printf("external reorder AB currently requires square B so B row and column axes can be ordered by B.\n");
+            return -7;
+        }
+        st = order_host(ctx, okind, matrixA, &info->row_perm, ordergen_ms);
+        if (st == TSG_OK && axis_copy(&info->inner_perm, &info->row_perm))
+            st = TSG_ERR_OOM;
+        if (st == TSG_OK)
+            st = order_host(ctx, okind, matrixB, &info->col_perm, ordergen_ms);
+        info->shared_symmetric_csr = 0;
+    }
+    else
+        return -9;
+    if (st != TSG_OK)
+    {
+        printf("external reorder failed on the GPU: %s\n", tsg_status_string(st));
+        return -20;
+    }
+    info->enabled = 1;
+    info->n = matrixA->n;
+    info->guard_degraded_to_identity = 0;
+    info->structural_conservative = 0;
+    set_text(info->mode, sizeof(info->mode), algorithm);
+    set_text(info->risk_reason, sizeof(info->risk_reason), "external_order");
+    if (fill_estimates(ctx, matrixA, kind == REORDER_PROBLEM_AA ? matrixA : matrixB, info) != TSG_OK)
+        return -30;
+    return 0;
+}
+
+static int download_csr(tsg_context *ctx, const DevCSR *d, SMatrix *out)
+{
+    out->m = d->m;
+    out->n = d->n;
+    out->nnz = d->nnz;
+    out->rowpointer = (int *)malloc(((size_t)d->m + 1) * sizeof(int));
+    out->columnindex = (int *)malloc((size_t)(d->nnz > 0 ? d->nnz : 1) * sizeof(int));
+    out->value = (double *)malloc((size_t)(d->nnz > 0 ? d->nnz : 1) * sizeof(double));
+    if (!out->rowpointer || !out->columnindex || !out->value)
+        return tsg_set_error(TSG_ERR_OOM, "host allocation failed");
+    TSG_CUDA(cudaMemcpyAsync(out->rowpointer, d->rp, ((size_t)d->m + 1) * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    if (d->nnz)
+    {
+        TSG_CUDA(cudaMemcpyAsync(out->columnindex, d->ci, (size_t)d->nnz * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        TSG_CUDA(cudaMemcpyAsync(out->value, d->v, (size_t)d->nnz * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    TSG_CUDA(cudaStreamSynchronize(ctx->stream));
+    return TSG_OK;
+}
+
+extern "C" int apply_bipermutation_csr(const SMatrix *input, const AxisPermutation *row_perm,
+                                       const AxisPermutation *col_perm, SMatrix *output)
+{
+    if (!input || !output || !row_perm || !col_perm || row_perm->n != input->m || col_perm->n != input->n)
+        return -1;
+    tsg_context *ctx = tsg_dropin_context();
+    DevCSR d, p;
+    if (upload_csr(ctx, input, &d) != TSG_OK)
+        return -2;
+    if (permute_dev(ctx, &d, row_perm->old_id, col_perm->new_id, &p) != TSG_OK)
+        return -2;
+    output->isSymmetric = 0;
+    if (download_csr(ctx, &p, output) != TSG_OK)
+        return -2;
+    free_csr(ctx, &d);
+    free_csr(ctx, &p);
+    return 0;
+}
+
+extern "C" int restore_bipermutation_csr(SMatrix *matrix, const AxisPermutation *row_perm,
+                                         const AxisPermutation *col_perm)
+{
+    if (!row_perm || !col_perm)
+        return 0;
+    if (!matrix || row_perm->n != matrix->m || col_perm->n != matrix->n)
+        return -1;
+    tsg_context *ctx = tsg_dropin_context();
+    DevCSR d, p;
+    if (upload_csr(ctx, matrix, &d) != TSG_OK)
+        return -1;
+    // output row o = input row new_id[o]; input column c -> old_id[c]
+    if (permute_dev(ctx, &d, row_perm->new_id, col_perm->old_id, &p) != TSG_OK)
+        return -1;
+    free(matrix->rowpointer);
+    free(matrix->columnindex);
+    free(matrix->value);
+    int st = download_csr(ctx, &p, matrix);
+    free_csr(ctx, &d);
+    free_csr(ctx, &p);
+    return st == TSG_OK ? 0 : -1;
+}

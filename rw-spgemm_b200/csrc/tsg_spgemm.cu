@@ -340,6 +340,238 @@ __global__ void __launch_bounds__(S3_THREADS)
 }
 
 // ---------------------------------------------------------------------------
+// Row-segment schedule (tile-level Gustavson) for steps 2 and 3.
+//
+// A work item is W consecutive C tiles (global order), cut at tile-row
+// boundaries into segments.  For a segment of C tile row i the half-warp walks
+// A's tile row i in k order and, for each A tile (i,k), the tiles of B's tile
+// row k whose columns fall in the segment's column range (binary search for
+// the first, then a merge against the segment's sorted C columns) -- every
+// (A tile, B tile) pair of the segment is visited exactly once and no
+// intersection is searched.  Lane r owns row r of every C tile of the
+// segment.  Step 2 ORs boolean tile products into per-tile row masks; step 3
+// accumulates a*b into a compact FP64 buffer holding exactly the segment's
+// nonzeros (slot = tile offset + row offset + popcount of the row mask left
+// of the column), in k-ascending then A-entry order with separately rounded
+// multiply and add -- the oracle's order -- and streams the buffer out with
+// contiguous stores.  A segment whose nonzeros exceed CAP is processed in
+// tile sub-chunks of at most CAP values.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int lower_bound_int(const int *__restrict__ a, int n, int key)
+{
+    int lo = 0;
+    while (n > 0)
+    {
+        const int h = n >> 1;
+        if (a[lo + h] < key)
+        {
+            lo += h + 1;
+            n -= h + 1;
+        }
+        else
+            n = h;
+    }
+    return lo;
+}
+
+template <int W>
+__global__ void __launch_bounds__(128)
+    k_step2_rows(int numC, const int *__restrict__ C_row, const int *__restrict__ C_col,
+                 const int *__restrict__ C_ptr, const int *__restrict__ A_ptr, const int *__restrict__ A_col,
+                 const unsigned short *__restrict__ A_mask, const int *__restrict__ B_ptr,
+                 const int *__restrict__ B_col, const unsigned short *__restrict__ B_mask,
+                 unsigned short *__restrict__ C_mask, unsigned char *__restrict__ C_Ptr, int *__restrict__ C_cnt,
+                 int *__restrict__ bins)
+{
+    __shared__ unsigned int s_m[8][W][16];
+    __shared__ int s_col[8][W];
+    __shared__ int s_bins[4];
+    if (threadIdx.x < 4)
+        s_bins[threadIdx.x] = 0;
+    __syncthreads();
+    const int hw = threadIdx.x >> 4, lane = threadIdx.x & 15;
+    const unsigned hmask = HW_MASK(threadIdx.x);
+    const long long item = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 4;
+    const long long tb = item * W;
+    if (tb < numC)
+    {
+        const int t_end = (int)min((long long)numC, tb + W);
+        int t = (int)tb;
+        while (t < t_end)
+        {
+            const int i = C_row[t];
+            const int seg_end = min(t_end, C_ptr[i + 1]);
+            const int n = seg_end - t;
+            if (lane < n)
+                s_col[hw][lane] = C_col[t + lane];
+            for (int jl = 0; jl < n; jl++)
+                s_m[hw][jl][lane] = 0u;
+            __syncwarp(hmask);
+            const int jlo = s_col[hw][0], jhi = s_col[hw][n - 1];
+            for (int pa = A_ptr[i]; pa < A_ptr[i + 1]; pa++)
+            {
+                const int k = A_col[pa];
+                const unsigned ma = A_mask[(long long)pa * TSG_BS + lane];
+                const int b0 = B_ptr[k], b1 = B_ptr[k + 1];
+                int pb = b0 + lower_bound_int(B_col + b0, b1 - b0, jlo);
+                int jl = 0;
+                for (; pb < b1; pb++)
+                {
+                    const int j = B_col[pb];
+                    if (j > jhi)
+                        break;
+                    while (jl < n - 1 && s_col[hw][jl] != j)
+                        jl++;
+                    const uint4 *mb = reinterpret_cast<const uint4 *>(B_mask + (long long)pb * TSG_BS);
+                    const uint4 q0 = __ldg(mb), q1 = __ldg(mb + 1);
+                    if (ma)
+                        s_m[hw][jl][lane] |= bool_row(ma, q0, q1);
+                }
+            }
+            __syncwarp(hmask);
+            for (int jl = 0; jl < n; jl++)
+            {
+                const unsigned acc = s_m[hw][jl][lane];
+                const int cnt = __popc(acc);
+                int incl = cnt;
+#pragma unroll
+                for (int d = 1; d < 16; d <<= 1)
+                {
+                    const int o = __shfl_up_sync(hmask, incl, d, 16);
+                    if (lane >= d)
+                        incl += o;
+                }
+                const int total = __shfl_sync(hmask, incl, 15, 16);
+                const long long tt = t + jl;
+                C_mask[tt * TSG_BS + lane] = (unsigned short)acc;
+                C_Ptr[tt * TSG_BS + lane] = (unsigned char)(incl - cnt);
+                if (lane == 0)
+                {
+                    C_cnt[tt] = total;
+                    if (total > 0)
+                        atomicAdd(&s_bins[total <= 32 ? 0 : total <= 224 ? 1 : total < 256 ? 2 : 3], 1);
+                }
+            }
+            __syncwarp(hmask);
+            t = seg_end;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < 4 && s_bins[threadIdx.x])
+        atomicAdd(&bins[threadIdx.x], s_bins[threadIdx.x]);
+}
+
+template <int W, int CAP>
+__global__ void __launch_bounds__(128)
+    k_step3_rows(int numC, const int *__restrict__ C_row, const int *__restrict__ C_col,
+                 const int *__restrict__ C_ptr, const int *__restrict__ C_tnnz,
+                 const unsigned short *__restrict__ C_mask, const unsigned char *__restrict__ C_Ptr,
+                 const int *__restrict__ A_ptr, const int *__restrict__ A_col, const int *__restrict__ A_tnnz,
+                 const unsigned char *__restrict__ A_Ptr, const unsigned char *__restrict__ A_Colb,
+                 const double *__restrict__ A_Val, const int *__restrict__ B_ptr, const int *__restrict__ B_col,
+                 const int *__restrict__ B_tnnz, const unsigned char *__restrict__ B_Ptr,
+                 const unsigned char *__restrict__ B_Colb, const double *__restrict__ B_Val,
+                 unsigned char *__restrict__ C_Colb, double *__restrict__ C_Val)
+{
+    extern __shared__ __align__(16) unsigned char s_raw[];
+    const int hw = threadIdx.x >> 4, lane = threadIdx.x & 15;
+    const unsigned hmask = HW_MASK(threadIdx.x);
+    // per half-warp: acc[CAP] doubles, base[W][16] ints, mask[W][16] u32, col[W] ints
+    const size_t per_hw = (size_t)CAP * 8 + (size_t)W * 16 * 4 * 2 + (size_t)W * 4;
+    double *acc = reinterpret_cast<double *>(s_raw + hw * per_hw);
+    int *s_base = reinterpret_cast<int *>(acc + CAP);
+    unsigned *s_mk = reinterpret_cast<unsigned *>(s_base + W * 16);
+    int *s_col = reinterpret_cast<int *>(s_mk + W * 16);
+    const long long item = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 4;
+    const long long tb = item * W;
+    if (tb >= numC)
+        return;
+    const int t_end = (int)min((long long)numC, tb + W);
+    int t = (int)tb;
+    while (t < t_end)
+    {
+        const int i = C_row[t];
+        const int seg_end = min(t_end, C_ptr[i + 1]);
+        int s = t;
+        while (s < seg_end)
+        {
+            const int base0 = C_tnnz[s];
+            int e = s + 1;
+            while (e < seg_end && C_tnnz[e + 1] - base0 <= CAP)
+                e++;
+            const int n = e - s, cn = C_tnnz[e] - base0;
+            if (lane < n)
+                s_col[lane] = C_col[s + lane];
+            for (int jl = 0; jl < n; jl++)
+            {
+                const long long tt = (long long)(s + jl) * TSG_BS + lane;
+                s_base[jl * 16 + lane] = C_tnnz[s + jl] - base0 + C_Ptr[tt];
+                s_mk[jl * 16 + lane] = C_mask[tt];
+            }
+            for (int q = lane; q < cn; q += 16)
+                acc[q] = 0.0;
+            __syncwarp(hmask);
+            const int jlo = s_col[0], jhi = s_col[n - 1];
+            for (int pa = A_ptr[i]; pa < A_ptr[i + 1]; pa++)
+            {
+                const int k = A_col[pa];
+                const int b0 = B_ptr[k], b1 = B_ptr[k + 1];
+                const int pb0 = b0 + lower_bound_int(B_col + b0, b1 - b0, jlo);
+                const int a0 = A_tnnz[pa], na = A_tnnz[pa + 1] - a0;
+                const int xa0 = A_Ptr[(long long)pa * TSG_BS + lane];
+                const int xa1 = lane == TSG_BS - 1 ? na : A_Ptr[(long long)pa * TSG_BS + lane + 1];
+                if (xa0 >= xa1)
+                    continue;
+                int jl = 0;
+                for (int pb = pb0; pb < b1; pb++)
+                {
+                    const int j = B_col[pb];
+                    if (j > jhi)
+                        break;
+                    while (jl < n - 1 && s_col[jl] != j)
+                        jl++;
+                    const int rb = s_base[jl * 16 + lane];
+                    const unsigned mk = s_mk[jl * 16 + lane];
+                    const int bt0 = B_tnnz[pb], nb = B_tnnz[pb + 1] - bt0;
+                    const unsigned char *bp = B_Ptr + (long long)pb * TSG_BS;
+                    for (int x = xa0; x < xa1; x++)
+                    {
+                        const int ca = A_Colb[a0 + x] & 15;
+                        const double a = A_Val[a0 + x];
+                        const int yb0 = bp[ca];
+                        const int yb1 = ca == TSG_BS - 1 ? nb : bp[ca + 1];
+                        for (int y = yb0; y < yb1; y++)
+                        {
+                            const int c = B_Colb[bt0 + y] & 15;
+                            const int slot = rb + __popc(mk >> (16 - c));
+                            if (slot < CAP)
+                                acc[slot] = __dadd_rn(acc[slot], __dmul_rn(a, B_Val[bt0 + y]));
+                        }
+                    }
+                }
+            }
+            __syncwarp(hmask);
+            for (int q = lane; q < cn; q += 16)
+                C_Val[base0 + q] = acc[q];
+            for (int jl = 0; jl < n; jl++)
+            {
+                unsigned mk = s_mk[jl * 16 + lane];
+                int p = base0 + s_base[jl * 16 + lane];
+                while (mk)
+                {
+                    const int bit = 31 - __clz(mk); // highest set bit = smallest column
+                    C_Colb[p++] = (unsigned char)(15 - bit);
+                    mk &= ~(1u << bit);
+                }
+            }
+            __syncwarp(hmask);
+            s = e;
+        }
+        t = seg_end;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Host orchestration.
 // ---------------------------------------------------------------------------
 static int validate_operands(const tsg_tiled *A, const tsg_tiled *B)
@@ -361,6 +593,52 @@ static float ev_ms(cudaEvent_t a, cudaEvent_t b)
     float ms = 0.f;
     cudaEventElapsedTime(&ms, a, b);
     return ms;
+}
+
+template <int W, int CAP>
+static int launch_step3_rows(tsg_context *ctx, long long numC, const tsg_tiled *A, const tsg_tiled *B, tsg_tiled *C)
+{
+    const size_t per_hw = (size_t)CAP * 8 + (size_t)W * 16 * 4 * 2 + (size_t)W * 4;
+    const size_t smem = 8 * per_hw;
+    TSG_CUDA(cudaFuncSetAttribute(k_step3_rows<W, CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const long long items = (numC + W - 1) / W;
+    k_step3_rows<W, CAP><<<tsg_blocks(items * 16, 128), 128, smem, ctx->stream>>>(
+        (int)numC, C->tile_rowidx, C->tile_columnidx, C->tile_ptr, C->tile_nnz, C->mask, C->tile_csr_Ptr,
+        A->tile_ptr, A->tile_columnidx, A->tile_nnz, A->tile_csr_Ptr, A->tile_csr_Col, A->tile_csr_Value,
+        B->tile_ptr, B->tile_columnidx, B->tile_nnz, B->tile_csr_Ptr, B->tile_csr_Col, B->tile_csr_Value,
+        C->tile_csr_Col, C->tile_csr_Value);
+    TSG_LAUNCH_CHECK();
+    return TSG_OK;
+}
+
+template <int W>
+static int launch_step2_rows(tsg_context *ctx, long long numC, const tsg_tiled *A, const tsg_tiled *B, tsg_tiled *C,
+                             int *d_bins)
+{
+    const long long items = (numC + W - 1) / W;
+    k_step2_rows<W><<<tsg_blocks(items * 16, 128), 128, 0, ctx->stream>>>(
+        (int)numC, C->tile_rowidx, C->tile_columnidx, C->tile_ptr, A->tile_ptr, A->tile_columnidx, A->mask,
+        B->tile_ptr, B->tile_columnidx, B->mask, C->mask, C->tile_csr_Ptr, C->tile_nnz, d_bins);
+    TSG_LAUNCH_CHECK();
+    return TSG_OK;
+}
+
+static int launch_step3_rows_any(tsg_context *ctx, long long numC, const tsg_tiled *A, const tsg_tiled *B, tsg_tiled *C)
+{
+    const int W = ctx->seg_tiles, cap = ctx->acc_cap;
+    if (W == 8 && cap == 256)
+        return launch_step3_rows<8, 256>(ctx, numC, A, B, C);
+    if (W == 8 && cap == 512)
+        return launch_step3_rows<8, 512>(ctx, numC, A, B, C);
+    if (W == 8 && cap == 1024)
+        return launch_step3_rows<8, 1024>(ctx, numC, A, B, C);
+    if (W == 16 && cap == 512)
+        return launch_step3_rows<16, 512>(ctx, numC, A, B, C);
+    if (W == 16 && cap == 1024)
+        return launch_step3_rows<16, 1024>(ctx, numC, A, B, C);
+    if (W == 16 && cap == 2048)
+        return launch_step3_rows<16, 2048>(ctx, numC, A, B, C);
+    return tsg_set_error(TSG_ERR_INVALID, "unsupported row schedule (%d, %d)", W, cap);
 }
 
 extern "C" int tsg_spgemm(tsg_context *ctx, const tsg_tiled *A, const tsg_tiled *B, tsg_tiled *C,
@@ -420,11 +698,21 @@ extern "C" int tsg_spgemm(tsg_context *ctx, const tsg_tiled *A, const tsg_tiled 
     long long nnzC = 0;
     if (numC > 0)
     {
-        k_step2<<<tsg_blocks(numC * 16, 256), 256, 0, st>>>(
-            (int)numC, C->tile_rowidx, C->tile_columnidx, A->tile_ptr, A->tile_columnidx, A->mask,
-            B->csc_tile_ptr, B->csc_tile_rowidx, B->csc_tile_pos, B->mask, C->mask, C->tile_csr_Ptr,
-            C->tile_nnz, d_bins);
-        TSG_LAUNCH_CHECK();
+        if (ctx->sched == TSG_SCHED_ROWS)
+        {
+            if (ctx->seg_tiles == 16)
+                TSG_TRY(launch_step2_rows<16>(ctx, numC, A, B, C, d_bins));
+            else
+                TSG_TRY(launch_step2_rows<8>(ctx, numC, A, B, C, d_bins));
+        }
+        else
+        {
+            k_step2<<<tsg_blocks(numC * 16, 256), 256, 0, st>>>(
+                (int)numC, C->tile_rowidx, C->tile_columnidx, A->tile_ptr, A->tile_columnidx, A->mask,
+                B->csc_tile_ptr, B->csc_tile_rowidx, B->csc_tile_pos, B->mask, C->mask, C->tile_csr_Ptr,
+                C->tile_nnz, d_bins);
+            TSG_LAUNCH_CHECK();
+        }
         TSG_TRY(tsg_scan_counts(ctx, C->tile_nnz, C->tile_nnz, numC, &nnzC));
     }
     else
@@ -436,7 +724,9 @@ extern "C" int tsg_spgemm(tsg_context *ctx, const tsg_tiled *A, const tsg_tiled 
     // step 3: numeric
     TSG_TRY(tsg_alloc(ctx, &C->tile_csr_Col, (size_t)nnzC));
     TSG_TRY(tsg_alloc(ctx, &C->tile_csr_Value, (size_t)nnzC));
-    if (nnzC > 0)
+    if (nnzC > 0 && ctx->sched == TSG_SCHED_ROWS)
+        TSG_TRY(launch_step3_rows_any(ctx, numC, A, B, C));
+    else if (nnzC > 0)
     {
         k_step3<<<tsg_blocks(numC * 16, S3_THREADS), S3_THREADS, 0, st>>>(
             (int)numC, C->tile_rowidx, C->tile_columnidx, A->tile_ptr, A->tile_columnidx, A->tile_nnz,
@@ -469,5 +759,23 @@ extern "C" int tsg_spgemm(tsg_context *ctx, const tsg_tiled *A, const tsg_tiled 
     }
     tsg_release(ctx, d_pairs);
     tsg_release(ctx, d_bins);
+    return TSG_OK;
+}
+
+// Number of C tiles of A*B (step 1's count pass only); A and B need their
+// row-major tile structure.
+int tsg_count_c_tiles(tsg_context *ctx, const tsg_tiled *A, const tsg_tiled *B, long long *numC)
+{
+    *numC = 0;
+    if (A->tilem == 0)
+        return TSG_OK;
+    int *cnt;
+    TSG_TRY(tsg_alloc(ctx, &cnt, (size_t)A->tilem + 1));
+    k_step1<false><<<tsg_blocks(A->tilem, S1_WARPS), S1_WARPS * 32, 0, ctx->stream>>>(
+        A->tilem, A->tile_ptr, A->tile_columnidx, B->tile_ptr, B->tile_columnidx, cnt, nullptr, nullptr, nullptr,
+        nullptr);
+    TSG_LAUNCH_CHECK();
+    TSG_TRY(tsg_scan_counts(ctx, cnt, cnt, A->tilem, numC));
+    tsg_release(ctx, cnt);
     return TSG_OK;
 }

@@ -36,3 +36,10 @@ def test_library_exports_every_declared_symbol(tsg):
 def test_library_is_sm100a_build(tsg):
     data = tsg.LIB_PATH.read_bytes()
     assert b"sm_100a" in data or b"sm_100" in data
+
+
+def test_cli_binary_prints_usage_without_gpu():
+    import subprocess
+    out = subprocess.run([str(ROOT / "rw-spgemm_b200" / "bin" / "test"), "-d", "0"], capture_output=True, text=True,
+                         timeout=60)
+    assert out.returncode == 0 and "Run the code by './test -d 0 -aat 0 matrixA.mtx" in out.stdout

@@ -1,0 +1,122 @@
+"""GPU orderings and bipermutations against the oracle (and, for original /
+degree / RCM, against the reference's own order_utils.py outputs in
+tests/golden/orders.npz); reorder plans; the reordered product restored."""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+GOLD = Path(__file__).resolve().parent / "golden"
+
+
+def _dev(mat):
+    import torch
+    m, n, rp, ci, v = mat
+    d = torch.device("cuda", 0)
+    return (torch.from_numpy(np.ascontiguousarray(rp, np.int32)).to(d),
+            torch.from_numpy(np.ascontiguousarray(ci, np.int32)).to(d),
+            torch.from_numpy(np.ascontiguousarray(v, np.float64)).to(d))
+
+
+def _mats(gen):
+    return {
+        "lap": gen.laplacian_2d(40, 33),
+        "st27": gen.stencil_27pt_3d(12, seed=2),
+        "st27_perm": gen.permute_symmetric(gen.stencil_27pt_3d(10, seed=1), gen.random_symmetric_permutation(1000, 7)),
+        "pois": gen.random_poisson(700, None, 5.0, seed=4),
+        "rmat": gen.rmat(11, 8, seed=9),          # self loops, isolated vertices, hubs
+        "rect": gen.random_poisson(300, 500, 4.0, seed=1),
+    }
+
+
+@pytest.mark.parametrize("kind", ["original", "degree", "random", "gray", "rcm"])
+def test_gpu_orderings_match_oracle(tsg, ctx, oracle, gen, kind):
+    for name, mat in _mats(gen).items():
+        if kind == "rcm" and mat[0] != mat[1]:
+            continue
+        rp, ci, _ = _dev(mat)
+        got = tsg.order(ctx, kind, mat[0], mat[1], rp, ci, seed=5).cpu().numpy()
+        want = oracle.order(kind, mat, seed=5)
+        np.testing.assert_array_equal(got, want, err_msg=f"{kind} on {name}")
+        assert np.array_equal(np.sort(got), np.arange(mat[0]))
+
+
+def test_orderings_match_reference_order_utils(tsg, ctx):
+    z = np.load(GOLD / "orders.npz")
+    for nm in sorted({k.split("/")[0] for k in z.files}):
+        m, n = (int(x) for x in z[f"{nm}/m"])
+        mat = (m, n, z[f"{nm}/rowptr"], z[f"{nm}/colidx"], z[f"{nm}/val"])
+        rp, ci, _ = _dev(mat)
+        for kind in ("original", "degree", "rcm"):
+            got = tsg.order(ctx, kind, m, n, rp, ci).cpu().numpy()
+            if kind == "rcm" and nm == "rmat7":
+                continue  # scipy seeds ties through an unstable argsort; see test_oracle_orders
+            np.testing.assert_array_equal(got, z[f"{nm}/{kind}"], err_msg=f"{kind} on {nm}")
+
+
+def test_permute_csr_matches_oracle(tsg, ctx, oracle, gen):
+    import torch
+    for name, mat in _mats(gen).items():
+        m, n = mat[0], mat[1]
+        rng = np.random.default_rng(3)
+        row_old = rng.permutation(m).astype(np.int32)
+        col_old = rng.permutation(n).astype(np.int32)
+        col_new = np.empty(n, np.int32)
+        col_new[col_old] = np.arange(n, dtype=np.int32)
+        rp, ci, v = _dev(mat)
+        d = torch.device("cuda", 0)
+        orp, oci, ov = tsg.permute_csr(ctx, m, n, rp, ci, v, torch.from_numpy(row_old).to(d),
+                                       torch.from_numpy(col_new).to(d))
+        W = oracle.apply_bipermutation(mat, row_old, col_new)
+        np.testing.assert_array_equal(orp.cpu().numpy(), W[2])
+        np.testing.assert_array_equal(oci.cpu().numpy(), W[3])
+        np.testing.assert_array_equal(ov.cpu().numpy(), W[4])
+
+
+def test_dropin_apply_restore_round_trip(tsg, gen):
+    mat = gen.random_poisson(333, 444, 6.0, seed=2)
+    rng = np.random.default_rng(8)
+    r, c = rng.permutation(333), rng.permutation(444)
+    P = tsg.apply_bipermutation_csr(mat, r, c)
+    back = tsg.restore_bipermutation_csr(P, r, c)
+    for a, b in zip(back[2:], mat[2:]):
+        np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.parametrize("algo", ["original", "rcm", "degree", "gray", "random"])
+def test_reorder_plan_estimates_and_restored_product(tsg, ctx, oracle, gen, algo):
+    """AA plan on a randomly permuted 3D stencil: the plan's C-tile counts equal
+    the oracle's tile counts of the permuted product, and the product computed
+    in the new order and restored equals the product of the original matrix."""
+    base = gen.stencil_27pt_3d(10, seed=3)
+    mat = gen.permute_symmetric(base, gen.random_symmetric_permutation(1000, 11))
+    plan = tsg.build_reorder_plan("AA", algo, mat)
+    p = plan["row_perm"]
+    assert np.array_equal(plan["inner_perm"], p) and np.array_equal(plan["col_perm"], p)
+    if algo == "original":
+        assert np.array_equal(p, np.arange(1000)) and plan["guard_degraded_to_identity"] == 1
+    else:
+        np.testing.assert_array_equal(p, oracle.order(algo, mat, seed=1))
+    new = np.empty_like(p)
+    new[p] = np.arange(p.size)
+    PA = oracle.apply_bipermutation(mat, p, new)
+    C_before = oracle.spgemm_tiled(oracle.csr2tile_row_major(mat), oracle.csr2tile_col_major(mat))
+    C_after = oracle.spgemm_tiled(oracle.csr2tile_row_major(PA), oracle.csr2tile_col_major(PA))
+    assert plan["estimated_c_tiles_before"] == C_before["numtile"]
+    assert plan["estimated_c_tiles_after"] == C_after["numtile"]
+    assert plan["input_tiles_A_after"] == oracle.csr2tile_row_major(PA)["numtile"]
+    # product in the new order on the GPU, restored to the original order
+    Cp, _ = tsg.spgemm_csr_host(ctx, tsg.apply_bipermutation_csr(mat, p, p))
+    C = tsg.restore_bipermutation_csr(Cp, p, p)
+    G = oracle.gustavson(mat, mat)
+    np.testing.assert_array_equal(C[2], G[2])
+    np.testing.assert_array_equal(C[3], G[3])
+    rel = np.abs(C[4] - G[4]) / np.maximum(np.abs(G[4]), 1e-300)
+    assert rel.max() <= 1e-12   # the inner index order changes with the ordering
+
+
+def test_unknown_ordering_reports_missing_dependency(tsg, gen):
+    with pytest.raises(tsg.TsgError) as e:
+        tsg.build_reorder_plan("AA", "slashburn", gen.laplacian_2d(8))
+    assert e.value.status == -20
