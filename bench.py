@@ -225,6 +225,7 @@ def run_ours(args, tsg, gen, world, rank, local):
     m, n, rp, ci, v = mat
     stream = torch.cuda.current_stream(dev)
     ctx = tsg.Context(local, stream=stream.cuda_stream)
+    ctx.set_schedule(args.sched, args.seg, args.cap)
     d_rp = torch.from_numpy(rp).to(dev)
     d_ci = torch.from_numpy(ci).to(dev)
     d_v = torch.from_numpy(v).to(dev)
@@ -309,6 +310,7 @@ def run_ours(args, tsg, gen, world, rank, local):
                                "uniform(0.5,1.5)), natural order, 16x16 tiles",
                    "products": prods, "tiles_A": A.numtile, "tiles_C": numC, "nnz_C": nnzC,
                    "window": "steps 1-3 incl. C allocation (reference tilespgemm window)",
+                   "schedule": f"{args.sched} seg={args.seg} cap={args.cap}",
                    "l2": "512 MiB write before every timed step, outside the timed events",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
         "hbm_gbs": round(comp / (ms_per_step * 1e-3) / 1e9, 2),
@@ -342,6 +344,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
+    ap.add_argument("--sched", default="rows", choices=["rows", "tiles"])
+    ap.add_argument("--seg", type=int, default=16)
+    ap.add_argument("--cap", type=int, default=1024)
     args = ap.parse_args()
     world, rank, local = dist_setup()
     tsg = _load("rw_spgemm_b200", PKG_DIR / "__init__.py", PKG_DIR)

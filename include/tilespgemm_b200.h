@@ -281,6 +281,9 @@ int tsg_context_set_stream(tsg_context *ctx, void *cuda_stream);
 #define TSG_SCHED_TILES 0
 #define TSG_SCHED_ROWS 1
 int tsg_context_set_schedule(tsg_context *ctx, int schedule, int seg_tiles, int acc_cap);
+/* 0 when all work queued on the context's stream has finished, 1 while
+ * some is pending, a negative status on error (non-blocking). */
+int tsg_context_query(tsg_context *ctx);
 /* Blocks until all work queued on the context's stream has finished. */
 int tsg_context_synchronize(tsg_context *ctx);
 /* Number of this library's kernels launched on the context so far. */
@@ -355,6 +358,94 @@ int tsg_permute_csr(tsg_context *ctx, int m, int n, int nnz,
                     const int *d_rowptr, const int *d_col, const double *d_val,
                     const int *d_row_old, const int *d_col_new,
                     int *d_out_rowptr, int *d_out_col, double *d_out_val);
+
+/* As tsg_spgemm_csr_host; with TSG_HOST_PINNED_OUTPUT in flags the three
+ * output arrays are page-locked host memory (faster device->host copies),
+ * released with tsg_host_free instead of free. */
+#define TSG_HOST_PINNED_OUTPUT 1
+int tsg_spgemm_csr_host_ex(tsg_context *ctx,
+                           int m, int k, int n,
+                           int nnzA, const int *a_rowptr, const int *a_colidx, const double *a_val,
+                           int nnzB, const int *b_rowptr, const int *b_colidx, const double *b_val,
+                           int *nnzC, int **c_rowptr, int **c_colidx, double **c_val,
+                           tsg_spgemm_info *info, int flags);
+void tsg_host_free(void *p);
+
+/* Host CSR -> device tiles in one call (copies through pooled device memory;
+ * the host arrays may be pageable or pinned). */
+int tsg_csr_host_to_tiled(tsg_context *ctx, int m, int n, int nnz,
+                          const int *h_rowptr, const int *h_colidx, const double *h_val,
+                          int flags, tsg_tiled *out);
+/* Device tiles -> host CSR; arrays allocated like tsg_spgemm_csr_host_ex
+ * (TSG_HOST_PINNED_OUTPUT: page-locked, release with tsg_host_free). */
+int tsg_tiled_to_csr_host(tsg_context *ctx, const tsg_tiled *C, int flags,
+                          int **rowptr, int **colidx, double **val);
+
+/* Upper bounds of one product from the tile structure alone: scalar
+ * products (= nnzCub >= nnz(C)) and matched tile pairs (>= C tiles). */
+int tsg_product_bounds(tsg_context *ctx, const tsg_tiled *A, const tsg_tiled *B,
+                       long long *products, long long *tile_pairs);
+
+/* ------------------------------------------------------------------------ */
+/* Batched products: many independent C_p = A_p * B_p of uneven size run in  */
+/* one persistent, cooperatively launched kernel captured in a CUDA graph.   */
+/* ------------------------------------------------------------------------ */
+typedef struct
+{
+    int schedule;  /* TSG_SCHED_TILES or TSG_SCHED_ROWS                  */
+    int seg_tiles; /* row schedule: C tiles per work item                */
+    int acc_cap;   /* row schedule: FP64 accumulator slots per half-warp */
+    int use_graph; /* capture the launch in a CUDA graph                 */
+} tsg_batch_params;
+
+typedef struct tsg_batch tsg_batch;
+
+/* Plans a batch over count device-resident operand pairs (A[p] row tiles,
+ * B[p] with column view; they must stay alive), computes per-product upper
+ * bounds on the device, allocates one result arena and captures the launch.
+ * params NULL = row schedule (16, 1024) with a graph. */
+int tsg_batch_create(tsg_context *ctx, int count, const tsg_tiled *A, const tsg_tiled *B,
+                     const tsg_batch_params *params, tsg_batch **out);
+/* Queues one execution of the whole batch on the context's stream. */
+int tsg_batch_run(tsg_batch *b);
+/* Waits for the last run and reads per-product sizes; reports a device wait
+ * that gave up (TSG_ERR_TIMEOUT) or an exceeded bound (TSG_ERR_OVERFLOW). */
+int tsg_batch_sync(tsg_batch *b, long long *total_tiles, long long *total_nnz);
+/* View of product p's result inside the arena (valid until the next run or
+ * destroy; tsg_tiled_free on it only clears the struct). */
+int tsg_batch_product(tsg_batch *b, int p, tsg_tiled *C);
+int tsg_batch_info(tsg_batch *b, int *graph, int *grid, size_t *arena_bytes, long long *launches);
+int tsg_batch_destroy(tsg_batch *b);
+
+/* ------------------------------------------------------------------------ */
+/* Learned selector: row statistics of a device CSR and a small FP32 MLP     */
+/* (F -> H -> H -> O, ReLU) trained and evaluated by hand-written kernels.   */
+/* ------------------------------------------------------------------------ */
+#define TSG_NFEAT_RAW 24
+/* out[0] sum of row lengths, [1] sum of squares, [2] max length, [3] sum of
+ * |i-j|, [4] max |i-j|, [5] empty rows, [6..17] row-length histogram
+ * (0, 1, 2-3, 4-7, ..., >= 1024), [18] entries with |i-j| < 16. */
+int tsg_row_features(tsg_context *ctx, int m, const int *d_rowptr, const int *d_col,
+                     unsigned long long *h_out);
+
+typedef struct tsg_mlp tsg_mlp;
+/* F <= 32 inputs, H <= 64 hidden units (two layers), O <= 32 outputs; He
+ * initialisation from seed. */
+int tsg_mlp_create(tsg_context *ctx, int F, int H, int O, unsigned long long seed, tsg_mlp **out);
+int tsg_mlp_destroy(tsg_mlp *m);
+int tsg_mlp_num_params(const tsg_mlp *m);
+/* One forward + backward (masked mean squared error) + Adam step on a device
+ * minibatch of B <= 64 rows: X[B][F], T[B][O], M[B][O] (NULL = all 1).
+ * lr <= 0 only computes the gradients (read them with tsg_mlp_get(m, 1, .)).
+ * *loss receives the minibatch loss before the update (NULL: no sync). */
+int tsg_mlp_train_step(tsg_mlp *m, int B, const float *d_X, const float *d_T, const float *d_M,
+                       float lr, float *loss);
+/* Y[n][O] = network(X[n][F]), device arrays. */
+int tsg_mlp_forward(tsg_mlp *m, int n, const float *d_X, float *d_Y);
+/* which = 0 parameters, 1 last gradients; layout W1[F][H] b1 W2[H][H] b2
+ * W3[H][O] b3, row-major. */
+int tsg_mlp_get(tsg_mlp *m, int which, float *host);
+int tsg_mlp_set(tsg_mlp *m, const float *host);
 
 /* Scalar product count nnzCub = sum over A nonzeros (i,k) of nnz(B row k),
  * computed on the device from device CSR arrays. */

@@ -110,6 +110,8 @@ def _declare(L):
     L.tsg_context_set_timing.argtypes = [vp, ip]
     L.tsg_context_launches.argtypes = [vp]
     L.tsg_context_synchronize.argtypes = [vp]
+    L.tsg_context_query.argtypes = [vp]
+    L.tsg_context_set_schedule.argtypes = [vp, ip, ip, ip]
     L.tsg_context_launches.restype = ctypes.c_longlong
     L.tsg_csr_to_tiled.argtypes = [vp, ip, ip, ip, vp, vp, vp, ip, ctypes.POINTER(TsgTiled)]
     L.tsg_tiled_free.argtypes = [vp, ctypes.POINTER(TsgTiled)]
@@ -124,6 +126,9 @@ def _declare(L):
                                       ip, vp, vp, vp, ip, vp, vp, vp,
                                       ctypes.POINTER(ip), ctypes.POINTER(vp), ctypes.POINTER(vp),
                                       ctypes.POINTER(vp), ctypes.POINTER(TsgInfo)]
+    L.tsg_spgemm_csr_host_ex.argtypes = list(L.tsg_spgemm_csr_host.argtypes) + [ip]
+    L.tsg_host_free.argtypes = [vp]
+    L.tsg_host_free.restype = None
     for name in ("csr2tile_row_major", "csr2tile_col_major", "tile2csr", "matrix_destroy"):
         getattr(L, name).argtypes = [ctypes.POINTER(SMatrix)]
         getattr(L, name).restype = None
@@ -280,6 +285,11 @@ class Context:
     def set_timing(self, on: bool):
         check(lib().tsg_context_set_timing(self.handle, 1 if on else 0))
 
+    def set_schedule(self, schedule: str = "rows", seg_tiles: int = 8, acc_cap: int = 512):
+        """'tiles' (half-warp per C tile, intersection) or 'rows' (half-warp per
+        run of seg_tiles C tiles of one tile row, acc_cap FP64 slots)."""
+        check(lib().tsg_context_set_schedule(self.handle, {"tiles": 0, "rows": 1}[schedule], seg_tiles, acc_cap))
+
     def synchronize(self):
         check(lib().tsg_context_synchronize(self.handle))
 
@@ -382,9 +392,34 @@ def count_products(ctx: Context, a_colidx, b_rowptr) -> int:
     return out.value
 
 
-def spgemm_csr_host(ctx: Context, matA, matB=None):
+class _PinnedHostArray:
+    """Owner of a page-locked result array; freed with tsg_host_free."""
+
+    def __init__(self, ptr):
+        self.ptr = ptr
+
+    def __del__(self):
+        try:
+            lib().tsg_host_free(self.ptr)
+        except Exception:
+            pass
+
+
+def _wrap_pinned(ptr, count, dtype):
+    owner = _PinnedHostArray(ptr)
+    if count == 0:
+        return np.zeros(0, dtype=dtype)
+    buf = (ctypes.c_char * (count * np.dtype(dtype).itemsize)).from_address(ptr.value)
+    arr = np.frombuffer(buf, dtype=dtype)
+    arr_owner = arr.view()  # keep the owner alive as long as the array
+    buf._owner = owner
+    return arr_owner
+
+
+def spgemm_csr_host(ctx: Context, matA, matB=None, pinned: bool = True):
     """End to end through the C ABI with host buffers: CSR A * CSR B -> CSR C
-    (numpy).  matB=None computes A*A."""
+    (numpy).  matB=None computes A*A.  pinned=True returns page-locked result
+    arrays without a copy."""
     hA = HostCSR(matA)
     hB = hA if matB is None else HostCSR(matB)
     nnzC = ctypes.c_int(0)
@@ -392,14 +427,20 @@ def spgemm_csr_host(ctx: Context, matA, matB=None):
     info = TsgInfo()
     m, k = hA.sm.m, hA.sm.n
     n = hB.sm.n
-    check(lib().tsg_spgemm_csr_host(
+    check(lib().tsg_spgemm_csr_host_ex(
         ctx.handle, m, k, n,
         hA.sm.nnz, hA.rp.ctypes.data, hA.ci.ctypes.data, hA.v.ctypes.data,
         hB.sm.nnz, hB.rp.ctypes.data, hB.ci.ctypes.data, hB.v.ctypes.data,
-        ctypes.byref(nnzC), ctypes.byref(prp), ctypes.byref(pci), ctypes.byref(pv), ctypes.byref(info)))
-    rp = _np_from(prp, m + 1, np.int32, True)
-    ci = _np_from(pci, nnzC.value, np.int32, True)
-    v = _np_from(pv, nnzC.value, np.float64, True)
+        ctypes.byref(nnzC), ctypes.byref(prp), ctypes.byref(pci), ctypes.byref(pv), ctypes.byref(info),
+        1 if pinned else 0))
+    if pinned:
+        rp = _wrap_pinned(prp, m + 1, np.int32)
+        ci = _wrap_pinned(pci, nnzC.value, np.int32)
+        v = _wrap_pinned(pv, nnzC.value, np.float64)
+    else:
+        rp = _np_from(prp, m + 1, np.int32, True)
+        ci = _np_from(pci, nnzC.value, np.int32, True)
+        v = _np_from(pv, nnzC.value, np.float64, True)
     return (m, n, rp, ci, v), info.as_dict()
 
 
@@ -563,3 +604,125 @@ def build_reorder_plan(kind: str, algorithm: str, matA, matB=None) -> dict:
     d["ordergen_ms"] = ms.value
     L.reorder_info_destroy(ctypes.byref(info))
     return d
+
+
+# ---------------------------------------------------------------------------
+# batched products (one persistent, graph-captured launch for many products)
+# ---------------------------------------------------------------------------
+class BatchParams(ctypes.Structure):
+    _fields_ = [("schedule", ctypes.c_int), ("seg_tiles", ctypes.c_int), ("acc_cap", ctypes.c_int),
+                ("use_graph", ctypes.c_int)]
+
+
+def _declare_batch(L):
+    vp, ip = ctypes.c_void_p, ctypes.c_int
+    L.tsg_batch_create.argtypes = [vp, ip, ctypes.POINTER(TsgTiled), ctypes.POINTER(TsgTiled),
+                                   ctypes.POINTER(BatchParams), ctypes.POINTER(vp)]
+    L.tsg_batch_run.argtypes = [vp]
+    L.tsg_batch_sync.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]
+    L.tsg_batch_product.argtypes = [vp, ip, ctypes.POINTER(TsgTiled)]
+    L.tsg_batch_info.argtypes = [vp, ctypes.POINTER(ip), ctypes.POINTER(ip), ctypes.POINTER(ctypes.c_size_t),
+                                 ctypes.POINTER(ctypes.c_longlong)]
+    L.tsg_batch_destroy.argtypes = [vp]
+    L.tsg_product_bounds.argtypes = [vp, ctypes.POINTER(TsgTiled), ctypes.POINTER(TsgTiled),
+                                     ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]
+
+
+_declare_prev = _declare
+
+
+def _declare(L):  # noqa: F811
+    _declare_prev(L)
+    _declare_batch(L)
+
+
+def product_bounds(ctx: Context, A: Tiled, B: Tiled):
+    """(scalar products, matched tile pairs) of A*B from the tile structure."""
+    pr, tp = ctypes.c_longlong(0), ctypes.c_longlong(0)
+    check(lib().tsg_product_bounds(ctx.handle, ctypes.byref(A.s), ctypes.byref(B.s), ctypes.byref(pr),
+                                   ctypes.byref(tp)))
+    return pr.value, tp.value
+
+
+class Batch:
+    """tsg_batch over device-resident (A, B) operand pairs."""
+
+    def __init__(self, ctx: Context, pairs, schedule: str = "rows", seg_tiles: int = 16, acc_cap: int = 1024,
+                 graph: bool = True):
+        self.ctx = ctx
+        self.pairs = list(pairs)  # keep operands alive
+        n = len(self.pairs)
+        arrA = (TsgTiled * n)(*[a.s for a, _ in self.pairs])
+        arrB = (TsgTiled * n)(*[b.s for _, b in self.pairs])
+        prm = BatchParams({"tiles": 0, "rows": 1}[schedule], seg_tiles, acc_cap, 1 if graph else 0)
+        self.handle = ctypes.c_void_p()
+        check(lib().tsg_batch_create(ctx.handle, n, arrA, arrB, ctypes.byref(prm), ctypes.byref(self.handle)))
+        self.count = n
+        self.params = dict(schedule=schedule, seg_tiles=seg_tiles, acc_cap=acc_cap)
+
+    def run(self):
+        check(lib().tsg_batch_run(self.handle))
+
+    def sync(self):
+        t, z = ctypes.c_longlong(0), ctypes.c_longlong(0)
+        check(lib().tsg_batch_sync(self.handle, ctypes.byref(t), ctypes.byref(z)))
+        return t.value, z.value
+
+    def product(self, p: int) -> Tiled:
+        """Borrowed view of product p's C (valid until the next run / close)."""
+        v = Tiled(self.ctx)
+        check(lib().tsg_batch_product(self.handle, int(p), ctypes.byref(v.s)))
+        return v
+
+    def info(self) -> dict:
+        g, gr = ctypes.c_int(0), ctypes.c_int(0)
+        ab, ln = ctypes.c_size_t(0), ctypes.c_longlong(0)
+        check(lib().tsg_batch_info(self.handle, ctypes.byref(g), ctypes.byref(gr), ctypes.byref(ab), ctypes.byref(ln)))
+        return dict(graph=bool(g.value), grid=gr.value, arena_bytes=ab.value, launches=ln.value)
+
+    def close(self):
+        if self.handle:
+            lib().tsg_batch_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _declare_host_io(L):
+    vp, ip = ctypes.c_void_p, ctypes.c_int
+    L.tsg_csr_host_to_tiled.argtypes = [vp, ip, ip, ip, vp, vp, vp, ip, ctypes.POINTER(TsgTiled)]
+    L.tsg_tiled_to_csr_host.argtypes = [vp, ctypes.POINTER(TsgTiled), ip, ctypes.POINTER(vp), ctypes.POINTER(vp),
+                                        ctypes.POINTER(vp)]
+
+
+_declare_prev2 = _declare
+
+
+def _declare(L):  # noqa: F811
+    _declare_prev2(L)
+    _declare_host_io(L)
+
+
+def csr_host_to_tiled(ctx: Context, mat, flags: int) -> Tiled:
+    """Host CSR (numpy) -> device tiles in one C call."""
+    h = HostCSR(mat)
+    t = Tiled(ctx)
+    check(lib().tsg_csr_host_to_tiled(ctx.handle, h.sm.m, h.sm.n, h.sm.nnz, h.rp.ctypes.data, h.ci.ctypes.data,
+                                      h.v.ctypes.data, int(flags), ctypes.byref(t.s)))
+    return t
+
+
+def tiled_to_csr_host(ctx: Context, C: Tiled, pinned: bool = True):
+    """Device tiles -> host CSR (numpy; page-locked without a copy when pinned)."""
+    prp, pci, pv = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
+    check(lib().tsg_tiled_to_csr_host(ctx.handle, ctypes.byref(C.s), 1 if pinned else 0, ctypes.byref(prp),
+                                      ctypes.byref(pci), ctypes.byref(pv)))
+    m, n, nnz = C.s.m, C.s.n, C.s.nnz
+    if pinned:
+        return m, n, _wrap_pinned(prp, m + 1, np.int32), _wrap_pinned(pci, nnz, np.int32), _wrap_pinned(pv, nnz, np.float64)
+    return (m, n, _np_from(prp, m + 1, np.int32, True), _np_from(pci, nnz, np.int32, True),
+            _np_from(pv, nnz, np.float64, True))

@@ -120,7 +120,8 @@ extern "C" int tsg_context_set_schedule(tsg_context *ctx, int schedule, int seg_
     if (schedule == TSG_SCHED_ROWS)
     {
         const bool ok = (seg_tiles == 8 && (acc_cap == 256 || acc_cap == 512 || acc_cap == 1024)) ||
-                        (seg_tiles == 16 && (acc_cap == 512 || acc_cap == 1024 || acc_cap == 2048));
+                        (seg_tiles == 16 && (acc_cap == 512 || acc_cap == 1024 || acc_cap == 2048)) ||
+                        (seg_tiles == 32 && (acc_cap == 1024 || acc_cap == 2048));
         if (!ok)
             return tsg_set_error(TSG_ERR_INVALID, "unsupported (seg_tiles, acc_cap) = (%d, %d)", seg_tiles, acc_cap);
         ctx->seg_tiles = seg_tiles;
@@ -128,6 +129,18 @@ extern "C" int tsg_context_set_schedule(tsg_context *ctx, int schedule, int seg_
     }
     ctx->sched = schedule;
     return TSG_OK;
+}
+
+extern "C" int tsg_context_query(tsg_context *ctx)
+{
+    if (!ctx)
+        return tsg_set_error(TSG_ERR_INVALID, "null context");
+    const cudaError_t e = cudaStreamQuery(ctx->stream);
+    if (e == cudaSuccess)
+        return 0;
+    if (e == cudaErrorNotReady)
+        return 1;
+    return tsg_set_error(TSG_ERR_CUDA, "stream query: %s", cudaGetErrorString(e));
 }
 
 extern "C" int tsg_context_synchronize(tsg_context *ctx)
@@ -152,6 +165,11 @@ extern "C" int tsg_tiled_free(tsg_context *ctx, tsg_tiled *t)
 {
     if (!ctx || !t)
         return TSG_OK;
+    if (t->_alloc) // borrowed view (batch arena): nothing to release
+    {
+        memset(t, 0, sizeof(*t));
+        return TSG_OK;
+    }
     tsg_release(ctx, t->tile_ptr);
     tsg_release(ctx, t->tile_columnidx);
     tsg_release(ctx, t->tile_rowidx);
@@ -333,10 +351,34 @@ extern "C" int tsg_tiled_download(tsg_context *ctx, const tsg_tiled *src, int co
 // ---------------------------------------------------------------------------
 // End-to-end CSR call with host buffers.
 // ---------------------------------------------------------------------------
+template <typename T>
+static int d2h_pinned(tsg_context *ctx, T **dst, const T *src, size_t count)
+{
+    TSG_CUDA(cudaMallocHost((void **)dst, (count ? count : 1) * sizeof(T)));
+    if (count && src)
+        TSG_CUDA(cudaMemcpyAsync(*dst, src, count * sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
+    return TSG_OK;
+}
+
+extern "C" void tsg_host_free(void *p)
+{
+    if (p)
+        cudaFreeHost(p);
+}
+
 extern "C" int tsg_spgemm_csr_host(tsg_context *ctx, int m, int k, int n, int nnzA, const int *a_rowptr,
                                    const int *a_colidx, const double *a_val, int nnzB, const int *b_rowptr,
                                    const int *b_colidx, const double *b_val, int *nnzC, int **c_rowptr,
                                    int **c_colidx, double **c_val, tsg_spgemm_info *info)
+{
+    return tsg_spgemm_csr_host_ex(ctx, m, k, n, nnzA, a_rowptr, a_colidx, a_val, nnzB, b_rowptr, b_colidx, b_val,
+                                  nnzC, c_rowptr, c_colidx, c_val, info, 0);
+}
+
+extern "C" int tsg_spgemm_csr_host_ex(tsg_context *ctx, int m, int k, int n, int nnzA, const int *a_rowptr,
+                                      const int *a_colidx, const double *a_val, int nnzB, const int *b_rowptr,
+                                      const int *b_colidx, const double *b_val, int *nnzC, int **c_rowptr,
+                                      int **c_colidx, double **c_val, tsg_spgemm_info *info, int flags)
 {
     if (!ctx || !a_rowptr || !b_rowptr || !nnzC || !c_rowptr || !c_colidx || !c_val)
         return tsg_set_error(TSG_ERR_INVALID, "null argument");
@@ -385,11 +427,22 @@ extern "C" int tsg_spgemm_csr_host(tsg_context *ctx, int m, int k, int n, int nn
     if (st == TSG_OK)
     {
         *nnzC = C.nnz;
-        st = d2h(ctx, c_rowptr, dC_rp, (size_t)m + 1);
-        if (st == TSG_OK)
-            st = d2h(ctx, c_colidx, dC_ci, (size_t)C.nnz);
-        if (st == TSG_OK)
-            st = d2h(ctx, c_val, dC_v, (size_t)C.nnz);
+        if (flags & TSG_HOST_PINNED_OUTPUT)
+        {
+            st = d2h_pinned(ctx, c_rowptr, dC_rp, (size_t)m + 1);
+            if (st == TSG_OK)
+                st = d2h_pinned(ctx, c_colidx, dC_ci, (size_t)C.nnz);
+            if (st == TSG_OK)
+                st = d2h_pinned(ctx, c_val, dC_v, (size_t)C.nnz);
+        }
+        else
+        {
+            st = d2h(ctx, c_rowptr, dC_rp, (size_t)m + 1);
+            if (st == TSG_OK)
+                st = d2h(ctx, c_colidx, dC_ci, (size_t)C.nnz);
+            if (st == TSG_OK)
+                st = d2h(ctx, c_val, dC_v, (size_t)C.nnz);
+        }
         cudaError_t e = cudaStreamSynchronize(ctx->stream);
         if (st == TSG_OK && e != cudaSuccess)
             st = tsg_set_error(TSG_ERR_CUDA, "%s", cudaGetErrorString(e));
@@ -590,4 +643,51 @@ extern "C" void tilespgemm(SMatrix *matrixA, SMatrix *matrixB, SMatrix *matrixC,
     tsg_tiled_free(ctx, &B);
     tsg_tiled_free(ctx, &C);
     cudaStreamSynchronize(ctx->stream);
+}
+
+extern "C" int tsg_csr_host_to_tiled(tsg_context *ctx, int m, int n, int nnz, const int *h_rowptr,
+                                     const int *h_colidx, const double *h_val, int flags, tsg_tiled *out)
+{
+    if (!ctx || !out || !h_rowptr)
+        return tsg_set_error(TSG_ERR_INVALID, "null argument");
+    int *rp, *ci;
+    double *v;
+    TSG_TRY(h2d(ctx, &rp, h_rowptr, (size_t)m + 1));
+    TSG_TRY(h2d(ctx, &ci, h_colidx, (size_t)nnz));
+    TSG_TRY(h2d(ctx, &v, h_val, (size_t)nnz));
+    const int st = tsg_csr_to_tiled(ctx, m, n, nnz, rp, ci, v, flags, out);
+    tsg_release(ctx, rp);
+    tsg_release(ctx, ci);
+    tsg_release(ctx, v);
+    return st;
+}
+
+extern "C" int tsg_tiled_to_csr_host(tsg_context *ctx, const tsg_tiled *C, int flags, int **rowptr, int **colidx,
+                                     double **val)
+{
+    if (!ctx || !C || !rowptr || !colidx || !val)
+        return tsg_set_error(TSG_ERR_INVALID, "null argument");
+    int *rp, *ci;
+    double *v;
+    TSG_TRY(tsg_alloc(ctx, &rp, (size_t)C->m + 1));
+    TSG_TRY(tsg_alloc(ctx, &ci, (size_t)C->nnz));
+    TSG_TRY(tsg_alloc(ctx, &v, (size_t)C->nnz));
+    TSG_TRY(tsg_tiled_to_csr(ctx, C, rp, ci, v));
+    if (flags & TSG_HOST_PINNED_OUTPUT)
+    {
+        TSG_TRY(d2h_pinned(ctx, rowptr, rp, (size_t)C->m + 1));
+        TSG_TRY(d2h_pinned(ctx, colidx, ci, (size_t)C->nnz));
+        TSG_TRY(d2h_pinned(ctx, val, v, (size_t)C->nnz));
+    }
+    else
+    {
+        TSG_TRY(d2h(ctx, rowptr, rp, (size_t)C->m + 1));
+        TSG_TRY(d2h(ctx, colidx, ci, (size_t)C->nnz));
+        TSG_TRY(d2h(ctx, val, v, (size_t)C->nnz));
+    }
+    TSG_CUDA(cudaStreamSynchronize(ctx->stream));
+    tsg_release(ctx, rp);
+    tsg_release(ctx, ci);
+    tsg_release(ctx, v);
+    return TSG_OK;
 }

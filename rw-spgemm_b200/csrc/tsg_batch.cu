@@ -1,0 +1,723 @@
+// Batched tiled SpGEMM: many independent products C_p = A_p * B_p of uneven
+// size in ONE persistent, cooperatively launched kernel, captured once in a
+// CUDA graph and replayed by tsg_batch_run.
+//
+// The kernel runs seven phases separated by a grid barrier; in each phase the
+// work of all products is one flattened index space (product found by binary
+// search over a prefix array), so small products do not leave the GPU idle:
+//   1 step-1 counts (warp per A tile row)        2 per-product scan of them
+//   3 item prefix over products (block 0)        4 step-1 emit
+//   5 step 2 (half-warp per item)                6 per-product scan of tile nnz
+//   7 step 3 (half-warp per item)
+// An item is one C tile (tile schedule) or seg_tiles C tiles (row schedule);
+// the per-item code is tsg_device.cuh's, identical to the one-product path.
+//
+// Memory: one arena per batch, sized at creation from per-product upper
+// bounds computed on the device (C tiles <= matched tile pairs, C nonzeros <=
+// scalar products), so a run needs no host round trip.  The grid barrier is
+// bounded: a wait that exceeds its iteration limit sets an error flag that
+// tsg_batch_sync reports, and every block leaves.
+#include <cooperative_groups.h>
+#include <stdlib.h>
+
+#include <vector>
+
+#include "tsg_device.cuh"
+
+int tsg_count_c_tiles(tsg_context *ctx, const tsg_tiled *A, const tsg_tiled *B, long long *numC);
+
+struct BatchProd
+{
+    ProdView P;
+    long long capT, capN;
+    int tilemA;
+    int status; // 0 ok, 1 tile capacity, 2 value capacity
+    int numC, nnzC;
+};
+
+struct tsg_batch
+{
+    tsg_context *ctx;
+    int count;
+    tsg_batch_params params;
+    std::vector<BatchProd> host;    // descriptors (host copy)
+    std::vector<long long> rowoff;  // prefix of tilemA over products
+    BatchProd *d_prod;
+    long long *d_rowoff;
+    long long *d_itemoff;
+    unsigned *d_bar; // [0] arrivals, [1] generation
+    int *d_err;
+    int *d_bins;
+    void *arena;
+    size_t arena_bytes;
+    int grid, block;
+    size_t smem;
+    cudaGraph_t graph;
+    cudaGraphExec_t exec;
+    int graph_ok;
+    std::vector<int> m, n, tilen; // per product C dimensions
+    long long launches;
+};
+
+#define BATCH_THREADS 128
+#define BATCH_BAR_LIMIT 4000000LL
+
+// ---------------------------------------------------------------------------
+// bounded grid barrier (all blocks co-resident: cooperative launch)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool grid_barrier(unsigned *bar, int *err)
+{
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        volatile unsigned *vgen = bar + 1;
+        const unsigned gen = *vgen;
+        __threadfence();
+        const unsigned arrived = atomicAdd(bar, 1u) + 1u;
+        if (arrived == gridDim.x)
+        {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        }
+        else
+        {
+            long long spins = 0;
+            while (*vgen == gen)
+            {
+                if (++spins > BATCH_BAR_LIMIT || *(volatile int *)err)
+                {
+                    atomicOr(err, 1);
+                    break;
+                }
+                __nanosleep(100);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return *(volatile int *)err == 0;
+}
+
+__device__ __forceinline__ int find_product(const long long *__restrict__ off, int count, long long x)
+{
+    int lo = 0, hi = count - 1; // largest p with off[p] <= x
+    while (lo < hi)
+    {
+        const int mid = (lo + hi + 1) >> 1;
+        if (off[mid] <= x)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+// Block-wide exclusive scan of a[0..n) in place, a[n] = total (BATCH_THREADS).
+__device__ long long block_scan_inplace(int *a, int n, long long *s_tmp)
+{
+    long long run = 0;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int base = 0; base < n; base += BATCH_THREADS)
+    {
+        const int i = base + threadIdx.x;
+        const long long v = i < n ? a[i] : 0;
+        long long incl = v;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1)
+        {
+            const long long o = __shfl_up_sync(TSG_FULL_MASK, incl, d);
+            if (lane >= d)
+                incl += o;
+        }
+        if (lane == 31)
+            s_tmp[warp] = incl;
+        __syncthreads();
+        long long woff = 0;
+        for (int w = 0; w < warp; w++)
+            woff += s_tmp[w];
+        const long long tot = s_tmp[0] + s_tmp[1] + s_tmp[2] + s_tmp[3];
+        if (i < n)
+            a[i] = (int)(run + woff + incl - v);
+        run += tot;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        a[n] = (int)run;
+    __syncthreads();
+    return run;
+}
+
+template <int SCHED, int W, int CAP>
+__global__ void __launch_bounds__(BATCH_THREADS)
+    k_batch(BatchProd *prods, int count, const long long *__restrict__ rowoff, long long *itemoff, unsigned *bar,
+            int *err, int *bins)
+{
+    extern __shared__ __align__(16) unsigned char s_raw[];
+    __shared__ long long s_tmp[4];
+    __shared__ int s_bins[4];
+    const int lane32 = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 15, hw = threadIdx.x >> 4;
+    const unsigned hmask = TSG_HW_MASK(threadIdx.x);
+    const long long nwarps = (long long)gridDim.x * (BATCH_THREADS / 32);
+    const long long nhw = (long long)gridDim.x * (BATCH_THREADS / 16);
+    const long long total_rows = rowoff[count];
+
+    // phase 1: step-1 counts
+    {
+        unsigned *bm = reinterpret_cast<unsigned *>(s_raw) + warp * S1_WORDS;
+        for (long long w = (long long)blockIdx.x * (BATCH_THREADS / 32) + warp; w < total_rows; w += nwarps)
+        {
+            const int p = find_product(rowoff, count, w);
+            const ProdView &P = prods[p].P;
+            const int i = (int)(w - rowoff[p]);
+            const int cnt = step1_row<false>(P, i, bm, lane32, nullptr);
+            if (lane32 == 0)
+                P.C_ptr[i] = cnt;
+        }
+    }
+    if (!grid_barrier(bar, err))
+        return;
+    // phase 2: per-product scan of C tile counts
+    for (int p = blockIdx.x; p < count; p += gridDim.x)
+    {
+        BatchProd &bp = prods[p];
+        const long long tot = block_scan_inplace(bp.P.C_ptr, bp.tilemA, s_tmp);
+        if (threadIdx.x == 0)
+        {
+            if (tot > bp.capT)
+            {
+                bp.status = 1;
+                bp.numC = 0;
+            }
+            else
+            {
+                bp.status = 0;
+                bp.numC = (int)tot;
+            }
+            bp.P.numC = bp.numC;
+        }
+    }
+    if (!grid_barrier(bar, err))
+        return;
+    // phase 3: item prefix over products (block 0)
+    if (blockIdx.x == 0)
+    {
+        if (threadIdx.x == 0)
+        {
+            long long run = 0;
+            for (int p = 0; p < count; p++)
+            {
+                itemoff[p] = run;
+                const long long nc = prods[p].numC;
+                run += SCHED ? (nc + W - 1) / W : nc;
+            }
+            itemoff[count] = run;
+        }
+        if (threadIdx.x < 4)
+            bins[threadIdx.x] = 0;
+    }
+    if (!grid_barrier(bar, err))
+        return;
+    // phase 4: step-1 emit
+    {
+        unsigned *bm = reinterpret_cast<unsigned *>(s_raw) + warp * S1_WORDS;
+        for (long long w = (long long)blockIdx.x * (BATCH_THREADS / 32) + warp; w < total_rows; w += nwarps)
+        {
+            const int p = find_product(rowoff, count, w);
+            if (prods[p].status)
+                continue;
+            step1_row<true>(prods[p].P, (int)(w - rowoff[p]), bm, lane32, nullptr);
+        }
+    }
+    if (!grid_barrier(bar, err))
+        return;
+    // phase 5: step 2
+    if (threadIdx.x < 4)
+        s_bins[threadIdx.x] = 0;
+    __syncthreads();
+    {
+        const long long total_items = itemoff[count];
+        for (long long h = (long long)blockIdx.x * (BATCH_THREADS / 16) + hw; h < total_items; h += nhw)
+        {
+            const int p = find_product(itemoff, count, h);
+            const ProdView &P = prods[p].P;
+            const long long item = h - itemoff[p];
+            if (SCHED)
+                step2_rows_item<W>(P, item, hmask, lane, reinterpret_cast<S2RowsSmem<W> *>(s_raw)[hw], s_bins);
+            else
+                step2_tile(P, (int)item, hmask, lane, s_bins);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < 4 && s_bins[threadIdx.x])
+        atomicAdd(&bins[threadIdx.x], s_bins[threadIdx.x]);
+    if (!grid_barrier(bar, err))
+        return;
+    // phase 6: per-product scan of tile nnz
+    for (int p = blockIdx.x; p < count; p += gridDim.x)
+    {
+        BatchProd &bp = prods[p];
+        const long long tot = block_scan_inplace(bp.P.C_tnnz, bp.numC, s_tmp);
+        if (threadIdx.x == 0)
+        {
+            if (tot > bp.capN)
+            {
+                bp.status = 2;
+                bp.nnzC = 0;
+            }
+            else
+                bp.nnzC = (int)tot;
+        }
+    }
+    if (!grid_barrier(bar, err))
+        return;
+    // phase 7: step 3
+    {
+        double *tacc = reinterpret_cast<double *>(s_raw) + hw * (TSG_BS * S3T_STRIDE);
+        if (!SCHED)
+        {
+            for (int q = lane; q < TSG_BS * S3T_STRIDE; q += 16)
+                tacc[q] = 0.0;
+            __syncwarp(hmask);
+        }
+        const long long total_items = itemoff[count];
+        for (long long h = (long long)blockIdx.x * (BATCH_THREADS / 16) + hw; h < total_items; h += nhw)
+        {
+            const int p = find_product(itemoff, count, h);
+            if (prods[p].status)
+                continue;
+            const ProdView &P = prods[p].P;
+            const long long item = h - itemoff[p];
+            if (SCHED)
+                step3_rows_item<W, CAP>(P, item, hmask, lane, reinterpret_cast<S3RowsSmem<W, CAP> *>(s_raw)[hw]);
+            else
+                step3_tile(P, (int)item, hmask, lane, tacc);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// upper bounds: matched tile pairs and scalar products per product
+// ---------------------------------------------------------------------------
+// half-warp per B tile row: element row lengths of B from the tile masks
+__global__ void k_brow_len(int tilem, int m, const int *__restrict__ tile_ptr, const unsigned short *__restrict__ mask,
+                           int *__restrict__ rowlen)
+{
+    const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int tr = (int)(gid >> 4), lane = threadIdx.x & 15;
+    if (tr >= tilem)
+        return;
+    int s = 0;
+    for (int t = tile_ptr[tr]; t < tile_ptr[tr + 1]; t++)
+        s += __popc((unsigned)mask[(long long)t * TSG_BS + lane]);
+    if (tr * TSG_BS + lane < m)
+        rowlen[tr * TSG_BS + lane] = s;
+}
+
+// half-warp per A tile: tile pairs and scalar products it generates
+__global__ void k_bounds(int T, const int *__restrict__ A_col, const unsigned short *__restrict__ A_mask,
+                         const int *__restrict__ B_ptr, const int *__restrict__ browlen, int mB,
+                         unsigned long long *__restrict__ out)
+{
+    const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = (int)(gid >> 4), lane = threadIdx.x & 15;
+    unsigned long long prods = 0, pairs = 0;
+    if (t < T)
+    {
+        const int k = A_col[t];
+        unsigned ma = A_mask[(long long)t * TSG_BS + lane];
+        while (ma)
+        {
+            const int bit = 31 - __clz(ma);
+            const int row = k * TSG_BS + (15 - bit);
+            if (row < mB)
+                prods += (unsigned long long)browlen[row];
+            ma ^= 1u << bit;
+        }
+        if (lane == 0)
+            pairs = (unsigned long long)(B_ptr[k + 1] - B_ptr[k]);
+    }
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1)
+    {
+        prods += __shfl_xor_sync(TSG_FULL_MASK, prods, d);
+        pairs += __shfl_xor_sync(TSG_FULL_MASK, pairs, d);
+    }
+    if ((threadIdx.x & 31) == 0 && (prods || pairs))
+    {
+        atomicAdd(out, prods);
+        atomicAdd(out + 1, pairs);
+    }
+}
+
+extern "C" int tsg_product_bounds(tsg_context *ctx, const tsg_tiled *A, const tsg_tiled *B, long long *products,
+                                  long long *tile_pairs)
+{
+    if (!ctx || !A || !B || !products || !tile_pairs)
+        return tsg_set_error(TSG_ERR_INVALID, "null argument");
+    int *rowlen;
+    unsigned long long *d;
+    TSG_TRY(tsg_alloc(ctx, &rowlen, (size_t)B->m + 1));
+    TSG_TRY(tsg_alloc(ctx, &d, 2));
+    TSG_CUDA(cudaMemsetAsync(d, 0, 2 * sizeof(unsigned long long), ctx->stream));
+    TSG_CUDA(cudaMemsetAsync(rowlen, 0, ((size_t)B->m + 1) * sizeof(int), ctx->stream));
+    if (B->tilem > 0)
+    {
+        k_brow_len<<<tsg_blocks((long long)B->tilem * 16, 256), 256, 0, ctx->stream>>>(B->tilem, B->m, B->tile_ptr,
+                                                                                       B->mask, rowlen);
+        TSG_LAUNCH_CHECK();
+    }
+    if (A->numtile > 0)
+    {
+        k_bounds<<<tsg_blocks((long long)A->numtile * 16, 256), 256, 0, ctx->stream>>>(
+            A->numtile, A->tile_columnidx, A->mask, B->tile_ptr, rowlen, B->m, d);
+        TSG_LAUNCH_CHECK();
+    }
+    TSG_CUDA(cudaMemcpyAsync(ctx->h_pinned, d, 2 * sizeof(long long), cudaMemcpyDeviceToHost, ctx->stream));
+    TSG_CUDA(cudaStreamSynchronize(ctx->stream));
+    *products = ctx->h_pinned[0];
+    *tile_pairs = ctx->h_pinned[1];
+    tsg_release(ctx, rowlen);
+    tsg_release(ctx, d);
+    return TSG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+typedef void (*batch_kernel_t)(BatchProd *, int, const long long *, long long *, unsigned *, int *, int *);
+
+static batch_kernel_t pick_kernel(const tsg_batch_params &p, size_t *smem)
+{
+    const size_t s1 = (size_t)(BATCH_THREADS / 32) * S1_WORDS * 4;
+    if (p.schedule == TSG_SCHED_TILES)
+    {
+        const size_t s3 = (size_t)(BATCH_THREADS / 16) * TSG_BS * S3T_STRIDE * 8;
+        *smem = s1 > s3 ? s1 : s3;
+        return k_batch<0, 8, 256>;
+    }
+#define TSG_PICK(w, c)                                                                          \
+    if (p.seg_tiles == w && p.acc_cap == c)                                                     \
+    {                                                                                           \
+        size_t s2 = (size_t)(BATCH_THREADS / 16) * sizeof(S2RowsSmem<w>);                       \
+        size_t s3 = (size_t)(BATCH_THREADS / 16) * sizeof(S3RowsSmem<w, c>);                    \
+        size_t mx = s1 > s2 ? s1 : s2;                                                          \
+        *smem = mx > s3 ? mx : s3;                                                              \
+        return k_batch<1, w, c>;                                                                \
+    }
+    TSG_ROW_CONFIGS(TSG_PICK)
+#undef TSG_PICK
+    return nullptr;
+}
+
+static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+static int record_run(tsg_batch *b, cudaStream_t st)
+{
+    size_t smem;
+    batch_kernel_t kern = pick_kernel(b->params, &smem);
+    TSG_CUDA(cudaMemsetAsync(b->d_err, 0, sizeof(int), st));
+    TSG_CUDA(cudaMemsetAsync(b->d_bar, 0, sizeof(unsigned), st));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)b->grid);
+    cfg.blockDim = dim3(BATCH_THREADS);
+    cfg.dynamicSmemBytes = b->smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    TSG_CUDA(cudaLaunchKernelEx(&cfg, kern, b->d_prod, b->count, (const long long *)b->d_rowoff, b->d_itemoff,
+                                b->d_bar, b->d_err, b->d_bins));
+    return TSG_OK;
+}
+
+extern "C" int tsg_batch_create(tsg_context *ctx, int count, const tsg_tiled *A, const tsg_tiled *B,
+                                const tsg_batch_params *params, tsg_batch **out)
+{
+    if (!ctx || !out || count <= 0 || !A || !B)
+        return tsg_set_error(TSG_ERR_INVALID, "bad batch arguments");
+    *out = nullptr;
+    tsg_batch_params prm;
+    if (params)
+        prm = *params;
+    else
+    {
+        prm.schedule = TSG_SCHED_ROWS;
+        prm.seg_tiles = 16;
+        prm.acc_cap = 1024;
+        prm.use_graph = 1;
+    }
+    size_t smem;
+    batch_kernel_t kern = pick_kernel(prm, &smem);
+    if (!kern)
+        return tsg_set_error(TSG_ERR_INVALID, "unsupported batch schedule (%d, %d, %d)", prm.schedule, prm.seg_tiles,
+                             prm.acc_cap);
+    for (int p = 0; p < count; p++)
+    {
+        if (A[p].n != B[p].m || !B[p].csc_tile_ptr)
+            return tsg_set_error(TSG_ERR_INVALID, "product %d: inner dimensions differ or B lacks its column view", p);
+    }
+    tsg_batch *b = new tsg_batch();
+    b->ctx = ctx;
+    b->count = count;
+    b->params = prm;
+    b->host.resize(count);
+    b->rowoff.resize(count + 1);
+    b->m.resize(count);
+    b->n.resize(count);
+    b->tilen.resize(count);
+    b->launches = 0;
+    // bounds and arena layout
+    size_t bytes = 0;
+    std::vector<size_t> off(count);
+    long long run = 0;
+    for (int p = 0; p < count; p++)
+    {
+        long long prods = 0, pairs = 0;
+        int st = tsg_product_bounds(ctx, &A[p], &B[p], &prods, &pairs);
+        if (st != TSG_OK)
+        {
+            delete b;
+            return st;
+        }
+        // exact C tile count (step 1's count pass) bounds both arrays tightly
+        long long capT = 0;
+        st = tsg_count_c_tiles(ctx, &A[p], &B[p], &capT);
+        if (st != TSG_OK)
+        {
+            delete b;
+            return st;
+        }
+        (void)pairs;
+        long long capN = prods < 256 * capT ? prods : 256 * capT;
+        if (capN > 2147483647LL || capT > 2147483647LL / 16)
+        {
+            delete b;
+            return tsg_set_error(TSG_ERR_OVERFLOW, "product %d exceeds 32-bit offsets", p);
+        }
+        BatchProd &h = b->host[p];
+        memset(&h, 0, sizeof(h));
+        h.capT = capT;
+        h.capN = capN;
+        h.tilemA = A[p].tilem;
+        b->rowoff[p] = run;
+        run += A[p].tilem;
+        b->m[p] = A[p].m;
+        b->n[p] = B[p].n;
+        b->tilen[p] = B[p].tilen;
+        off[p] = bytes;
+        bytes += align256(((size_t)A[p].tilem + 1) * 4) + 2 * align256((size_t)capT * 4) + align256(((size_t)capT + 1) * 4) +
+                 align256((size_t)capT * 32) + align256((size_t)capT * 16) + align256((size_t)capN) +
+                 align256((size_t)capN * 8);
+    }
+    b->rowoff[count] = run;
+    b->arena_bytes = bytes;
+    int st = TSG_OK;
+    if ((st = tsg_alloc(ctx, (char **)&b->arena, bytes ? bytes : 256)) != TSG_OK)
+    {
+        delete b;
+        return st;
+    }
+    for (int p = 0; p < count; p++)
+    {
+        BatchProd &h = b->host[p];
+        char *q = (char *)b->arena + off[p];
+        auto take = [&](size_t nbytes) {
+            char *r = q;
+            q += align256(nbytes);
+            return r;
+        };
+        ProdView &P = h.P;
+        P.A_ptr = A[p].tile_ptr;
+        P.A_col = A[p].tile_columnidx;
+        P.A_tnnz = A[p].tile_nnz;
+        P.A_Ptr = A[p].tile_csr_Ptr;
+        P.A_Colb = A[p].tile_csr_Col;
+        P.A_Val = A[p].tile_csr_Value;
+        P.A_mask = A[p].mask;
+        P.tilemA = A[p].tilem;
+        P.B_ptr = B[p].tile_ptr;
+        P.B_col = B[p].tile_columnidx;
+        P.B_cptr = B[p].csc_tile_ptr;
+        P.B_crow = B[p].csc_tile_rowidx;
+        P.B_cpos = B[p].csc_tile_pos;
+        P.B_tnnz = B[p].tile_nnz;
+        P.B_Ptr = B[p].tile_csr_Ptr;
+        P.B_Colb = B[p].tile_csr_Col;
+        P.B_Val = B[p].tile_csr_Value;
+        P.B_mask = B[p].mask;
+        P.tilenB = B[p].tilen;
+        P.C_ptr = (int *)take(((size_t)A[p].tilem + 1) * 4);
+        P.C_col = (int *)take((size_t)h.capT * 4);
+        P.C_row = (int *)take((size_t)h.capT * 4);
+        P.C_tnnz = (int *)take(((size_t)h.capT + 1) * 4);
+        P.C_mask = (unsigned short *)take((size_t)h.capT * 32);
+        P.C_Ptr = (unsigned char *)take((size_t)h.capT * 16);
+        P.C_Colb = (unsigned char *)take((size_t)h.capN);
+        P.C_Val = (double *)take((size_t)h.capN * 8);
+        P.numC = 0;
+    }
+    if ((st = tsg_alloc(ctx, &b->d_prod, (size_t)count)) != TSG_OK || (st = tsg_alloc(ctx, &b->d_rowoff, (size_t)count + 1)) ||
+        (st = tsg_alloc(ctx, &b->d_itemoff, (size_t)count + 1)) || (st = tsg_alloc(ctx, &b->d_bar, 2)) ||
+        (st = tsg_alloc(ctx, &b->d_err, 1)) || (st = tsg_alloc(ctx, &b->d_bins, 4)))
+    {
+        tsg_batch_destroy(b);
+        return st;
+    }
+    cudaStream_t s = ctx->stream;
+    cudaMemcpyAsync(b->d_prod, b->host.data(), sizeof(BatchProd) * count, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(b->d_rowoff, b->rowoff.data(), sizeof(long long) * (count + 1), cudaMemcpyHostToDevice, s);
+    cudaMemsetAsync(b->d_bar, 0, 2 * sizeof(unsigned), s);
+    cudaMemsetAsync(b->d_err, 0, sizeof(int), s);
+    // co-resident grid
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    {
+        tsg_batch_destroy(b);
+        return tsg_set_error(TSG_ERR_CUDA, "cannot reserve %zu bytes of shared memory", smem);
+    }
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, BATCH_THREADS, smem);
+    if (per_sm < 1)
+    {
+        tsg_batch_destroy(b);
+        return tsg_set_error(TSG_ERR_CUDA, "batch kernel cannot be resident");
+    }
+    b->grid = per_sm * ctx->num_sms;
+    b->block = BATCH_THREADS;
+    b->smem = smem;
+    b->graph_ok = 0;
+    if (prm.use_graph)
+    {
+        cudaStream_t cs;
+        if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) == cudaSuccess)
+        {
+            cudaStreamSynchronize(s);
+            if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) == cudaSuccess)
+            {
+                int rs = record_run(b, cs);
+                cudaGraph_t g = nullptr;
+                cudaError_t e = cudaStreamEndCapture(cs, &g);
+                if (rs == TSG_OK && e == cudaSuccess && g &&
+                    cudaGraphInstantiate(&b->exec, g, 0) == cudaSuccess)
+                {
+                    b->graph = g;
+                    b->graph_ok = 1;
+                }
+                else if (g)
+                    cudaGraphDestroy(g);
+            }
+            cudaGetLastError(); // a failed capture falls back to direct launches
+            cudaStreamDestroy(cs);
+        }
+    }
+    TSG_CUDA(cudaStreamSynchronize(s));
+    *out = b;
+    return TSG_OK;
+}
+
+extern "C" int tsg_batch_run(tsg_batch *b)
+{
+    if (!b)
+        return tsg_set_error(TSG_ERR_INVALID, "null batch");
+    tsg_context *ctx = b->ctx;
+    if (b->graph_ok)
+        TSG_CUDA(cudaGraphLaunch(b->exec, ctx->stream));
+    else
+        TSG_TRY(record_run(b, ctx->stream));
+    ctx->launches++;
+    b->launches++;
+    return TSG_OK;
+}
+
+extern "C" int tsg_batch_sync(tsg_batch *b, long long *total_tiles, long long *total_nnz)
+{
+    if (!b)
+        return tsg_set_error(TSG_ERR_INVALID, "null batch");
+    tsg_context *ctx = b->ctx;
+    int err = 0;
+    TSG_CUDA(cudaMemcpyAsync(b->host.data(), b->d_prod, sizeof(BatchProd) * b->count, cudaMemcpyDeviceToHost,
+                             ctx->stream));
+    TSG_CUDA(cudaMemcpyAsync(&err, b->d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    TSG_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (err)
+        return tsg_set_error(TSG_ERR_TIMEOUT, "batch grid barrier gave up waiting");
+    long long tt = 0, tn = 0;
+    for (int p = 0; p < b->count; p++)
+    {
+        if (b->host[p].status)
+            return tsg_set_error(TSG_ERR_OVERFLOW, "product %d exceeded its bound (%d)", p, b->host[p].status);
+        tt += b->host[p].numC;
+        tn += b->host[p].nnzC;
+    }
+    if (total_tiles)
+        *total_tiles = tt;
+    if (total_nnz)
+        *total_nnz = tn;
+    return TSG_OK;
+}
+
+extern "C" int tsg_batch_product(tsg_batch *b, int p, tsg_tiled *C)
+{
+    if (!b || !C || p < 0 || p >= b->count)
+        return tsg_set_error(TSG_ERR_INVALID, "bad batch product index");
+    const BatchProd &h = b->host[p];
+    memset(C, 0, sizeof(*C));
+    C->m = b->m[p];
+    C->n = b->n[p];
+    C->tilem = h.tilemA;
+    C->tilen = b->tilen[p];
+    C->numtile = h.numC;
+    C->nnz = h.nnzC;
+    C->tile_ptr = h.P.C_ptr;
+    C->tile_columnidx = h.P.C_col;
+    C->tile_rowidx = h.P.C_row;
+    C->tile_nnz = h.P.C_tnnz;
+    C->mask = h.P.C_mask;
+    C->tile_csr_Ptr = h.P.C_Ptr;
+    C->tile_csr_Col = h.P.C_Colb;
+    C->tile_csr_Value = h.P.C_Val;
+    C->_alloc = (void *)b; // borrowed view into the batch arena
+    return TSG_OK;
+}
+
+extern "C" int tsg_batch_info(tsg_batch *b, int *graph, int *grid, size_t *arena_bytes, long long *launches)
+{
+    if (!b)
+        return tsg_set_error(TSG_ERR_INVALID, "null batch");
+    if (graph)
+        *graph = b->graph_ok;
+    if (grid)
+        *grid = b->grid;
+    if (arena_bytes)
+        *arena_bytes = b->arena_bytes;
+    if (launches)
+        *launches = b->launches;
+    return TSG_OK;
+}
+
+extern "C" int tsg_batch_destroy(tsg_batch *b)
+{
+    if (!b)
+        return TSG_OK;
+    tsg_context *ctx = b->ctx;
+    cudaStreamSynchronize(ctx->stream);
+    if (b->graph_ok)
+    {
+        cudaGraphExecDestroy(b->exec);
+        cudaGraphDestroy(b->graph);
+    }
+    tsg_release(ctx, b->d_prod);
+    tsg_release(ctx, b->d_rowoff);
+    tsg_release(ctx, b->d_itemoff);
+    tsg_release(ctx, b->d_bar);
+    tsg_release(ctx, b->d_err);
+    tsg_release(ctx, b->d_bins);
+    char *a = (char *)b->arena;
+    tsg_release(ctx, a);
+    cudaStreamSynchronize(ctx->stream);
+    delete b;
+    return TSG_OK;
+}

@@ -1,0 +1,511 @@
+// Device-side building blocks of the tiled SpGEMM, shared by the
+// one-product kernels (tsg_spgemm.cu) and the batched persistent kernel
+// (tsg_batch.cu), so both compute with identical code and order.
+//
+// Restates the three steps of the reference's tilespgemm()
+// (src/tilespgemm-cuda.h:2610-3221): step 1 tile structure of C (:257-369),
+// step 2 per-tile bitmask symbolic (:371-755), step 3 numeric (:1505-2608).
+// Every C entry is accumulated as 0.0 + p1 + p2 + ... in k-ascending, then
+// A-entry order with separately rounded multiply and add: the order and
+// rounding of the reference's CPU oracle (src/spgemm-cpu.h:330), so the
+// results are bit-identical to it and deterministic -- no FP64 atomics.
+#pragma once
+
+#include <limits.h>
+
+#include "tsg_internal.h"
+
+#define TSG_FULL_MASK 0xffffffffu
+#define TSG_HW_MASK(tid) (0xFFFFu << ((tid) & 16))
+
+// Pointers of one product C = A*B.  A: row-major tiles; B: row-major tiles
+// plus the column view; C: outputs.
+struct ProdView
+{
+    const int *A_ptr, *A_col, *A_tnnz;
+    const unsigned char *A_Ptr, *A_Colb;
+    const double *A_Val;
+    const unsigned short *A_mask;
+    int tilemA;
+    const int *B_ptr, *B_col, *B_cptr, *B_crow, *B_cpos, *B_tnnz;
+    const unsigned char *B_Ptr, *B_Colb;
+    const double *B_Val;
+    const unsigned short *B_mask;
+    int tilenB;
+    int *C_ptr, *C_col, *C_row, *C_tnnz;
+    unsigned short *C_mask;
+    unsigned char *C_Ptr, *C_Colb;
+    double *C_Val;
+    int numC;
+};
+
+// ---------------------------------------------------------------------------
+// Step 1 (warp per A tile row): the tile-column lists of the B tile rows the
+// A tile row touches are ORed into a shared-memory bitmap restricted to the
+// row's column window (S1_WORDS words per pass); popcount gives the count,
+// an ordered bit walk emits the sorted C tile columns.
+// ---------------------------------------------------------------------------
+#define S1_WORDS 1024
+
+template <bool EMIT>
+__device__ __forceinline__ int step1_row(const ProdView &P, int i, unsigned int *bm, int lane,
+                                         unsigned long long *pairs)
+{
+    const int a0 = P.A_ptr[i], a1 = P.A_ptr[i + 1];
+    int lo = INT_MAX, hi = -1;
+    unsigned long long np = 0;
+    for (int pa = a0 + lane; pa < a1; pa += 32)
+    {
+        const int k = P.A_col[pa];
+        const int b0 = P.B_ptr[k], b1 = P.B_ptr[k + 1];
+        if (b1 > b0)
+        {
+            lo = min(lo, P.B_col[b0]);
+            hi = max(hi, P.B_col[b1 - 1]);
+            np += (unsigned long long)(b1 - b0);
+        }
+    }
+    lo = __reduce_min_sync(TSG_FULL_MASK, lo);
+    hi = __reduce_max_sync(TSG_FULL_MASK, hi);
+    if (!EMIT && pairs)
+    {
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1)
+            np += __shfl_xor_sync(TSG_FULL_MASK, np, d);
+        if (lane == 0 && np)
+            atomicAdd(pairs, np);
+    }
+    int out = 0;
+    const int cbase = EMIT ? P.C_ptr[i] : 0;
+    if (hi >= 0)
+    {
+        for (int c0 = lo & ~31; c0 <= hi; c0 += S1_WORDS * 32)
+        {
+            const int c1 = min(hi + 1, c0 + S1_WORDS * 32);
+            const int nw = (c1 - c0 + 31) >> 5;
+            for (int w = lane; w < nw; w += 32)
+                bm[w] = 0;
+            __syncwarp();
+            for (int pa = a0; pa < a1; pa++)
+            {
+                const int k = P.A_col[pa];
+                const int b0 = P.B_ptr[k], b1 = P.B_ptr[k + 1];
+                for (int pb = b0 + lane; pb < b1; pb += 32)
+                {
+                    const int j = P.B_col[pb];
+                    if (j >= c0 && j < c1)
+                        atomicOr(&bm[(j - c0) >> 5], 1u << ((j - c0) & 31));
+                }
+            }
+            __syncwarp();
+            for (int wb = 0; wb < nw; wb += 32)
+            {
+                const int w = wb + lane;
+                unsigned bits = w < nw ? bm[w] : 0u;
+                const int cnt = __popc(bits);
+                if (EMIT)
+                {
+                    int incl = cnt;
+#pragma unroll
+                    for (int d = 1; d < 32; d <<= 1)
+                    {
+                        const int o = __shfl_up_sync(TSG_FULL_MASK, incl, d);
+                        if (lane >= d)
+                            incl += o;
+                    }
+                    int pos = cbase + out + incl - cnt;
+                    while (bits)
+                    {
+                        const int b = __ffs(bits) - 1;
+                        bits &= bits - 1;
+                        P.C_col[pos] = c0 + (w << 5) + b;
+                        P.C_row[pos] = i;
+                        pos++;
+                    }
+                    out += __shfl_sync(TSG_FULL_MASK, incl, 31);
+                }
+                else
+                {
+                    out += __reduce_add_sync(TSG_FULL_MASK, cnt);
+                }
+            }
+            __syncwarp();
+        }
+    }
+    return out;
+}
+
+// ---------------------------------------------------------------------------
+// Helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int lower_bound_int(const int *__restrict__ a, int n, int key)
+{
+    int lo = 0;
+    while (n > 0)
+    {
+        const int h = n >> 1;
+        if (a[lo + h] < key)
+        {
+            lo += h + 1;
+            n -= h + 1;
+        }
+        else
+            n = h;
+    }
+    return lo;
+}
+
+// Row r of a 16x16 boolean tile product: OR of B's row masks c for every
+// column c set in A's row mask (bit 15-c).  q0/q1 hold B's 16 row masks
+// (rows 2w and 2w+1 in the low and high halves of word w).
+__device__ __forceinline__ unsigned bool_row(unsigned ma, uint4 q0, uint4 q1)
+{
+    unsigned r = 0;
+    const unsigned w[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
+#pragma unroll
+    for (int c = 0; c < 16; c++)
+    {
+        const unsigned row = (c & 1) ? (w[c >> 1] >> 16) : (w[c >> 1] & 0xFFFFu);
+        r |= ((ma >> (15 - c)) & 1u) ? row : 0u;
+    }
+    return r;
+}
+
+// Exclusive half-warp scan of cnt; returns the exclusive value, total via ref.
+__device__ __forceinline__ int hw_excl_scan(unsigned hmask, int lane, int cnt, int &total)
+{
+    int incl = cnt;
+#pragma unroll
+    for (int d = 1; d < 16; d <<= 1)
+    {
+        const int o = __shfl_up_sync(hmask, incl, d, 16);
+        if (lane >= d)
+            incl += o;
+    }
+    total = __shfl_sync(hmask, incl, 15, 16);
+    return incl - cnt;
+}
+
+__device__ __forceinline__ int nnz_bin(int total)
+{
+    return total <= 32 ? 0 : total <= 224 ? 1 : total < 256 ? 2 : 3;
+}
+
+// Writes row r's mask, offset and (lane 0) the tile count / bin of tile t.
+__device__ __forceinline__ void step2_store(const ProdView &P, long long t, unsigned hmask, int lane, unsigned acc,
+                                            int *s_bins)
+{
+    int total;
+    const int excl = hw_excl_scan(hmask, lane, __popc(acc), total);
+    P.C_mask[t * TSG_BS + lane] = (unsigned short)acc;
+    P.C_Ptr[t * TSG_BS + lane] = (unsigned char)excl;
+    if (lane == 0)
+    {
+        P.C_tnnz[t] = total;
+        if (total > 0 && s_bins)
+            atomicAdd(&s_bins[nnz_bin(total)], 1);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Tile schedule: half-warp per C tile, A's tile row intersected with B's tile
+// column 16 elements at a time, the chunks held in lanes' registers (shuffle
+// binary search + ballot); f(posA, posB) is called for every matched k in
+// ascending order, uniformly across the half-warp.
+// ---------------------------------------------------------------------------
+template <typename F>
+__device__ __forceinline__ void intersect_tiles(unsigned hmask, int lane, const int *__restrict__ a_list,
+                                                int abase, int la, const int *__restrict__ b_list,
+                                                const int *__restrict__ b_pos, int bbase, int lb, F f)
+{
+    int ia = 0, ib = 0;
+    while (ia < la && ib < lb)
+    {
+        const int va = ia + lane < la ? a_list[abase + ia + lane] : INT_MAX;
+        const int vb = ib + lane < lb ? b_list[bbase + ib + lane] : INT_MAX;
+        int pos = 0;
+#pragma unroll
+        for (int s = 8; s >= 1; s >>= 1)
+        {
+            const int v = __shfl_sync(hmask, vb, pos + s - 1, 16);
+            if (v < va)
+                pos += s;
+        }
+        const int cand = __shfl_sync(hmask, vb, pos, 16);
+        const bool found = (cand == va) && (va != INT_MAX);
+        unsigned bal = __ballot_sync(hmask, found);
+        bal = (bal >> (threadIdx.x & 16)) & 0xFFFFu;
+        while (bal)
+        {
+            const int x = __ffs(bal) - 1;
+            bal &= bal - 1;
+            const int y = __shfl_sync(hmask, pos, x, 16);
+            const int q = bbase + ib + y;
+            const int posB = b_pos ? b_pos[q] : q;
+            f(abase + ia + x, posB);
+        }
+        const int amax = __shfl_sync(hmask, va, 15, 16);
+        const int bmax = __shfl_sync(hmask, vb, 15, 16);
+        if (amax <= bmax)
+            ia += 16;
+        if (bmax <= amax)
+            ib += 16;
+    }
+}
+
+__device__ __forceinline__ void step2_tile(const ProdView &P, int t, unsigned hmask, int lane, int *s_bins)
+{
+    const int i = P.C_row[t], j = P.C_col[t];
+    const int abase = P.A_ptr[i], la = P.A_ptr[i + 1] - abase;
+    const int bbase = P.B_cptr[j], lb = P.B_cptr[j + 1] - bbase;
+    unsigned acc = 0;
+    intersect_tiles(hmask, lane, P.A_col, abase, la, P.B_crow, P.B_cpos, bbase, lb, [&](int posA, int posB) {
+        const unsigned ma = P.A_mask[(long long)posA * TSG_BS + lane];
+        const uint4 *mb = reinterpret_cast<const uint4 *>(P.B_mask + (long long)posB * TSG_BS);
+        const uint4 q0 = __ldg(mb), q1 = __ldg(mb + 1);
+        acc |= bool_row(ma, q0, q1);
+    });
+    step2_store(P, t, hmask, lane, acc, s_bins);
+}
+
+#define S3T_STRIDE 17
+
+// acc: 16 x S3T_STRIDE doubles of this half-warp, all zero on entry and on exit
+__device__ __forceinline__ void step3_tile(const ProdView &P, int t, unsigned hmask, int lane, double *acc)
+{
+    const int cb = P.C_tnnz[t], cn = P.C_tnnz[t + 1] - cb;
+    if (cn == 0)
+        return;
+    const int i = P.C_row[t], j = P.C_col[t];
+    const int abase = P.A_ptr[i], la = P.A_ptr[i + 1] - abase;
+    const int bbase = P.B_cptr[j], lb = P.B_cptr[j + 1] - bbase;
+    double *myrow = acc + lane * S3T_STRIDE;
+    intersect_tiles(hmask, lane, P.A_col, abase, la, P.B_crow, P.B_cpos, bbase, lb, [&](int posA, int posB) {
+        const int a0 = P.A_tnnz[posA], na = P.A_tnnz[posA + 1] - a0;
+        const int sa = P.A_Ptr[(long long)posA * TSG_BS + lane];
+        const int ea = lane == TSG_BS - 1 ? na : P.A_Ptr[(long long)posA * TSG_BS + lane + 1];
+        const int b0 = P.B_tnnz[posB], nb = P.B_tnnz[posB + 1] - b0;
+        const unsigned char *bp = P.B_Ptr + (long long)posB * TSG_BS;
+        for (int x = sa; x < ea; x++)
+        {
+            const int ca = P.A_Colb[a0 + x] & 15;
+            const double a = P.A_Val[a0 + x];
+            const int sb = bp[ca];
+            const int eb = ca == TSG_BS - 1 ? nb : bp[ca + 1];
+            for (int y = sb; y < eb; y++)
+            {
+                const int c = P.B_Colb[b0 + y] & 15;
+                myrow[c] = __dadd_rn(myrow[c], __dmul_rn(a, P.B_Val[b0 + y]));
+            }
+        }
+    });
+    __syncwarp(hmask);
+    const int excl = P.C_Ptr[(long long)t * TSG_BS + lane];
+    const unsigned mrev = __brev((unsigned)P.C_mask[(long long)t * TSG_BS + lane]) >> 16;
+    // every lane runs the same trip count so the shuffles see all 16 lanes
+    for (int pb = 0; pb < cn; pb += 16)
+    {
+        const int p = pb + lane;
+        int r = 0;
+#pragma unroll
+        for (int s = 8; s >= 1; s >>= 1)
+        {
+            const int v = __shfl_sync(hmask, excl, r + s, 16);
+            if (v <= p)
+                r += s;
+        }
+        const unsigned mr = __shfl_sync(hmask, mrev, r, 16);
+        const int rank = p - __shfl_sync(hmask, excl, r, 16);
+        if (p < cn)
+        {
+            const int c = (int)__fns(mr, 0, rank + 1) & 15;
+            double *cell = acc + r * S3T_STRIDE + c;
+            P.C_Colb[cb + p] = (unsigned char)c;
+            P.C_Val[cb + p] = *cell;
+            *cell = 0.0;
+        }
+    }
+    __syncwarp(hmask);
+}
+
+// ---------------------------------------------------------------------------
+// Row-segment schedule (tile-level Gustavson).  A work item is W consecutive
+// C tiles (global order), cut at tile-row boundaries into segments.  For a
+// segment of C tile row i the half-warp walks A's tile row i in k order and,
+// for each A tile (i,k), the tiles of B's tile row k whose columns fall in
+// the segment's range (binary search for the first, then a merge against the
+// segment's sorted C columns): every (A tile, B tile) pair is visited once
+// and no intersection is searched.  Lane r owns row r of every C tile of the
+// segment.
+// ---------------------------------------------------------------------------
+template <int W>
+struct S2RowsSmem
+{
+    unsigned m[W][16];
+    int col[W];
+};
+
+template <int W>
+__device__ __forceinline__ void step2_rows_item(const ProdView &P, long long item, unsigned hmask, int lane,
+                                                S2RowsSmem<W> &sm, int *s_bins)
+{
+    const long long tb = item * W;
+    if (tb >= P.numC)
+        return;
+    const int t_end = (int)min((long long)P.numC, tb + W);
+    int t = (int)tb;
+    while (t < t_end)
+    {
+        const int i = P.C_row[t];
+        const int seg_end = min(t_end, P.C_ptr[i + 1]);
+        const int n = seg_end - t;
+        for (int jl = lane; jl < n; jl += 16)
+            sm.col[jl] = P.C_col[t + jl];
+        for (int jl = 0; jl < n; jl++)
+            sm.m[jl][lane] = 0u;
+        __syncwarp(hmask);
+        const int jlo = sm.col[0], jhi = sm.col[n - 1];
+        for (int pa = P.A_ptr[i]; pa < P.A_ptr[i + 1]; pa++)
+        {
+            const int k = P.A_col[pa];
+            const unsigned ma = P.A_mask[(long long)pa * TSG_BS + lane];
+            const int b0 = P.B_ptr[k], b1 = P.B_ptr[k + 1];
+            int jl = 0;
+            for (int pb = b0 + lower_bound_int(P.B_col + b0, b1 - b0, jlo); pb < b1; pb++)
+            {
+                const int j = P.B_col[pb];
+                if (j > jhi)
+                    break;
+                while (jl < n - 1 && sm.col[jl] != j)
+                    jl++;
+                const uint4 *mb = reinterpret_cast<const uint4 *>(P.B_mask + (long long)pb * TSG_BS);
+                const uint4 q0 = __ldg(mb), q1 = __ldg(mb + 1);
+                if (ma)
+                    sm.m[jl][lane] |= bool_row(ma, q0, q1);
+            }
+        }
+        __syncwarp(hmask);
+        for (int jl = 0; jl < n; jl++)
+            step2_store(P, t + jl, hmask, lane, sm.m[jl][lane], s_bins);
+        __syncwarp(hmask);
+        t = seg_end;
+    }
+}
+
+// Per half-warp shared memory of the numeric row-segment step.
+template <int W, int CAP>
+struct S3RowsSmem
+{
+    double acc[CAP];
+    unsigned bm[W * 16]; // (first slot of the row in the sub-chunk << 16) | row mask
+    int col[W];
+};
+
+// Accumulates a*b into a compact FP64 buffer holding exactly the sub-chunk's
+// nonzeros (slot = tile offset + row offset + popcount of the row mask left
+// of the column); B rows are walked through their 16-bit masks (no column
+// byte loads); the buffer is written out with contiguous stores.  A segment
+// with more than CAP nonzeros is processed in tile sub-chunks.
+template <int W, int CAP>
+__device__ __forceinline__ void step3_rows_item(const ProdView &P, long long item, unsigned hmask, int lane,
+                                                S3RowsSmem<W, CAP> &sm)
+{
+    const long long tb = item * W;
+    if (tb >= P.numC)
+        return;
+    const int t_end = (int)min((long long)P.numC, tb + W);
+    int t = (int)tb;
+    while (t < t_end)
+    {
+        const int i = P.C_row[t];
+        const int seg_end = min(t_end, P.C_ptr[i + 1]);
+        int s = t;
+        while (s < seg_end)
+        {
+            const int base0 = P.C_tnnz[s];
+            int e = s + 1;
+            while (e < seg_end && P.C_tnnz[e + 1] - base0 <= CAP)
+                e++;
+            const int n = e - s, cn = P.C_tnnz[e] - base0;
+            for (int jl = lane; jl < n; jl += 16)
+                sm.col[jl] = P.C_col[s + jl];
+            for (int jl = 0; jl < n; jl++)
+            {
+                const long long tt = (long long)(s + jl) * TSG_BS + lane;
+                const unsigned b = (unsigned)(P.C_tnnz[s + jl] - base0 + P.C_Ptr[tt]);
+                sm.bm[jl * 16 + lane] = (b << 16) | P.C_mask[tt];
+            }
+            for (int q = lane; q < cn; q += 16)
+                sm.acc[q] = 0.0;
+            __syncwarp(hmask);
+            const int jlo = sm.col[0], jhi = sm.col[n - 1];
+            for (int pa = P.A_ptr[i]; pa < P.A_ptr[i + 1]; pa++)
+            {
+                const int k = P.A_col[pa];
+                const int b0 = P.B_ptr[k], b1 = P.B_ptr[k + 1];
+                const int pb0 = b0 + lower_bound_int(P.B_col + b0, b1 - b0, jlo);
+                const int a0 = P.A_tnnz[pa];
+                const int xa0 = a0 + P.A_Ptr[(long long)pa * TSG_BS + lane];
+                const int xa1 = a0 + (lane == TSG_BS - 1 ? P.A_tnnz[pa + 1] - a0
+                                                          : P.A_Ptr[(long long)pa * TSG_BS + lane + 1]);
+                if (xa0 >= xa1)
+                    continue;
+                int jl = 0;
+                for (int pb = pb0; pb < b1; pb++)
+                {
+                    const int j = P.B_col[pb];
+                    if (j > jhi)
+                        break;
+                    while (jl < n - 1 && sm.col[jl] != j)
+                        jl++;
+                    const unsigned bm = sm.bm[jl * 16 + lane];
+                    const int rb = (int)(bm >> 16);
+                    const unsigned mk = bm & 0xFFFFu;
+                    const double *bv = P.B_Val + P.B_tnnz[pb];
+                    const unsigned short *bmask = P.B_mask + (long long)pb * TSG_BS;
+                    const unsigned char *bp = P.B_Ptr + (long long)pb * TSG_BS;
+                    for (int x = xa0; x < xa1; x++)
+                    {
+                        const int ca = P.A_Colb[x] & 15;
+                        unsigned mb = bmask[ca];
+                        if (!mb)
+                            continue;
+                        const double a = P.A_Val[x];
+                        int y = bp[ca];
+                        do // B row ca's columns, ascending (highest mask bit first)
+                        {
+                            const int bit = 31 - __clz(mb);
+                            const int slot = rb + __popc(mk >> (bit + 1));
+                            if (slot < CAP)
+                                sm.acc[slot] = __dadd_rn(sm.acc[slot], __dmul_rn(a, bv[y]));
+                            y++;
+                            mb ^= 1u << bit;
+                        } while (mb);
+                    }
+                }
+            }
+            __syncwarp(hmask);
+            for (int q = lane; q < cn; q += 16)
+                P.C_Val[base0 + q] = sm.acc[q];
+            for (int jl = 0; jl < n; jl++)
+            {
+                const unsigned bm = sm.bm[jl * 16 + lane];
+                unsigned mk = bm & 0xFFFFu;
+                int p = base0 + (int)(bm >> 16);
+                while (mk)
+                {
+                    const int bit = 31 - __clz(mk);
+                    P.C_Colb[p++] = (unsigned char)(15 - bit);
+                    mk ^= 1u << bit;
+                }
+            }
+            __syncwarp(hmask);
+            s = e;
+        }
+        t = seg_end;
+    }
+}
+
+// Supported (W, CAP) pairs of the row schedule; the dispatch macro expands
+// X(W, CAP) for each.
+#define TSG_ROW_CONFIGS(X) X(8, 256) X(8, 512) X(8, 1024) X(16, 512) X(16, 1024) X(16, 2048) X(32, 1024) X(32, 2048)

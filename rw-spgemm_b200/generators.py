@@ -86,18 +86,18 @@ def rmat(scale: int, edge_factor: int, a=0.57, b=0.19, c=0.19, seed: int = 1,
 
 
 def banded(n: int, half_bandwidth: int, seed: int = 0, low=-1.0, high=1.0):
-    """Full band |i-j| <= half_bandwidth, values uniform(low, high)."""
-    rows, cols = [], []
-    idx = np.arange(n, dtype=np.int64)
-    for d in range(-half_bandwidth, half_bandwidth + 1):
-        ok = (idx + d >= 0) & (idx + d < n)
-        rows.append(idx[ok])
-        cols.append(idx[ok] + d)
-    rows = np.concatenate(rows)
-    cols = np.concatenate(cols)
-    m, n_, rp, ci, _ = _coo_to_csr(n, n, rows, cols, np.zeros(rows.size))
+    """Full band |i-j| <= half_bandwidth, values uniform(low, high); built
+    directly in CSR order."""
+    i = np.arange(n, dtype=np.int64)
+    start = np.maximum(i - half_bandwidth, 0)
+    stop = np.minimum(i + half_bandwidth, n - 1)
+    lens = stop - start + 1
+    rp = np.zeros(n + 1, dtype=np.int64)
+    np.cumsum(lens, out=rp[1:])
+    pos = np.arange(int(rp[-1]), dtype=np.int64)
+    ci = (np.repeat(start - rp[:-1], lens) + pos).astype(np.int32)
     rng = np.random.default_rng(seed)
-    return m, n_, rp, ci, rng.uniform(low, high, ci.size)
+    return n, n, rp.astype(np.int32), ci, rng.uniform(low, high, ci.size)
 
 
 def random_poisson(m: int, n: int | None = None, lam: float = 8.0, seed: int = 0, low=-1.0, high=1.0):
@@ -145,3 +145,24 @@ def products(matA, matB) -> int:
     _, _, _, ci, _ = matA
     _, _, rpB, _, _ = matB
     return int(np.diff(rpB.astype(np.int64))[ci].sum())
+
+
+def batched_products(count: int = 512, seed: int = 0, n_min: int = 1024, n_max: int = 65536,
+                     hb_min: int = 8, hb_max: int = 64, lam: float = 8.0):
+    """Independent square products C_i = A_i * B_i: n_i log-uniform in
+    [n_min, n_max]; each of A_i, B_i banded (half-bandwidth uniform in
+    [hb_min, hb_max]) or random with Poisson(lam) nonzeros per row; values
+    uniform(-1, 1); a fixed seed per product."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        n = int(round(np.exp(rng.uniform(np.log(n_min), np.log(n_max)))))
+        mats = []
+        for side in range(2):
+            s = int(rng.integers(0, 2**31 - 1))
+            if rng.random() < 0.5:
+                mats.append(banded(n, int(rng.integers(hb_min, hb_max + 1)), seed=s))
+            else:
+                mats.append(random_poisson(n, None, lam, seed=s))
+        out.append((mats[0], mats[1]))
+    return out

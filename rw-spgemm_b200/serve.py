@@ -1,0 +1,278 @@
+"""Serving layer: a continuous-batching request loop over the batched engine.
+
+Jobs (C = A*B or C = A*A^T over registered matrices) arrive at any time.  A
+dispatcher thread
+  * keeps every operand resident on the device as tiles (one tiled copy per
+    matrix serves both the A and B roles; A^T is registered on first use) in
+    an LRU cache,
+  * admits queued jobs in arrival order while the device memory in use --
+    resident operands + result arenas of batches in flight + the new job's
+    predicted bytes -- stays under the cap; the prediction comes from the
+    job's step-1/step-2 bounds on the device (matched tile pairs, scalar
+    products),
+  * packs admitted jobs into a batch (tsg_batch: one persistent,
+    graph-captured launch) on a free stream slot while earlier batches are
+    still running on the other slots, so their work overlaps on the GPU,
+  * when a batch finishes, copies each result to host CSR and completes the
+    job's future with its latency (submit -> result on the host).
+Results are bit-identical whether a job runs alone or inside any mix: each
+output entry is accumulated in a fixed order independent of batching.
+"""
+from __future__ import annotations
+
+import collections
+import threading
+import time
+from concurrent.futures import Future
+
+import numpy as np
+
+from . import (TSG_TILED_CSC_VIEW, Batch, Context, csr_host_to_tiled, lib, product_bounds, tiled_to_csr_host)
+
+
+class Job:
+    __slots__ = ("jid", "kind", "a_key", "b_key", "t_submit", "t_done", "future", "pred_bytes", "result_nnz")
+
+    def __init__(self, jid, kind, a_key, b_key):
+        self.jid, self.kind, self.a_key, self.b_key = jid, kind, a_key, b_key
+        self.t_submit = time.perf_counter()
+        self.t_done = None
+        self.future = Future()
+        self.pred_bytes = 0
+        self.result_nnz = 0
+
+
+def _transpose(mat):
+    m, n, rp, ci, v = mat
+    rows = np.repeat(np.arange(m, dtype=np.int64), np.diff(rp))
+    order = np.lexsort((rows, ci))
+    rp_t = np.zeros(n + 1, dtype=np.int64)
+    np.add.at(rp_t, ci.astype(np.int64) + 1, 1)
+    return n, m, np.cumsum(rp_t).astype(np.int32), rows[order].astype(np.int32), np.asarray(v)[order]
+
+
+class OperandCache:
+    """Device-resident tiled operands (row tiles + column view), LRU."""
+
+    def __init__(self, ctx: Context):
+        self.ctx = ctx
+        self.tiles = collections.OrderedDict()
+        self.bytes = 0
+        self.hits = 0
+        self.misses = 0
+
+    @staticmethod
+    def tiled_bytes(t):
+        s = t.s
+        return (s.tilem + 1) * 4 + s.numtile * (4 + 4 + 4 + 16 + 32 + 8) + s.nnz * 9 + (s.tilen + 1) * 4
+
+    def get(self, key, host_mat):
+        if key in self.tiles:
+            self.tiles.move_to_end(key)
+            self.hits += 1
+            return self.tiles[key]
+        self.misses += 1
+        t = csr_host_to_tiled(self.ctx, host_mat, TSG_TILED_CSC_VIEW)
+        self.tiles[key] = t
+        self.bytes += self.tiled_bytes(t)
+        return t
+
+    def evict_until(self, limit, pinned_keys):
+        for key in list(self.tiles.keys()):
+            if self.bytes <= limit:
+                break
+            if key in pinned_keys:
+                continue
+            t = self.tiles.pop(key)
+            self.bytes -= self.tiled_bytes(t)
+            t.free()
+
+
+class _Slot:
+    """One in-flight batch position with its own stream."""
+
+    def __init__(self, device):
+        self.ctx = Context(device, own_stream=True)
+        self.batch = None
+        self.jobs = []
+        self.arena = 0
+        self.t_launch = 0.0
+
+    def idle_stream(self) -> bool:
+        return lib().tsg_context_query(self.ctx.handle) == 0
+
+
+class SpGEMMServer:
+    """Continuous-batching SpGEMM server on one GPU.
+
+    mem_cap   bytes of device memory the server may hold (operands + arenas)
+    slots     batches that may be in flight at once (one stream each)
+    max_batch jobs per batch
+    schedule  (schedule, seg_tiles, acc_cap) of the batched kernel, e.g. the
+              autotuner's choice
+    """
+
+    def __init__(self, device=0, mem_cap=40 << 30, slots=2, max_batch=64, schedule=("rows", 16, 1024)):
+        self.device = device
+        self.mem_cap = int(mem_cap)
+        self.max_batch = max_batch
+        self.schedule = schedule
+        self.matrices = {}
+        self.slots = [_Slot(device) for _ in range(slots)]
+        self.stage_ctx = Context(device, own_stream=True)  # operand staging and bounds
+        self.cache = OperandCache(self.stage_ctx)
+        self.queue = collections.deque()
+        self.lock = threading.Condition()
+        self.running = False
+        self.thread = None
+        self.next_id = 0
+        self.done = []
+        self.batches = 0
+        self.rejected = 0
+
+    # -- registration / submission -------------------------------------------
+    def register(self, key, mat):
+        self.matrices[key] = mat
+
+    def submit(self, kind, a_key, b_key=None) -> Future:
+        if kind not in ("AB", "AAT"):
+            raise ValueError(kind)
+        if kind == "AAT":
+            tkey = (a_key, "T")
+            if tkey not in self.matrices:
+                self.matrices[tkey] = _transpose(self.matrices[a_key])
+            b_key = tkey
+        with self.lock:
+            job = Job(self.next_id, kind, a_key, b_key)
+            self.next_id += 1
+            self.queue.append(job)
+            self.lock.notify()
+        return job.future
+
+    # -- lifecycle ---------------------------------------------------------------
+    def start(self):
+        self.running = True
+        self.thread = threading.Thread(target=self._loop, name="spgemm-dispatch", daemon=True)
+        self.thread.start()
+        return self
+
+    def stop(self, drain=True):
+        if drain:
+            while True:
+                with self.lock:
+                    idle = not self.queue and all(s.batch is None for s in self.slots)
+                if idle:
+                    break
+                time.sleep(0.0005)
+        self.running = False
+        with self.lock:
+            self.lock.notify()
+        if self.thread:
+            self.thread.join()
+        for s in self.slots:
+            if s.batch is not None:
+                s.batch.close()
+            s.ctx.synchronize()
+
+    def close(self):
+        self.stop()
+        for t in self.cache.tiles.values():
+            t.free()
+        self.cache.tiles.clear()
+        for s in self.slots:
+            s.ctx.close()
+        self.stage_ctx.close()
+
+    # -- dispatcher ----------------------------------------------------------------
+    def _in_use(self):
+        return self.cache.bytes + sum(s.arena for s in self.slots if s.batch is not None)
+
+    def _predict(self, A, B):
+        prods, pairs = product_bounds(self.cache.ctx, A, B)
+        tiles = pairs
+        full = A.s.tilem * B.s.tilen
+        tiles = min(tiles, full)
+        vals = min(prods, 256 * tiles)
+        return tiles * (4 * 3 + 4 + 32 + 16) + vals * 9 + (A.s.tilem + 1) * 4
+
+    def _form_batch(self, slot):
+        jobs, pairs, pred = [], [], 0
+        # operands of batches still running must stay resident
+        pinned = {k for s in self.slots if s.batch is not None for j in s.jobs for k in (j.a_key, j.b_key)}
+        while self.queue and len(jobs) < self.max_batch:
+            job = self.queue[0]
+            A = self.cache.get(job.a_key, self.matrices[job.a_key])
+            B = self.cache.get(job.b_key, self.matrices[job.b_key])
+            pinned.update((job.a_key, job.b_key))
+            job.pred_bytes = self._predict(A, B)
+            if job.pred_bytes > self.mem_cap:
+                self.queue.popleft()
+                self.rejected += 1
+                job.future.set_exception(MemoryError(f"job {job.jid} needs {job.pred_bytes} bytes, cap {self.mem_cap}"))
+                continue
+            if self._in_use() + pred + job.pred_bytes > self.mem_cap:
+                self.cache.evict_until(self.mem_cap - pred - job.pred_bytes -
+                                       sum(s.arena for s in self.slots if s.batch is not None), pinned)
+                if self._in_use() + pred + job.pred_bytes > self.mem_cap:
+                    break  # wait for memory to free up (arrival order kept)
+            self.queue.popleft()
+            jobs.append(job)
+            pairs.append((A, B))
+            pred += job.pred_bytes
+        if not jobs:
+            return False
+        sch, seg, cap = self.schedule
+        slot.batch = Batch(slot.ctx, pairs, sch, seg, cap, graph=False)
+        slot.arena = slot.batch.info()["arena_bytes"]
+        slot.jobs = jobs
+        slot.t_launch = time.perf_counter()
+        slot.batch.run()
+        self.batches += 1
+        return True
+
+    def _finish(self, slot):
+        slot.batch.sync()
+        for p, job in enumerate(slot.jobs):
+            C = slot.batch.product(p)
+            res = tiled_to_csr_host(slot.ctx, C, pinned=True)
+            job.t_done = time.perf_counter()
+            job.result_nnz = C.s.nnz
+            job.future.set_result(res)
+            self.done.append(job)
+        slot.batch.close()
+        slot.batch = None
+        slot.jobs = []
+        slot.arena = 0
+
+    def _loop(self):
+        # only this thread consumes the queue (deque appends/pops are atomic)
+        while self.running:
+            progressed = False
+            for slot in self.slots:
+                if slot.batch is not None and slot.idle_stream():
+                    self._finish(slot)
+                    progressed = True
+            for slot in self.slots:
+                if slot.batch is None and self.queue:
+                    progressed |= self._form_batch(slot)
+            if not progressed:
+                with self.lock:
+                    if not self.queue and all(s.batch is None for s in self.slots):
+                        self.lock.wait(timeout=0.002)
+                time.sleep(0.0001)
+
+    # -- statistics ----------------------------------------------------------------
+    def stats(self):
+        lat = np.array([(j.t_done - j.t_submit) * 1e3 for j in self.done]) if self.done else np.zeros(0)
+        t0 = min((j.t_submit for j in self.done), default=0.0)
+        t1 = max((j.t_done for j in self.done), default=0.0)
+        return {
+            "jobs": len(self.done),
+            "jobs_per_s": len(self.done) / (t1 - t0) if t1 > t0 else 0.0,
+            "p50_ms": float(np.percentile(lat, 50)) if lat.size else None,
+            "p99_ms": float(np.percentile(lat, 99)) if lat.size else None,
+            "batches": self.batches,
+            "mean_batch": len(self.done) / self.batches if self.batches else 0.0,
+            "rejected": self.rejected,
+            "operand_cache": {"hits": self.cache.hits, "misses": self.cache.misses, "bytes": self.cache.bytes},
+        }

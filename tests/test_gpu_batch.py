@@ -1,0 +1,82 @@
+"""Batched products in one persistent launch: every product equals the
+oracle (bit for bit) and the one-product path, under both schedules, and
+graph replays reproduce the same bits."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+C_KEYS = ["tile_ptr", "tile_columnidx", "tile_rowidx", "tile_nnz", "tile_csr_Ptr", "tile_csr_Col", "mask",
+          "tile_csr_Value"]
+
+
+def _tiled(tsg, ctx, mat, flags):
+    import torch
+    d = torch.device("cuda", 0)
+    m, n, rp, ci, v = mat
+    t = [torch.from_numpy(np.ascontiguousarray(x)).to(d) for x in (rp.astype(np.int32), ci.astype(np.int32),
+                                                                    v.astype(np.float64))]
+    torch.cuda.synchronize()
+    T = tsg.csr_to_tiled(ctx, m, n, *t, flags)
+    T._keep = t
+    return T
+
+
+def _pairs(gen):
+    rng = np.random.default_rng(5)
+    mats = []
+    for i in range(14):
+        m, k, n = (int(x) for x in rng.integers(1, 400, 3))
+        mats.append((gen.random_poisson(m, k, float(rng.uniform(0.5, 10)), seed=i),
+                     gen.random_poisson(k, n, float(rng.uniform(0.5, 10)), seed=100 + i)))
+    mats.append((gen.banded(300, 40, seed=1), gen.banded(300, 20, seed=2)))   # dense / full tiles
+    mats.append((gen.rmat(10, 8, seed=3), gen.rmat(10, 8, seed=4)))          # hubs
+    mats.append((gen.laplacian_2d(30), gen.laplacian_2d(30)))
+    mats.append(((5, 6, np.zeros(6, np.int32), np.zeros(0, np.int32), np.zeros(0)),
+                 gen.random_poisson(6, 9, 2.0, seed=9)))                    # empty A
+    return mats
+
+
+@pytest.mark.parametrize("cfg", [("rows", 16, 1024), ("rows", 8, 256), ("rows", 32, 2048), ("tiles", 8, 256)])
+def test_batch_matches_oracle_and_single_path(tsg, ctx, oracle, gen, cfg):
+    mats = _pairs(gen)
+    pairs = [(_tiled(tsg, ctx, a, tsg.TSG_TILED_PACKED_COL), _tiled(tsg, ctx, b, tsg.TSG_TILED_CSC_VIEW))
+             for a, b in mats]
+    batch = tsg.Batch(ctx, pairs, *cfg)
+    batch.run()
+    tiles, nnz = batch.sync()
+    first = []
+    for p, (a, b) in enumerate(mats):
+        got = batch.product(p).download()
+        want = oracle.spgemm_tiled(oracle.csr2tile_row_major(a), oracle.csr2tile_col_major(b))
+        for k in C_KEYS:
+            np.testing.assert_array_equal(np.asarray(got[k]).view(np.uint8), np.asarray(want[k]).view(np.uint8),
+                                          err_msg=f"product {p} {k}")
+        first.append(got)
+    assert tiles == sum(f["numtile"] for f in first) and nnz == sum(f["nnz"] for f in first)
+    # replay: same bits
+    batch.run()
+    batch.sync()
+    for p in range(len(mats)):
+        again = batch.product(p).download()
+        for k in C_KEYS:
+            np.testing.assert_array_equal(np.asarray(again[k]).view(np.uint8), np.asarray(first[p][k]).view(np.uint8))
+    info = batch.info()
+    assert info["launches"] == 2 and info["grid"] > 0
+    batch.close()
+
+
+def test_batch_uses_graph(tsg, ctx, gen):
+    mats = _pairs(gen)[:3]
+    pairs = [(_tiled(tsg, ctx, a, 1), _tiled(tsg, ctx, b, 2)) for a, b in mats]
+    batch = tsg.Batch(ctx, pairs)
+    assert batch.info()["graph"], "the persistent launch was not captured in a CUDA graph"
+    batch.close()
+
+
+def test_product_bounds_bound_the_result(tsg, ctx, oracle, gen):
+    for a, b in _pairs(gen)[:6]:
+        A, B = _tiled(tsg, ctx, a, 1), _tiled(tsg, ctx, b, 2)
+        prods, pairs = tsg.product_bounds(ctx, A, B)
+        assert prods == oracle.count_products(a, b)
+        C, info = tsg.spgemm(ctx, A, B)
+        assert info["nnz_C"] <= prods and info["numtile_C"] <= pairs

@@ -81,6 +81,7 @@ def test_conversion_random_and_edges(tsg, gen, oracle):
 # ---------------------------------------------------------------------------
 @pytest.mark.parametrize("name", sorted(CASES))
 def test_dropin_tilespgemm_matches_oracle(tsg, oracle, name):
+    """Drop-in path: host column-major B is converted to the internal layout."""
     z, mat = CASES[name]
     if mat[0] != mat[1]:
         pytest.skip("rectangular")
@@ -119,8 +120,18 @@ def _handle_product(tsg, ctx, matA, matB):
     return A, B, C, info
 
 
+SCHEDULES = [("tiles", 8, 512), ("rows", 8, 256), ("rows", 8, 512), ("rows", 16, 1024), ("rows", 16, 2048)]
+
+
+@pytest.fixture(params=SCHEDULES, ids=lambda p: f"{p[0]}{p[1]}-{p[2]}")
+def sched(request, ctx):
+    ctx.set_schedule(*request.param)
+    yield request.param
+    ctx.set_schedule("rows", 8, 512)
+
+
 @pytest.mark.parametrize("seed", range(6))
-def test_handle_spgemm_random_rectangular(tsg, ctx, oracle, gen, seed):
+def test_handle_spgemm_random_rectangular(tsg, ctx, sched, oracle, gen, seed):
     rng = np.random.default_rng(100 + seed)
     m, k, n = (int(x) for x in rng.integers(1, 700, 3))
     matA = gen.random_poisson(m, k, float(rng.uniform(0.5, 14)), seed=seed)
@@ -131,7 +142,7 @@ def test_handle_spgemm_random_rectangular(tsg, ctx, oracle, gen, seed):
     assert info["numtile_C"] == Co["numtile"] and info["nnz_C"] == Co["nnz"]
 
 
-def test_aat_and_dense_tiles(tsg, ctx, oracle, gen):
+def test_aat_and_dense_tiles(tsg, ctx, sched, oracle, gen):
     cases = [(gen.random_poisson(300, 200, 9.0, seed=4), None),
              (gen.banded(257, 48, seed=5), None),             # full (256) and dense (225-255) C tiles
              (gen.rmat(11, 16, seed=7), None)]                # hub rows
@@ -143,7 +154,7 @@ def test_aat_and_dense_tiles(tsg, ctx, oracle, gen):
             assert_tiles(C.download(), Co, C_KEYS + ["tile_csr_Value"])
 
 
-def test_laplacian_256_known_answers(tsg, ctx, oracle, gen):
+def test_laplacian_256_known_answers(tsg, ctx, sched, oracle, gen):
     facts = json.loads((GOLD / "known_answers.json").read_text())["laplacian_256x256"]
     mat = gen.laplacian_2d(256)
     A, B, C, info = _handle_product(tsg, ctx, mat, mat)
@@ -157,7 +168,7 @@ def test_laplacian_256_known_answers(tsg, ctx, oracle, gen):
     assert v[rp[0]:rp[1]].tolist() == facts["row0_vals"]
 
 
-def test_stencil27_full_size_against_gustavson(tsg, ctx, oracle, gen):
+def test_stencil27_full_size_against_gustavson(tsg, ctx, sched, oracle, gen):
     """27-point stencil 64^3 (n=262,144): structure and every value against the
     element-level oracle; the known answers pin the counts."""
     facts = json.loads((GOLD / "known_answers.json").read_text())["stencil27_64"]
@@ -172,7 +183,7 @@ def test_stencil27_full_size_against_gustavson(tsg, ctx, oracle, gen):
     assert_values(v, G[4])
 
 
-def test_spgemm_is_deterministic(tsg, ctx, gen):
+def test_spgemm_is_deterministic(tsg, ctx, sched, gen):
     mat = gen.rmat(12, 8, seed=2)
     _, _, C1, _ = _handle_product(tsg, ctx, mat, mat)
     _, _, C2, _ = _handle_product(tsg, ctx, mat, mat)
