@@ -52,14 +52,16 @@ def measured_peak_hbm():
     return 6650.0, "fallback"
 
 
-def profiled_traffic(workload_key):
-    """Per-launch DRAM bytes of the dominant kernel from the committed ncu
-    summary (profiles/k_step3_<workload>.md, line 'traffic_bytes_per_launch:')."""
-    p = ROOT / "profiles" / f"k_step3_{workload_key}.md"
+def profiled_traffic(workload_key, sched):
+    """Per-launch DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of
+    the numeric kernel from the committed ncu summary
+    (profiles/numeric_step_<workload>.md, line 'traffic_bytes_per_launch[<sched>]:')."""
+    p = ROOT / "profiles" / f"numeric_step_{workload_key}.md"
     if not p.exists():
         return None
+    tag = f"traffic_bytes_per_launch[{sched}]:"
     for line in p.read_text().splitlines():
-        if line.strip().startswith("traffic_bytes_per_launch:"):
+        if line.strip().startswith(tag):
             try:
                 return int(float(line.split(":", 1)[1].strip()))
             except ValueError:
@@ -210,6 +212,185 @@ def run_cpu_reference(args, gen, world, rank):
 
 
 # ---------------------------------------------------------------------------
+# batched (512 uneven products in one persistent, graph-captured launch) vs
+# the plain one-product-at-a-time path on the same GPU
+# ---------------------------------------------------------------------------
+def run_batched(args, tsg, gen, ctx, steps):
+    import torch
+    at = _load("rw_spgemm_b200.autotune", PKG_DIR / "autotune.py")
+    mats = gen.batched_products(args.batch_count, seed=0)
+    pairs = [(tsg.csr_host_to_tiled(ctx, a, tsg.TSG_TILED_CSC_VIEW), tsg.csr_host_to_tiled(ctx, b, tsg.TSG_TILED_CSC_VIEW))
+             for a, b in mats]
+    total_products = sum(tsg.product_bounds(ctx, A, B)[0] for A, B in pairs)
+    del mats
+    tuner = at.Autotuner()
+    choice = tuner.tune_batch(ctx, pairs, reps=1, use_cache=False)
+    tune_ms = at.summarize(tuner.last_timings)
+    batch = tsg.Batch(ctx, pairs, *choice, graph=True)
+    stream = torch.cuda.current_stream()
+    batch.run()
+    batch.sync()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    ctx.synchronize()
+    ev[0].record(stream)
+    for _ in range(steps):
+        batch.run()
+    ev[1].record(stream)
+    ev[1].synchronize()
+    ms_batched = ev[0].elapsed_time(ev[1]) / steps
+    tiles, nnz = batch.sync()
+    info = batch.info()
+    batch.close()
+    # plain path: one tsg_spgemm per product (its own launches, read-backs and allocations)
+    ctx.set_schedule(*choice)
+    for A, B in pairs[:8]:
+        C, _ = tsg.spgemm(ctx, A, B)
+        C.free()
+    ctx.synchronize()
+    ev[0].record(stream)
+    for _ in range(max(1, steps // 2)):
+        for A, B in pairs:
+            C, _ = tsg.spgemm(ctx, A, B)
+            C.free()
+    ev[1].record(stream)
+    ev[1].synchronize()
+    ms_plain = ev[0].elapsed_time(ev[1]) / max(1, steps // 2)
+    for A, B in pairs:
+        A.free()
+        B.free()
+    gf_b = 2.0 * total_products / (ms_batched * 1e-3) / 1e9
+    gf_p = 2.0 * total_products / (ms_plain * 1e-3) / 1e9
+    return {"workload": f"{len(pairs)} independent FP64 products C_i = A_i*B_i, n_i log-uniform in [1024, 65536], "
+                        "A_i/B_i banded (half-bandwidth 8-64) or random Poisson(8) per row, values U(-1,1)",
+            "products": int(total_products), "C_tiles": int(tiles), "C_nnz": int(nnz),
+            "gflops_batched": round(gf_b, 2), "gflops_plain": round(gf_p, 2), "speedup_vs_plain": round(gf_b / gf_p, 3),
+            "ms_batched": round(ms_batched, 3), "ms_plain": round(ms_plain, 3),
+            "schedule": list(choice), "autotune_ms": tune_ms, "graph": info["graph"], "grid": info["grid"],
+            "arena_gb": round(info["arena_bytes"] / 1e9, 3)}
+
+
+# ---------------------------------------------------------------------------
+# served: Poisson arrivals into the continuous-batching server
+# ---------------------------------------------------------------------------
+def served_pool(gen, seed=0):
+    """Fixed mix: 40 small matrices from the batched generators (n 1k-16k),
+    R-MAT scale 14 (edge factor 8, 16), 15 (8, 16) and 16 (8)."""
+    rng = np.random.default_rng(seed)
+    small = []
+    for i in range(40):
+        n = int(round(np.exp(rng.uniform(np.log(1024), np.log(16384)))))
+        s = int(rng.integers(0, 2**31 - 1))
+        small.append(gen.banded(n, int(rng.integers(8, 65)), seed=s) if rng.random() < 0.5
+                     else gen.random_poisson(n, None, 8.0, seed=s))
+    rmat = {14: [gen.rmat(14, 8, seed=1), gen.rmat(14, 16, seed=2)],
+            15: [gen.rmat(15, 8, seed=3), gen.rmat(15, 16, seed=4)],
+            16: [gen.rmat(16, 8, seed=5)]}
+    return small, rmat
+
+
+def run_served(args, tsg, gen, device):
+    srv_mod = _load("rw_spgemm_b200.serve", PKG_DIR / "serve.py")
+    small, rmat = served_pool(gen)
+    srv = srv_mod.SpGEMMServer(device, mem_cap=40 << 30, slots=2, max_batch=64, schedule=tuple(args.served_schedule))
+    keys = []
+    for i, m in enumerate(small):
+        srv.register(f"s{i}", m)
+        keys.append(("small", f"s{i}", m))
+    for sc, lst in rmat.items():
+        for i, m in enumerate(lst):
+            srv.register(f"r{sc}_{i}", m)
+            keys.append((sc, f"r{sc}_{i}", m))
+    rng = np.random.default_rng(1)
+    jobs = []
+    by_kind = {"small": [k for k in keys if k[0] == "small"], 14: [k for k in keys if k[0] == 14],
+               15: [k for k in keys if k[0] == 15], 16: [k for k in keys if k[0] == 16]}
+    for _ in range(args.served_jobs):
+        u = rng.random()
+        cls = "small" if u < 0.85 else 14 if u < 0.95 else 15 if u < 0.99 else 16
+        _, key, mat = by_kind[cls][int(rng.integers(0, len(by_kind[cls])))]
+        if rng.random() < 0.5:
+            jobs.append(("AAT", key, None, gen.products(mat, gen.transpose(mat))))
+        else:
+            same = [k for k in by_kind[cls] if k[2][0] == mat[1]] or [(None, key, mat)]
+            _, bkey, bmat = same[int(rng.integers(0, len(same)))]
+            jobs.append(("AB", key, bkey, gen.products(mat, bmat)))
+    # warm the operand cache and the kernels with one pass of distinct jobs
+    srv.start()
+    for f in [srv.submit(k, a, b) for k, a, b, _ in jobs[:64]]:
+        f.result(timeout=600)
+    srv.done.clear()
+    srv.batches = 0
+    gaps = rng.exponential(1.0 / args.served_rate, len(jobs))
+    futs = []
+    t0 = time.perf_counter()
+    t_next = t0
+    for (kind, a, b, _), g in zip(jobs, gaps):
+        t_next += g
+        while True:
+            now = time.perf_counter()
+            if now >= t_next:
+                break
+            time.sleep(min(t_next - now, 0.0005))
+        futs.append(srv.submit(kind, a, b))
+    for f in futs:
+        f.result(timeout=600)
+    wall = time.perf_counter() - t0
+    st = srv.stats()
+    srv.close()
+    prods = sum(j[3] for j in jobs)
+    return {"workload": "Poisson arrivals at %d jobs/s; mix 85%% small batched-generator products (n 1k-16k), 10%% "
+                        "R-MAT scale 14, 4%% scale 15, 1%% scale 16 (edge factor 8/16); 50%% A*B, 50%% A*A^T"
+                        % args.served_rate,
+            "jobs": st["jobs"], "jobs_per_s": round(st["jobs_per_s"], 1), "p50_ms": round(st["p50_ms"], 3),
+            "p99_ms": round(st["p99_ms"], 3), "gflops": round(2.0 * prods / wall / 1e9, 2),
+            "batches": st["batches"], "mean_batch": round(st["mean_batch"], 2), "rejected": st["rejected"],
+            "operand_cache": st["operand_cache"], "schedule": list(args.served_schedule), "mem_cap_gb": 40}
+
+
+# ---------------------------------------------------------------------------
+# learned selector: trained on method-generated timings, judged by exhaustive
+# search on held-out matrices
+# ---------------------------------------------------------------------------
+def run_selector(args, tsg, gen, ctx):
+    sel = _load("rw_spgemm_b200.selector", PKG_DIR / "selector.py")
+    n_mat = max(10, args.selector_samples // len(sel.CONFIGS))
+    mats = sel.training_matrices(gen, n_mat, seed=21)
+    t0 = time.perf_counter()
+    data = [sel.time_configs(ctx, m, repeats=2) for m in mats]
+    collect_s = time.perf_counter() - t0
+    feats = np.stack([d[0] for d in data])
+    times = np.stack([d[1] for d in data])
+    order_ms = np.array([[d[2][o] for o in sel.ORDERINGS] for d in data])
+    n_tr = int(0.8 * n_mat)
+    net = sel.MLP(ctx, seed=3)
+    t0 = time.perf_counter()
+    losses = net.fit(feats[:n_tr], times[:n_tr], epochs=300, lr=2e-3)
+    train_s = time.perf_counter() - t0
+    te = slice(n_tr, n_mat)
+    picks = np.argmin(net.predict(feats[te]), axis=1)
+    fixed_best = int(np.argmin(np.log(times[:n_tr]).mean(0)))
+    res = {
+        "timing_samples": int(times.size), "matrices": n_mat, "train": n_tr, "held_out": n_mat - n_tr,
+        "configs": [f"{o}/{a[0]}-{a[1]}-{a[2]}" for o, a in sel.CONFIGS],
+        "regret_model": sel.regret(times[te], picks),
+        "regret_without_model": sel.regret(times[te], np.zeros(n_mat - n_tr, dtype=int)),
+        "regret_best_fixed": sel.regret(times[te], np.full(n_mat - n_tr, fixed_best)),
+        "best_fixed_config": res_name(sel, fixed_best),
+        "final_train_loss": round(float(losses[-1]), 5), "collect_s": round(collect_s, 1),
+        "train_s": round(train_s, 2), "mean_ordering_ms": {o: round(float(order_ms[:, k].mean()), 3)
+                                                           for k, o in enumerate(sel.ORDERINGS)},
+        "within_10pct_of_exhaustive": bool(sel.regret(times[te], picks)[0] <= 0.10),
+    }
+    net.close()
+    return res
+
+
+def res_name(sel, idx):
+    o, a = sel.CONFIGS[idx]
+    return f"{o}/{a[0]}-{a[1]}-{a[2]}"
+
+
+# ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
 def run_ours(args, tsg, gen, world, rank, local):
@@ -231,6 +412,7 @@ def run_ours(args, tsg, gen, world, rank, local):
     d_v = torch.from_numpy(v).to(dev)
     A = tsg.csr_to_tiled(ctx, m, n, d_rp, d_ci, d_v, tsg.TSG_TILED_CSC_VIEW)  # serves as A and B
     prods = tsg.count_products(ctx, d_ci, d_rp)
+    tiles_A = A.numtile
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
 
     def one_step():
@@ -281,34 +463,42 @@ def run_ours(args, tsg, gen, world, rank, local):
     achieved = alg3 / (s3 * 1e-3) / 1e9
     comp = compulsory_bytes(A, A, numC, nnzC)
 
-    # end to end through the C ABI with host buffers (pinned inputs)
+    # end to end through the C ABI with host buffers: pinned inputs, results
+    # copied into reused pinned output buffers (two-phase call)
     e2e_t, h2d, d2h = float("nan"), 0, 0
     if not args.no_e2e:
         pin = lambda x: torch.from_numpy(x).pin_memory().numpy()  # noqa: E731
         hmat = (m, n, pin(rp), pin(ci), pin(v))
-        tsg.spgemm_csr_host(ctx, hmat)
+        outbuf = tsg.HostResultBuffers(m, nnzC)
+        tsg.spgemm_csr_host_into(ctx, hmat, None, outbuf)
         e2e_ms = []
         for _ in range(max(2, min(args.steps, 5))):
             flush.zero_()
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            Cc, _ = tsg.spgemm_csr_host(ctx, hmat)
+            Cc, _ = tsg.spgemm_csr_host_into(ctx, hmat, None, outbuf)
             torch.cuda.synchronize()
             e2e_ms.append((time.perf_counter() - t0) * 1e3)
         e2e_t = float(np.mean(e2e_ms))
         h2d = rp.nbytes + ci.nbytes + v.nbytes
         d2h = Cc[2].nbytes + Cc[3].nbytes + Cc[4].nbytes
-
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = run_cpu_reference(argparse.Namespace(warmup=0, steps=1), gen, 1, 0)
+    batched = served = None
+    A.free()
+    if "batched" in args.sections:
+        batched = run_batched(args, tsg, gen, ctx, max(2, min(args.steps, 5)))
+    if "served" in args.sections:
+        served = run_served(args, tsg, gen, local)
+    selector = run_selector(args, tsg, gen, ctx) if "selector" in args.sections else None
     out = {
         "metric": METRIC, "value": round(value, 3), "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": "C = A*A, 27-point stencil on a 64^3 grid (n=262,144, nnz=6,859,000, FP64 "
                                "uniform(0.5,1.5)), natural order, 16x16 tiles",
-                   "products": prods, "tiles_A": A.numtile, "tiles_C": numC, "nnz_C": nnzC,
+                   "products": prods, "tiles_A": tiles_A, "tiles_C": numC, "nnz_C": nnzC,
                    "window": "steps 1-3 incl. C allocation (reference tilespgemm window)",
                    "schedule": f"{args.sched} seg={args.seg} cap={args.cap}",
                    "l2": "512 MiB write before every timed step, outside the timed events",
@@ -317,17 +507,23 @@ def run_ours(args, tsg, gen, world, rank, local):
         "hbm_frac": round(comp / (ms_per_step * 1e-3) / 1e9 / peak, 4),
         "compulsory_bytes": comp,
         "step_ms": {k: round(float(np.mean([i[k] for i in infos])), 4) for k in ("ms_step1", "ms_step2", "ms_step3")},
-        "roofline": {"bound": "hbm", "kernel": "k_step3 (numeric)", "achieved": round(achieved, 2),
+        "roofline": {"bound": "hbm", "kernel": {"tiles": "k_step3", "elems": "k_step3_elems", "rows": "k_step3_rows"}[args.sched] + " (numeric)", "achieved": round(achieved, 2),
                      "peak": peak, "peak_source": peak_src, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                     "algorithmic_bytes": alg3, "traffic": profiled_traffic("stencil27_64")},
+                     "algorithmic_bytes": alg3, "traffic": profiled_traffic("stencil27_64", args.sched)},
         "e2e": {"value": round(2.0 * prods / (e2e_t * 1e-3) / 1e9, 3), "unit": "GFLOP/s", "ms": round(e2e_t, 3),
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-                "path": "tsg_spgemm_csr_host (host CSR in -> host CSR out, pinned inputs)"},
+                "path": "tsg_spgemm_csr_host_start + tsg_result_copy (host CSR in -> host CSR out, pinned buffers)"},
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
     }
     if cpu:
         out["cpu_baseline"] = cpu
+    if batched:
+        out["batched"] = batched
+    if served:
+        out["served"] = served
+    if selector:
+        out["selector"] = selector
     if rank == 0:
         print(json.dumps(out), flush=True)
     ctx.close()
@@ -344,10 +540,19 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
-    ap.add_argument("--sched", default="rows", choices=["rows", "tiles"])
+    ap.add_argument("--sched", default="elems", choices=["rows", "tiles", "elems"])
+    ap.add_argument("--sections", default="plain,batched,served",
+                    help="comma list: plain (always), batched, served, selector")
+    ap.add_argument("--batch-count", type=int, default=512)
+    ap.add_argument("--selector-samples", type=int, default=5000)
+    ap.add_argument("--served-jobs", type=int, default=2000)
+    ap.add_argument("--served-rate", type=float, default=2000.0)
+    ap.add_argument("--served-schedule", nargs=3, default=["elems", "8", "512"])
     ap.add_argument("--seg", type=int, default=16)
     ap.add_argument("--cap", type=int, default=1024)
     args = ap.parse_args()
+    args.sections = set(args.sections.split(","))
+    args.served_schedule = (args.served_schedule[0], int(args.served_schedule[1]), int(args.served_schedule[2]))
     world, rank, local = dist_setup()
     tsg = _load("rw_spgemm_b200", PKG_DIR / "__init__.py", PKG_DIR)
     gen = _load("rw_spgemm_b200.generators", PKG_DIR / "generators.py")

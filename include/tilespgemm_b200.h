@@ -248,7 +248,8 @@ typedef struct
     int *csc_tile_ptr;
     int *csc_tile_rowidx;
     int *csc_tile_pos;
-    void *_alloc; /* internal: single backing allocation */
+    unsigned short *mask_t; /* B operand: per tile column masks, bit (15-row) */
+    void *_alloc;           /* internal: non-NULL marks a borrowed view      */
 } tsg_tiled;
 
 /* Per-product statistics filled by tsg_spgemm. */
@@ -280,7 +281,16 @@ int tsg_context_set_stream(tsg_context *ctx, void *cuda_stream);
  *                  {256, 512, 1024, 2048}. */
 #define TSG_SCHED_TILES 0
 #define TSG_SCHED_ROWS 1
+/* TSG_SCHED_ELEMS  step 2 as TILES; step 3 with one warp per C tile and one
+ *                  lane per C nonzero, accumulating across matched tile pairs
+ *                  through A's row masks and B's column masks (register
+ *                  accumulator, no shared-memory scatter). */
+#define TSG_SCHED_ELEMS 2
 int tsg_context_set_schedule(tsg_context *ctx, int schedule, int seg_tiles, int acc_cap);
+/* 1 (default): step-1 emit and step 2 run as one row-wise pass for tile rows
+ * with at most 128 C tiles (others fall back to step 2 per tile); 0: separate
+ * step 2 of the schedule.  Results are identical. */
+int tsg_context_set_fusion(tsg_context *ctx, int fuse_step12);
 /* 0 when all work queued on the context's stream has finished, 1 while
  * some is pending, a negative status on error (non-blocking). */
 int tsg_context_query(tsg_context *ctx);
@@ -370,6 +380,20 @@ int tsg_spgemm_csr_host_ex(tsg_context *ctx,
                            int *nnzC, int **c_rowptr, int **c_colidx, double **c_val,
                            tsg_spgemm_info *info, int flags);
 void tsg_host_free(void *p);
+
+/* Two-phase end-to-end call for callers that own their output buffers
+ * (e.g. reused page-locked buffers): _start copies the host CSR inputs to the
+ * device and computes C there (as CSR), returning nnz(C); tsg_result_copy
+ * copies it into rowptr[m+1], colidx[nnzC], val[nnzC]; tsg_result_free
+ * releases the device result. */
+typedef struct tsg_result tsg_result;
+int tsg_spgemm_csr_host_start(tsg_context *ctx,
+                              int m, int k, int n,
+                              int nnzA, const int *a_rowptr, const int *a_colidx, const double *a_val,
+                              int nnzB, const int *b_rowptr, const int *b_colidx, const double *b_val,
+                              tsg_result **res, int *nnzC, tsg_spgemm_info *info);
+int tsg_result_copy(tsg_result *res, int *rowptr, int *colidx, double *val);
+int tsg_result_free(tsg_result *res);
 
 /* Host CSR -> device tiles in one call (copies through pooled device memory;
  * the host arrays may be pageable or pinned). */

@@ -59,7 +59,7 @@ class TsgTiled(ctypes.Structure):
         ("tile_nnz", ctypes.c_void_p), ("tile_csr_Ptr", ctypes.c_void_p), ("tile_csr_Col", ctypes.c_void_p),
         ("tile_csr_Value", ctypes.c_void_p), ("mask", ctypes.c_void_p),
         ("csc_tile_ptr", ctypes.c_void_p), ("csc_tile_rowidx", ctypes.c_void_p), ("csc_tile_pos", ctypes.c_void_p),
-        ("_alloc", ctypes.c_void_p),
+        ("mask_t", ctypes.c_void_p), ("_alloc", ctypes.c_void_p),
     ]
 
 
@@ -111,6 +111,7 @@ def _declare(L):
     L.tsg_context_launches.argtypes = [vp]
     L.tsg_context_synchronize.argtypes = [vp]
     L.tsg_context_query.argtypes = [vp]
+    L.tsg_context_set_fusion.argtypes = [vp, ip]
     L.tsg_context_set_schedule.argtypes = [vp, ip, ip, ip]
     L.tsg_context_launches.restype = ctypes.c_longlong
     L.tsg_csr_to_tiled.argtypes = [vp, ip, ip, ip, vp, vp, vp, ip, ctypes.POINTER(TsgTiled)]
@@ -288,7 +289,11 @@ class Context:
     def set_schedule(self, schedule: str = "rows", seg_tiles: int = 8, acc_cap: int = 512):
         """'tiles' (half-warp per C tile, intersection) or 'rows' (half-warp per
         run of seg_tiles C tiles of one tile row, acc_cap FP64 slots)."""
-        check(lib().tsg_context_set_schedule(self.handle, {"tiles": 0, "rows": 1}[schedule], seg_tiles, acc_cap))
+        check(lib().tsg_context_set_schedule(self.handle, {"tiles": 0, "rows": 1, "elems": 2}[schedule], seg_tiles,
+                                             acc_cap))
+
+    def set_fusion(self, on: bool):
+        check(lib().tsg_context_set_fusion(self.handle, 1 if on else 0))
 
     def synchronize(self):
         check(lib().tsg_context_synchronize(self.handle))
@@ -654,7 +659,7 @@ class Batch:
         n = len(self.pairs)
         arrA = (TsgTiled * n)(*[a.s for a, _ in self.pairs])
         arrB = (TsgTiled * n)(*[b.s for _, b in self.pairs])
-        prm = BatchParams({"tiles": 0, "rows": 1}[schedule], seg_tiles, acc_cap, 1 if graph else 0)
+        prm = BatchParams({"tiles": 0, "rows": 1, "elems": 2}[schedule], seg_tiles, acc_cap, 1 if graph else 0)
         self.handle = ctypes.c_void_p()
         check(lib().tsg_batch_create(ctx.handle, n, arrA, arrB, ctypes.byref(prm), ctypes.byref(self.handle)))
         self.count = n
@@ -726,3 +731,64 @@ def tiled_to_csr_host(ctx: Context, C: Tiled, pinned: bool = True):
         return m, n, _wrap_pinned(prp, m + 1, np.int32), _wrap_pinned(pci, nnz, np.int32), _wrap_pinned(pv, nnz, np.float64)
     return (m, n, _np_from(prp, m + 1, np.int32, True), _np_from(pci, nnz, np.int32, True),
             _np_from(pv, nnz, np.float64, True))
+
+
+def _declare_result(L):
+    vp, ip = ctypes.c_void_p, ctypes.c_int
+    L.tsg_spgemm_csr_host_start.argtypes = [vp, ip, ip, ip, ip, vp, vp, vp, ip, vp, vp, vp, ctypes.POINTER(vp),
+                                            ctypes.POINTER(ip), ctypes.POINTER(TsgInfo)]
+    L.tsg_result_copy.argtypes = [vp, vp, vp, vp]
+    L.tsg_result_free.argtypes = [vp]
+
+
+_declare_prev3 = _declare
+
+
+def _declare(L):  # noqa: F811
+    _declare_prev3(L)
+    _declare_result(L)
+
+
+class HostResultBuffers:
+    """Reusable (page-locked when torch is available) output buffers for the
+    two-phase end-to-end call."""
+
+    def __init__(self, m: int, nnz_cap: int, pinned: bool = True):
+        self.resize(m, nnz_cap, pinned)
+
+    def resize(self, m, nnz_cap, pinned=True):
+        self.m, self.cap = m, nnz_cap
+        if pinned:
+            import torch
+            self._t = [torch.empty(m + 1, dtype=torch.int32).pin_memory(),
+                       torch.empty(max(nnz_cap, 1), dtype=torch.int32).pin_memory(),
+                       torch.empty(max(nnz_cap, 1), dtype=torch.float64).pin_memory()]
+            self.rp, self.ci, self.v = (t.numpy() for t in self._t)
+        else:
+            self.rp = np.empty(m + 1, np.int32)
+            self.ci = np.empty(max(nnz_cap, 1), np.int32)
+            self.v = np.empty(max(nnz_cap, 1), np.float64)
+
+
+def spgemm_csr_host_into(ctx: Context, matA, matB, out: HostResultBuffers):
+    """End to end with host buffers through the two-phase C call; the result
+    lands in out (grown if too small).  Returns (m, n, rowptr, colidx, val)
+    views into out, and the info dict."""
+    hA = HostCSR(matA)
+    hB = hA if matB is None else HostCSR(matB)
+    res = ctypes.c_void_p()
+    nnzC = ctypes.c_int(0)
+    info = TsgInfo()
+    m, k, n = hA.sm.m, hA.sm.n, hB.sm.n
+    check(lib().tsg_spgemm_csr_host_start(
+        ctx.handle, m, k, n, hA.sm.nnz, hA.rp.ctypes.data, hA.ci.ctypes.data, hA.v.ctypes.data,
+        hB.sm.nnz, hB.rp.ctypes.data, hB.ci.ctypes.data, hB.v.ctypes.data,
+        ctypes.byref(res), ctypes.byref(nnzC), ctypes.byref(info)))
+    try:
+        if out.m != m or out.cap < nnzC.value:
+            out.resize(m, nnzC.value)
+        check(lib().tsg_result_copy(res, out.rp.ctypes.data, out.ci.ctypes.data, out.v.ctypes.data))
+    finally:
+        lib().tsg_result_free(res)
+    nz = nnzC.value
+    return (m, n, out.rp, out.ci[:nz], out.v[:nz]), info.as_dict()

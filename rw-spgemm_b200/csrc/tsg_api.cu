@@ -60,9 +60,10 @@ extern "C" int tsg_context_create(int device, tsg_context **out)
         return tsg_set_error(TSG_ERR_CUDA, "context creation failed: %s", cudaGetErrorString(e));
     }
     ctx->own_stream = 1;
-    ctx->sched = TSG_SCHED_ROWS;
+    ctx->sched = TSG_SCHED_ELEMS;
     ctx->seg_tiles = 8;
     ctx->acc_cap = 512;
+    ctx->fuse12 = 1;
     // keep freed pool memory cached so repeated products do not return pages
     cudaMemPool_t pool;
     if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess)
@@ -115,7 +116,7 @@ extern "C" int tsg_context_set_schedule(tsg_context *ctx, int schedule, int seg_
 {
     if (!ctx)
         return tsg_set_error(TSG_ERR_INVALID, "null context");
-    if (schedule != TSG_SCHED_TILES && schedule != TSG_SCHED_ROWS)
+    if (schedule != TSG_SCHED_TILES && schedule != TSG_SCHED_ROWS && schedule != TSG_SCHED_ELEMS)
         return tsg_set_error(TSG_ERR_INVALID, "unknown schedule %d", schedule);
     if (schedule == TSG_SCHED_ROWS)
     {
@@ -128,6 +129,14 @@ extern "C" int tsg_context_set_schedule(tsg_context *ctx, int schedule, int seg_
         ctx->acc_cap = acc_cap;
     }
     ctx->sched = schedule;
+    return TSG_OK;
+}
+
+extern "C" int tsg_context_set_fusion(tsg_context *ctx, int fuse_step12)
+{
+    if (!ctx)
+        return tsg_set_error(TSG_ERR_INVALID, "null context");
+    ctx->fuse12 = fuse_step12 ? 1 : 0;
     return TSG_OK;
 }
 
@@ -181,6 +190,7 @@ extern "C" int tsg_tiled_free(tsg_context *ctx, tsg_tiled *t)
     tsg_release(ctx, t->csc_tile_ptr);
     tsg_release(ctx, t->csc_tile_rowidx);
     tsg_release(ctx, t->csc_tile_pos);
+    tsg_release(ctx, t->mask_t);
     memset(t, 0, sizeof(*t));
     return TSG_OK;
 }
@@ -689,5 +699,91 @@ extern "C" int tsg_tiled_to_csr_host(tsg_context *ctx, const tsg_tiled *C, int f
     tsg_release(ctx, rp);
     tsg_release(ctx, ci);
     tsg_release(ctx, v);
+    return TSG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Two-phase end-to-end call (caller-owned output buffers).
+// ---------------------------------------------------------------------------
+struct tsg_result
+{
+    tsg_context *ctx;
+    int m, nnz;
+    int *rp, *ci;
+    double *v;
+};
+
+extern "C" int tsg_spgemm_csr_host_start(tsg_context *ctx, int m, int k, int n, int nnzA, const int *a_rowptr,
+                                         const int *a_colidx, const double *a_val, int nnzB, const int *b_rowptr,
+                                         const int *b_colidx, const double *b_val, tsg_result **res, int *nnzC,
+                                         tsg_spgemm_info *info)
+{
+    if (!ctx || !res || !nnzC || !a_rowptr || !b_rowptr)
+        return tsg_set_error(TSG_ERR_INVALID, "null argument");
+    *res = nullptr;
+    const bool alias = (a_rowptr == b_rowptr && a_colidx == b_colidx && a_val == b_val && m == k && k == n);
+    tsg_tiled A, B, C;
+    memset(&A, 0, sizeof(A));
+    memset(&B, 0, sizeof(B));
+    memset(&C, 0, sizeof(C));
+    int st = alias ? tsg_csr_host_to_tiled(ctx, m, k, nnzA, a_rowptr, a_colidx, a_val, TSG_TILED_CSC_VIEW, &A)
+                   : tsg_csr_host_to_tiled(ctx, m, k, nnzA, a_rowptr, a_colidx, a_val, TSG_TILED_PACKED_COL, &A);
+    if (st == TSG_OK && !alias)
+        st = tsg_csr_host_to_tiled(ctx, k, n, nnzB, b_rowptr, b_colidx, b_val, TSG_TILED_CSC_VIEW, &B);
+    if (st == TSG_OK)
+        st = tsg_spgemm(ctx, &A, alias ? &A : &B, &C, info);
+    tsg_result *r = nullptr;
+    if (st == TSG_OK)
+    {
+        r = (tsg_result *)calloc(1, sizeof(tsg_result));
+        r->ctx = ctx;
+        r->m = m;
+        r->nnz = C.nnz;
+        st = tsg_alloc(ctx, &r->rp, (size_t)m + 1);
+        if (st == TSG_OK)
+            st = tsg_alloc(ctx, &r->ci, (size_t)C.nnz);
+        if (st == TSG_OK)
+            st = tsg_alloc(ctx, &r->v, (size_t)C.nnz);
+        if (st == TSG_OK)
+            st = tsg_tiled_to_csr(ctx, &C, r->rp, r->ci, r->v);
+    }
+    tsg_tiled_free(ctx, &A);
+    tsg_tiled_free(ctx, &B);
+    tsg_tiled_free(ctx, &C);
+    if (st != TSG_OK)
+    {
+        if (r)
+            tsg_result_free(r);
+        return st;
+    }
+    *nnzC = r->nnz;
+    *res = r;
+    return TSG_OK;
+}
+
+extern "C" int tsg_result_copy(tsg_result *r, int *rowptr, int *colidx, double *val)
+{
+    if (!r || !rowptr)
+        return tsg_set_error(TSG_ERR_INVALID, "null argument");
+    tsg_context *ctx = r->ctx;
+    TSG_CUDA(cudaMemcpyAsync(rowptr, r->rp, ((size_t)r->m + 1) * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    if (r->nnz)
+    {
+        TSG_CUDA(cudaMemcpyAsync(colidx, r->ci, (size_t)r->nnz * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        TSG_CUDA(cudaMemcpyAsync(val, r->v, (size_t)r->nnz * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    TSG_CUDA(cudaStreamSynchronize(ctx->stream));
+    return TSG_OK;
+}
+
+extern "C" int tsg_result_free(tsg_result *r)
+{
+    if (!r)
+        return TSG_OK;
+    tsg_context *ctx = r->ctx;
+    tsg_release(ctx, r->rp);
+    tsg_release(ctx, r->ci);
+    tsg_release(ctx, r->v);
+    free(r);
     return TSG_OK;
 }

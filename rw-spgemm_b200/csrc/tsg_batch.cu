@@ -29,6 +29,7 @@ int tsg_count_c_tiles(tsg_context *ctx, const tsg_tiled *A, const tsg_tiled *B, 
 struct BatchProd
 {
     ProdView P;
+    int *wide; // per A tile row: 1 when step 2 runs per tile (fused pass declined)
     long long capT, capN;
     int tilemA;
     int status; // 0 ok, 1 tile capacity, 2 value capacity
@@ -210,7 +211,7 @@ __global__ void __launch_bounds__(BATCH_THREADS)
             {
                 itemoff[p] = run;
                 const long long nc = prods[p].numC;
-                run += SCHED ? (nc + W - 1) / W : nc;
+                run += SCHED == 1 ? (nc + W - 1) / W : nc;
             }
             itemoff[count] = run;
         }
@@ -219,23 +220,39 @@ __global__ void __launch_bounds__(BATCH_THREADS)
     }
     if (!grid_barrier(bar, err))
         return;
-    // phase 4: step-1 emit
+    // phase 4: step-1 emit (fused with step 2 for narrow rows unless the
+    // row schedule runs its own step 2)
+    if (threadIdx.x < 4)
+        s_bins[threadIdx.x] = 0;
+    __syncthreads();
     {
         unsigned *bm = reinterpret_cast<unsigned *>(s_raw) + warp * S1_WORDS;
+        S12Smem *s12 = reinterpret_cast<S12Smem *>(s_raw) + warp;
         for (long long w = (long long)blockIdx.x * (BATCH_THREADS / 32) + warp; w < total_rows; w += nwarps)
         {
             const int p = find_product(rowoff, count, w);
             if (prods[p].status)
                 continue;
-            step1_row<true>(prods[p].P, (int)(w - rowoff[p]), bm, lane32, nullptr);
+            const int i = (int)(w - rowoff[p]);
+            if (SCHED == 1)
+                step1_row<true>(prods[p].P, i, bm, lane32, nullptr);
+            else
+            {
+                const int done = step12_row(prods[p].P, i, *s12, lane32, s_bins);
+                if (!done)
+                {
+                    __syncwarp();
+                    step1_row<true>(prods[p].P, i, reinterpret_cast<unsigned *>(s12), lane32, nullptr);
+                }
+                if (lane32 == 0)
+                    prods[p].wide[i] = done ? 0 : 1;
+                __syncwarp();
+            }
         }
     }
     if (!grid_barrier(bar, err))
         return;
-    // phase 5: step 2
-    if (threadIdx.x < 4)
-        s_bins[threadIdx.x] = 0;
-    __syncthreads();
+    // phase 5: step 2 (all tiles for the row schedule, tiles of wide rows otherwise)
     {
         const long long total_items = itemoff[count];
         for (long long h = (long long)blockIdx.x * (BATCH_THREADS / 16) + hw; h < total_items; h += nhw)
@@ -243,9 +260,9 @@ __global__ void __launch_bounds__(BATCH_THREADS)
             const int p = find_product(itemoff, count, h);
             const ProdView &P = prods[p].P;
             const long long item = h - itemoff[p];
-            if (SCHED)
+            if (SCHED == 1)
                 step2_rows_item<W>(P, item, hmask, lane, reinterpret_cast<S2RowsSmem<W> *>(s_raw)[hw], s_bins);
-            else
+            else if (prods[p].wide[P.C_row[item]])
                 step2_tile(P, (int)item, hmask, lane, s_bins);
         }
     }
@@ -273,6 +290,19 @@ __global__ void __launch_bounds__(BATCH_THREADS)
     if (!grid_barrier(bar, err))
         return;
     // phase 7: step 3
+    if (SCHED == 2)
+    {
+        int2 *pairs = reinterpret_cast<int2 *>(s_raw) + warp * S3E_PAIRS;
+        const long long total_items = itemoff[count];
+        for (long long w = (long long)blockIdx.x * (BATCH_THREADS / 32) + warp; w < total_items; w += nwarps)
+        {
+            const int p = find_product(itemoff, count, w);
+            if (prods[p].status)
+                continue;
+            step3_elems_tile(prods[p].P, (int)(w - itemoff[p]), pairs);
+        }
+    }
+    else
     {
         double *tacc = reinterpret_cast<double *>(s_raw) + hw * (TSG_BS * S3T_STRIDE);
         if (!SCHED)
@@ -289,7 +319,7 @@ __global__ void __launch_bounds__(BATCH_THREADS)
                 continue;
             const ProdView &P = prods[p].P;
             const long long item = h - itemoff[p];
-            if (SCHED)
+            if (SCHED == 1)
                 step3_rows_item<W, CAP>(P, item, hmask, lane, reinterpret_cast<S3RowsSmem<W, CAP> *>(s_raw)[hw]);
             else
                 step3_tile(P, (int)item, hmask, lane, tacc);
@@ -390,7 +420,15 @@ typedef void (*batch_kernel_t)(BatchProd *, int, const long long *, long long *,
 
 static batch_kernel_t pick_kernel(const tsg_batch_params &p, size_t *smem)
 {
-    const size_t s1 = (size_t)(BATCH_THREADS / 32) * S1_WORDS * 4;
+    const size_t s1a = (size_t)(BATCH_THREADS / 32) * S1_WORDS * 4;
+    const size_t s12 = (size_t)(BATCH_THREADS / 32) * sizeof(S12Smem);
+    const size_t s1 = s1a > s12 ? s1a : s12;
+    if (p.schedule == TSG_SCHED_ELEMS)
+    {
+        const size_t s3 = (size_t)(BATCH_THREADS / 32) * S3E_PAIRS * sizeof(int2);
+        *smem = s1 > s3 ? s1 : s3;
+        return k_batch<2, 8, 256>;
+    }
     if (p.schedule == TSG_SCHED_TILES)
     {
         const size_t s3 = (size_t)(BATCH_THREADS / 16) * TSG_BS * S3T_STRIDE * 8;
@@ -459,6 +497,8 @@ extern "C" int tsg_batch_create(tsg_context *ctx, int count, const tsg_tiled *A,
     {
         if (A[p].n != B[p].m || !B[p].csc_tile_ptr)
             return tsg_set_error(TSG_ERR_INVALID, "product %d: inner dimensions differ or B lacks its column view", p);
+        if (prm.schedule == TSG_SCHED_ELEMS && !B[p].mask_t)
+            return tsg_set_error(TSG_ERR_INVALID, "product %d: element schedule needs B's column masks", p);
     }
     tsg_batch *b = new tsg_batch();
     b->ctx = ctx;
@@ -509,7 +549,8 @@ extern "C" int tsg_batch_create(tsg_context *ctx, int count, const tsg_tiled *A,
         b->n[p] = B[p].n;
         b->tilen[p] = B[p].tilen;
         off[p] = bytes;
-        bytes += align256(((size_t)A[p].tilem + 1) * 4) + 2 * align256((size_t)capT * 4) + align256(((size_t)capT + 1) * 4) +
+        bytes += align256(((size_t)A[p].tilem + 1) * 4) + align256((size_t)A[p].tilem * 4) + 2 * align256((size_t)capT * 4) +
+                 align256(((size_t)capT + 1) * 4) +
                  align256((size_t)capT * 32) + align256((size_t)capT * 16) + align256((size_t)capN) +
                  align256((size_t)capN * 8);
     }
@@ -549,8 +590,10 @@ extern "C" int tsg_batch_create(tsg_context *ctx, int count, const tsg_tiled *A,
         P.B_Colb = B[p].tile_csr_Col;
         P.B_Val = B[p].tile_csr_Value;
         P.B_mask = B[p].mask;
+        P.B_maskT = B[p].mask_t;
         P.tilenB = B[p].tilen;
         P.C_ptr = (int *)take(((size_t)A[p].tilem + 1) * 4);
+        h.wide = (int *)take((size_t)A[p].tilem * 4);
         P.C_col = (int *)take((size_t)h.capT * 4);
         P.C_row = (int *)take((size_t)h.capT * 4);
         P.C_tnnz = (int *)take(((size_t)h.capT + 1) * 4);

@@ -230,8 +230,42 @@ static int bits_for(long long v)
     return b;
 }
 
+// transposed masks: mask_t[t][c] has bit (15-r) when mask[t][r] has bit (15-c)
+__global__ void k_mask_transpose(int T, const unsigned short *__restrict__ mask, unsigned short *__restrict__ mask_t)
+{
+    const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = (int)(gid >> 4), c = threadIdx.x & 15;
+    if (t >= T)
+        return;
+    const uint4 *mb = reinterpret_cast<const uint4 *>(mask + (long long)t * TSG_BS);
+    const uint4 q0 = mb[0], q1 = mb[1];
+    const unsigned w[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
+    unsigned out = 0;
+#pragma unroll
+    for (int r = 0; r < 16; r++)
+    {
+        const unsigned row = (r & 1) ? (w[r >> 1] >> 16) : (w[r >> 1] & 0xFFFFu);
+        out |= ((row >> (15 - c)) & 1u) << (15 - r);
+    }
+    mask_t[(long long)t * TSG_BS + c] = (unsigned short)out;
+}
+
+int tsg_build_mask_t(tsg_context *ctx, tsg_tiled *mat)
+{
+    const int T = mat->numtile;
+    if (!mat->mask_t)
+        TSG_TRY(tsg_alloc(ctx, &mat->mask_t, (size_t)T * TSG_BS));
+    if (T > 0)
+    {
+        k_mask_transpose<<<tsg_blocks((long long)T * 16, 256), 256, 0, ctx->stream>>>(T, mat->mask, mat->mask_t);
+        TSG_LAUNCH_CHECK();
+    }
+    return TSG_OK;
+}
+
 int tsg_build_csc_view(tsg_context *ctx, tsg_tiled *mat)
 {
+    TSG_TRY(tsg_build_mask_t(ctx, mat));
     const int T = mat->numtile, tilen = mat->tilen;
     if (!mat->csc_tile_ptr)
     {
@@ -512,5 +546,5 @@ int tsg_colmajor_data_to_rowmajor(tsg_context *ctx, tsg_tiled *mat)
     mat->mask = mask;
     mat->tile_csr_Col = Col;
     mat->tile_csr_Value = Val;
-    return TSG_OK;
+    return tsg_build_mask_t(ctx, mat);
 }

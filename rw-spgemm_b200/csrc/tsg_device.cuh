@@ -31,6 +31,7 @@ struct ProdView
     const unsigned char *B_Ptr, *B_Colb;
     const double *B_Val;
     const unsigned short *B_mask;
+    const unsigned short *B_maskT;
     int tilenB;
     int *C_ptr, *C_col, *C_row, *C_tnnz;
     unsigned short *C_mask;
@@ -133,6 +134,144 @@ __device__ __forceinline__ int step1_row(const ProdView &P, int i, unsigned int 
         }
     }
     return out;
+}
+
+// forward declarations of helpers defined below
+__device__ __forceinline__ unsigned bool_row(unsigned ma, uint4 q0, uint4 q1);
+__device__ __forceinline__ int hw_excl_scan(unsigned hmask, int lane, int cnt, int &total);
+__device__ __forceinline__ int nnz_bin(int total);
+
+// ---------------------------------------------------------------------------
+// Fused step 1 (emit) + step 2 for one A tile row (warp).  The row's C tile
+// columns come from the window bitmap as in step1_row; when the window fits
+// one pass of S12_WORDS words and the row has at most S12_MAXT C tiles, the
+// bitmap's word-prefix popcounts give each B tile's C slot in O(1), and the
+// warp ORs the 16x16 boolean products of every (A tile, B tile) pair of the
+// row into per-slot row masks in shared memory (two B tiles at a time, one
+// per half-warp, lane = row), then writes masks, row offsets and tile counts.
+// No intersection is searched.  Returns 1 if the row was completed, 0 if it
+// needs the tile-schedule step 2 (C columns are emitted either way).
+// ---------------------------------------------------------------------------
+#define S12_WORDS 256
+#define S12_MAXT 128
+
+struct S12Smem
+{
+    unsigned bm[S12_WORDS];
+    unsigned short pre[S12_WORDS];
+    unsigned short acc[S12_MAXT][16];
+};
+
+__device__ __forceinline__ int step12_row(const ProdView &P, int i, S12Smem &sm, int lane, int *s_bins)
+{
+    const int a0 = P.A_ptr[i], a1 = P.A_ptr[i + 1];
+    int lo = INT_MAX, hi = -1;
+    for (int pa = a0 + lane; pa < a1; pa += 32)
+    {
+        const int k = P.A_col[pa];
+        const int b0 = P.B_ptr[k], b1 = P.B_ptr[k + 1];
+        if (b1 > b0)
+        {
+            lo = min(lo, P.B_col[b0]);
+            hi = max(hi, P.B_col[b1 - 1]);
+        }
+    }
+    lo = __reduce_min_sync(TSG_FULL_MASK, lo);
+    hi = __reduce_max_sync(TSG_FULL_MASK, hi);
+    const int cbase = P.C_ptr[i];
+    const int ntiles = P.C_ptr[i + 1] - cbase;
+    if (hi < 0)
+        return 1;
+    const int c0 = lo & ~31;
+    const int nw = (hi - c0 + 32) >> 5;
+    if (nw > S12_WORDS || ntiles > S12_MAXT)
+        return 0; // wide row: the caller emits it with step1_row and runs step 2 per tile
+    for (int w = lane; w < nw; w += 32)
+        sm.bm[w] = 0;
+    __syncwarp();
+    for (int pa = a0; pa < a1; pa++)
+    {
+        const int k = P.A_col[pa];
+        const int b0 = P.B_ptr[k], b1 = P.B_ptr[k + 1];
+        for (int pb = b0 + lane; pb < b1; pb += 32)
+        {
+            const int j = P.B_col[pb] - c0;
+            atomicOr(&sm.bm[j >> 5], 1u << (j & 31));
+        }
+    }
+    __syncwarp();
+    // word prefix popcounts (exclusive) and the sorted C columns
+    int run = 0;
+    for (int wb = 0; wb < nw; wb += 32)
+    {
+        const int w = wb + lane;
+        unsigned bits = w < nw ? sm.bm[w] : 0u;
+        const int cnt = __popc(bits);
+        int incl = cnt;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1)
+        {
+            const int o = __shfl_up_sync(TSG_FULL_MASK, incl, d);
+            if (lane >= d)
+                incl += o;
+        }
+        int pos = run + incl - cnt;
+        if (w < nw)
+            sm.pre[w] = (unsigned short)pos;
+        while (bits)
+        {
+            const int b = __ffs(bits) - 1;
+            bits &= bits - 1;
+            P.C_col[cbase + pos] = c0 + (w << 5) + b;
+            P.C_row[cbase + pos] = i;
+            pos++;
+        }
+        run += __shfl_sync(TSG_FULL_MASK, incl, 31);
+    }
+    const int r = lane & 15, half = lane >> 4;
+    for (int q = half; q < ntiles; q += 2)
+        sm.acc[q][r] = 0;
+    __syncwarp();
+    // OR the boolean products of all (A tile, B tile) pairs of the row
+    for (int pa = a0; pa < a1; pa++)
+    {
+        const int k = P.A_col[pa];
+        const unsigned ma = P.A_mask[(long long)pa * TSG_BS + r];
+        const int b0 = P.B_ptr[k], b1 = P.B_ptr[k + 1];
+        for (int pb = b0 + half; pb < b1; pb += 2)
+        {
+            const int j = P.B_col[pb] - c0;
+            const int slot = sm.pre[j >> 5] + __popc(sm.bm[j >> 5] & ((1u << (j & 31)) - 1u));
+            const uint4 *mb = reinterpret_cast<const uint4 *>(P.B_mask + (long long)pb * TSG_BS);
+            const uint4 q0 = __ldg(mb), q1 = __ldg(mb + 1);
+            if (ma)
+                sm.acc[slot][r] |= (unsigned short)bool_row(ma, q0, q1);
+        }
+        __syncwarp();
+    }
+    // row offsets, masks and counts, one C tile per half-warp
+    const unsigned hmask = TSG_HW_MASK(threadIdx.x);
+    for (int q0 = 0; q0 < ntiles; q0 += 2)
+    {
+        const int q = q0 + half;
+        const unsigned accm = q < ntiles ? sm.acc[q][r] : 0u;
+        int total;
+        const int excl = hw_excl_scan(hmask, r, __popc(accm), total);
+        if (q < ntiles)
+        {
+            const long long t = cbase + q;
+            P.C_mask[t * TSG_BS + r] = (unsigned short)accm;
+            P.C_Ptr[t * TSG_BS + r] = (unsigned char)excl;
+            if (r == 0)
+            {
+                P.C_tnnz[t] = total;
+                if (total > 0 && s_bins)
+                    atomicAdd(&s_bins[nnz_bin(total)], 1);
+            }
+        }
+    }
+    __syncwarp();
+    return 1;
 }
 
 // ---------------------------------------------------------------------------
@@ -504,6 +643,104 @@ __device__ __forceinline__ void step3_rows_item(const ProdView &P, long long ite
         }
         t = seg_end;
     }
+}
+
+// ---------------------------------------------------------------------------
+// Element schedule for step 3: one warp per C tile, lane = one nonzero
+// (r, c) of the tile (from step 2's masks), for chunks of 32 nonzeros.  For
+// every matched tile pair (A tile (i,k), B tile (k,j)), the A columns that
+// meet B rows with an entry in column c are maskA[r] & maskT_B[c]; each such
+// ca contributes A(r,ca) * B(ca,c), both fetched by popcount rank.  The
+// accumulator lives in a register, the order is k ascending then ca
+// ascending -- the oracle's order for row-sorted inputs -- and the results
+// are stored with coalesced writes.  The matched pairs are found once per
+// tile (half-warp intersection, identical in both halves) and cached in
+// shared memory for the chunks of dense tiles.
+// ---------------------------------------------------------------------------
+#define S3E_PAIRS 96
+
+__device__ __forceinline__ double elem_pair(const ProdView &P, int posA, int posB, int r, int c, double acc)
+{
+    const unsigned ma = P.A_mask[(long long)posA * TSG_BS + r];
+    unsigned tb = ma & P.B_maskT[(long long)posB * TSG_BS + c];
+    if (tb)
+    {
+        const double *av = P.A_Val + P.A_tnnz[posA] + P.A_Ptr[(long long)posA * TSG_BS + r];
+        const double *bv = P.B_Val + P.B_tnnz[posB];
+        const unsigned short *bm = P.B_mask + (long long)posB * TSG_BS;
+        const unsigned char *bp = P.B_Ptr + (long long)posB * TSG_BS;
+        do
+        {
+            const int bit = 31 - __clz(tb); // bit 15-ca: highest first = ca ascending
+            const int ca = 15 - bit;
+            const double a = av[__popc(ma >> (bit + 1))];
+            const double b = bv[bp[ca] + __popc((unsigned)bm[ca] >> (16 - c))];
+            acc = __dadd_rn(acc, __dmul_rn(a, b));
+            tb ^= 1u << bit;
+        } while (tb);
+    }
+    return acc;
+}
+
+// warp per C tile t; s_pairs: S3E_PAIRS int2 of this warp
+__device__ __forceinline__ void step3_elems_tile(const ProdView &P, int t, int2 *s_pairs)
+{
+    const int lane = threadIdx.x & 31, l16 = lane & 15;
+    const unsigned hmask = TSG_HW_MASK(threadIdx.x);
+    const int cb = P.C_tnnz[t], cn = P.C_tnnz[t + 1] - cb;
+    if (cn == 0)
+        return;
+    const int i = P.C_row[t], j = P.C_col[t];
+    const int abase = P.A_ptr[i], la = P.A_ptr[i + 1] - abase;
+    const int bbase = P.B_cptr[j], lb = P.B_cptr[j + 1] - bbase;
+    int np = 0;
+    intersect_tiles(hmask, l16, P.A_col, abase, la, P.B_crow, P.B_cpos, bbase, lb, [&](int posA, int posB) {
+        if (np < S3E_PAIRS && lane == 0)
+            s_pairs[np] = make_int2(posA, posB);
+        np++;
+    });
+    __syncwarp();
+    const int excl = P.C_Ptr[(long long)t * TSG_BS + l16];
+    const unsigned mrev = __brev((unsigned)P.C_mask[(long long)t * TSG_BS + l16]) >> 16;
+    for (int e0 = 0; e0 < cn; e0 += 32)
+    {
+        const int e = e0 + lane;
+        int r = 0;
+#pragma unroll
+        for (int s = 8; s >= 1; s >>= 1)
+        {
+            const int v = __shfl_sync(TSG_FULL_MASK, excl, r + s, 16);
+            if (v <= e)
+                r += s;
+        }
+        const unsigned mr = __shfl_sync(TSG_FULL_MASK, mrev, r, 16);
+        const int rank = e - __shfl_sync(TSG_FULL_MASK, excl, r, 16);
+        const bool valid = e < cn;
+        const int c = valid ? ((int)__fns(mr, 0, rank + 1) & 15) : 0;
+        double acc = 0.0;
+        if (np <= S3E_PAIRS)
+        {
+            for (int q = 0; q < np; q++)
+            {
+                const int2 pr = s_pairs[q];
+                if (valid)
+                    acc = elem_pair(P, pr.x, pr.y, r, c, acc);
+            }
+        }
+        else
+        {
+            intersect_tiles(hmask, l16, P.A_col, abase, la, P.B_crow, P.B_cpos, bbase, lb, [&](int posA, int posB) {
+                if (valid)
+                    acc = elem_pair(P, posA, posB, r, c, acc);
+            });
+        }
+        if (valid)
+        {
+            P.C_Colb[cb + e] = (unsigned char)c;
+            P.C_Val[cb + e] = acc;
+        }
+    }
+    __syncwarp();
 }
 
 // Supported (W, CAP) pairs of the row schedule; the dispatch macro expands

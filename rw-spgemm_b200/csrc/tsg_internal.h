@@ -23,6 +23,7 @@ struct tsg_context
     int sched;           // TSG_SCHED_TILES / TSG_SCHED_ROWS for steps 2-3
     int seg_tiles;       // row schedule: C tiles per work item (8 or 16)
     int acc_cap;         // row schedule: FP64 accumulator slots per half-warp
+    int fuse12;          // step-1 emit fused with step 2 for narrow tile rows
 };
 
 // Records a formatted message as the thread's last error and returns code.

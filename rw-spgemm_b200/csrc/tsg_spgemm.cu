@@ -28,6 +28,49 @@ __global__ void __launch_bounds__(S1_WARPS * 32) k_step1(ProdView P, int *__rest
         C_cnt[i] = cnt;
 }
 
+// fused step-1 emit + step 2 (warp per A tile row); wide rows are emitted by
+// step1_row and flagged for k_step2_wide
+__global__ void __launch_bounds__(256) k_step12(ProdView P, int *__restrict__ wide, int *__restrict__ bins)
+{
+    __shared__ S12Smem sm[8];
+    __shared__ int s_bins[4];
+    if (threadIdx.x < 4)
+        s_bins[threadIdx.x] = 0;
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int i = blockIdx.x * 8 + warp;
+    if (i < P.tilemA)
+    {
+        const int done = step12_row(P, i, sm[warp], lane, s_bins);
+        if (!done)
+        {
+            static_assert(sizeof(S12Smem) >= S1_WORDS * sizeof(unsigned), "bitmap scratch");
+            __syncwarp();
+            step1_row<true>(P, i, reinterpret_cast<unsigned *>(&sm[warp]), lane, nullptr);
+        }
+        if (lane == 0)
+            wide[i] = done ? 0 : 1;
+    }
+    __syncthreads();
+    if (threadIdx.x < 4 && s_bins[threadIdx.x])
+        atomicAdd(&bins[threadIdx.x], s_bins[threadIdx.x]);
+}
+
+// step 2 (tile schedule) for the C tiles of rows k_step12 left to it
+__global__ void __launch_bounds__(256) k_step2_wide(ProdView P, const int *__restrict__ wide, int *__restrict__ bins)
+{
+    __shared__ int s_bins[4];
+    if (threadIdx.x < 4)
+        s_bins[threadIdx.x] = 0;
+    __syncthreads();
+    const long long t = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 4;
+    if (t < P.numC && wide[P.C_row[t]])
+        step2_tile(P, (int)t, TSG_HW_MASK(threadIdx.x), threadIdx.x & 15, s_bins);
+    __syncthreads();
+    if (threadIdx.x < 4 && s_bins[threadIdx.x])
+        atomicAdd(&bins[threadIdx.x], s_bins[threadIdx.x]);
+}
+
 __global__ void __launch_bounds__(256) k_step2(ProdView P, int *__restrict__ bins)
 {
     __shared__ int s_bins[4];
@@ -57,6 +100,14 @@ __global__ void __launch_bounds__(S3_THREADS) k_step3(ProdView P)
     const long long t = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 4;
     if (t < P.numC)
         step3_tile(P, (int)t, hmask, lane, acc);
+}
+
+__global__ void __launch_bounds__(256) k_step3_elems(ProdView P)
+{
+    __shared__ int2 s_pairs[8][S3E_PAIRS];
+    const long long t = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (t < P.numC)
+        step3_elems_tile(P, (int)t, s_pairs[threadIdx.x >> 5]);
 }
 
 template <int W>
@@ -128,6 +179,7 @@ static ProdView make_view(const tsg_tiled *A, const tsg_tiled *B, tsg_tiled *C)
     P.B_Colb = B->tile_csr_Col;
     P.B_Val = B->tile_csr_Value;
     P.B_mask = B->mask;
+    P.B_maskT = B->mask_t;
     P.tilenB = B->tilen;
     P.C_ptr = C->tile_ptr;
     P.C_col = C->tile_columnidx;
@@ -188,6 +240,14 @@ static int launch_step3(tsg_context *ctx, const ProdView &P)
 #undef TSG_DISPATCH3
         return tsg_set_error(TSG_ERR_INVALID, "unsupported row schedule (%d, %d)", W, cap);
     }
+    if (ctx->sched == TSG_SCHED_ELEMS)
+    {
+        if (!P.B_maskT)
+            return tsg_set_error(TSG_ERR_INVALID, "element schedule needs B's column masks (mask_t)");
+        k_step3_elems<<<tsg_blocks((long long)P.numC * 32, 256), 256, 0, ctx->stream>>>(P);
+        TSG_LAUNCH_CHECK();
+        return TSG_OK;
+    }
     k_step3<<<tsg_blocks((long long)P.numC * 16, S3_THREADS), S3_THREADS, 0, ctx->stream>>>(P);
     TSG_LAUNCH_CHECK();
     return TSG_OK;
@@ -232,27 +292,46 @@ extern "C" int tsg_spgemm(tsg_context *ctx, const tsg_tiled *A, const tsg_tiled 
     C->numtile = (int)numC;
     TSG_TRY(tsg_alloc(ctx, &C->tile_columnidx, (size_t)numC));
     TSG_TRY(tsg_alloc(ctx, &C->tile_rowidx, (size_t)numC));
-    if (numC > 0)
-    {
-        ProdView P = make_view(A, B, C);
-        k_step1<true><<<tsg_blocks(tilem, S1_WARPS), S1_WARPS * 32, 0, st>>>(P, nullptr, nullptr);
-        TSG_LAUNCH_CHECK();
-    }
-    if (timing)
-        TSG_CUDA(cudaEventRecord(ctx->ev[1], st));
-
-    // step 2: symbolic
     TSG_TRY(tsg_alloc(ctx, &C->mask, (size_t)numC * TSG_BS));
     TSG_TRY(tsg_alloc(ctx, &C->tile_csr_Ptr, (size_t)numC * TSG_BS));
     TSG_TRY(tsg_alloc(ctx, &C->tile_nnz, (size_t)numC + 1));
     long long nnzC = 0;
+    const bool fused = ctx->fuse12 && ctx->sched != TSG_SCHED_ROWS;
+    int *d_wide = nullptr;
     if (numC > 0)
     {
-        TSG_TRY(launch_step2(ctx, make_view(A, B, C), d_bins));
+        ProdView P = make_view(A, B, C);
+        if (fused)
+        {
+            TSG_TRY(tsg_alloc(ctx, &d_wide, (size_t)tilem));
+            k_step12<<<tsg_blocks(tilem, 8), 256, 0, st>>>(P, d_wide, d_bins);
+            TSG_LAUNCH_CHECK();
+        }
+        else
+        {
+            k_step1<true><<<tsg_blocks(tilem, S1_WARPS), S1_WARPS * 32, 0, st>>>(P, nullptr, nullptr);
+            TSG_LAUNCH_CHECK();
+        }
+    }
+    if (timing)
+        TSG_CUDA(cudaEventRecord(ctx->ev[1], st));
+
+    // step 2: symbolic (rows the fused kernel left, or all tiles)
+    if (numC > 0)
+    {
+        ProdView P = make_view(A, B, C);
+        if (fused)
+        {
+            k_step2_wide<<<tsg_blocks(numC * 16, 256), 256, 0, st>>>(P, d_wide, d_bins);
+            TSG_LAUNCH_CHECK();
+        }
+        else
+            TSG_TRY(launch_step2(ctx, P, d_bins));
         TSG_TRY(tsg_scan_counts(ctx, C->tile_nnz, C->tile_nnz, numC, &nnzC));
     }
     else
         TSG_CUDA(cudaMemsetAsync(C->tile_nnz, 0, sizeof(int), st));
+    tsg_release(ctx, d_wide);
     C->nnz = (int)nnzC;
     if (timing)
         TSG_CUDA(cudaEventRecord(ctx->ev[2], st));

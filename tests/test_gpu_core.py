@@ -120,14 +120,17 @@ def _handle_product(tsg, ctx, matA, matB):
     return A, B, C, info
 
 
-SCHEDULES = [("tiles", 8, 512), ("rows", 8, 256), ("rows", 8, 512), ("rows", 16, 1024), ("rows", 16, 2048)]
+SCHEDULES = [("tiles", 8, 512, True), ("elems", 8, 512, True), ("elems", 8, 512, False), ("tiles", 8, 512, False),
+             ("rows", 8, 256, False), ("rows", 16, 1024, False), ("rows", 32, 2048, False)]
 
 
-@pytest.fixture(params=SCHEDULES, ids=lambda p: f"{p[0]}{p[1]}-{p[2]}")
+@pytest.fixture(params=SCHEDULES, ids=lambda p: f"{p[0]}{p[1]}-{p[2]}{'-fused' if p[3] else ''}")
 def sched(request, ctx):
-    ctx.set_schedule(*request.param)
+    ctx.set_schedule(*request.param[:3])
+    ctx.set_fusion(request.param[3])
     yield request.param
-    ctx.set_schedule("rows", 8, 512)
+    ctx.set_schedule("elems", 8, 512)
+    ctx.set_fusion(True)
 
 
 @pytest.mark.parametrize("seed", range(6))
@@ -229,3 +232,14 @@ def test_malformed_csr_is_rejected(tsg, ctx):
         with pytest.raises(tsg.TsgError) as e:
             tsg.csr_to_tiled(ctx, 2, 8, rp, ci, v, tsg.TSG_TILED_PACKED_COL)
         assert e.value.status == -4
+
+
+def test_two_phase_end_to_end_into_caller_buffers(tsg, ctx, oracle, gen):
+    out = tsg.HostResultBuffers(10, 10)
+    for matA, matB in [(gen.laplacian_2d(60), None), (gen.random_poisson(200, 150, 5.0, seed=3),
+                                                       gen.random_poisson(150, 90, 5.0, seed=4))]:
+        C, info = tsg.spgemm_csr_host_into(ctx, matA, matB, out)
+        G = oracle.gustavson(matA, matA if matB is None else matB)
+        np.testing.assert_array_equal(C[2], G[2])
+        np.testing.assert_array_equal(C[3], G[3])
+        assert_values(C[4], G[4])
