@@ -325,6 +325,27 @@ int tsg_spgemm(tsg_context *ctx, const tsg_tiled *A, const tsg_tiled *B,
 int tsg_tiled_to_csr(tsg_context *ctx, const tsg_tiled *C,
                      int *d_rowptr, int *d_colidx, double *d_val);
 
+/* Tiles -> CSR with no allocation at all (no counterpart in the reference;
+ * its tile2csr, src/tile2csr.h:71, is a host conversion).  Same outputs as
+ * tsg_tiled_to_csr.  The row-pointer scan keeps its block sums in a fixed
+ * file-scope device array of 4096 entries (32 KB per device) instead of
+ * taking them from the context's memory pool, so C may have at most
+ * 4096 * 8192 = 33,554,432 rows; larger C returns TSG_ERR_INVALID before
+ * anything is launched.  For callers that must not allocate here: those that
+ * have handed all device memory to their own fixed arena or admission budget
+ * (the pool would grow behind it), and those on a path where a pool growth,
+ * which can synchronise the device, is not allowed.
+ *   - Nothing in the scratch has to start at zero: each call writes every
+ *     block sum it reads.
+ *   - The scratch is one per device, shared by all contexts, streams and
+ *     threads: calls that may overlap on one device race on it; order them
+ *     (same stream, or an event between them).
+ *   - The first call on a device looks up the scratch address
+ *     (cudaGetSymbolAddress, with that device current); make that first call
+ *     before any stream capture. */
+int tsg_tiled_to_csr_noalloc(tsg_context *ctx, const tsg_tiled *C,
+                             int *d_rowptr, int *d_colidx, double *d_val);
+
 /* Copy a device tiled matrix into host arrays of an SMatrix (malloc'd,
  * caller frees).  colmajor != 0 writes B's reference layout (column-major
  * tile data, plain Col bytes, csc_tile_ptr/csc_tile_rowidx). */
