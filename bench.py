@@ -385,6 +385,50 @@ def run_selector(args, tsg, gen, ctx):
     return res
 
 
+def run_orderings(args, tsg, gen, ctx, reps=3):
+    """27-point stencil on a 64^3 grid after a seeded random symmetric
+    permutation; every GPU ordering is applied (permutation + CSR permute timed
+    on the device), then C = A*A (steps 1-3, min of reps): tile count of C and
+    run time per ordering."""
+    import torch
+    dev = torch.device("cuda", torch.cuda.current_device())
+    base = gen.stencil_27pt_3d(64, seed=0)
+    mat = gen.permute_symmetric(base, gen.random_symmetric_permutation(base[0], 7))
+    m, n, rp, ci, v = mat
+    d_rp, d_ci, d_v = (torch.from_numpy(x).to(dev) for x in (rp, ci, v))
+    prods = tsg.count_products(ctx, d_ci, d_rp)
+    out = {"workload": "27-point stencil 64^3 (n=262,144), seeded random symmetric permutation, then each ordering; "
+                       "C = A*A", "products": int(prods), "per_ordering": {}}
+    ctx.set_timing(True)
+    for name in ["original", "rcm", "degree", "gray", "random"]:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        best_order = float("inf")
+        for _ in range(2):
+            e0.record()
+            perm = tsg.order(ctx, name, m, n, d_rp, d_ci, seed=1)
+            inv = torch.empty_like(perm)
+            inv[perm.long()] = torch.arange(m, dtype=torch.int32, device=dev)
+            prp, pci, pv = tsg.permute_csr(ctx, m, n, d_rp, d_ci, d_v, perm, inv)
+            e1.record()
+            e1.synchronize()
+            best_order = min(best_order, e0.elapsed_time(e1))
+        T = tsg.csr_to_tiled(ctx, m, n, prp, pci, pv, tsg.TSG_TILED_CSC_VIEW)
+        best, info = float("inf"), None
+        for _ in range(reps):
+            C, inf = tsg.spgemm(ctx, T, T)
+            if inf["ms_total"] < best:
+                best, info = inf["ms_total"], inf
+            C.free()
+        out["per_ordering"][name] = {"ordering_ms": round(best_order, 3), "tiles_A": int(T.numtile),
+                                     "tiles_C": int(info["numtile_C"]), "nnz_C": int(info["nnz_C"]),
+                                     "ms_steps_1_3": round(best, 4),
+                                     "gflops": round(2.0 * prods / (best * 1e-3) / 1e9, 2)}
+        T.free()
+        del prp, pci, pv
+    ctx.set_timing(False)
+    return out
+
+
 def res_name(sel, idx):
     o, a = sel.CONFIGS[idx]
     return f"{o}/{a[0]}-{a[1]}-{a[2]}"
@@ -404,7 +448,8 @@ def run_ours(args, tsg, gen, world, rank, local):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
     mat = workload_matrix(gen)
     m, n, rp, ci, v = mat
-    stream = torch.cuda.current_stream(dev)
+    stream = torch.cuda.Stream(dev)  # one non-default stream for torch and the library
+    torch.cuda.set_stream(stream)
     ctx = tsg.Context(local, stream=stream.cuda_stream)
     ctx.set_schedule(args.sched, args.seg, args.cap)
     d_rp = torch.from_numpy(rp).to(dev)
@@ -492,6 +537,7 @@ def run_ours(args, tsg, gen, world, rank, local):
     if "served" in args.sections:
         served = run_served(args, tsg, gen, local)
     selector = run_selector(args, tsg, gen, ctx) if "selector" in args.sections else None
+    orderings = run_orderings(args, tsg, gen, ctx) if "orderings" in args.sections else None
     out = {
         "metric": METRIC, "value": round(value, 3), "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,
@@ -524,6 +570,8 @@ def run_ours(args, tsg, gen, world, rank, local):
         out["served"] = served
     if selector:
         out["selector"] = selector
+    if orderings:
+        out["orderings"] = orderings
     if rank == 0:
         print(json.dumps(out), flush=True)
     ctx.close()
@@ -541,7 +589,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--sched", default="elems", choices=["rows", "tiles", "elems"])
-    ap.add_argument("--sections", default="plain,batched,served",
+    ap.add_argument("--sections", default="plain,batched,served,orderings",
                     help="comma list: plain (always), batched, served, selector")
     ap.add_argument("--batch-count", type=int, default=512)
     ap.add_argument("--selector-samples", type=int, default=5000)

@@ -269,7 +269,9 @@ const char *tsg_last_error(void);
 
 int tsg_context_create(int device, tsg_context **ctx);
 int tsg_context_destroy(tsg_context *ctx);
-/* Use an existing cudaStream_t (passed as void*) for all work; NULL = own. */
+/* Use an existing cudaStream_t (passed as void*) for all work; NULL = the
+ * context's own stream again.  For the legacy default stream pass
+ * cudaStreamLegacy, not 0. */
 int tsg_context_set_stream(tsg_context *ctx, void *cuda_stream);
 /* Work schedule of steps 2 and 3 (results are bit-identical either way):
  * TSG_SCHED_TILES  one half-warp per C tile, intersecting A's tile row with

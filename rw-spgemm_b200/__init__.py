@@ -260,6 +260,9 @@ def tilespgemm(tilesA: dict, tilesB: dict, nnzCub: int = 0) -> tuple[dict, dict]
 # ---------------------------------------------------------------------------
 # handle API (device-resident)
 # ---------------------------------------------------------------------------
+CUDA_STREAM_LEGACY = 0x1
+
+
 class Context:
     """tsg_context on one device.  Work goes to ``stream`` (a cudaStream_t as
     int) when given, else to torch's current stream on that device when torch
@@ -276,7 +279,9 @@ class Context:
             except Exception:
                 stream = None
         if stream is not None:
-            self.set_stream(stream)
+            # torch reports its legacy default stream as 0, which the C API
+            # reads as "own stream": name it explicitly (cudaStreamLegacy)
+            self.set_stream(stream if int(stream) != 0 else CUDA_STREAM_LEGACY)
         if timing:
             self.set_timing(True)
 

@@ -21,13 +21,14 @@ output entry is accumulated in a fixed order independent of batching.
 from __future__ import annotations
 
 import collections
+import ctypes
 import threading
 import time
 from concurrent.futures import Future
 
 import numpy as np
 
-from . import (TSG_TILED_CSC_VIEW, Batch, Context, csr_host_to_tiled, lib, product_bounds, tiled_to_csr_host)
+from . import TSG_TILED_CSC_VIEW, Batch, Context, check, csr_host_to_tiled, lib, product_bounds
 
 
 class Job:
@@ -231,12 +232,27 @@ class SpGEMMServer:
         return True
 
     def _finish(self, slot):
+        """Converts every product of the finished batch to CSR on the device
+        (all conversions queued, one synchronisation), then copies each result
+        to host arrays and completes its future."""
+        import torch
         slot.batch.sync()
+        dev = torch.device("cuda", self.device)
+        pending = []
         for p, job in enumerate(slot.jobs):
             C = slot.batch.product(p)
-            res = tiled_to_csr_host(slot.ctx, C, pinned=True)
+            m, nnz = C.s.m, C.s.nnz
+            rp = torch.empty(m + 1, dtype=torch.int32, device=dev)
+            ci = torch.empty(max(nnz, 1), dtype=torch.int32, device=dev)
+            v = torch.empty(max(nnz, 1), dtype=torch.float64, device=dev)
+            check(lib().tsg_tiled_to_csr(slot.ctx.handle, ctypes.byref(C.s), ctypes.c_void_p(rp.data_ptr()),
+                                         ctypes.c_void_p(ci.data_ptr()), ctypes.c_void_p(v.data_ptr())))
+            pending.append((job, C.s.m, C.s.n, nnz, rp, ci, v))
+        slot.ctx.synchronize()
+        for job, m, n, nnz, rp, ci, v in pending:
+            res = (m, n, rp.cpu().numpy(), ci[:nnz].cpu().numpy(), v[:nnz].cpu().numpy())
             job.t_done = time.perf_counter()
-            job.result_nnz = C.s.nnz
+            job.result_nnz = nnz
             job.future.set_result(res)
             self.done.append(job)
         slot.batch.close()
