@@ -553,7 +553,7 @@ def run_ours(args, tsg, gen, world, rank, local):
         "hbm_frac": round(comp / (ms_per_step * 1e-3) / 1e9 / peak, 4),
         "compulsory_bytes": comp,
         "step_ms": {k: round(float(np.mean([i[k] for i in infos])), 4) for k in ("ms_step1", "ms_step2", "ms_step3")},
-        "roofline": {"bound": "hbm", "kernel": {"tiles": "k_step3", "elems": "k_step3_elems", "rows": "k_step3_rows"}[args.sched] + " (numeric)", "achieved": round(achieved, 2),
+        "roofline": {"bound": "hbm", "kernel": {"tiles": "k_step3", "elems": "k_step3_elems", "rows": "k_step3_rows", "spa": "k_step3_spa"}[args.sched] + " (numeric)", "achieved": round(achieved, 2),
                      "peak": peak, "peak_source": peak_src, "unit": "GB/s", "frac": round(achieved / peak, 4),
                      "algorithmic_bytes": alg3, "traffic": profiled_traffic("stencil27_64", args.sched)},
         "e2e": {"value": round(2.0 * prods / (e2e_t * 1e-3) / 1e9, 3), "unit": "GFLOP/s", "ms": round(e2e_t, 3),
@@ -588,7 +588,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
-    ap.add_argument("--sched", default="elems", choices=["rows", "tiles", "elems"])
+    ap.add_argument("--sched", default="elems", choices=["rows", "tiles", "elems", "spa"])
     ap.add_argument("--sections", default="plain,batched,served,orderings",
                     help="comma list: plain (always), batched, served, selector")
     ap.add_argument("--batch-count", type=int, default=512)

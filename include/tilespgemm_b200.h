@@ -231,6 +231,9 @@ typedef struct tsg_context tsg_context;
 /* Device-resident tiled matrix.  Tile data is stored in row-major tile order;
  * the optional column view lists, per tile column, the tile rows
  * (csc_tile_rowidx) and the row-major tile index (csc_tile_pos) of each tile.
+ * Matrices converted for the B role (TSG_TILED_CSC_VIEW) also carry a row
+ * view: the same matrix as scalar CSR (row_ptr[m+1], row_col[nnz],
+ * row_val[nnz]), read by the numeric step of TSG_SCHED_SPA.
  * All pointers are device pointers owned by the library. */
 typedef struct
 {
@@ -249,6 +252,9 @@ typedef struct
     int *csc_tile_rowidx;
     int *csc_tile_pos;
     unsigned short *mask_t; /* B operand: per tile column masks, bit (15-row) */
+    int *row_ptr;           /* B operand: row view (scalar CSR)             */
+    int *row_col;
+    double *row_val;
     void *_alloc;           /* internal: non-NULL marks a borrowed view      */
 } tsg_tiled;
 
@@ -288,6 +294,12 @@ int tsg_context_set_stream(tsg_context *ctx, void *cuda_stream);
  *                  through A's row masks and B's column masks (register
  *                  accumulator, no shared-memory scatter). */
 #define TSG_SCHED_ELEMS 2
+/* TSG_SCHED_SPA    step 2 as TILES; step 3 as a row Gustavson over B's row
+ *                  view (scalar CSR): a CTA per run of C tiles of one tile
+ *                  row, a warp per C row, products accumulated in shared
+ *                  memory in C's tiled layout.  B without a row view runs
+ *                  TSG_SCHED_TILES. */
+#define TSG_SCHED_SPA 3
 int tsg_context_set_schedule(tsg_context *ctx, int schedule, int seg_tiles, int acc_cap);
 /* 1 (default): step-1 emit and step 2 run as one row-wise pass for tile rows
  * with at most 128 C tiles (others fall back to step 2 per tile); 0: separate

@@ -59,7 +59,9 @@ class TsgTiled(ctypes.Structure):
         ("tile_nnz", ctypes.c_void_p), ("tile_csr_Ptr", ctypes.c_void_p), ("tile_csr_Col", ctypes.c_void_p),
         ("tile_csr_Value", ctypes.c_void_p), ("mask", ctypes.c_void_p),
         ("csc_tile_ptr", ctypes.c_void_p), ("csc_tile_rowidx", ctypes.c_void_p), ("csc_tile_pos", ctypes.c_void_p),
-        ("mask_t", ctypes.c_void_p), ("_alloc", ctypes.c_void_p),
+        ("mask_t", ctypes.c_void_p),
+        ("row_ptr", ctypes.c_void_p), ("row_col", ctypes.c_void_p), ("row_val", ctypes.c_void_p),
+        ("_alloc", ctypes.c_void_p),
     ]
 
 
@@ -294,7 +296,7 @@ class Context:
     def set_schedule(self, schedule: str = "rows", seg_tiles: int = 8, acc_cap: int = 512):
         """'tiles' (half-warp per C tile, intersection) or 'rows' (half-warp per
         run of seg_tiles C tiles of one tile row, acc_cap FP64 slots)."""
-        check(lib().tsg_context_set_schedule(self.handle, {"tiles": 0, "rows": 1, "elems": 2}[schedule], seg_tiles,
+        check(lib().tsg_context_set_schedule(self.handle, {"tiles": 0, "rows": 1, "elems": 2, "spa": 3}[schedule], seg_tiles,
                                              acc_cap))
 
     def set_fusion(self, on: bool):

@@ -116,7 +116,8 @@ extern "C" int tsg_context_set_schedule(tsg_context *ctx, int schedule, int seg_
 {
     if (!ctx)
         return tsg_set_error(TSG_ERR_INVALID, "null context");
-    if (schedule != TSG_SCHED_TILES && schedule != TSG_SCHED_ROWS && schedule != TSG_SCHED_ELEMS)
+    if (schedule != TSG_SCHED_TILES && schedule != TSG_SCHED_ROWS && schedule != TSG_SCHED_ELEMS &&
+        schedule != TSG_SCHED_SPA)
         return tsg_set_error(TSG_ERR_INVALID, "unknown schedule %d", schedule);
     if (schedule == TSG_SCHED_ROWS)
     {
@@ -191,6 +192,9 @@ extern "C" int tsg_tiled_free(tsg_context *ctx, tsg_tiled *t)
     tsg_release(ctx, t->csc_tile_rowidx);
     tsg_release(ctx, t->csc_tile_pos);
     tsg_release(ctx, t->mask_t);
+    tsg_release(ctx, t->row_ptr);
+    tsg_release(ctx, t->row_col);
+    tsg_release(ctx, t->row_val);
     memset(t, 0, sizeof(*t));
     return TSG_OK;
 }

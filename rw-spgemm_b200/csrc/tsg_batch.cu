@@ -591,6 +591,9 @@ extern "C" int tsg_batch_create(tsg_context *ctx, int count, const tsg_tiled *A,
         P.B_Val = B[p].tile_csr_Value;
         P.B_mask = B[p].mask;
         P.B_maskT = B[p].mask_t;
+        P.B_rptr = B[p].row_ptr;
+        P.B_rcol = B[p].row_col;
+        P.B_rval = B[p].row_val;
         P.tilenB = B[p].tilen;
         P.C_ptr = (int *)take(((size_t)A[p].tilem + 1) * 4);
         h.wide = (int *)take((size_t)A[p].tilem * 4);

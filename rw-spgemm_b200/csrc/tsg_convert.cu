@@ -263,9 +263,22 @@ int tsg_build_mask_t(tsg_context *ctx, tsg_tiled *mat)
     return TSG_OK;
 }
 
+// Row view (scalar CSR of the matrix), from its tiles.
+int tsg_build_row_view(tsg_context *ctx, tsg_tiled *mat)
+{
+    if (!mat->row_ptr)
+    {
+        TSG_TRY(tsg_alloc(ctx, &mat->row_ptr, (size_t)mat->m + 1));
+        TSG_TRY(tsg_alloc(ctx, &mat->row_col, (size_t)mat->nnz));
+        TSG_TRY(tsg_alloc(ctx, &mat->row_val, (size_t)mat->nnz));
+    }
+    return tsg_tiled_to_csr(ctx, mat, mat->row_ptr, mat->row_col, mat->row_val);
+}
+
 int tsg_build_csc_view(tsg_context *ctx, tsg_tiled *mat)
 {
     TSG_TRY(tsg_build_mask_t(ctx, mat));
+    TSG_TRY(tsg_build_row_view(ctx, mat));
     const int T = mat->numtile, tilen = mat->tilen;
     if (!mat->csc_tile_ptr)
     {
@@ -546,5 +559,6 @@ int tsg_colmajor_data_to_rowmajor(tsg_context *ctx, tsg_tiled *mat)
     mat->mask = mask;
     mat->tile_csr_Col = Col;
     mat->tile_csr_Value = Val;
-    return tsg_build_mask_t(ctx, mat);
+    TSG_TRY(tsg_build_mask_t(ctx, mat));
+    return tsg_build_row_view(ctx, mat);
 }

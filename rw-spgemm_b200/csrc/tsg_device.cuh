@@ -32,6 +32,8 @@ struct ProdView
     const double *B_Val;
     const unsigned short *B_mask;
     const unsigned short *B_maskT;
+    const int *B_rptr, *B_rcol; // row view of B (scalar CSR), may be null
+    const double *B_rval;
     int tilenB;
     int *C_ptr, *C_col, *C_row, *C_tnnz;
     unsigned short *C_mask;
@@ -232,20 +234,40 @@ __device__ __forceinline__ int step12_row(const ProdView &P, int i, S12Smem &sm,
     for (int q = half; q < ntiles; q += 2)
         sm.acc[q][r] = 0;
     __syncwarp();
-    // OR the boolean products of all (A tile, B tile) pairs of the row
+    // OR the boolean products of all (A tile, B tile) pairs of the row: unit
+    // (row r, B tile) ORs the B rows its A row meets -- one 16-bit load per
+    // set bit of a sparse A row, two 16-byte loads for a dense one
     for (int pa = a0; pa < a1; pa++)
     {
         const int k = P.A_col[pa];
         const unsigned ma = P.A_mask[(long long)pa * TSG_BS + r];
         const int b0 = P.B_ptr[k], b1 = P.B_ptr[k + 1];
-        for (int pb = b0 + half; pb < b1; pb += 2)
+        if (ma)
         {
-            const int j = P.B_col[pb] - c0;
-            const int slot = sm.pre[j >> 5] + __popc(sm.bm[j >> 5] & ((1u << (j & 31)) - 1u));
-            const uint4 *mb = reinterpret_cast<const uint4 *>(P.B_mask + (long long)pb * TSG_BS);
-            const uint4 q0 = __ldg(mb), q1 = __ldg(mb + 1);
-            if (ma)
-                sm.acc[slot][r] |= (unsigned short)bool_row(ma, q0, q1);
+            const bool dense_row = __popc(ma) > 4;
+            for (int pb = b0 + half; pb < b1; pb += 2)
+            {
+                const int j = P.B_col[pb] - c0;
+                const int slot = sm.pre[j >> 5] + __popc(sm.bm[j >> 5] & ((1u << (j & 31)) - 1u));
+                const unsigned short *mbk = P.B_mask + (long long)pb * TSG_BS;
+                unsigned acc = 0;
+                if (dense_row)
+                {
+                    const uint4 *mb = reinterpret_cast<const uint4 *>(mbk);
+                    acc = bool_row(ma, __ldg(mb), __ldg(mb + 1));
+                }
+                else
+                {
+                    unsigned bits = ma;
+                    do
+                    {
+                        const int bit = 31 - __clz(bits);
+                        bits ^= 1u << bit;
+                        acc |= __ldg(mbk + (15 - bit));
+                    } while (bits);
+                }
+                sm.acc[slot][r] |= (unsigned short)acc;
+            }
         }
         __syncwarp();
     }
@@ -400,9 +422,22 @@ __device__ __forceinline__ void step2_tile(const ProdView &P, int t, unsigned hm
     unsigned acc = 0;
     intersect_tiles(hmask, lane, P.A_col, abase, la, P.B_crow, P.B_cpos, bbase, lb, [&](int posA, int posB) {
         const unsigned ma = P.A_mask[(long long)posA * TSG_BS + lane];
-        const uint4 *mb = reinterpret_cast<const uint4 *>(P.B_mask + (long long)posB * TSG_BS);
-        const uint4 q0 = __ldg(mb), q1 = __ldg(mb + 1);
-        acc |= bool_row(ma, q0, q1);
+        const unsigned short *mbk = P.B_mask + (long long)posB * TSG_BS;
+        if (__popc(ma) > 4)
+        {
+            const uint4 *mb = reinterpret_cast<const uint4 *>(mbk);
+            acc |= bool_row(ma, __ldg(mb), __ldg(mb + 1));
+        }
+        else
+        {
+            unsigned bits = ma;
+            while (bits)
+            {
+                const int bit = 31 - __clz(bits);
+                bits ^= 1u << bit;
+                acc |= __ldg(mbk + (15 - bit));
+            }
+        }
     });
     step2_store(P, t, hmask, lane, acc, s_bins);
 }
@@ -643,6 +678,202 @@ __device__ __forceinline__ void step3_rows_item(const ProdView &P, long long ite
         }
         t = seg_end;
     }
+}
+
+// ---------------------------------------------------------------------------
+// Numeric step, SPA schedule (row Gustavson over B's row view).  One CTA of
+// SPA_WARPS warps owns a segment of consecutive C tiles of one tile row I
+// (at most SPA_CAP values, SPA_SEGT tiles, a tile-column window of SPA_WIN);
+// warp r owns C row 16 I + r.  The segment's values are accumulated in shared
+// memory in C's own output layout: the slot of C(r, c) is the tile's value
+// offset + its row-r offset + the popcount of the row mask left of c, the
+// tile found through a window map.  Warp r walks A's row r through the row's
+// tiles in column order; for every A(r, k) it streams B's row k (scalar CSR:
+// coalesced column and value loads, the next row's first 32 entries
+// prefetched) and each lane adds a * b into the slot of its entry's column.
+// A's entries of one row are applied one after another (warp barrier between
+// them), so every C entry sums its products in k order -- the reference's
+// order -- with multiply and add rounded separately.
+// ---------------------------------------------------------------------------
+#define SPA_WARPS 16
+#define SPA_THREADS (SPA_WARPS * 32)
+#define SPA_CAP 4096
+#define SPA_SEGT 256
+#define SPA_WIN 2048
+#define SPA_STAGE 64
+
+struct SpaStage
+{
+    int bs[SPA_STAGE], be[SPA_STAGE];
+    double a[SPA_STAGE];
+};
+
+struct SpaSmem
+{
+    double acc[SPA_CAP];
+    unsigned cm[SPA_SEGT * TSG_BS]; // (row's first slot << 16) | C row mask
+    unsigned short map[SPA_WIN];    // tile column - J0 -> segment tile, 0xFFFF none
+    SpaStage stage[SPA_WARPS];
+};
+
+__device__ __forceinline__ void spa_add(SpaSmem &S, int r, int J0, int J1, int col, double a, double b)
+{
+    const int J = col >> 4;
+    if (J < J0 || J >= J1 || J - J0 >= SPA_WIN)
+        return;
+    const int slot = S.map[J - J0];
+    if (slot >= SPA_SEGT)
+        return;
+    const unsigned cmw = S.cm[slot * TSG_BS + r];
+    const int pos = (int)(cmw >> 16) + __popc((cmw & 0xFFFFu) >> (16 - (col & 15)));
+    if (pos < SPA_CAP)
+        S.acc[pos] = __dadd_rn(S.acc[pos], __dmul_rn(a, b));
+}
+
+// The CTA computes C tiles [t0, t1) (one tile row, limits as above).
+__device__ __forceinline__ void step3_spa_segment(const ProdView &P, SpaSmem &S, int t0, int t1)
+{
+    const int tid = threadIdx.x, lane = tid & 31, r = tid >> 5;
+    const int I = P.C_row[t0];
+    const int J0 = P.C_col[t0], J1 = P.C_col[t1 - 1] + 1;
+    const int base0 = P.C_tnnz[t0], cn = min(P.C_tnnz[t1] - base0, SPA_CAP);
+    const int nt = min(t1 - t0, SPA_SEGT);
+    const int win = min(J1 - J0, SPA_WIN);
+    __syncthreads();
+    for (int q = tid; q < cn; q += SPA_THREADS)
+        S.acc[q] = 0.0;
+    for (int q = tid; q < win; q += SPA_THREADS)
+        S.map[q] = 0xFFFF;
+    __syncthreads();
+    for (int u = tid; u < nt * TSG_BS; u += SPA_THREADS)
+    {
+        const int jl = u >> 4, rr = u & 15;
+        const long long tt = (long long)(t0 + jl) * TSG_BS + rr;
+        const unsigned b = (unsigned)(P.C_tnnz[t0 + jl] - base0 + P.C_Ptr[tt]);
+        S.cm[u] = (b << 16) | P.C_mask[tt];
+        if (rr == 0)
+        {
+            const int w = P.C_col[t0 + jl] - J0;
+            if (w < win)
+                S.map[w] = (unsigned short)jl;
+        }
+    }
+    __syncthreads();
+    SpaStage &G = S.stage[r];
+    const int pa_beg = P.A_ptr[I], pa_end = P.A_ptr[I + 1];
+    for (int g = pa_beg; g < pa_end; g += 32)
+    {
+        const int pa = g + lane;
+        unsigned mr = 0;
+        int st = 0, kb = 0;
+        if (pa < pa_end)
+        {
+            mr = P.A_mask[(long long)pa * TSG_BS + r];
+            st = P.A_tnnz[pa] + P.A_Ptr[(long long)pa * TSG_BS + r];
+            kb = P.A_col[pa] * TSG_BS;
+        }
+        const int cnt = __popc(mr);
+        int incl = cnt;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1)
+        {
+            const int o = __shfl_up_sync(TSG_FULL_MASK, incl, d);
+            if (lane >= d)
+                incl += o;
+        }
+        const int total = __shfl_sync(TSG_FULL_MASK, incl, 31);
+        for (int base = 0; base < total; base += SPA_STAGE)
+        {
+            __syncwarp();
+            // stage A(r, k) entries [base, base + SPA_STAGE) of this group in
+            // column order: B row bounds and the A value
+            unsigned bits = mr;
+            for (int x = 0; x < cnt; x++)
+            {
+                const int bit = 31 - __clz(bits);
+                bits ^= 1u << bit;
+                const int e = incl - cnt + x - base;
+                if (e >= 0 && e < SPA_STAGE)
+                {
+                    const int k = kb + (15 - bit);
+                    G.bs[e] = P.B_rptr[k];
+                    G.be[e] = P.B_rptr[k + 1];
+                    G.a[e] = P.A_Val[st + x];
+                }
+            }
+            __syncwarp();
+            const int ne = min(SPA_STAGE, total - base);
+            int c_cur = -1;
+            double v_cur = 0.0;
+            {
+                const int e = G.bs[0] + lane;
+                if (e < G.be[0])
+                {
+                    c_cur = P.B_rcol[e];
+                    v_cur = P.B_rval[e];
+                }
+            }
+            for (int i = 0; i < ne; i++)
+            {
+                int c_nxt = -1;
+                double v_nxt = 0.0;
+                if (i + 1 < ne)
+                {
+                    const int e = G.bs[i + 1] + lane;
+                    if (e < G.be[i + 1])
+                    {
+                        c_nxt = P.B_rcol[e];
+                        v_nxt = P.B_rval[e];
+                    }
+                }
+                const double a = G.a[i];
+                if (c_cur >= 0)
+                    spa_add(S, r, J0, J1, c_cur, a, v_cur);
+                for (int e = G.bs[i] + 32 + lane; e < G.be[i]; e += 32)
+                    spa_add(S, r, J0, J1, P.B_rcol[e], a, P.B_rval[e]);
+                __syncwarp();
+                c_cur = c_nxt;
+                v_cur = v_nxt;
+            }
+        }
+    }
+    __syncthreads();
+    for (int q = tid; q < cn; q += SPA_THREADS)
+        P.C_Val[base0 + q] = S.acc[q];
+    for (int u = tid; u < nt * TSG_BS; u += SPA_THREADS)
+    {
+        const unsigned cmw = S.cm[u];
+        unsigned mk = cmw & 0xFFFFu;
+        int p = base0 + (int)(cmw >> 16);
+        while (mk)
+        {
+            const int bit = 31 - __clz(mk);
+            P.C_Colb[p++] = (unsigned char)(15 - bit);
+            mk ^= 1u << bit;
+        }
+    }
+}
+
+// Segments of C tile row I: greedy runs of tiles with at most SPA_CAP values,
+// SPA_SEGT tiles and a SPA_WIN column window.  With segs == nullptr only the
+// count is written.
+__device__ __forceinline__ void spa_row_segments(const ProdView &P, int I, int *count, const int *offs, int2 *segs)
+{
+    int t = P.C_ptr[I];
+    const int tend = P.C_ptr[I + 1];
+    int n = 0;
+    while (t < tend)
+    {
+        const int t0 = t, v0 = P.C_tnnz[t0], j0 = P.C_col[t0];
+        t++;
+        while (t < tend && t - t0 < SPA_SEGT && P.C_tnnz[t + 1] - v0 <= SPA_CAP && P.C_col[t] - j0 < SPA_WIN)
+            t++;
+        if (segs)
+            segs[offs[I] + n] = make_int2(t0, t);
+        n++;
+    }
+    if (count)
+        *count = n;
 }
 
 // ---------------------------------------------------------------------------

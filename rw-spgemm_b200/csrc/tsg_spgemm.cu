@@ -134,6 +134,34 @@ __global__ void __launch_bounds__(128) k_step3_rows(ProdView P)
     step3_rows_item<W, CAP>(P, item, TSG_HW_MASK(threadIdx.x), threadIdx.x & 15, sm[threadIdx.x >> 4]);
 }
 
+__global__ void k_spa_count(ProdView P, int tilem, int *__restrict__ counts)
+{
+    const long long I = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (I < tilem)
+        spa_row_segments(P, (int)I, &counts[I], nullptr, nullptr);
+}
+
+__global__ void k_spa_fill(ProdView P, int tilem, const int *__restrict__ offs, int2 *__restrict__ segs)
+{
+    const long long I = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (I < tilem)
+        spa_row_segments(P, (int)I, nullptr, offs, segs);
+}
+
+// persistent: CTAs take segments in turn (the count is read on the device)
+__global__ void __launch_bounds__(SPA_THREADS) k_step3_spa(ProdView P, const int2 *__restrict__ segs,
+                                                           const int *__restrict__ nseg)
+{
+    extern __shared__ __align__(16) unsigned char s_raw[];
+    SpaSmem &S = *reinterpret_cast<SpaSmem *>(s_raw);
+    const int ns = *nseg;
+    for (int sg = blockIdx.x; sg < ns; sg += gridDim.x)
+    {
+        const int2 se = segs[sg];
+        step3_spa_segment(P, S, se.x, se.y);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Host orchestration.
 // ---------------------------------------------------------------------------
@@ -180,6 +208,9 @@ static ProdView make_view(const tsg_tiled *A, const tsg_tiled *B, tsg_tiled *C)
     P.B_Val = B->tile_csr_Value;
     P.B_mask = B->mask;
     P.B_maskT = B->mask_t;
+    P.B_rptr = B->row_ptr;
+    P.B_rcol = B->row_col;
+    P.B_rval = B->row_val;
     P.tilenB = B->tilen;
     P.C_ptr = C->tile_ptr;
     P.C_col = C->tile_columnidx;
@@ -228,8 +259,36 @@ static int launch_step2(tsg_context *ctx, const ProdView &P, int *d_bins)
     return TSG_OK;
 }
 
+static int launch_step3_spa(tsg_context *ctx, const ProdView &P)
+{
+    const int tilem = P.tilemA;
+    int *counts = nullptr;
+    int2 *segs = nullptr;
+    TSG_TRY(tsg_alloc(ctx, &counts, (size_t)tilem + 1));
+    TSG_TRY(tsg_alloc(ctx, &segs, (size_t)P.numC));
+    k_spa_count<<<tsg_blocks(tilem, 128), 128, 0, ctx->stream>>>(P, tilem, counts);
+    TSG_LAUNCH_CHECK();
+    TSG_TRY(tsg_scan_counts(ctx, counts, counts, tilem, nullptr));
+    k_spa_fill<<<tsg_blocks(tilem, 128), 128, 0, ctx->stream>>>(P, tilem, counts, segs);
+    TSG_LAUNCH_CHECK();
+    const int smem = (int)sizeof(SpaSmem);
+    TSG_CUDA(cudaFuncSetAttribute(k_step3_spa, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    int per_sm = 0;
+    TSG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step3_spa, SPA_THREADS, smem));
+    const long long want = (long long)ctx->num_sms * (per_sm > 0 ? per_sm : 1);
+    const unsigned grid = (unsigned)(want < P.numC ? want : P.numC);
+    k_step3_spa<<<grid, SPA_THREADS, smem, ctx->stream>>>(P, segs, counts + tilem);
+    TSG_LAUNCH_CHECK();
+    tsg_release(ctx, counts);
+    tsg_release(ctx, segs);
+    return TSG_OK;
+}
+
 static int launch_step3(tsg_context *ctx, const ProdView &P)
 {
+    // B without a row view (borrowed foreign buffers) takes the tile schedule
+    if (ctx->sched == TSG_SCHED_SPA && P.B_rptr)
+        return launch_step3_spa(ctx, P);
     if (ctx->sched == TSG_SCHED_ROWS)
     {
         const int W = ctx->seg_tiles, cap = ctx->acc_cap;

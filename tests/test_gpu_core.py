@@ -121,6 +121,7 @@ def _handle_product(tsg, ctx, matA, matB):
 
 
 SCHEDULES = [("tiles", 8, 512, True), ("elems", 8, 512, True), ("elems", 8, 512, False), ("tiles", 8, 512, False),
+             ("spa", 8, 512, True), ("spa", 8, 512, False),
              ("rows", 8, 256, False), ("rows", 16, 1024, False), ("rows", 32, 2048, False)]
 
 
@@ -155,6 +156,19 @@ def test_aat_and_dense_tiles(tsg, ctx, sched, oracle, gen):
             A_, B_, C, info = _handle_product(tsg, ctx, matA, B)
             Co = oracle.spgemm_tiled(oracle.csr2tile_row_major(matA), oracle.csr2tile_col_major(B))
             assert_tiles(C.download(), Co, C_KEYS + ["tile_csr_Value"])
+
+
+def test_many_pairs_per_c_tile(tsg, ctx, sched, oracle, gen):
+    """C tiles with ~100 matched tile pairs (long A rows and B columns): every
+    product still folds in k order."""
+    matA = gen.random_poisson(1600, 1600, 120.0, seed=8)
+    matB = gen.random_poisson(1600, 1500, 30.0, seed=9)
+    A_, B_, C, info = _handle_product(tsg, ctx, matA, matB)
+    rp, ci, v = (x.cpu().numpy() for x in tsg.tiled_to_csr(ctx, C))
+    G = oracle.gustavson(matA, matB)
+    np.testing.assert_array_equal(rp, G[2])
+    np.testing.assert_array_equal(ci, G[3])
+    assert np.array_equal(v.view(np.uint64), G[4].view(np.uint64))
 
 
 def test_laplacian_256_known_answers(tsg, ctx, sched, oracle, gen):
