@@ -263,6 +263,7 @@ def tilespgemm(tilesA: dict, tilesB: dict, nnzCub: int = 0) -> tuple[dict, dict]
 # handle API (device-resident)
 # ---------------------------------------------------------------------------
 CUDA_STREAM_LEGACY = 0x1
+SCHEDULE_IDS = {"tiles": 0, "rows": 1, "elems": 2, "spa": 3}
 
 
 class Context:
@@ -296,7 +297,7 @@ class Context:
     def set_schedule(self, schedule: str = "rows", seg_tiles: int = 8, acc_cap: int = 512):
         """'tiles' (half-warp per C tile, intersection) or 'rows' (half-warp per
         run of seg_tiles C tiles of one tile row, acc_cap FP64 slots)."""
-        check(lib().tsg_context_set_schedule(self.handle, {"tiles": 0, "rows": 1, "elems": 2, "spa": 3}[schedule], seg_tiles,
+        check(lib().tsg_context_set_schedule(self.handle, SCHEDULE_IDS[schedule], seg_tiles,
                                              acc_cap))
 
     def set_fusion(self, on: bool):
@@ -666,7 +667,7 @@ class Batch:
         n = len(self.pairs)
         arrA = (TsgTiled * n)(*[a.s for a, _ in self.pairs])
         arrB = (TsgTiled * n)(*[b.s for _, b in self.pairs])
-        prm = BatchParams({"tiles": 0, "rows": 1, "elems": 2}[schedule], seg_tiles, acc_cap, 1 if graph else 0)
+        prm = BatchParams(SCHEDULE_IDS[schedule], seg_tiles, acc_cap, 1 if graph else 0)
         self.handle = ctypes.c_void_p()
         check(lib().tsg_batch_create(ctx.handle, n, arrA, arrB, ctypes.byref(prm), ctypes.byref(self.handle)))
         self.count = n

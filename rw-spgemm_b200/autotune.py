@@ -24,7 +24,7 @@ import numpy as np
 
 from . import Batch, Context, product_bounds, spgemm
 
-CANDIDATES = [("elems", 8, 512), ("tiles", 8, 512), ("rows", 16, 1024), ("rows", 8, 256), ("rows", 32, 2048)]
+CANDIDATES = [("spa", 8, 512), ("elems", 8, 512), ("tiles", 8, 512), ("rows", 16, 1024), ("rows", 8, 256), ("rows", 32, 2048)]
 
 
 def batch_key(ctx: Context, pairs) -> str:

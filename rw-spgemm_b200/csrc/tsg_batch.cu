@@ -46,7 +46,7 @@ struct tsg_batch
     BatchProd *d_prod;
     long long *d_rowoff;
     long long *d_itemoff;
-    unsigned *d_bar; // [0] arrivals, [1] generation
+    unsigned *d_bar; // [0] arrivals, [1] generation, [2] next tile row (SPA step 3)
     int *d_err;
     int *d_bins;
     void *arena;
@@ -114,12 +114,14 @@ __device__ __forceinline__ int find_product(const long long *__restrict__ off, i
     return lo;
 }
 
-// Block-wide exclusive scan of a[0..n) in place, a[n] = total (BATCH_THREADS).
+// Block-wide exclusive scan of a[0..n) in place, a[n] = total (NT threads;
+// s_tmp holds NT / 32 partial sums).
+template <int NT>
 __device__ long long block_scan_inplace(int *a, int n, long long *s_tmp)
 {
     long long run = 0;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int base = 0; base < n; base += BATCH_THREADS)
+    for (int base = 0; base < n; base += NT)
     {
         const int i = base + threadIdx.x;
         const long long v = i < n ? a[i] : 0;
@@ -137,7 +139,10 @@ __device__ long long block_scan_inplace(int *a, int n, long long *s_tmp)
         long long woff = 0;
         for (int w = 0; w < warp; w++)
             woff += s_tmp[w];
-        const long long tot = s_tmp[0] + s_tmp[1] + s_tmp[2] + s_tmp[3];
+        long long tot = 0;
+#pragma unroll
+        for (int w = 0; w < NT / 32; w++)
+            tot += s_tmp[w];
         if (i < n)
             a[i] = (int)(run + woff + incl - v);
         run += tot;
@@ -149,25 +154,26 @@ __device__ long long block_scan_inplace(int *a, int n, long long *s_tmp)
     return run;
 }
 
-template <int SCHED, int W, int CAP>
-__global__ void __launch_bounds__(BATCH_THREADS)
+template <int SCHED, int W, int CAP, int NT>
+__global__ void __launch_bounds__(NT)
     k_batch(BatchProd *prods, int count, const long long *__restrict__ rowoff, long long *itemoff, unsigned *bar,
             int *err, int *bins)
 {
     extern __shared__ __align__(16) unsigned char s_raw[];
-    __shared__ long long s_tmp[4];
+    __shared__ long long s_tmp[NT / 32];
+    __shared__ int s_row;
     __shared__ int s_bins[4];
     const int lane32 = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 15, hw = threadIdx.x >> 4;
     const unsigned hmask = TSG_HW_MASK(threadIdx.x);
-    const long long nwarps = (long long)gridDim.x * (BATCH_THREADS / 32);
-    const long long nhw = (long long)gridDim.x * (BATCH_THREADS / 16);
+    const long long nwarps = (long long)gridDim.x * (NT / 32);
+    const long long nhw = (long long)gridDim.x * (NT / 16);
     const long long total_rows = rowoff[count];
 
     // phase 1: step-1 counts
     {
         unsigned *bm = reinterpret_cast<unsigned *>(s_raw) + warp * S1_WORDS;
-        for (long long w = (long long)blockIdx.x * (BATCH_THREADS / 32) + warp; w < total_rows; w += nwarps)
+        for (long long w = (long long)blockIdx.x * (NT / 32) + warp; w < total_rows; w += nwarps)
         {
             const int p = find_product(rowoff, count, w);
             const ProdView &P = prods[p].P;
@@ -183,7 +189,7 @@ __global__ void __launch_bounds__(BATCH_THREADS)
     for (int p = blockIdx.x; p < count; p += gridDim.x)
     {
         BatchProd &bp = prods[p];
-        const long long tot = block_scan_inplace(bp.P.C_ptr, bp.tilemA, s_tmp);
+        const long long tot = block_scan_inplace<NT>(bp.P.C_ptr, bp.tilemA, s_tmp);
         if (threadIdx.x == 0)
         {
             if (tot > bp.capT)
@@ -214,6 +220,7 @@ __global__ void __launch_bounds__(BATCH_THREADS)
                 run += SCHED == 1 ? (nc + W - 1) / W : nc;
             }
             itemoff[count] = run;
+            bar[2] = 0;
         }
         if (threadIdx.x < 4)
             bins[threadIdx.x] = 0;
@@ -228,7 +235,7 @@ __global__ void __launch_bounds__(BATCH_THREADS)
     {
         unsigned *bm = reinterpret_cast<unsigned *>(s_raw) + warp * S1_WORDS;
         S12Smem *s12 = reinterpret_cast<S12Smem *>(s_raw) + warp;
-        for (long long w = (long long)blockIdx.x * (BATCH_THREADS / 32) + warp; w < total_rows; w += nwarps)
+        for (long long w = (long long)blockIdx.x * (NT / 32) + warp; w < total_rows; w += nwarps)
         {
             const int p = find_product(rowoff, count, w);
             if (prods[p].status)
@@ -255,7 +262,7 @@ __global__ void __launch_bounds__(BATCH_THREADS)
     // phase 5: step 2 (all tiles for the row schedule, tiles of wide rows otherwise)
     {
         const long long total_items = itemoff[count];
-        for (long long h = (long long)blockIdx.x * (BATCH_THREADS / 16) + hw; h < total_items; h += nhw)
+        for (long long h = (long long)blockIdx.x * (NT / 16) + hw; h < total_items; h += nhw)
         {
             const int p = find_product(itemoff, count, h);
             const ProdView &P = prods[p].P;
@@ -275,7 +282,7 @@ __global__ void __launch_bounds__(BATCH_THREADS)
     for (int p = blockIdx.x; p < count; p += gridDim.x)
     {
         BatchProd &bp = prods[p];
-        const long long tot = block_scan_inplace(bp.P.C_tnnz, bp.numC, s_tmp);
+        const long long tot = block_scan_inplace<NT>(bp.P.C_tnnz, bp.numC, s_tmp);
         if (threadIdx.x == 0)
         {
             if (tot > bp.capN)
@@ -290,11 +297,43 @@ __global__ void __launch_bounds__(BATCH_THREADS)
     if (!grid_barrier(bar, err))
         return;
     // phase 7: step 3
-    if (SCHED == 2)
+    if (SCHED == 3)
+    {
+        // CTAs take whole tile rows from a counter; each row goes in
+        // segments whose end is the last tile within the SPA limits
+        SpaSmem &S = *reinterpret_cast<SpaSmem *>(s_raw);
+        for (;;)
+        {
+            __syncthreads();
+            if (threadIdx.x == 0)
+                s_row = (int)atomicAdd(&bar[2], 1u);
+            __syncthreads();
+            const long long row = s_row;
+            if (row >= total_rows)
+                break;
+            const int p = find_product(rowoff, count, row);
+            if (prods[p].status)
+                continue;
+            const ProdView &P = prods[p].P;
+            const int I = (int)(row - rowoff[p]);
+            const int te = P.C_ptr[I + 1];
+            for (int t0 = P.C_ptr[I]; t0 < te;)
+            {
+                const int cand = t0 + 1 + (int)threadIdx.x;
+                const bool ok = threadIdx.x < SPA_SEGT && cand <= te &&
+                                P.C_tnnz[cand] - P.C_tnnz[t0] <= SPA_CAP && P.C_col[cand - 1] - P.C_col[t0] < SPA_WIN;
+                const int n = __syncthreads_count(ok);
+                const int t1 = t0 + (n > 0 ? n : 1);
+                step3_spa_segment(P, S, t0, t1);
+                t0 = t1;
+            }
+        }
+    }
+    else if (SCHED == 2)
     {
         int2 *pairs = reinterpret_cast<int2 *>(s_raw) + warp * S3E_PAIRS;
         const long long total_items = itemoff[count];
-        for (long long w = (long long)blockIdx.x * (BATCH_THREADS / 32) + warp; w < total_items; w += nwarps)
+        for (long long w = (long long)blockIdx.x * (NT / 32) + warp; w < total_items; w += nwarps)
         {
             const int p = find_product(itemoff, count, w);
             if (prods[p].status)
@@ -312,7 +351,7 @@ __global__ void __launch_bounds__(BATCH_THREADS)
             __syncwarp(hmask);
         }
         const long long total_items = itemoff[count];
-        for (long long h = (long long)blockIdx.x * (BATCH_THREADS / 16) + hw; h < total_items; h += nhw)
+        for (long long h = (long long)blockIdx.x * (NT / 16) + hw; h < total_items; h += nhw)
         {
             const int p = find_product(itemoff, count, h);
             if (prods[p].status)
@@ -418,22 +457,33 @@ extern "C" int tsg_product_bounds(tsg_context *ctx, const tsg_tiled *A, const ts
 // ---------------------------------------------------------------------------
 typedef void (*batch_kernel_t)(BatchProd *, int, const long long *, long long *, unsigned *, int *, int *);
 
-static batch_kernel_t pick_kernel(const tsg_batch_params &p, size_t *smem)
+// Kernel, dynamic shared memory and block size of a batch schedule.
+static batch_kernel_t pick_kernel(const tsg_batch_params &p, size_t *smem, int *threads)
 {
+    *threads = BATCH_THREADS;
     const size_t s1a = (size_t)(BATCH_THREADS / 32) * S1_WORDS * 4;
     const size_t s12 = (size_t)(BATCH_THREADS / 32) * sizeof(S12Smem);
     const size_t s1 = s1a > s12 ? s1a : s12;
+    if (p.schedule == TSG_SCHED_SPA)
+    {
+        *threads = SPA_THREADS;
+        const size_t t1a = (size_t)(SPA_THREADS / 32) * S1_WORDS * 4;
+        const size_t t12 = (size_t)(SPA_THREADS / 32) * sizeof(S12Smem);
+        const size_t t1 = t1a > t12 ? t1a : t12;
+        *smem = t1 > sizeof(SpaSmem) ? t1 : sizeof(SpaSmem);
+        return k_batch<3, 8, 256, SPA_THREADS>;
+    }
     if (p.schedule == TSG_SCHED_ELEMS)
     {
         const size_t s3 = (size_t)(BATCH_THREADS / 32) * S3E_PAIRS * sizeof(int2);
         *smem = s1 > s3 ? s1 : s3;
-        return k_batch<2, 8, 256>;
+        return k_batch<2, 8, 256, BATCH_THREADS>;
     }
     if (p.schedule == TSG_SCHED_TILES)
     {
         const size_t s3 = (size_t)(BATCH_THREADS / 16) * TSG_BS * S3T_STRIDE * 8;
         *smem = s1 > s3 ? s1 : s3;
-        return k_batch<0, 8, 256>;
+        return k_batch<0, 8, 256, BATCH_THREADS>;
     }
 #define TSG_PICK(w, c)                                                                          \
     if (p.seg_tiles == w && p.acc_cap == c)                                                     \
@@ -442,7 +492,7 @@ static batch_kernel_t pick_kernel(const tsg_batch_params &p, size_t *smem)
         size_t s3 = (size_t)(BATCH_THREADS / 16) * sizeof(S3RowsSmem<w, c>);                    \
         size_t mx = s1 > s2 ? s1 : s2;                                                          \
         *smem = mx > s3 ? mx : s3;                                                              \
-        return k_batch<1, w, c>;                                                                \
+        return k_batch<1, w, c, BATCH_THREADS>;                                                 \
     }
     TSG_ROW_CONFIGS(TSG_PICK)
 #undef TSG_PICK
@@ -454,12 +504,13 @@ static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 static int record_run(tsg_batch *b, cudaStream_t st)
 {
     size_t smem;
-    batch_kernel_t kern = pick_kernel(b->params, &smem);
+    int threads;
+    batch_kernel_t kern = pick_kernel(b->params, &smem, &threads);
     TSG_CUDA(cudaMemsetAsync(b->d_err, 0, sizeof(int), st));
     TSG_CUDA(cudaMemsetAsync(b->d_bar, 0, sizeof(unsigned), st));
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)b->grid);
-    cfg.blockDim = dim3(BATCH_THREADS);
+    cfg.blockDim = dim3(threads);
     cfg.dynamicSmemBytes = b->smem;
     cfg.stream = st;
     cudaLaunchAttribute attr[1];
@@ -489,7 +540,8 @@ extern "C" int tsg_batch_create(tsg_context *ctx, int count, const tsg_tiled *A,
         prm.use_graph = 1;
     }
     size_t smem;
-    batch_kernel_t kern = pick_kernel(prm, &smem);
+    int threads;
+    batch_kernel_t kern = pick_kernel(prm, &smem, &threads);
     if (!kern)
         return tsg_set_error(TSG_ERR_INVALID, "unsupported batch schedule (%d, %d, %d)", prm.schedule, prm.seg_tiles,
                              prm.acc_cap);
@@ -499,6 +551,8 @@ extern "C" int tsg_batch_create(tsg_context *ctx, int count, const tsg_tiled *A,
             return tsg_set_error(TSG_ERR_INVALID, "product %d: inner dimensions differ or B lacks its column view", p);
         if (prm.schedule == TSG_SCHED_ELEMS && !B[p].mask_t)
             return tsg_set_error(TSG_ERR_INVALID, "product %d: element schedule needs B's column masks", p);
+        if (prm.schedule == TSG_SCHED_SPA && !B[p].row_ptr)
+            return tsg_set_error(TSG_ERR_INVALID, "product %d: SPA schedule needs B's row view", p);
     }
     tsg_batch *b = new tsg_batch();
     b->ctx = ctx;
@@ -607,7 +661,7 @@ extern "C" int tsg_batch_create(tsg_context *ctx, int count, const tsg_tiled *A,
         P.numC = 0;
     }
     if ((st = tsg_alloc(ctx, &b->d_prod, (size_t)count)) != TSG_OK || (st = tsg_alloc(ctx, &b->d_rowoff, (size_t)count + 1)) ||
-        (st = tsg_alloc(ctx, &b->d_itemoff, (size_t)count + 1)) || (st = tsg_alloc(ctx, &b->d_bar, 2)) ||
+        (st = tsg_alloc(ctx, &b->d_itemoff, (size_t)count + 1)) || (st = tsg_alloc(ctx, &b->d_bar, 3)) ||
         (st = tsg_alloc(ctx, &b->d_err, 1)) || (st = tsg_alloc(ctx, &b->d_bins, 4)))
     {
         tsg_batch_destroy(b);
@@ -616,7 +670,7 @@ extern "C" int tsg_batch_create(tsg_context *ctx, int count, const tsg_tiled *A,
     cudaStream_t s = ctx->stream;
     cudaMemcpyAsync(b->d_prod, b->host.data(), sizeof(BatchProd) * count, cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(b->d_rowoff, b->rowoff.data(), sizeof(long long) * (count + 1), cudaMemcpyHostToDevice, s);
-    cudaMemsetAsync(b->d_bar, 0, 2 * sizeof(unsigned), s);
+    cudaMemsetAsync(b->d_bar, 0, 3 * sizeof(unsigned), s);
     cudaMemsetAsync(b->d_err, 0, sizeof(int), s);
     // co-resident grid
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
@@ -625,14 +679,14 @@ extern "C" int tsg_batch_create(tsg_context *ctx, int count, const tsg_tiled *A,
         return tsg_set_error(TSG_ERR_CUDA, "cannot reserve %zu bytes of shared memory", smem);
     }
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, BATCH_THREADS, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
     if (per_sm < 1)
     {
         tsg_batch_destroy(b);
         return tsg_set_error(TSG_ERR_CUDA, "batch kernel cannot be resident");
     }
     b->grid = per_sm * ctx->num_sms;
-    b->block = BATCH_THREADS;
+    b->block = threads;
     b->smem = smem;
     b->graph_ok = 0;
     if (prm.use_graph)

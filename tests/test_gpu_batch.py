@@ -37,7 +37,7 @@ def _pairs(gen):
 
 
 @pytest.mark.parametrize("cfg", [("rows", 16, 1024), ("rows", 8, 256), ("rows", 32, 2048), ("tiles", 8, 256),
-                                 ("elems", 8, 256)])
+                                 ("elems", 8, 256), ("spa", 8, 512)])
 def test_batch_matches_oracle_and_single_path(tsg, ctx, oracle, gen, cfg):
     mats = _pairs(gen)
     pairs = [(_tiled(tsg, ctx, a, tsg.TSG_TILED_PACKED_COL), _tiled(tsg, ctx, b, tsg.TSG_TILED_CSC_VIEW))
