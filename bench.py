@@ -588,14 +588,14 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
-    ap.add_argument("--sched", default="elems", choices=["rows", "tiles", "elems", "spa"])
+    ap.add_argument("--sched", default="spa", choices=["rows", "tiles", "elems", "spa"])
     ap.add_argument("--sections", default="plain,batched,served,orderings",
                     help="comma list: plain (always), batched, served, selector")
     ap.add_argument("--batch-count", type=int, default=512)
     ap.add_argument("--selector-samples", type=int, default=5000)
     ap.add_argument("--served-jobs", type=int, default=2000)
     ap.add_argument("--served-rate", type=float, default=2000.0)
-    ap.add_argument("--served-schedule", nargs=3, default=["elems", "8", "512"])
+    ap.add_argument("--served-schedule", nargs=3, default=["spa", "8", "512"])
     ap.add_argument("--seg", type=int, default=16)
     ap.add_argument("--cap", type=int, default=1024)
     args = ap.parse_args()

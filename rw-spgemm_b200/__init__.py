@@ -294,7 +294,7 @@ class Context:
     def set_timing(self, on: bool):
         check(lib().tsg_context_set_timing(self.handle, 1 if on else 0))
 
-    def set_schedule(self, schedule: str = "rows", seg_tiles: int = 8, acc_cap: int = 512):
+    def set_schedule(self, schedule: str = "spa", seg_tiles: int = 8, acc_cap: int = 512):
         """'tiles' (half-warp per C tile, intersection) or 'rows' (half-warp per
         run of seg_tiles C tiles of one tile row, acc_cap FP64 slots)."""
         check(lib().tsg_context_set_schedule(self.handle, SCHEDULE_IDS[schedule], seg_tiles,
@@ -660,7 +660,7 @@ def product_bounds(ctx: Context, A: Tiled, B: Tiled):
 class Batch:
     """tsg_batch over device-resident (A, B) operand pairs."""
 
-    def __init__(self, ctx: Context, pairs, schedule: str = "rows", seg_tiles: int = 16, acc_cap: int = 1024,
+    def __init__(self, ctx: Context, pairs, schedule: str = "spa", seg_tiles: int = 8, acc_cap: int = 512,
                  graph: bool = True):
         self.ctx = ctx
         self.pairs = list(pairs)  # keep operands alive

@@ -60,7 +60,7 @@ extern "C" int tsg_context_create(int device, tsg_context **out)
         return tsg_set_error(TSG_ERR_CUDA, "context creation failed: %s", cudaGetErrorString(e));
     }
     ctx->own_stream = 1;
-    ctx->sched = TSG_SCHED_ELEMS;
+    ctx->sched = TSG_SCHED_SPA;
     ctx->seg_tiles = 8;
     ctx->acc_cap = 512;
     ctx->fuse12 = 1;

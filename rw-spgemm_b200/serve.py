@@ -113,7 +113,7 @@ class SpGEMMServer:
               autotuner's choice
     """
 
-    def __init__(self, device=0, mem_cap=40 << 30, slots=2, max_batch=64, schedule=("rows", 16, 1024)):
+    def __init__(self, device=0, mem_cap=40 << 30, slots=2, max_batch=64, schedule=("spa", 8, 512)):
         self.device = device
         self.mem_cap = int(mem_cap)
         self.max_batch = max_batch

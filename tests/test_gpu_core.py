@@ -130,7 +130,7 @@ def sched(request, ctx):
     ctx.set_schedule(*request.param[:3])
     ctx.set_fusion(request.param[3])
     yield request.param
-    ctx.set_schedule("elems", 8, 512)
+    ctx.set_schedule("spa", 8, 512)
     ctx.set_fusion(True)
 
 
