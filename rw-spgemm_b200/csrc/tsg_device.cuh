@@ -704,7 +704,8 @@ __device__ __forceinline__ void step3_rows_item(const ProdView &P, long long ite
 
 struct SpaStage
 {
-    int bs[SPA_STAGE], be[SPA_STAGE];
+    int bs[SPA_STAGE];      // first entry of the B row
+    int off[SPA_STAGE + 1]; // exclusive prefix of the B row lengths
     double a[SPA_STAGE];
 };
 
@@ -716,10 +717,10 @@ struct SpaSmem
     SpaStage stage[SPA_WARPS];
 };
 
-__device__ __forceinline__ void spa_add(SpaSmem &S, int r, int J0, int J1, int col, double a, double b)
+__device__ __forceinline__ void spa_add(SpaSmem &S, int r, int J0, int J1, bool full, int col, double a, double b)
 {
     const int J = col >> 4;
-    if (J < J0 || J >= J1 || J - J0 >= SPA_WIN)
+    if (!full && (J < J0 || J >= J1 || J - J0 >= SPA_WIN))
         return;
     const int slot = S.map[J - J0];
     if (slot >= SPA_SEGT)
@@ -739,6 +740,8 @@ __device__ __forceinline__ void step3_spa_segment(const ProdView &P, SpaSmem &S,
     const int base0 = P.C_tnnz[t0], cn = min(P.C_tnnz[t1] - base0, SPA_CAP);
     const int nt = min(t1 - t0, SPA_SEGT);
     const int win = min(J1 - J0, SPA_WIN);
+    // a segment holding the whole C tile row meets only its own columns
+    const bool full = t0 == P.C_ptr[I] && t1 == P.C_ptr[I + 1] && J1 - J0 <= SPA_WIN;
     __syncthreads();
     for (int q = tid; q < cn; q += SPA_THREADS)
         S.acc[q] = 0.0;
@@ -796,44 +799,76 @@ __device__ __forceinline__ void step3_spa_segment(const ProdView &P, SpaSmem &S,
                 if (e >= 0 && e < SPA_STAGE)
                 {
                     const int k = kb + (15 - bit);
-                    G.bs[e] = P.B_rptr[k];
-                    G.be[e] = P.B_rptr[k + 1];
+                    const int b0 = P.B_rptr[k];
+                    G.bs[e] = b0;
+                    G.off[e] = P.B_rptr[k + 1] - b0;
                     G.a[e] = P.A_Val[st + x];
                 }
             }
             __syncwarp();
             const int ne = min(SPA_STAGE, total - base);
-            int c_cur = -1;
-            double v_cur = 0.0;
+            // B row lengths -> exclusive offsets of the flattened item list
             {
-                const int e = G.bs[0] + lane;
-                if (e < G.be[0])
+                const int l0 = lane < ne ? G.off[lane] : 0;
+                const int l1 = lane + 32 < ne ? G.off[lane + 32] : 0;
+                int i0 = l0, i1 = l1;
+#pragma unroll
+                for (int d = 1; d < 32; d <<= 1)
                 {
-                    c_cur = P.B_rcol[e];
-                    v_cur = P.B_rval[e];
-                }
-            }
-            for (int i = 0; i < ne; i++)
-            {
-                int c_nxt = -1;
-                double v_nxt = 0.0;
-                if (i + 1 < ne)
-                {
-                    const int e = G.bs[i + 1] + lane;
-                    if (e < G.be[i + 1])
+                    const int o0 = __shfl_up_sync(TSG_FULL_MASK, i0, d);
+                    const int o1 = __shfl_up_sync(TSG_FULL_MASK, i1, d);
+                    if (lane >= d)
                     {
-                        c_nxt = P.B_rcol[e];
-                        v_nxt = P.B_rval[e];
+                        i0 += o0;
+                        i1 += o1;
                     }
                 }
-                const double a = G.a[i];
-                if (c_cur >= 0)
-                    spa_add(S, r, J0, J1, c_cur, a, v_cur);
-                for (int e = G.bs[i] + 32 + lane; e < G.be[i]; e += 32)
-                    spa_add(S, r, J0, J1, P.B_rcol[e], a, P.B_rval[e]);
+                const int t0s = __shfl_sync(TSG_FULL_MASK, i0, 31);
                 __syncwarp();
-                c_cur = c_nxt;
-                v_cur = v_nxt;
+                if (lane < ne)
+                    G.off[lane] = i0 - l0;
+                if (lane + 32 < ne)
+                    G.off[lane + 32] = t0s + i1 - l1;
+                if (lane == 31)
+                    G.off[ne] = t0s + i1;
+                __syncwarp();
+            }
+            // items (entry, B element) in entry order, 32 at a time; a column
+            // met twice in one window (two entries) is added in item order
+            const int ni = G.off[ne];
+            int ent = 0;
+            for (int wb = 0; wb < ni; wb += 32)
+            {
+                const int item = wb + lane;
+                int col = -1;
+                double bv = 0.0, av = 0.0;
+                if (item < ni)
+                {
+                    while (G.off[ent + 1] <= item)
+                        ent++;
+                    const int e = G.bs[ent] + (item - G.off[ent]);
+                    col = P.B_rcol[e];
+                    bv = P.B_rval[e];
+                    av = G.a[ent];
+                }
+                const unsigned same = __match_any_sync(TSG_FULL_MASK, col);
+                if (col >= 0)
+                {
+                    if (same == (1u << lane))
+                        spa_add(S, r, J0, J1, full, col, av, bv);
+                    else
+                    {
+                        unsigned grp = same;
+                        while (grp)
+                        {
+                            if (lane == __ffs(grp) - 1)
+                                spa_add(S, r, J0, J1, full, col, av, bv);
+                            __syncwarp(same);
+                            grp &= grp - 1;
+                        }
+                    }
+                }
+                __syncwarp();
             }
         }
     }
