@@ -46,7 +46,7 @@ struct tsg_batch
     BatchProd *d_prod;
     long long *d_rowoff;
     long long *d_itemoff;
-    unsigned *d_bar; // [0] arrivals, [1] generation, [2] next tile row (SPA step 3)
+    unsigned *d_bar; // [0] arrivals, [1] generation, [2] / [3] next tile row (SPA steps 3 / 2)
     int *d_err;
     int *d_bins;
     void *arena;
@@ -221,6 +221,7 @@ __global__ void __launch_bounds__(NT)
             }
             itemoff[count] = run;
             bar[2] = 0;
+            bar[3] = 0;
         }
         if (threadIdx.x < 4)
             bins[threadIdx.x] = 0;
@@ -260,6 +261,41 @@ __global__ void __launch_bounds__(NT)
     if (!grid_barrier(bar, err))
         return;
     // phase 5: step 2 (all tiles for the row schedule, tiles of wide rows otherwise)
+    if (SCHED == 3)
+    {
+        // wide rows through B's row view; CTAs take 32 tile rows at a time
+        Spa2Smem &S2 = *reinterpret_cast<Spa2Smem *>(s_raw);
+        for (;;)
+        {
+            __syncthreads();
+            if (threadIdx.x == 0)
+                s_row = (int)atomicAdd(&bar[3], 32u);
+            __syncthreads();
+            const long long r0 = s_row;
+            if (r0 >= total_rows)
+                break;
+            const long long r1 = r0 + 32 < total_rows ? r0 + 32 : total_rows;
+            for (long long row = r0; row < r1; row++)
+            {
+                const int p = find_product(rowoff, count, row);
+                const int I = (int)(row - rowoff[p]);
+                if (prods[p].status || !prods[p].wide[I])
+                    continue;
+                const ProdView &P = prods[p].P;
+                const int te = P.C_ptr[I + 1];
+                for (int t0 = P.C_ptr[I]; t0 < te;)
+                {
+                    const int cand = t0 + 1 + (int)threadIdx.x;
+                    const bool ok = threadIdx.x < SP2_SEGT && cand <= te && P.C_col[cand - 1] - P.C_col[t0] < SP2_WIN;
+                    const int n = __syncthreads_count(ok);
+                    const int t1 = t0 + (n > 0 ? n : 1);
+                    step2_spa_segment(P, S2, t0, t1, s_bins);
+                    t0 = t1;
+                }
+            }
+        }
+    }
+    else
     {
         const long long total_items = itemoff[count];
         for (long long h = (long long)blockIdx.x * (NT / 16) + hw; h < total_items; h += nhw)
@@ -306,27 +342,49 @@ __global__ void __launch_bounds__(NT)
         {
             __syncthreads();
             if (threadIdx.x == 0)
-                s_row = (int)atomicAdd(&bar[2], 1u);
+                s_row = (int)atomicAdd(&bar[2], 4u);
             __syncthreads();
-            const long long row = s_row;
-            if (row >= total_rows)
+            const long long r0 = s_row;
+            if (r0 >= total_rows)
                 break;
-            const int p = find_product(rowoff, count, row);
-            if (prods[p].status)
-                continue;
-            const ProdView &P = prods[p].P;
-            const int I = (int)(row - rowoff[p]);
-            const int te = P.C_ptr[I + 1];
-            for (int t0 = P.C_ptr[I]; t0 < te;)
+            const long long r1 = r0 + 4 < total_rows ? r0 + 4 : total_rows;
+            for (long long row = r0; row < r1; row++)
             {
-                const int cand = t0 + 1 + (int)threadIdx.x;
-                const bool ok = threadIdx.x < SPA_SEGT && cand <= te &&
-                                P.C_tnnz[cand] - P.C_tnnz[t0] <= SPA_CAP && P.C_col[cand - 1] - P.C_col[t0] < SPA_WIN;
-                const int n = __syncthreads_count(ok);
-                const int t1 = t0 + (n > 0 ? n : 1);
-                step3_spa_segment(P, S, t0, t1);
-                t0 = t1;
+                const int p = find_product(rowoff, count, row);
+                if (prods[p].status || prods[p].nnzC >= (long long)SPA_DENSE * prods[p].numC)
+                    continue;
+                const ProdView &P = prods[p].P;
+                const int I = (int)(row - rowoff[p]);
+                const int te = P.C_ptr[I + 1];
+                for (int t0 = P.C_ptr[I]; t0 < te;)
+                {
+                    const int cand = t0 + 1 + (int)threadIdx.x;
+                    const bool ok = threadIdx.x < SPA_SEGT && cand <= te &&
+                                    P.C_tnnz[cand] - P.C_tnnz[t0] <= SPA_CAP &&
+                                    P.C_col[cand - 1] - P.C_col[t0] < SPA_WIN;
+                    const int n = __syncthreads_count(ok);
+                    const int t1 = t0 + (n > 0 ? n : 1);
+                    step3_spa_segment(P, S, t0, t1);
+                    t0 = t1;
+                }
             }
+        }
+    }
+    if (SCHED == 3)
+    {
+        // products with dense C tiles: tile kernel, half-warp per C tile
+        __syncthreads();
+        double *tacc = reinterpret_cast<double *>(s_raw) + hw * (TSG_BS * S3T_STRIDE);
+        for (int q = lane; q < TSG_BS * S3T_STRIDE; q += 16)
+            tacc[q] = 0.0;
+        __syncwarp(hmask);
+        const long long total_items = itemoff[count];
+        for (long long h = (long long)blockIdx.x * (NT / 16) + hw; h < total_items; h += nhw)
+        {
+            const int p = find_product(itemoff, count, h);
+            if (prods[p].status || prods[p].nnzC < (long long)SPA_DENSE * prods[p].numC)
+                continue;
+            step3_tile(prods[p].P, (int)(h - itemoff[p]), hmask, lane, tacc);
         }
     }
     else if (SCHED == 2)
@@ -470,7 +528,8 @@ static batch_kernel_t pick_kernel(const tsg_batch_params &p, size_t *smem, int *
         const size_t t1a = (size_t)(SPA_THREADS / 32) * S1_WORDS * 4;
         const size_t t12 = (size_t)(SPA_THREADS / 32) * sizeof(S12Smem);
         const size_t t1 = t1a > t12 ? t1a : t12;
-        *smem = t1 > sizeof(SpaSmem) ? t1 : sizeof(SpaSmem);
+        const size_t t3 = sizeof(SpaSmem) > sizeof(Spa2Smem) ? sizeof(SpaSmem) : sizeof(Spa2Smem);
+        *smem = t1 > t3 ? t1 : t3;
         return k_batch<3, 8, 256, SPA_THREADS>;
     }
     if (p.schedule == TSG_SCHED_ELEMS)
@@ -661,7 +720,7 @@ extern "C" int tsg_batch_create(tsg_context *ctx, int count, const tsg_tiled *A,
         P.numC = 0;
     }
     if ((st = tsg_alloc(ctx, &b->d_prod, (size_t)count)) != TSG_OK || (st = tsg_alloc(ctx, &b->d_rowoff, (size_t)count + 1)) ||
-        (st = tsg_alloc(ctx, &b->d_itemoff, (size_t)count + 1)) || (st = tsg_alloc(ctx, &b->d_bar, 3)) ||
+        (st = tsg_alloc(ctx, &b->d_itemoff, (size_t)count + 1)) || (st = tsg_alloc(ctx, &b->d_bar, 4)) ||
         (st = tsg_alloc(ctx, &b->d_err, 1)) || (st = tsg_alloc(ctx, &b->d_bins, 4)))
     {
         tsg_batch_destroy(b);
@@ -670,7 +729,7 @@ extern "C" int tsg_batch_create(tsg_context *ctx, int count, const tsg_tiled *A,
     cudaStream_t s = ctx->stream;
     cudaMemcpyAsync(b->d_prod, b->host.data(), sizeof(BatchProd) * count, cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(b->d_rowoff, b->rowoff.data(), sizeof(long long) * (count + 1), cudaMemcpyHostToDevice, s);
-    cudaMemsetAsync(b->d_bar, 0, 3 * sizeof(unsigned), s);
+    cudaMemsetAsync(b->d_bar, 0, 4 * sizeof(unsigned), s);
     cudaMemsetAsync(b->d_err, 0, sizeof(int), s);
     // co-resident grid
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)

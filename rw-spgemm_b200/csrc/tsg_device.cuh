@@ -701,11 +701,11 @@ __device__ __forceinline__ void step3_rows_item(const ProdView &P, long long ite
 #define SPA_SEGT 256
 #define SPA_WIN 2048
 #define SPA_STAGE 64
+#define SPA_DENSE 64 // C values per tile from which the tile kernel is faster
 
 struct SpaStage
 {
-    int bs[SPA_STAGE];      // first entry of the B row
-    int off[SPA_STAGE + 1]; // exclusive prefix of the B row lengths
+    int bs[SPA_STAGE], be[SPA_STAGE]; // B row bounds
     double a[SPA_STAGE];
 };
 
@@ -799,15 +799,171 @@ __device__ __forceinline__ void step3_spa_segment(const ProdView &P, SpaSmem &S,
                 if (e >= 0 && e < SPA_STAGE)
                 {
                     const int k = kb + (15 - bit);
-                    const int b0 = P.B_rptr[k];
-                    G.bs[e] = b0;
-                    G.off[e] = P.B_rptr[k + 1] - b0;
+                    G.bs[e] = P.B_rptr[k];
+                    G.be[e] = P.B_rptr[k + 1];
                     G.a[e] = P.A_Val[st + x];
                 }
             }
             __syncwarp();
             const int ne = min(SPA_STAGE, total - base);
-            // B row lengths -> exclusive offsets of the flattened item list
+            int c_cur = -1;
+            double v_cur = 0.0;
+            {
+                const int e = G.bs[0] + lane;
+                if (e < G.be[0])
+                {
+                    c_cur = P.B_rcol[e];
+                    v_cur = P.B_rval[e];
+                }
+            }
+            for (int i = 0; i < ne; i++)
+            {
+                int c_nxt = -1;
+                double v_nxt = 0.0;
+                if (i + 1 < ne)
+                {
+                    const int e = G.bs[i + 1] + lane;
+                    if (e < G.be[i + 1])
+                    {
+                        c_nxt = P.B_rcol[e];
+                        v_nxt = P.B_rval[e];
+                    }
+                }
+                const double a = G.a[i];
+                if (c_cur >= 0)
+                    spa_add(S, r, J0, J1, full, c_cur, a, v_cur);
+                for (int e = G.bs[i] + 32 + lane; e < G.be[i]; e += 32)
+                    spa_add(S, r, J0, J1, full, P.B_rcol[e], a, P.B_rval[e]);
+                __syncwarp();
+                c_cur = c_nxt;
+                v_cur = v_nxt;
+            }
+        }
+    }
+    __syncthreads();
+    for (int q = tid; q < cn; q += SPA_THREADS)
+        P.C_Val[base0 + q] = S.acc[q];
+    for (int u = tid; u < nt * TSG_BS; u += SPA_THREADS)
+    {
+        const unsigned cmw = S.cm[u];
+        unsigned mk = cmw & 0xFFFFu;
+        int p = base0 + (int)(cmw >> 16);
+        while (mk)
+        {
+            const int bit = 31 - __clz(mk);
+            P.C_Colb[p++] = (unsigned char)(15 - bit);
+            mk ^= 1u << bit;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Step 2 for wide tile rows (more C tiles or a wider column window than the
+// fused row pass holds), through B's row view.  One CTA owns a segment of
+// consecutive C tiles of tile row I (at most SP2_SEGT tiles, a SP2_WIN
+// tile-column window); warp r walks A's row r and, for every A(r, k), B's
+// row k: each entry's column sets its bit in the 32-bit row-r mask word of
+// its C tile (shared-memory atomicOr; the order does not matter for an OR).
+// The masks then go out through step2_store like every other step-2 path.
+// ---------------------------------------------------------------------------
+#define SP2_SEGT 1024
+#define SP2_WIN 4096
+
+struct Spa2Stage
+{
+    int bs[SPA_STAGE];
+    int off[SPA_STAGE + 1];
+};
+
+struct Spa2Smem
+{
+    unsigned m[SP2_SEGT * TSG_BS];
+    unsigned short map[SP2_WIN];
+    Spa2Stage stage[SPA_WARPS];
+};
+
+// Segments of tile row I for the scalar step 2 (tile and window limits only).
+__device__ __forceinline__ void spa2_row_segments(const ProdView &P, int I, int *count, const int *offs, int2 *segs)
+{
+    int t = P.C_ptr[I];
+    const int tend = P.C_ptr[I + 1];
+    int n = 0;
+    while (t < tend)
+    {
+        const int t0 = t, j0 = P.C_col[t0];
+        t++;
+        while (t < tend && t - t0 < SP2_SEGT && P.C_col[t] - j0 < SP2_WIN)
+            t++;
+        if (segs)
+            segs[offs[I] + n] = make_int2(t0, t);
+        n++;
+    }
+    if (count)
+        *count = n;
+}
+
+// The CTA (SPA_THREADS threads) computes the masks of C tiles [t0, t1).
+__device__ __forceinline__ void step2_spa_segment(const ProdView &P, Spa2Smem &S, int t0, int t1, int *s_bins)
+{
+    const int tid = threadIdx.x, lane = tid & 31, r = tid >> 5;
+    const int I = P.C_row[t0];
+    const int J0 = P.C_col[t0], J1 = P.C_col[t1 - 1] + 1;
+    const int nt = min(t1 - t0, SP2_SEGT);
+    const int win = min(J1 - J0, SP2_WIN);
+    __syncthreads();
+    for (int q = tid; q < nt * TSG_BS; q += SPA_THREADS)
+        S.m[q] = 0u;
+    for (int q = tid; q < win; q += SPA_THREADS)
+        S.map[q] = 0xFFFF;
+    __syncthreads();
+    for (int jl = tid; jl < nt; jl += SPA_THREADS)
+    {
+        const int w = P.C_col[t0 + jl] - J0;
+        if (w < win)
+            S.map[w] = (unsigned short)jl;
+    }
+    __syncthreads();
+    Spa2Stage &G = S.stage[r];
+    const int pa_beg = P.A_ptr[I], pa_end = P.A_ptr[I + 1];
+    for (int g = pa_beg; g < pa_end; g += 32)
+    {
+        const int pa = g + lane;
+        unsigned mr = 0;
+        int kb = 0;
+        if (pa < pa_end)
+        {
+            mr = P.A_mask[(long long)pa * TSG_BS + r];
+            kb = P.A_col[pa] * TSG_BS;
+        }
+        const int cnt = __popc(mr);
+        int incl = cnt;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1)
+        {
+            const int o = __shfl_up_sync(TSG_FULL_MASK, incl, d);
+            if (lane >= d)
+                incl += o;
+        }
+        const int total = __shfl_sync(TSG_FULL_MASK, incl, 31);
+        for (int base = 0; base < total; base += SPA_STAGE)
+        {
+            __syncwarp();
+            unsigned bits = mr;
+            for (int x = 0; x < cnt; x++)
+            {
+                const int bit = 31 - __clz(bits);
+                bits ^= 1u << bit;
+                const int e = incl - cnt + x - base;
+                if (e >= 0 && e < SPA_STAGE)
+                {
+                    const int k = kb + (15 - bit);
+                    const int b0 = P.B_rptr[k];
+                    G.bs[e] = b0;
+                    G.off[e] = P.B_rptr[k + 1] - b0;
+                }
+            }
+            __syncwarp();
+            const int ne = min(SPA_STAGE, total - base);
             {
                 const int l0 = lane < ne ? G.off[lane] : 0;
                 const int l1 = lane + 32 < ne ? G.off[lane + 32] : 0;
@@ -833,60 +989,27 @@ __device__ __forceinline__ void step3_spa_segment(const ProdView &P, SpaSmem &S,
                     G.off[ne] = t0s + i1;
                 __syncwarp();
             }
-            // items (entry, B element) in entry order, 32 at a time; a column
-            // met twice in one window (two entries) is added in item order
             const int ni = G.off[ne];
             int ent = 0;
-            for (int wb = 0; wb < ni; wb += 32)
+            for (int item = lane; item < ni; item += 32)
             {
-                const int item = wb + lane;
-                int col = -1;
-                double bv = 0.0, av = 0.0;
-                if (item < ni)
-                {
-                    while (G.off[ent + 1] <= item)
-                        ent++;
-                    const int e = G.bs[ent] + (item - G.off[ent]);
-                    col = P.B_rcol[e];
-                    bv = P.B_rval[e];
-                    av = G.a[ent];
-                }
-                const unsigned same = __match_any_sync(TSG_FULL_MASK, col);
-                if (col >= 0)
-                {
-                    if (same == (1u << lane))
-                        spa_add(S, r, J0, J1, full, col, av, bv);
-                    else
-                    {
-                        unsigned grp = same;
-                        while (grp)
-                        {
-                            if (lane == __ffs(grp) - 1)
-                                spa_add(S, r, J0, J1, full, col, av, bv);
-                            __syncwarp(same);
-                            grp &= grp - 1;
-                        }
-                    }
-                }
-                __syncwarp();
+                while (G.off[ent + 1] <= item)
+                    ent++;
+                const int col = P.B_rcol[G.bs[ent] + (item - G.off[ent])];
+                const int J = col >> 4;
+                if (J < J0 || J - J0 >= win)
+                    continue;
+                const int slot = S.map[J - J0];
+                if (slot < nt)
+                    atomicOr(&S.m[slot * TSG_BS + r], 1u << (15 - (col & 15)));
             }
         }
     }
     __syncthreads();
-    for (int q = tid; q < cn; q += SPA_THREADS)
-        P.C_Val[base0 + q] = S.acc[q];
-    for (int u = tid; u < nt * TSG_BS; u += SPA_THREADS)
-    {
-        const unsigned cmw = S.cm[u];
-        unsigned mk = cmw & 0xFFFFu;
-        int p = base0 + (int)(cmw >> 16);
-        while (mk)
-        {
-            const int bit = 31 - __clz(mk);
-            P.C_Colb[p++] = (unsigned char)(15 - bit);
-            mk ^= 1u << bit;
-        }
-    }
+    // half-warp per C tile: row offsets, masks, tile count, bin
+    const unsigned hmask = TSG_HW_MASK(tid);
+    for (int jl = tid >> 4; jl < nt; jl += SPA_THREADS / 16)
+        step2_store(P, t0 + jl, hmask, tid & 15, S.m[jl * TSG_BS + (tid & 15)], s_bins);
 }
 
 // Segments of C tile row I: greedy runs of tiles with at most SPA_CAP values,

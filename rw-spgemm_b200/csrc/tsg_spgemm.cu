@@ -71,6 +71,46 @@ __global__ void __launch_bounds__(256) k_step2_wide(ProdView P, const int *__res
         atomicAdd(&bins[threadIdx.x], s_bins[threadIdx.x]);
 }
 
+// scalar step 2 for wide rows: segments of the rows k_step12 left
+__global__ void k_spa2_count(ProdView P, int tilem, const int *__restrict__ wide, int *__restrict__ counts)
+{
+    const long long I = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (I < tilem)
+    {
+        if (wide[I])
+            spa2_row_segments(P, (int)I, &counts[I], nullptr, nullptr);
+        else
+            counts[I] = 0;
+    }
+}
+
+__global__ void k_spa2_fill(ProdView P, int tilem, const int *__restrict__ wide, const int *__restrict__ offs,
+                            int2 *__restrict__ segs)
+{
+    const long long I = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (I < tilem && wide[I])
+        spa2_row_segments(P, (int)I, nullptr, offs, segs);
+}
+
+__global__ void __launch_bounds__(SPA_THREADS) k_step2_spa(ProdView P, const int2 *__restrict__ segs,
+                                                           const int *__restrict__ nseg, int *__restrict__ bins)
+{
+    extern __shared__ __align__(16) unsigned char s_raw[];
+    Spa2Smem &S = *reinterpret_cast<Spa2Smem *>(s_raw);
+    __shared__ int s_bins[4];
+    if (threadIdx.x < 4)
+        s_bins[threadIdx.x] = 0;
+    const int ns = *nseg;
+    for (int sg = blockIdx.x; sg < ns; sg += gridDim.x)
+    {
+        const int2 se = segs[sg];
+        step2_spa_segment(P, S, se.x, se.y, s_bins);
+    }
+    __syncthreads();
+    if (threadIdx.x < 4 && s_bins[threadIdx.x])
+        atomicAdd(&bins[threadIdx.x], s_bins[threadIdx.x]);
+}
+
 __global__ void __launch_bounds__(256) k_step2(ProdView P, int *__restrict__ bins)
 {
     __shared__ int s_bins[4];
@@ -259,6 +299,32 @@ static int launch_step2(tsg_context *ctx, const ProdView &P, int *d_bins)
     return TSG_OK;
 }
 
+// step 2 for the rows k_step12 declined, through B's row view
+static int launch_step2_spa(tsg_context *ctx, const ProdView &P, const int *d_wide, int *d_bins)
+{
+    const int tilem = P.tilemA;
+    int *counts = nullptr;
+    int2 *segs = nullptr;
+    TSG_TRY(tsg_alloc(ctx, &counts, (size_t)tilem + 1));
+    TSG_TRY(tsg_alloc(ctx, &segs, (size_t)P.numC));
+    k_spa2_count<<<tsg_blocks(tilem, 128), 128, 0, ctx->stream>>>(P, tilem, d_wide, counts);
+    TSG_LAUNCH_CHECK();
+    TSG_TRY(tsg_scan_counts(ctx, counts, counts, tilem, nullptr));
+    k_spa2_fill<<<tsg_blocks(tilem, 128), 128, 0, ctx->stream>>>(P, tilem, d_wide, counts, segs);
+    TSG_LAUNCH_CHECK();
+    const int smem = (int)sizeof(Spa2Smem);
+    TSG_CUDA(cudaFuncSetAttribute(k_step2_spa, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    int per_sm = 0;
+    TSG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step2_spa, SPA_THREADS, smem));
+    const long long want = (long long)ctx->num_sms * (per_sm > 0 ? per_sm : 1);
+    const unsigned grid = (unsigned)(want < P.numC ? want : P.numC);
+    k_step2_spa<<<grid, SPA_THREADS, smem, ctx->stream>>>(P, segs, counts + tilem, d_bins);
+    TSG_LAUNCH_CHECK();
+    tsg_release(ctx, counts);
+    tsg_release(ctx, segs);
+    return TSG_OK;
+}
+
 static int launch_step3_spa(tsg_context *ctx, const ProdView &P)
 {
     const int tilem = P.tilemA;
@@ -284,10 +350,11 @@ static int launch_step3_spa(tsg_context *ctx, const ProdView &P)
     return TSG_OK;
 }
 
-static int launch_step3(tsg_context *ctx, const ProdView &P)
+static int launch_step3(tsg_context *ctx, const ProdView &P, long long nnzC)
 {
-    // B without a row view (borrowed foreign buffers) takes the tile schedule
-    if (ctx->sched == TSG_SCHED_SPA && P.B_rptr)
+    // SPA: products whose C tiles are dense on average (>= SPA_DENSE values)
+    // and B without a row view (borrowed foreign buffers) take the tile kernel
+    if (ctx->sched == TSG_SCHED_SPA && P.B_rptr && nnzC < (long long)SPA_DENSE * P.numC)
         return launch_step3_spa(ctx, P);
     if (ctx->sched == TSG_SCHED_ROWS)
     {
@@ -379,7 +446,9 @@ extern "C" int tsg_spgemm(tsg_context *ctx, const tsg_tiled *A, const tsg_tiled 
     if (numC > 0)
     {
         ProdView P = make_view(A, B, C);
-        if (fused)
+        if (fused && P.B_rptr)
+            TSG_TRY(launch_step2_spa(ctx, P, d_wide, d_bins));
+        else if (fused)
         {
             k_step2_wide<<<tsg_blocks(numC * 16, 256), 256, 0, st>>>(P, d_wide, d_bins);
             TSG_LAUNCH_CHECK();
@@ -399,7 +468,7 @@ extern "C" int tsg_spgemm(tsg_context *ctx, const tsg_tiled *A, const tsg_tiled 
     TSG_TRY(tsg_alloc(ctx, &C->tile_csr_Col, (size_t)nnzC));
     TSG_TRY(tsg_alloc(ctx, &C->tile_csr_Value, (size_t)nnzC));
     if (nnzC > 0)
-        TSG_TRY(launch_step3(ctx, make_view(A, B, C)));
+        TSG_TRY(launch_step3(ctx, make_view(A, B, C), nnzC));
     if (timing)
         TSG_CUDA(cudaEventRecord(ctx->ev[3], st));
 
