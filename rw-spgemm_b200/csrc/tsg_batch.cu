@@ -281,17 +281,7 @@ __global__ void __launch_bounds__(NT)
                 const int I = (int)(row - rowoff[p]);
                 if (prods[p].status || !prods[p].wide[I])
                     continue;
-                const ProdView &P = prods[p].P;
-                const int te = P.C_ptr[I + 1];
-                for (int t0 = P.C_ptr[I]; t0 < te;)
-                {
-                    const int cand = t0 + 1 + (int)threadIdx.x;
-                    const bool ok = threadIdx.x < SP2_SEGT && cand <= te && P.C_col[cand - 1] - P.C_col[t0] < SP2_WIN;
-                    const int n = __syncthreads_count(ok);
-                    const int t1 = t0 + (n > 0 ? n : 1);
-                    step2_spa_segment(P, S2, t0, t1, s_bins);
-                    t0 = t1;
-                }
+                step2_spa_row(prods[p].P, S2, I, s_bins);
             }
         }
     }
@@ -353,20 +343,7 @@ __global__ void __launch_bounds__(NT)
                 const int p = find_product(rowoff, count, row);
                 if (prods[p].status || prods[p].nnzC >= (long long)SPA_DENSE * prods[p].numC)
                     continue;
-                const ProdView &P = prods[p].P;
-                const int I = (int)(row - rowoff[p]);
-                const int te = P.C_ptr[I + 1];
-                for (int t0 = P.C_ptr[I]; t0 < te;)
-                {
-                    const int cand = t0 + 1 + (int)threadIdx.x;
-                    const bool ok = threadIdx.x < SPA_SEGT && cand <= te &&
-                                    P.C_tnnz[cand] - P.C_tnnz[t0] <= SPA_CAP &&
-                                    P.C_col[cand - 1] - P.C_col[t0] < SPA_WIN;
-                    const int n = __syncthreads_count(ok);
-                    const int t1 = t0 + (n > 0 ? n : 1);
-                    step3_spa_segment(P, S, t0, t1);
-                    t0 = t1;
-                }
+                step3_spa_row(prods[p].P, S, (int)(row - rowoff[p]));
             }
         }
     }

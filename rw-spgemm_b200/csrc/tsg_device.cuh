@@ -882,26 +882,6 @@ struct Spa2Smem
     Spa2Stage stage[SPA_WARPS];
 };
 
-// Segments of tile row I for the scalar step 2 (tile and window limits only).
-__device__ __forceinline__ void spa2_row_segments(const ProdView &P, int I, int *count, const int *offs, int2 *segs)
-{
-    int t = P.C_ptr[I];
-    const int tend = P.C_ptr[I + 1];
-    int n = 0;
-    while (t < tend)
-    {
-        const int t0 = t, j0 = P.C_col[t0];
-        t++;
-        while (t < tend && t - t0 < SP2_SEGT && P.C_col[t] - j0 < SP2_WIN)
-            t++;
-        if (segs)
-            segs[offs[I] + n] = make_int2(t0, t);
-        n++;
-    }
-    if (count)
-        *count = n;
-}
-
 // The CTA (SPA_THREADS threads) computes the masks of C tiles [t0, t1).
 __device__ __forceinline__ void step2_spa_segment(const ProdView &P, Spa2Smem &S, int t0, int t1, int *s_bins)
 {
@@ -1012,26 +992,36 @@ __device__ __forceinline__ void step2_spa_segment(const ProdView &P, Spa2Smem &S
         step2_store(P, t0 + jl, hmask, tid & 15, S.m[jl * TSG_BS + (tid & 15)], s_bins);
 }
 
-// Segments of C tile row I: greedy runs of tiles with at most SPA_CAP values,
-// SPA_SEGT tiles and a SPA_WIN column window.  With segs == nullptr only the
-// count is written.
-__device__ __forceinline__ void spa_row_segments(const ProdView &P, int I, int *count, const int *offs, int2 *segs)
+// All segments of tile row I, numeric (the CTA splits the row on the fly:
+// each segment ends at the last tile within the SPA limits).
+__device__ __forceinline__ void step3_spa_row(const ProdView &P, SpaSmem &S, int I)
 {
-    int t = P.C_ptr[I];
-    const int tend = P.C_ptr[I + 1];
-    int n = 0;
-    while (t < tend)
+    const int te = P.C_ptr[I + 1];
+    for (int t0 = P.C_ptr[I]; t0 < te;)
     {
-        const int t0 = t, v0 = P.C_tnnz[t0], j0 = P.C_col[t0];
-        t++;
-        while (t < tend && t - t0 < SPA_SEGT && P.C_tnnz[t + 1] - v0 <= SPA_CAP && P.C_col[t] - j0 < SPA_WIN)
-            t++;
-        if (segs)
-            segs[offs[I] + n] = make_int2(t0, t);
-        n++;
+        const int cand = t0 + 1 + (int)threadIdx.x;
+        const bool ok = threadIdx.x < SPA_SEGT && cand <= te && P.C_tnnz[cand] - P.C_tnnz[t0] <= SPA_CAP &&
+                        P.C_col[cand - 1] - P.C_col[t0] < SPA_WIN;
+        const int n = __syncthreads_count(ok);
+        const int t1 = t0 + (n > 0 ? n : 1);
+        step3_spa_segment(P, S, t0, t1);
+        t0 = t1;
     }
-    if (count)
-        *count = n;
+}
+
+// All segments of tile row I, symbolic.
+__device__ __forceinline__ void step2_spa_row(const ProdView &P, Spa2Smem &S, int I, int *s_bins)
+{
+    const int te = P.C_ptr[I + 1];
+    for (int t0 = P.C_ptr[I]; t0 < te;)
+    {
+        const int cand = t0 + 1 + (int)threadIdx.x;
+        const bool ok = threadIdx.x < SP2_SEGT && cand <= te && P.C_col[cand - 1] - P.C_col[t0] < SP2_WIN;
+        const int n = __syncthreads_count(ok);
+        const int t1 = t0 + (n > 0 ? n : 1);
+        step2_spa_segment(P, S, t0, t1, s_bins);
+        t0 = t1;
+    }
 }
 
 // ---------------------------------------------------------------------------

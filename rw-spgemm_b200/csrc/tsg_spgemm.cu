@@ -71,40 +71,30 @@ __global__ void __launch_bounds__(256) k_step2_wide(ProdView P, const int *__res
         atomicAdd(&bins[threadIdx.x], s_bins[threadIdx.x]);
 }
 
-// scalar step 2 for wide rows: segments of the rows k_step12 left
-__global__ void k_spa2_count(ProdView P, int tilem, const int *__restrict__ wide, int *__restrict__ counts)
-{
-    const long long I = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (I < tilem)
-    {
-        if (wide[I])
-            spa2_row_segments(P, (int)I, &counts[I], nullptr, nullptr);
-        else
-            counts[I] = 0;
-    }
-}
-
-__global__ void k_spa2_fill(ProdView P, int tilem, const int *__restrict__ wide, const int *__restrict__ offs,
-                            int2 *__restrict__ segs)
-{
-    const long long I = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (I < tilem && wide[I])
-        spa2_row_segments(P, (int)I, nullptr, offs, segs);
-}
-
-__global__ void __launch_bounds__(SPA_THREADS) k_step2_spa(ProdView P, const int2 *__restrict__ segs,
-                                                           const int *__restrict__ nseg, int *__restrict__ bins)
+// scalar step 2 for the wide rows k_step12 left: CTAs take 32 tile rows at a
+// time from a device counter and run the wide ones
+__global__ void __launch_bounds__(SPA_THREADS) k_step2_spa(ProdView P, const int *__restrict__ wide,
+                                                           unsigned *__restrict__ ctr, int *__restrict__ bins)
 {
     extern __shared__ __align__(16) unsigned char s_raw[];
     Spa2Smem &S = *reinterpret_cast<Spa2Smem *>(s_raw);
     __shared__ int s_bins[4];
+    __shared__ int s_row;
     if (threadIdx.x < 4)
         s_bins[threadIdx.x] = 0;
-    const int ns = *nseg;
-    for (int sg = blockIdx.x; sg < ns; sg += gridDim.x)
+    for (;;)
     {
-        const int2 se = segs[sg];
-        step2_spa_segment(P, S, se.x, se.y, s_bins);
+        __syncthreads();
+        if (threadIdx.x == 0)
+            s_row = (int)atomicAdd(ctr, 32u);
+        __syncthreads();
+        const int r0 = s_row;
+        if (r0 >= P.tilemA)
+            break;
+        const int r1 = min(r0 + 32, P.tilemA);
+        for (int I = r0; I < r1; I++)
+            if (wide[I])
+                step2_spa_row(P, S, I, s_bins);
     }
     __syncthreads();
     if (threadIdx.x < 4 && s_bins[threadIdx.x])
@@ -174,31 +164,25 @@ __global__ void __launch_bounds__(128) k_step3_rows(ProdView P)
     step3_rows_item<W, CAP>(P, item, TSG_HW_MASK(threadIdx.x), threadIdx.x & 15, sm[threadIdx.x >> 4]);
 }
 
-__global__ void k_spa_count(ProdView P, int tilem, int *__restrict__ counts)
-{
-    const long long I = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (I < tilem)
-        spa_row_segments(P, (int)I, &counts[I], nullptr, nullptr);
-}
-
-__global__ void k_spa_fill(ProdView P, int tilem, const int *__restrict__ offs, int2 *__restrict__ segs)
-{
-    const long long I = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (I < tilem)
-        spa_row_segments(P, (int)I, nullptr, offs, segs);
-}
-
-// persistent: CTAs take segments in turn (the count is read on the device)
-__global__ void __launch_bounds__(SPA_THREADS) k_step3_spa(ProdView P, const int2 *__restrict__ segs,
-                                                           const int *__restrict__ nseg)
+// persistent: CTAs take tile rows from a device counter, SPA_ROWS at a time
+#define SPA_ROWS 4
+__global__ void __launch_bounds__(SPA_THREADS) k_step3_spa(ProdView P, unsigned *__restrict__ ctr)
 {
     extern __shared__ __align__(16) unsigned char s_raw[];
     SpaSmem &S = *reinterpret_cast<SpaSmem *>(s_raw);
-    const int ns = *nseg;
-    for (int sg = blockIdx.x; sg < ns; sg += gridDim.x)
+    __shared__ int s_row;
+    for (;;)
     {
-        const int2 se = segs[sg];
-        step3_spa_segment(P, S, se.x, se.y);
+        __syncthreads();
+        if (threadIdx.x == 0)
+            s_row = (int)atomicAdd(ctr, (unsigned)SPA_ROWS);
+        __syncthreads();
+        const int r0 = s_row;
+        if (r0 >= P.tilemA)
+            break;
+        const int r1 = min(r0 + SPA_ROWS, P.tilemA);
+        for (int I = r0; I < r1; I++)
+            step3_spa_row(P, S, I);
     }
 }
 
@@ -299,54 +283,41 @@ static int launch_step2(tsg_context *ctx, const ProdView &P, int *d_bins)
     return TSG_OK;
 }
 
+// persistent grid of a SPA kernel: resident CTAs on every SM
+template <typename K>
+static int spa_grid(tsg_context *ctx, K kern, int smem, unsigned *grid)
+{
+    TSG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    int per_sm = 0;
+    TSG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, SPA_THREADS, smem));
+    *grid = (unsigned)(ctx->num_sms * (per_sm > 0 ? per_sm : 1));
+    return TSG_OK;
+}
+
 // step 2 for the rows k_step12 declined, through B's row view
 static int launch_step2_spa(tsg_context *ctx, const ProdView &P, const int *d_wide, int *d_bins)
 {
-    const int tilem = P.tilemA;
-    int *counts = nullptr;
-    int2 *segs = nullptr;
-    TSG_TRY(tsg_alloc(ctx, &counts, (size_t)tilem + 1));
-    TSG_TRY(tsg_alloc(ctx, &segs, (size_t)P.numC));
-    k_spa2_count<<<tsg_blocks(tilem, 128), 128, 0, ctx->stream>>>(P, tilem, d_wide, counts);
-    TSG_LAUNCH_CHECK();
-    TSG_TRY(tsg_scan_counts(ctx, counts, counts, tilem, nullptr));
-    k_spa2_fill<<<tsg_blocks(tilem, 128), 128, 0, ctx->stream>>>(P, tilem, d_wide, counts, segs);
-    TSG_LAUNCH_CHECK();
+    unsigned *ctr = nullptr, grid = 0;
     const int smem = (int)sizeof(Spa2Smem);
-    TSG_CUDA(cudaFuncSetAttribute(k_step2_spa, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    int per_sm = 0;
-    TSG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step2_spa, SPA_THREADS, smem));
-    const long long want = (long long)ctx->num_sms * (per_sm > 0 ? per_sm : 1);
-    const unsigned grid = (unsigned)(want < P.numC ? want : P.numC);
-    k_step2_spa<<<grid, SPA_THREADS, smem, ctx->stream>>>(P, segs, counts + tilem, d_bins);
+    TSG_TRY(spa_grid(ctx, k_step2_spa, smem, &grid));
+    TSG_TRY(tsg_alloc(ctx, &ctr, 1));
+    TSG_CUDA(cudaMemsetAsync(ctr, 0, sizeof(unsigned), ctx->stream));
+    k_step2_spa<<<grid, SPA_THREADS, smem, ctx->stream>>>(P, d_wide, ctr, d_bins);
     TSG_LAUNCH_CHECK();
-    tsg_release(ctx, counts);
-    tsg_release(ctx, segs);
+    tsg_release(ctx, ctr);
     return TSG_OK;
 }
 
 static int launch_step3_spa(tsg_context *ctx, const ProdView &P)
 {
-    const int tilem = P.tilemA;
-    int *counts = nullptr;
-    int2 *segs = nullptr;
-    TSG_TRY(tsg_alloc(ctx, &counts, (size_t)tilem + 1));
-    TSG_TRY(tsg_alloc(ctx, &segs, (size_t)P.numC));
-    k_spa_count<<<tsg_blocks(tilem, 128), 128, 0, ctx->stream>>>(P, tilem, counts);
-    TSG_LAUNCH_CHECK();
-    TSG_TRY(tsg_scan_counts(ctx, counts, counts, tilem, nullptr));
-    k_spa_fill<<<tsg_blocks(tilem, 128), 128, 0, ctx->stream>>>(P, tilem, counts, segs);
-    TSG_LAUNCH_CHECK();
+    unsigned *ctr = nullptr, grid = 0;
     const int smem = (int)sizeof(SpaSmem);
-    TSG_CUDA(cudaFuncSetAttribute(k_step3_spa, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    int per_sm = 0;
-    TSG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step3_spa, SPA_THREADS, smem));
-    const long long want = (long long)ctx->num_sms * (per_sm > 0 ? per_sm : 1);
-    const unsigned grid = (unsigned)(want < P.numC ? want : P.numC);
-    k_step3_spa<<<grid, SPA_THREADS, smem, ctx->stream>>>(P, segs, counts + tilem);
+    TSG_TRY(spa_grid(ctx, k_step3_spa, smem, &grid));
+    TSG_TRY(tsg_alloc(ctx, &ctr, 1));
+    TSG_CUDA(cudaMemsetAsync(ctr, 0, sizeof(unsigned), ctx->stream));
+    k_step3_spa<<<grid, SPA_THREADS, smem, ctx->stream>>>(P, ctr);
     TSG_LAUNCH_CHECK();
-    tsg_release(ctx, counts);
-    tsg_release(ctx, segs);
+    tsg_release(ctx, ctr);
     return TSG_OK;
 }
 
