@@ -233,24 +233,33 @@ class SpGEMMServer:
 
     def _finish(self, slot):
         """Converts every product of the finished batch to CSR on the device
-        (all conversions queued, one synchronisation), then copies each result
-        to host arrays and completes its future."""
+        into one buffer (all conversions queued on the slot's stream), brings
+        the buffer to page-locked host memory in one copy and completes each
+        job's future with numpy views into it (they keep it alive)."""
         import torch
         slot.batch.sync()
         dev = torch.device("cuda", self.device)
-        pending = []
+        layout, total = [], 0
         for p, job in enumerate(slot.jobs):
             C = slot.batch.product(p)
             m, nnz = C.s.m, C.s.nnz
-            rp = torch.empty(m + 1, dtype=torch.int32, device=dev)
-            ci = torch.empty(max(nnz, 1), dtype=torch.int32, device=dev)
-            v = torch.empty(max(nnz, 1), dtype=torch.float64, device=dev)
-            check(lib().tsg_tiled_to_csr(slot.ctx.handle, ctypes.byref(C.s), ctypes.c_void_p(rp.data_ptr()),
-                                         ctypes.c_void_p(ci.data_ptr()), ctypes.c_void_p(v.data_ptr())))
-            pending.append((job, C.s.m, C.s.n, nnz, rp, ci, v))
+            v_off = total
+            rp_off = v_off + 8 * nnz
+            ci_off = rp_off + 4 * (m + 1)
+            total = (ci_off + 4 * nnz + 7) & ~7
+            layout.append((job, C, m, C.s.n, nnz, v_off, rp_off, ci_off))
+        dbuf = torch.empty(max(total, 8), dtype=torch.uint8, device=dev)
+        base = dbuf.data_ptr()
+        for job, C, m, n, nnz, v_off, rp_off, ci_off in layout:
+            check(lib().tsg_tiled_to_csr(slot.ctx.handle, ctypes.byref(C.s), ctypes.c_void_p(base + rp_off),
+                                         ctypes.c_void_p(base + ci_off), ctypes.c_void_p(base + v_off)))
         slot.ctx.synchronize()
-        for job, m, n, nnz, rp, ci, v in pending:
-            res = (m, n, rp.cpu().numpy(), ci[:nnz].cpu().numpy(), v[:nnz].cpu().numpy())
+        hbuf = torch.empty(max(total, 8), dtype=torch.uint8, pin_memory=True)
+        hbuf.copy_(dbuf)
+        raw = hbuf.numpy()
+        for job, C, m, n, nnz, v_off, rp_off, ci_off in layout:
+            res = (m, n, raw[rp_off:rp_off + 4 * (m + 1)].view(np.int32), raw[ci_off:ci_off + 4 * nnz].view(np.int32),
+                   raw[v_off:v_off + 8 * nnz].view(np.float64))
             job.t_done = time.perf_counter()
             job.result_nnz = nnz
             job.future.set_result(res)
