@@ -269,12 +269,12 @@ __global__ void __launch_bounds__(NT)
         {
             __syncthreads();
             if (threadIdx.x == 0)
-                s_row = (int)atomicAdd(&bar[3], 32u);
+                s_row = (int)atomicAdd(&bar[3], 8u);
             __syncthreads();
             const long long r0 = s_row;
             if (r0 >= total_rows)
                 break;
-            const long long r1 = r0 + 32 < total_rows ? r0 + 32 : total_rows;
+            const long long r1 = r0 + 8 < total_rows ? r0 + 8 : total_rows;
             for (long long row = r0; row < r1; row++)
             {
                 const int p = find_product(rowoff, count, row);
@@ -332,12 +332,12 @@ __global__ void __launch_bounds__(NT)
         {
             __syncthreads();
             if (threadIdx.x == 0)
-                s_row = (int)atomicAdd(&bar[2], 4u);
+                s_row = (int)atomicAdd(&bar[2], 1u);
             __syncthreads();
             const long long r0 = s_row;
             if (r0 >= total_rows)
                 break;
-            const long long r1 = r0 + 4 < total_rows ? r0 + 4 : total_rows;
+            const long long r1 = r0 + 1;
             for (long long row = r0; row < r1; row++)
             {
                 const int p = find_product(rowoff, count, row);

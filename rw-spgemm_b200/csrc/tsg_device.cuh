@@ -799,8 +799,15 @@ __device__ __forceinline__ void step3_spa_segment(const ProdView &P, SpaSmem &S,
                 if (e >= 0 && e < SPA_STAGE)
                 {
                     const int k = kb + (15 - bit);
-                    G.bs[e] = P.B_rptr[k];
-                    G.be[e] = P.B_rptr[k + 1];
+                    int b0 = P.B_rptr[k], b1 = P.B_rptr[k + 1];
+                    if (!full)
+                    {
+                        // only B's entries inside this segment's columns
+                        b0 += lower_bound_int(P.B_rcol + b0, b1 - b0, J0 * TSG_BS);
+                        b1 = b0 + lower_bound_int(P.B_rcol + b0, b1 - b0, J1 * TSG_BS);
+                    }
+                    G.bs[e] = b0;
+                    G.be[e] = b1;
                     G.a[e] = P.A_Val[st + x];
                 }
             }
@@ -890,6 +897,7 @@ __device__ __forceinline__ void step2_spa_segment(const ProdView &P, Spa2Smem &S
     const int J0 = P.C_col[t0], J1 = P.C_col[t1 - 1] + 1;
     const int nt = min(t1 - t0, SP2_SEGT);
     const int win = min(J1 - J0, SP2_WIN);
+    const bool full = t0 == P.C_ptr[I] && t1 == P.C_ptr[I + 1];
     __syncthreads();
     for (int q = tid; q < nt * TSG_BS; q += SPA_THREADS)
         S.m[q] = 0u;
@@ -937,9 +945,14 @@ __device__ __forceinline__ void step2_spa_segment(const ProdView &P, Spa2Smem &S
                 if (e >= 0 && e < SPA_STAGE)
                 {
                     const int k = kb + (15 - bit);
-                    const int b0 = P.B_rptr[k];
+                    int b0 = P.B_rptr[k], b1 = P.B_rptr[k + 1];
+                    if (!full)
+                    {
+                        b0 += lower_bound_int(P.B_rcol + b0, b1 - b0, J0 * TSG_BS);
+                        b1 = b0 + lower_bound_int(P.B_rcol + b0, b1 - b0, J1 * TSG_BS);
+                    }
                     G.bs[e] = b0;
-                    G.off[e] = P.B_rptr[k + 1] - b0;
+                    G.off[e] = b1 - b0;
                 }
             }
             __syncwarp();

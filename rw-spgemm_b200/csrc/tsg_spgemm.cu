@@ -86,12 +86,12 @@ __global__ void __launch_bounds__(SPA_THREADS) k_step2_spa(ProdView P, const int
     {
         __syncthreads();
         if (threadIdx.x == 0)
-            s_row = (int)atomicAdd(ctr, 32u);
+            s_row = (int)atomicAdd(ctr, 8u);
         __syncthreads();
         const int r0 = s_row;
         if (r0 >= P.tilemA)
             break;
-        const int r1 = min(r0 + 32, P.tilemA);
+        const int r1 = min(r0 + 8, P.tilemA);
         for (int I = r0; I < r1; I++)
             if (wide[I])
                 step2_spa_row(P, S, I, s_bins);
@@ -165,7 +165,7 @@ __global__ void __launch_bounds__(128) k_step3_rows(ProdView P)
 }
 
 // persistent: CTAs take tile rows from a device counter, SPA_ROWS at a time
-#define SPA_ROWS 4
+#define SPA_ROWS 1
 __global__ void __launch_bounds__(SPA_THREADS) k_step3_spa(ProdView P, unsigned *__restrict__ ctr)
 {
     extern __shared__ __align__(16) unsigned char s_raw[];
