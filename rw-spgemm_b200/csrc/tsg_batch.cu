@@ -46,7 +46,7 @@ struct tsg_batch
     BatchProd *d_prod;
     long long *d_rowoff;
     long long *d_itemoff;
-    unsigned *d_bar; // [0] arrivals, [1] generation, [2] / [3] next tile row (SPA steps 3 / 2)
+    unsigned *d_bar; // [0] arrivals, [1] generation, [2] / [3] next tile block (SPA steps 3 / 2)
     int *d_err;
     int *d_bins;
     void *arena;
@@ -220,6 +220,15 @@ __global__ void __launch_bounds__(NT)
                 run += SCHED == 1 ? (nc + W - 1) / W : nc;
             }
             itemoff[count] = run;
+            // SPA: blocks of SPA_BLK C tiles per product, prefix after itemoff
+            long long *blkoff = itemoff + count + 1;
+            run = 0;
+            for (int p = 0; p < count; p++)
+            {
+                blkoff[p] = run;
+                run += ((long long)prods[p].numC + SPA_BLK - 1) / SPA_BLK;
+            }
+            blkoff[count] = run;
             bar[2] = 0;
             bar[3] = 0;
         }
@@ -263,26 +272,24 @@ __global__ void __launch_bounds__(NT)
     // phase 5: step 2 (all tiles for the row schedule, tiles of wide rows otherwise)
     if (SCHED == 3)
     {
-        // wide rows through B's row view; CTAs take 32 tile rows at a time
+        // wide rows through B's row view; CTAs take blocks of C tiles
         Spa2Smem &S2 = *reinterpret_cast<Spa2Smem *>(s_raw);
+        const long long *blkoff = itemoff + count + 1;
         for (;;)
         {
             __syncthreads();
             if (threadIdx.x == 0)
-                s_row = (int)atomicAdd(&bar[3], 8u);
+                s_row = (int)atomicAdd(&bar[3], 1u);
             __syncthreads();
-            const long long r0 = s_row;
-            if (r0 >= total_rows)
+            const long long blk = s_row;
+            if (blk >= blkoff[count])
                 break;
-            const long long r1 = r0 + 8 < total_rows ? r0 + 8 : total_rows;
-            for (long long row = r0; row < r1; row++)
-            {
-                const int p = find_product(rowoff, count, row);
-                const int I = (int)(row - rowoff[p]);
-                if (prods[p].status || !prods[p].wide[I])
-                    continue;
-                step2_spa_row(prods[p].P, S2, I, s_bins);
-            }
+            const int p = find_product(blkoff, count, blk);
+            if (prods[p].status)
+                continue;
+            const ProdView &P = prods[p].P;
+            const long long tb = (blk - blkoff[p]) * SPA_BLK;
+            step2_spa_block(P, S2, (int)tb, (int)min((long long)P.numC, tb + SPA_BLK), prods[p].wide, s_bins);
         }
     }
     else
@@ -325,26 +332,25 @@ __global__ void __launch_bounds__(NT)
     // phase 7: step 3
     if (SCHED == 3)
     {
-        // CTAs take whole tile rows from a counter; each row goes in
-        // segments whose end is the last tile within the SPA limits
+        // CTAs take blocks of C tiles from a counter (products with sparse
+        // C tiles); a block goes in row parts and SPA-limited segments
         SpaSmem &S = *reinterpret_cast<SpaSmem *>(s_raw);
+        const long long *blkoff = itemoff + count + 1;
         for (;;)
         {
             __syncthreads();
             if (threadIdx.x == 0)
                 s_row = (int)atomicAdd(&bar[2], 1u);
             __syncthreads();
-            const long long r0 = s_row;
-            if (r0 >= total_rows)
+            const long long blk = s_row;
+            if (blk >= blkoff[count])
                 break;
-            const long long r1 = r0 + 1;
-            for (long long row = r0; row < r1; row++)
-            {
-                const int p = find_product(rowoff, count, row);
-                if (prods[p].status || prods[p].nnzC >= (long long)SPA_DENSE * prods[p].numC)
-                    continue;
-                step3_spa_row(prods[p].P, S, (int)(row - rowoff[p]));
-            }
+            const int p = find_product(blkoff, count, blk);
+            if (prods[p].status || prods[p].nnzC >= (long long)SPA_DENSE * prods[p].numC)
+                continue;
+            const ProdView &P = prods[p].P;
+            const long long tb = (blk - blkoff[p]) * SPA_BLK;
+            step3_spa_block(P, S, (int)tb, (int)min((long long)P.numC, tb + SPA_BLK));
         }
     }
     if (SCHED == 3)
@@ -697,7 +703,7 @@ extern "C" int tsg_batch_create(tsg_context *ctx, int count, const tsg_tiled *A,
         P.numC = 0;
     }
     if ((st = tsg_alloc(ctx, &b->d_prod, (size_t)count)) != TSG_OK || (st = tsg_alloc(ctx, &b->d_rowoff, (size_t)count + 1)) ||
-        (st = tsg_alloc(ctx, &b->d_itemoff, (size_t)count + 1)) || (st = tsg_alloc(ctx, &b->d_bar, 4)) ||
+        (st = tsg_alloc(ctx, &b->d_itemoff, 2 * ((size_t)count + 1))) || (st = tsg_alloc(ctx, &b->d_bar, 4)) ||
         (st = tsg_alloc(ctx, &b->d_err, 1)) || (st = tsg_alloc(ctx, &b->d_bins, 4)))
     {
         tsg_batch_destroy(b);

@@ -1005,35 +1005,53 @@ __device__ __forceinline__ void step2_spa_segment(const ProdView &P, Spa2Smem &S
         step2_store(P, t0 + jl, hmask, tid & 15, S.m[jl * TSG_BS + (tid & 15)], s_bins);
 }
 
-// All segments of tile row I, numeric (the CTA splits the row on the fly:
-// each segment ends at the last tile within the SPA limits).
-__device__ __forceinline__ void step3_spa_row(const ProdView &P, SpaSmem &S, int I)
+// Work item of the SPA steps: a block of SPA_BLK consecutive C tiles (global
+// tile order, any rows).  The CTA cuts the block at row ends and, inside a
+// row, into segments within the SPA limits (each segment ends at the last
+// tile that still fits), so a long row is spread over many blocks/CTAs.
+#define SPA_BLK 256
+
+__device__ __forceinline__ void step3_spa_block(const ProdView &P, SpaSmem &S, int tb, int te)
 {
-    const int te = P.C_ptr[I + 1];
-    for (int t0 = P.C_ptr[I]; t0 < te;)
+    for (int t = tb; t < te;)
     {
-        const int cand = t0 + 1 + (int)threadIdx.x;
-        const bool ok = threadIdx.x < SPA_SEGT && cand <= te && P.C_tnnz[cand] - P.C_tnnz[t0] <= SPA_CAP &&
-                        P.C_col[cand - 1] - P.C_col[t0] < SPA_WIN;
-        const int n = __syncthreads_count(ok);
-        const int t1 = t0 + (n > 0 ? n : 1);
-        step3_spa_segment(P, S, t0, t1);
-        t0 = t1;
+        const int I = P.C_row[t];
+        const int rend = min(te, P.C_ptr[I + 1]);
+        for (int t0 = t; t0 < rend;)
+        {
+            const int cand = t0 + 1 + (int)threadIdx.x;
+            const bool ok = threadIdx.x < SPA_SEGT && cand <= rend && P.C_tnnz[cand] - P.C_tnnz[t0] <= SPA_CAP &&
+                            P.C_col[cand - 1] - P.C_col[t0] < SPA_WIN;
+            const int n = __syncthreads_count(ok);
+            const int t1 = t0 + (n > 0 ? n : 1);
+            step3_spa_segment(P, S, t0, t1);
+            t0 = t1;
+        }
+        t = rend;
     }
 }
 
-// All segments of tile row I, symbolic.
-__device__ __forceinline__ void step2_spa_row(const ProdView &P, Spa2Smem &S, int I, int *s_bins)
+// Symbolic counterpart, for the tiles of wide rows only (wide[I] != 0).
+__device__ __forceinline__ void step2_spa_block(const ProdView &P, Spa2Smem &S, int tb, int te,
+                                                const int *__restrict__ wide, int *s_bins)
 {
-    const int te = P.C_ptr[I + 1];
-    for (int t0 = P.C_ptr[I]; t0 < te;)
+    for (int t = tb; t < te;)
     {
-        const int cand = t0 + 1 + (int)threadIdx.x;
-        const bool ok = threadIdx.x < SP2_SEGT && cand <= te && P.C_col[cand - 1] - P.C_col[t0] < SP2_WIN;
-        const int n = __syncthreads_count(ok);
-        const int t1 = t0 + (n > 0 ? n : 1);
-        step2_spa_segment(P, S, t0, t1, s_bins);
-        t0 = t1;
+        const int I = P.C_row[t];
+        const int rend = min(te, P.C_ptr[I + 1]);
+        if (wide[I])
+        {
+            for (int t0 = t; t0 < rend;)
+            {
+                const int cand = t0 + 1 + (int)threadIdx.x;
+                const bool ok = threadIdx.x < SP2_SEGT && cand <= rend && P.C_col[cand - 1] - P.C_col[t0] < SP2_WIN;
+                const int n = __syncthreads_count(ok);
+                const int t1 = t0 + (n > 0 ? n : 1);
+                step2_spa_segment(P, S, t0, t1, s_bins);
+                t0 = t1;
+            }
+        }
+        t = rend;
     }
 }
 

@@ -71,30 +71,27 @@ __global__ void __launch_bounds__(256) k_step2_wide(ProdView P, const int *__res
         atomicAdd(&bins[threadIdx.x], s_bins[threadIdx.x]);
 }
 
-// scalar step 2 for the wide rows k_step12 left: CTAs take 32 tile rows at a
-// time from a device counter and run the wide ones
+// scalar step 2 for the wide rows k_step12 left: CTAs take blocks of C tiles
+// from a device counter and run the wide rows' parts
 __global__ void __launch_bounds__(SPA_THREADS) k_step2_spa(ProdView P, const int *__restrict__ wide,
                                                            unsigned *__restrict__ ctr, int *__restrict__ bins)
 {
     extern __shared__ __align__(16) unsigned char s_raw[];
     Spa2Smem &S = *reinterpret_cast<Spa2Smem *>(s_raw);
     __shared__ int s_bins[4];
-    __shared__ int s_row;
+    __shared__ int s_blk;
     if (threadIdx.x < 4)
         s_bins[threadIdx.x] = 0;
     for (;;)
     {
         __syncthreads();
         if (threadIdx.x == 0)
-            s_row = (int)atomicAdd(ctr, 8u);
+            s_blk = (int)atomicAdd(ctr, 1u);
         __syncthreads();
-        const int r0 = s_row;
-        if (r0 >= P.tilemA)
+        const long long tb = (long long)s_blk * SPA_BLK;
+        if (tb >= P.numC)
             break;
-        const int r1 = min(r0 + 8, P.tilemA);
-        for (int I = r0; I < r1; I++)
-            if (wide[I])
-                step2_spa_row(P, S, I, s_bins);
+        step2_spa_block(P, S, (int)tb, (int)min((long long)P.numC, tb + SPA_BLK), wide, s_bins);
     }
     __syncthreads();
     if (threadIdx.x < 4 && s_bins[threadIdx.x])
@@ -164,25 +161,22 @@ __global__ void __launch_bounds__(128) k_step3_rows(ProdView P)
     step3_rows_item<W, CAP>(P, item, TSG_HW_MASK(threadIdx.x), threadIdx.x & 15, sm[threadIdx.x >> 4]);
 }
 
-// persistent: CTAs take tile rows from a device counter, SPA_ROWS at a time
-#define SPA_ROWS 1
+// persistent: CTAs take blocks of C tiles from a device counter
 __global__ void __launch_bounds__(SPA_THREADS) k_step3_spa(ProdView P, unsigned *__restrict__ ctr)
 {
     extern __shared__ __align__(16) unsigned char s_raw[];
     SpaSmem &S = *reinterpret_cast<SpaSmem *>(s_raw);
-    __shared__ int s_row;
+    __shared__ int s_blk;
     for (;;)
     {
         __syncthreads();
         if (threadIdx.x == 0)
-            s_row = (int)atomicAdd(ctr, (unsigned)SPA_ROWS);
+            s_blk = (int)atomicAdd(ctr, 1u);
         __syncthreads();
-        const int r0 = s_row;
-        if (r0 >= P.tilemA)
+        const long long tb = (long long)s_blk * SPA_BLK;
+        if (tb >= P.numC)
             break;
-        const int r1 = min(r0 + SPA_ROWS, P.tilemA);
-        for (int I = r0; I < r1; I++)
-            step3_spa_row(P, S, I);
+        step3_spa_block(P, S, (int)tb, (int)min((long long)P.numC, tb + SPA_BLK));
     }
 }
 
