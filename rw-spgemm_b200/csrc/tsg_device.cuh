@@ -1006,53 +1006,76 @@ __device__ __forceinline__ void step2_spa_segment(const ProdView &P, Spa2Smem &S
 }
 
 // Work item of the SPA steps: a block of SPA_BLK consecutive C tiles (global
-// tile order, any rows).  The CTA cuts the block at row ends and, inside a
-// row, into segments within the SPA limits (each segment ends at the last
-// tile that still fits), so a long row is spread over many blocks/CTAs.
+// tile order).  Ownership: a row of at most SPA_BLK tiles belongs, whole, to
+// the block holding its first tile; a longer row is cut into SPA_BLK-tile
+// chunks from its start, each belonging to the block holding the chunk's
+// first tile.  So every tile is done once, short rows are never cut, and a
+// long row is spread over many blocks (and CTAs).  The CTA cuts each piece
+// further into segments within the SPA limits.
 #define SPA_BLK 256
+
+// calls piece(t0, t1) for the pieces [t0, t1) owned by block [tb, te)
+template <typename F>
+__device__ __forceinline__ void spa_block_pieces(const ProdView &P, int tb, int te, F piece)
+{
+    int t = tb;
+    {
+        const int I = P.C_row[tb];
+        const int rs = P.C_ptr[I], re = P.C_ptr[I + 1];
+        if (rs < tb)
+        {
+            if (re - rs > SPA_BLK)
+                for (int cs = rs + ((tb - rs + SPA_BLK - 1) / SPA_BLK) * SPA_BLK; cs < te && cs < re; cs += SPA_BLK)
+                    piece(I, cs, min(cs + SPA_BLK, re));
+            t = re;
+        }
+    }
+    while (t < te)
+    {
+        const int I = P.C_row[t];
+        const int re = P.C_ptr[I + 1];
+        if (re - t <= SPA_BLK)
+            piece(I, t, re);
+        else
+            for (int cs = t; cs < te && cs < re; cs += SPA_BLK)
+                piece(I, cs, min(cs + SPA_BLK, re));
+        t = re;
+    }
+}
 
 __device__ __forceinline__ void step3_spa_block(const ProdView &P, SpaSmem &S, int tb, int te)
 {
-    for (int t = tb; t < te;)
-    {
-        const int I = P.C_row[t];
-        const int rend = min(te, P.C_ptr[I + 1]);
-        for (int t0 = t; t0 < rend;)
+    spa_block_pieces(P, tb, te, [&](int I, int ps, int pe) {
+        for (int t0 = ps; t0 < pe;)
         {
             const int cand = t0 + 1 + (int)threadIdx.x;
-            const bool ok = threadIdx.x < SPA_SEGT && cand <= rend && P.C_tnnz[cand] - P.C_tnnz[t0] <= SPA_CAP &&
+            const bool ok = threadIdx.x < SPA_SEGT && cand <= pe && P.C_tnnz[cand] - P.C_tnnz[t0] <= SPA_CAP &&
                             P.C_col[cand - 1] - P.C_col[t0] < SPA_WIN;
             const int n = __syncthreads_count(ok);
             const int t1 = t0 + (n > 0 ? n : 1);
             step3_spa_segment(P, S, t0, t1);
             t0 = t1;
         }
-        t = rend;
-    }
+    });
 }
 
-// Symbolic counterpart, for the tiles of wide rows only (wide[I] != 0).
+// Symbolic counterpart, for the pieces of wide rows only (wide[I] != 0).
 __device__ __forceinline__ void step2_spa_block(const ProdView &P, Spa2Smem &S, int tb, int te,
                                                 const int *__restrict__ wide, int *s_bins)
 {
-    for (int t = tb; t < te;)
-    {
-        const int I = P.C_row[t];
-        const int rend = min(te, P.C_ptr[I + 1]);
-        if (wide[I])
+    spa_block_pieces(P, tb, te, [&](int I, int ps, int pe) {
+        if (!wide[I])
+            return;
+        for (int t0 = ps; t0 < pe;)
         {
-            for (int t0 = t; t0 < rend;)
-            {
-                const int cand = t0 + 1 + (int)threadIdx.x;
-                const bool ok = threadIdx.x < SP2_SEGT && cand <= rend && P.C_col[cand - 1] - P.C_col[t0] < SP2_WIN;
-                const int n = __syncthreads_count(ok);
-                const int t1 = t0 + (n > 0 ? n : 1);
-                step2_spa_segment(P, S, t0, t1, s_bins);
-                t0 = t1;
-            }
+            const int cand = t0 + 1 + (int)threadIdx.x;
+            const bool ok = threadIdx.x < SP2_SEGT && cand <= pe && P.C_col[cand - 1] - P.C_col[t0] < SP2_WIN;
+            const int n = __syncthreads_count(ok);
+            const int t1 = t0 + (n > 0 ? n : 1);
+            step2_spa_segment(P, S, t0, t1, s_bins);
+            t0 = t1;
         }
-        t = rend;
-    }
+    });
 }
 
 // ---------------------------------------------------------------------------
