@@ -32,7 +32,8 @@ from . import TSG_TILED_CSC_VIEW, Batch, Context, check, csr_host_to_tiled, lib,
 
 
 class Job:
-    __slots__ = ("jid", "kind", "a_key", "b_key", "t_submit", "t_done", "future", "pred_bytes", "result_nnz")
+    __slots__ = ("jid", "kind", "a_key", "b_key", "t_submit", "t_done", "future", "pred_bytes", "pred_prods",
+                 "result_nnz")
 
     def __init__(self, jid, kind, a_key, b_key):
         self.jid, self.kind, self.a_key, self.b_key = jid, kind, a_key, b_key
@@ -40,6 +41,7 @@ class Job:
         self.t_done = None
         self.future = Future()
         self.pred_bytes = 0
+        self.pred_prods = 0
         self.result_nnz = 0
 
 
@@ -109,14 +111,20 @@ class SpGEMMServer:
     mem_cap   bytes of device memory the server may hold (operands + arenas)
     slots     batches that may be in flight at once (one stream each)
     max_batch jobs per batch
+    batch_products  scalar-product budget of a batch (the jobs' step-1
+              bounds): a batch closes once it holds this much work, so a few
+              large jobs do not hold many small ones back (a single job
+              above it still runs, alone)
     schedule  (schedule, seg_tiles, acc_cap) of the batched kernel, e.g. the
               autotuner's choice
     """
 
-    def __init__(self, device=0, mem_cap=40 << 30, slots=2, max_batch=64, schedule=("spa", 8, 512)):
+    def __init__(self, device=0, mem_cap=40 << 30, slots=2, max_batch=64, schedule=("spa", 8, 512),
+                 batch_products=2e8):
         self.device = device
         self.mem_cap = int(mem_cap)
         self.max_batch = max_batch
+        self.batch_products = float(batch_products)
         self.schedule = schedule
         self.matrices = {}
         self.slots = [_Slot(device) for _ in range(slots)]
@@ -189,15 +197,17 @@ class SpGEMMServer:
         return self.cache.bytes + sum(s.arena for s in self.slots if s.batch is not None)
 
     def _predict(self, A, B):
+        """(device bytes of the result arena, scalar products) from the step-1
+        bounds."""
         prods, pairs = product_bounds(self.cache.ctx, A, B)
         tiles = pairs
         full = A.s.tilem * B.s.tilen
         tiles = min(tiles, full)
         vals = min(prods, 256 * tiles)
-        return tiles * (4 * 3 + 4 + 32 + 16) + vals * 9 + (A.s.tilem + 1) * 4
+        return tiles * (4 * 3 + 4 + 32 + 16) + vals * 9 + (A.s.tilem + 1) * 4, prods
 
     def _form_batch(self, slot):
-        jobs, pairs, pred = [], [], 0
+        jobs, pairs, pred, work = [], [], 0, 0
         # operands of batches still running must stay resident
         pinned = {k for s in self.slots if s.batch is not None for j in s.jobs for k in (j.a_key, j.b_key)}
         while self.queue and len(jobs) < self.max_batch:
@@ -205,7 +215,9 @@ class SpGEMMServer:
             A = self.cache.get(job.a_key, self.matrices[job.a_key])
             B = self.cache.get(job.b_key, self.matrices[job.b_key])
             pinned.update((job.a_key, job.b_key))
-            job.pred_bytes = self._predict(A, B)
+            job.pred_bytes, job.pred_prods = self._predict(A, B)
+            if jobs and work + job.pred_prods > self.batch_products:
+                break  # the batch holds its share of work; this job opens the next
             if job.pred_bytes > self.mem_cap:
                 self.queue.popleft()
                 self.rejected += 1
@@ -220,6 +232,7 @@ class SpGEMMServer:
             jobs.append(job)
             pairs.append((A, B))
             pred += job.pred_bytes
+            work += job.pred_prods
         if not jobs:
             return False
         sch, seg, cap = self.schedule
