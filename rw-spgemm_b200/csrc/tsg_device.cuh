@@ -712,7 +712,7 @@ struct SpaStage
 struct SpaSmem
 {
     double acc[SPA_CAP];
-    unsigned cm[SPA_SEGT * TSG_BS]; // (row's first slot << 16) | C row mask
+    unsigned cm[TSG_BS * SPA_SEGT]; // [row][tile]: (row's first slot << 16) | C row mask
     unsigned short map[SPA_WIN];    // tile column - J0 -> segment tile, 0xFFFF none
     SpaStage stage[SPA_WARPS];
 };
@@ -725,7 +725,7 @@ __device__ __forceinline__ void spa_add(SpaSmem &S, int r, int J0, int J1, bool 
     const int slot = S.map[J - J0];
     if (slot >= SPA_SEGT)
         return;
-    const unsigned cmw = S.cm[slot * TSG_BS + r];
+    const unsigned cmw = S.cm[r * SPA_SEGT + slot];
     const int pos = (int)(cmw >> 16) + __popc((cmw & 0xFFFFu) >> (16 - (col & 15)));
     if (pos < SPA_CAP)
         S.acc[pos] = __dadd_rn(S.acc[pos], __dmul_rn(a, b));
@@ -753,7 +753,7 @@ __device__ __forceinline__ void step3_spa_segment(const ProdView &P, SpaSmem &S,
         const int jl = u >> 4, rr = u & 15;
         const long long tt = (long long)(t0 + jl) * TSG_BS + rr;
         const unsigned b = (unsigned)(P.C_tnnz[t0 + jl] - base0 + P.C_Ptr[tt]);
-        S.cm[u] = (b << 16) | P.C_mask[tt];
+        S.cm[rr * SPA_SEGT + jl] = (b << 16) | P.C_mask[tt];
         if (rr == 0)
         {
             const int w = P.C_col[t0 + jl] - J0;
@@ -852,7 +852,7 @@ __device__ __forceinline__ void step3_spa_segment(const ProdView &P, SpaSmem &S,
         P.C_Val[base0 + q] = S.acc[q];
     for (int u = tid; u < nt * TSG_BS; u += SPA_THREADS)
     {
-        const unsigned cmw = S.cm[u];
+        const unsigned cmw = S.cm[(u & 15) * SPA_SEGT + (u >> 4)];
         unsigned mk = cmw & 0xFFFFu;
         int p = base0 + (int)(cmw >> 16);
         while (mk)
@@ -884,7 +884,7 @@ struct Spa2Stage
 
 struct Spa2Smem
 {
-    unsigned m[SP2_SEGT * TSG_BS];
+    unsigned m[TSG_BS * SP2_SEGT]; // [row][tile] mask words
     unsigned short map[SP2_WIN];
     Spa2Stage stage[SPA_WARPS];
 };
@@ -900,7 +900,7 @@ __device__ __forceinline__ void step2_spa_segment(const ProdView &P, Spa2Smem &S
     const bool full = t0 == P.C_ptr[I] && t1 == P.C_ptr[I + 1];
     __syncthreads();
     for (int q = tid; q < nt * TSG_BS; q += SPA_THREADS)
-        S.m[q] = 0u;
+        S.m[(q & 15) * SP2_SEGT + (q >> 4)] = 0u;
     for (int q = tid; q < win; q += SPA_THREADS)
         S.map[q] = 0xFFFF;
     __syncthreads();
@@ -994,7 +994,7 @@ __device__ __forceinline__ void step2_spa_segment(const ProdView &P, Spa2Smem &S
                     continue;
                 const int slot = S.map[J - J0];
                 if (slot < nt)
-                    atomicOr(&S.m[slot * TSG_BS + r], 1u << (15 - (col & 15)));
+                    atomicOr(&S.m[r * SP2_SEGT + slot], 1u << (15 - (col & 15)));
             }
         }
     }
@@ -1002,7 +1002,7 @@ __device__ __forceinline__ void step2_spa_segment(const ProdView &P, Spa2Smem &S
     // half-warp per C tile: row offsets, masks, tile count, bin
     const unsigned hmask = TSG_HW_MASK(tid);
     for (int jl = tid >> 4; jl < nt; jl += SPA_THREADS / 16)
-        step2_store(P, t0 + jl, hmask, tid & 15, S.m[jl * TSG_BS + (tid & 15)], s_bins);
+        step2_store(P, t0 + jl, hmask, tid & 15, S.m[(tid & 15) * SP2_SEGT + jl], s_bins);
 }
 
 // Work item of the SPA steps: a block of SPA_BLK consecutive C tiles (global
