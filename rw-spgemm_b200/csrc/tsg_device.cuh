@@ -1014,8 +1014,9 @@ __device__ __forceinline__ void step2_spa_segment(const ProdView &P, Spa2Smem &S
 // further into segments within the SPA limits.
 #define SPA_BLK 256
 
-// calls piece(t0, t1) for the pieces [t0, t1) owned by block [tb, te)
-template <typename F>
+// calls piece(I, t0, t1) for the pieces [t0, t1) owned by block [tb, te),
+// rows longer than CH tiles being cut into CH-tile chunks
+template <int CH, typename F>
 __device__ __forceinline__ void spa_block_pieces(const ProdView &P, int tb, int te, F piece)
 {
     int t = tb;
@@ -1024,9 +1025,9 @@ __device__ __forceinline__ void spa_block_pieces(const ProdView &P, int tb, int 
         const int rs = P.C_ptr[I], re = P.C_ptr[I + 1];
         if (rs < tb)
         {
-            if (re - rs > SPA_BLK)
-                for (int cs = rs + ((tb - rs + SPA_BLK - 1) / SPA_BLK) * SPA_BLK; cs < te && cs < re; cs += SPA_BLK)
-                    piece(I, cs, min(cs + SPA_BLK, re));
+            if (re - rs > CH)
+                for (int cs = rs + ((tb - rs + CH - 1) / CH) * CH; cs < te && cs < re; cs += CH)
+                    piece(I, cs, min(cs + CH, re));
             t = re;
         }
     }
@@ -1034,18 +1035,18 @@ __device__ __forceinline__ void spa_block_pieces(const ProdView &P, int tb, int 
     {
         const int I = P.C_row[t];
         const int re = P.C_ptr[I + 1];
-        if (re - t <= SPA_BLK)
+        if (re - t <= CH)
             piece(I, t, re);
         else
-            for (int cs = t; cs < te && cs < re; cs += SPA_BLK)
-                piece(I, cs, min(cs + SPA_BLK, re));
+            for (int cs = t; cs < te && cs < re; cs += CH)
+                piece(I, cs, min(cs + CH, re));
         t = re;
     }
 }
 
 __device__ __forceinline__ void step3_spa_block(const ProdView &P, SpaSmem &S, int tb, int te)
 {
-    spa_block_pieces(P, tb, te, [&](int I, int ps, int pe) {
+    spa_block_pieces<SPA_BLK>(P, tb, te, [&](int I, int ps, int pe) {
         for (int t0 = ps; t0 < pe;)
         {
             const int cand = t0 + 1 + (int)threadIdx.x;
@@ -1063,7 +1064,7 @@ __device__ __forceinline__ void step3_spa_block(const ProdView &P, SpaSmem &S, i
 __device__ __forceinline__ void step2_spa_block(const ProdView &P, Spa2Smem &S, int tb, int te,
                                                 const int *__restrict__ wide, int *s_bins)
 {
-    spa_block_pieces(P, tb, te, [&](int I, int ps, int pe) {
+    spa_block_pieces<SP2_SEGT>(P, tb, te, [&](int I, int ps, int pe) {
         if (!wide[I])
             return;
         for (int t0 = ps; t0 < pe;)
