@@ -49,7 +49,11 @@ __global__ void __launch_bounds__(256) k_step12(ProdView P, int *__restrict__ wi
             step1_row<true>(P, i, reinterpret_cast<unsigned *>(&sm[warp]), lane, nullptr);
         }
         if (lane == 0)
+        {
             wide[i] = done ? 0 : 1;
+            if (!done)
+                atomicAdd(&wide[P.tilemA], 1); // count of wide rows
+        }
     }
     __syncthreads();
     if (threadIdx.x < 4 && s_bins[threadIdx.x])
@@ -80,6 +84,8 @@ __global__ void __launch_bounds__(SPA_THREADS) k_step2_spa(ProdView P, const int
     Spa2Smem &S = *reinterpret_cast<Spa2Smem *>(s_raw);
     __shared__ int s_bins[4];
     __shared__ int s_blk;
+    if (wide[P.tilemA] == 0) // no wide row (k_step12 counted them)
+        return;
     if (threadIdx.x < 4)
         s_bins[threadIdx.x] = 0;
     for (;;)
@@ -394,7 +400,8 @@ extern "C" int tsg_spgemm(tsg_context *ctx, const tsg_tiled *A, const tsg_tiled 
         ProdView P = make_view(A, B, C);
         if (fused)
         {
-            TSG_TRY(tsg_alloc(ctx, &d_wide, (size_t)tilem));
+            TSG_TRY(tsg_alloc(ctx, &d_wide, (size_t)tilem + 1));
+            TSG_CUDA(cudaMemsetAsync(d_wide + tilem, 0, sizeof(int), st));
             k_step12<<<tsg_blocks(tilem, 8), 256, 0, st>>>(P, d_wide, d_bins);
             TSG_LAUNCH_CHECK();
         }
