@@ -161,7 +161,7 @@ struct S12Smem
 {
     unsigned bm[S12_WORDS];
     unsigned short pre[S12_WORDS];
-    unsigned short acc[S12_MAXT][16];
+    unsigned short acc[16][S12_MAXT + 2]; // [row][slot], padded: both access forms spread over banks
 };
 
 __device__ __forceinline__ int step12_row(const ProdView &P, int i, S12Smem &sm, int lane, int *s_bins)
@@ -232,7 +232,7 @@ __device__ __forceinline__ int step12_row(const ProdView &P, int i, S12Smem &sm,
     }
     const int r = lane & 15, half = lane >> 4;
     for (int q = half; q < ntiles; q += 2)
-        sm.acc[q][r] = 0;
+        sm.acc[r][q] = 0;
     __syncwarp();
     // OR the boolean products of all (A tile, B tile) pairs of the row: unit
     // (row r, B tile) ORs the B rows its A row meets -- one 16-bit load per
@@ -240,8 +240,55 @@ __device__ __forceinline__ int step12_row(const ProdView &P, int i, S12Smem &sm,
     for (int pa = a0; pa < a1; pa++)
     {
         const int k = P.A_col[pa];
-        const unsigned ma = P.A_mask[(long long)pa * TSG_BS + r];
         const int b0 = P.B_ptr[k], b1 = P.B_ptr[k + 1];
+        if (b1 - b0 >= 8)
+        {
+            // lane per B tile; the A tile's row masks are the same for all
+            // lanes, so the walk over its set bits does not diverge
+            const uint4 *amq = reinterpret_cast<const uint4 *>(P.A_mask + (long long)pa * TSG_BS);
+            const uint4 aq0 = __ldg(amq), aq1 = __ldg(amq + 1);
+            const unsigned aw[8] = {aq0.x, aq0.y, aq0.z, aq0.w, aq1.x, aq1.y, aq1.z, aq1.w};
+            // A tile with a dense row: B's masks as two 16-byte loads
+            const bool adense = __popc(aq0.x) + __popc(aq0.y) + __popc(aq0.z) + __popc(aq0.w) + __popc(aq1.x) +
+                                    __popc(aq1.y) + __popc(aq1.z) + __popc(aq1.w) > 64;
+            for (int pb = b0 + lane; pb < b1; pb += 32)
+            {
+                const int j = P.B_col[pb] - c0;
+                const int slot = sm.pre[j >> 5] + __popc(sm.bm[j >> 5] & ((1u << (j & 31)) - 1u));
+                const unsigned short *mbk = P.B_mask + (long long)pb * TSG_BS;
+                if (adense)
+                {
+                    const uint4 *mb = reinterpret_cast<const uint4 *>(mbk);
+                    const uint4 q0 = __ldg(mb), q1 = __ldg(mb + 1);
+#pragma unroll
+                    for (int rr = 0; rr < 16; rr++)
+                    {
+                        const unsigned mrow = (rr & 1) ? (aw[rr >> 1] >> 16) : (aw[rr >> 1] & 0xFFFFu);
+                        if (mrow)
+                            sm.acc[rr][slot] |= (unsigned short)bool_row(mrow, q0, q1);
+                    }
+                    continue;
+                }
+#pragma unroll
+                for (int rr = 0; rr < 16; rr++)
+                {
+                    const unsigned mrow = (rr & 1) ? (aw[rr >> 1] >> 16) : (aw[rr >> 1] & 0xFFFFu);
+                    if (!mrow)
+                        continue;
+                    unsigned acc = 0, bits = mrow;
+                    do
+                    {
+                        const int bit = 31 - __clz(bits);
+                        bits ^= 1u << bit;
+                        acc |= __ldg(mbk + (15 - bit));
+                    } while (bits);
+                    sm.acc[rr][slot] |= (unsigned short)acc;
+                }
+            }
+            __syncwarp();
+            continue;
+        }
+        const unsigned ma = P.A_mask[(long long)pa * TSG_BS + r];
         if (ma)
         {
             const bool dense_row = __popc(ma) > 4;
@@ -266,7 +313,7 @@ __device__ __forceinline__ int step12_row(const ProdView &P, int i, S12Smem &sm,
                         acc |= __ldg(mbk + (15 - bit));
                     } while (bits);
                 }
-                sm.acc[slot][r] |= (unsigned short)acc;
+                sm.acc[r][slot] |= (unsigned short)acc;
             }
         }
         __syncwarp();
@@ -276,7 +323,7 @@ __device__ __forceinline__ int step12_row(const ProdView &P, int i, S12Smem &sm,
     for (int q0 = 0; q0 < ntiles; q0 += 2)
     {
         const int q = q0 + half;
-        const unsigned accm = q < ntiles ? sm.acc[q][r] : 0u;
+        const unsigned accm = q < ntiles ? sm.acc[r][q] : 0u;
         int total;
         const int excl = hw_excl_scan(hmask, r, __popc(accm), total);
         if (q < ntiles)
