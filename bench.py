@@ -81,11 +81,16 @@ class ClockSampler:
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        self.q = q
         try:
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                          "--format=csv,noheader,nounits", "-lms", "10"],
                                          stdout=self.fh, stderr=subprocess.DEVNULL)
+            # the timed region can be a few ms: start it only once sampling runs
+            t0 = time.time()
+            while time.time() - t0 < 5.0 and self.path.stat().st_size == 0 and self.proc.poll() is None:
+                time.sleep(0.01)
         except (OSError, FileNotFoundError):
             self.proc = None
         return self
@@ -98,6 +103,14 @@ class ClockSampler:
             except subprocess.TimeoutExpired:
                 self.proc.kill()
             self.fh.close()
+            # and one reading right at the end of the region
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=20)
+                with open(self.path, "a") as fh:
+                    fh.write(out.stdout)
+            except (OSError, subprocess.SubprocessError):
+                pass
 
     def summary(self):
         if not self.proc or not self.path.exists():

@@ -96,6 +96,7 @@ class _Slot:
 
     def __init__(self, device):
         self.ctx = Context(device, own_stream=True)
+        self.staging = None  # page-locked result staging, grown on demand
         self.batch = None
         self.jobs = []
         self.arena = 0
@@ -117,10 +118,16 @@ class SpGEMMServer:
               above it still runs, alone)
     schedule  (schedule, seg_tiles, acc_cap) of the batched kernel, e.g. the
               autotuner's choice
+    deliver   "host": a job's result is (m, n, rowptr, colidx, val) as numpy
+              arrays; "device": the same as torch tensors on the GPU (for a
+              consumer that stays on the device; nothing crosses the bus)
     """
 
     def __init__(self, device=0, mem_cap=40 << 30, slots=2, max_batch=64, schedule=("spa", 8, 512),
-                 batch_products=2e8):
+                 batch_products=2e8, deliver="host"):
+        if deliver not in ("host", "device"):
+            raise ValueError(deliver)
+        self.deliver = deliver
         self.device = device
         self.mem_cap = int(mem_cap)
         self.max_batch = max_batch
@@ -246,9 +253,10 @@ class SpGEMMServer:
 
     def _finish(self, slot):
         """Converts every product of the finished batch to CSR on the device
-        into one buffer (all conversions queued on the slot's stream), brings
-        the buffer to page-locked host memory in one copy and completes each
-        job's future with numpy views into it (they keep it alive)."""
+        (all conversions queued on the slot's stream, one synchronisation).
+        deliver="device": each job gets its device tensors.  deliver="host":
+        the batch's results go through the slot's reusable page-locked
+        staging buffer (one copy) into numpy arrays of each job."""
         import torch
         slot.batch.sync()
         dev = torch.device("cuda", self.device)
@@ -267,16 +275,29 @@ class SpGEMMServer:
             check(lib().tsg_tiled_to_csr(slot.ctx.handle, ctypes.byref(C.s), ctypes.c_void_p(base + rp_off),
                                          ctypes.c_void_p(base + ci_off), ctypes.c_void_p(base + v_off)))
         slot.ctx.synchronize()
-        hbuf = torch.empty(max(total, 8), dtype=torch.uint8, pin_memory=True)
-        hbuf.copy_(dbuf)
-        raw = hbuf.numpy()
-        for job, C, m, n, nnz, v_off, rp_off, ci_off in layout:
-            res = (m, n, raw[rp_off:rp_off + 4 * (m + 1)].view(np.int32), raw[ci_off:ci_off + 4 * nnz].view(np.int32),
-                   raw[v_off:v_off + 8 * nnz].view(np.float64))
-            job.t_done = time.perf_counter()
-            job.result_nnz = nnz
-            job.future.set_result(res)
-            self.done.append(job)
+        if self.deliver == "device":
+            for job, C, m, n, nnz, v_off, rp_off, ci_off in layout:
+                res = (m, n, dbuf[rp_off:rp_off + 4 * (m + 1)].view(torch.int32),
+                       dbuf[ci_off:ci_off + 4 * nnz].view(torch.int32), dbuf[v_off:v_off + 8 * nnz].view(torch.float64))
+                self._complete(job, nnz, res)
+        else:
+            if slot.staging is None or slot.staging.numel() < total:
+                slot.staging = torch.empty(max(total, 1 << 20), dtype=torch.uint8, pin_memory=True)
+            slot.staging[:max(total, 8)].copy_(dbuf)
+            raw = slot.staging.numpy()
+            for job, C, m, n, nnz, v_off, rp_off, ci_off in layout:
+                res = (m, n, raw[rp_off:rp_off + 4 * (m + 1)].view(np.int32).copy(),
+                       raw[ci_off:ci_off + 4 * nnz].view(np.int32).copy(), raw[v_off:v_off + 8 * nnz].view(np.float64).copy())
+                self._complete(job, nnz, res)
+        self._release(slot)
+
+    def _complete(self, job, nnz, res):
+        job.t_done = time.perf_counter()
+        job.result_nnz = nnz
+        job.future.set_result(res)
+        self.done.append(job)
+
+    def _release(self, slot):
         slot.batch.close()
         slot.batch = None
         slot.jobs = []

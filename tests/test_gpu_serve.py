@@ -116,3 +116,21 @@ def test_concurrent_submitters(srv_mod, gen):
     st = srv.stats()
     srv.close()
     assert st["jobs"] == 60 and st["batches"] >= 2
+
+
+def test_device_delivery_matches_host_delivery(srv_mod, gen):
+    mats = _matrices(gen)
+    jobs = _jobs(mats, random.Random(11), 12)
+    res = {}
+    for mode in ("host", "device"):
+        srv = srv_mod.SpGEMMServer(0, mem_cap=8 << 30, slots=2, max_batch=8, deliver=mode)
+        for k, m in mats.items():
+            srv.register(k, m)
+        srv.start()
+        futs = [srv.submit(kind, a, b) for kind, a, b in jobs]
+        res[mode] = [f.result(timeout=120) for f in futs]
+        srv.close()
+    for h, d in zip(res["host"], res["device"]):
+        assert h[0] == d[0] and h[1] == d[1]
+        for x, y in zip(h[2:], d[2:]):
+            assert np.array_equal(np.asarray(x).view(np.uint8), y.cpu().numpy().view(np.uint8))
