@@ -323,10 +323,14 @@ def _served_stream(srv, jobs, rate, rng):
     return srv.stats(), time.perf_counter() - t0
 
 
-def run_served(args, tsg, gen, device):
+def run_served(args, tsg, gen, device, deliver="device", n_jobs=None, half_capacity=True):
+    """deliver="device": results handed over as device tensors (the GPU
+    service alone); "host": as numpy arrays in page-locked memory (every
+    result crosses the bus)."""
     srv_mod = _load("rw_spgemm_b200.serve", PKG_DIR / "serve.py")
     small, rmat = served_pool(gen)
-    srv = srv_mod.SpGEMMServer(device, mem_cap=40 << 30, slots=2, max_batch=64, schedule=tuple(args.served_schedule))
+    srv = srv_mod.SpGEMMServer(device, mem_cap=40 << 30, slots=2, max_batch=64, schedule=tuple(args.served_schedule),
+                               deliver=deliver)
     keys = []
     for i, m in enumerate(small):
         srv.register(f"s{i}", m)
@@ -339,7 +343,7 @@ def run_served(args, tsg, gen, device):
     jobs = []
     by_kind = {"small": [k for k in keys if k[0] == "small"], 14: [k for k in keys if k[0] == 14],
                15: [k for k in keys if k[0] == 15], 16: [k for k in keys if k[0] == 16]}
-    for _ in range(args.served_jobs):
+    for _ in range(n_jobs or args.served_jobs):
         u = rng.random()
         cls = "small" if u < 0.85 else 14 if u < 0.95 else 15 if u < 0.99 else 16
         _, key, mat = by_kind[cls][int(rng.integers(0, len(by_kind[cls])))]
@@ -361,7 +365,11 @@ def run_served(args, tsg, gen, device):
            "jobs": st["jobs"], "jobs_per_s": round(st["jobs_per_s"], 1), "p50_ms": round(st["p50_ms"], 3),
            "p99_ms": round(st["p99_ms"], 3), "gflops": round(2.0 * prods / wall / 1e9, 2),
            "batches": st["batches"], "mean_batch": round(st["mean_batch"], 2), "rejected": st["rejected"],
-           "operand_cache": st["operand_cache"], "schedule": list(args.served_schedule), "mem_cap_gb": 40}
+           "operand_cache": st["operand_cache"], "schedule": list(args.served_schedule), "mem_cap_gb": 40,
+           "deliver": deliver}
+    if not half_capacity:
+        srv.close()
+        return out
     # the same mix below saturation: half the throughput the stream above reached
     rate2 = max(1.0, 0.5 * st["jobs_per_s"])
     sub = jobs[:max(100, min(len(jobs), int(rate2 * 10)))]
@@ -560,8 +568,11 @@ def run_ours(args, tsg, gen, world, rank, local):
     A.free()
     if "batched" in args.sections:
         batched = run_batched(args, tsg, gen, ctx, max(2, min(args.steps, 5)))
+    served_host = None
     if "served" in args.sections:
-        served = run_served(args, tsg, gen, local)
+        served = run_served(args, tsg, gen, local, deliver="device")
+        served_host = run_served(args, tsg, gen, local, deliver="host", n_jobs=min(args.served_jobs, 600),
+                                 half_capacity=False)
     selector = run_selector(args, tsg, gen, ctx) if "selector" in args.sections else None
     orderings = run_orderings(args, tsg, gen, ctx) if "orderings" in args.sections else None
     out = {
@@ -594,6 +605,8 @@ def run_ours(args, tsg, gen, world, rank, local):
         out["batched"] = batched
     if served:
         out["served"] = served
+    if served_host:
+        out["served_host_delivery"] = served_host
     if selector:
         out["selector"] = selector
     if orderings:
