@@ -96,6 +96,7 @@ class _Slot:
 
     def __init__(self, device):
         self.ctx = Context(device, own_stream=True)
+        self.staging = None  # page-locked result staging, grown on demand
         self.batch = None
         self.jobs = []
         self.arena = 0
@@ -254,8 +255,9 @@ class SpGEMMServer:
         """Converts every product of the finished batch to CSR on the device
         (all conversions queued on the slot's stream, one synchronisation).
         deliver="device": each job gets its device tensors.  deliver="host":
-        the batch's results come to page-locked host memory in one copy and
-        each job gets numpy views of it."""
+        the batch's results go through the slot's reusable page-locked
+        staging buffer (one copy; pinning fresh memory per batch costs more)
+        into numpy arrays of each job."""
         import torch
         slot.batch.sync()
         dev = torch.device("cuda", self.device)
@@ -280,15 +282,13 @@ class SpGEMMServer:
                        dbuf[ci_off:ci_off + 4 * nnz].view(torch.int32), dbuf[v_off:v_off + 8 * nnz].view(torch.float64))
                 self._complete(job, nnz, res)
         else:
-            # one page-locked buffer per batch (recycled by torch's caching
-            # host allocator once every job has dropped its arrays); results
-            # are numpy views of it
-            hbuf = torch.empty(max(total, 8), dtype=torch.uint8, pin_memory=True)
-            hbuf.copy_(dbuf)
-            raw = hbuf.numpy()
+            if slot.staging is None or slot.staging.numel() < total:
+                slot.staging = torch.empty(max(total, 1 << 20), dtype=torch.uint8, pin_memory=True)
+            slot.staging[:max(total, 8)].copy_(dbuf)
+            raw = slot.staging.numpy()
             for job, C, m, n, nnz, v_off, rp_off, ci_off in layout:
-                res = (m, n, raw[rp_off:rp_off + 4 * (m + 1)].view(np.int32), raw[ci_off:ci_off + 4 * nnz].view(np.int32),
-                       raw[v_off:v_off + 8 * nnz].view(np.float64))
+                res = (m, n, raw[rp_off:rp_off + 4 * (m + 1)].view(np.int32).copy(),
+                       raw[ci_off:ci_off + 4 * nnz].view(np.int32).copy(), raw[v_off:v_off + 8 * nnz].view(np.float64).copy())
                 self._complete(job, nnz, res)
         self._release(slot)
 
