@@ -141,6 +141,23 @@ def dist_setup():
     return world, rank, local
 
 
+def max_over_ranks(value, dist=None, device=None):
+    """The largest of every rank's value (the job's time is its slowest
+    rank's); the value itself without a process group."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_gflops(products_per_rank, world, ms_per_step):
+    """Whole-job GFLOP/s of `world` independent replicas, each computing
+    products_per_rank scalar products per step (2 flops each)."""
+    return 2.0 * products_per_rank * world / (ms_per_step * 1e-3) / 1e9
+
+
 def workload_matrix(gen):
     return gen.stencil_27pt_3d(64, seed=0)
 
@@ -527,13 +544,9 @@ def run_ours(args, tsg, gen, world, rank, local):
     if dist:
         dist.barrier()
     ctx.set_timing(False)
-    total_ms = float(np.sum(step_ms))
-    if dist:
-        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(float(np.sum(step_ms)), dist, dev)
     ms_per_step = total_ms / args.steps
-    value = 2.0 * prods * world / (ms_per_step * 1e-3) / 1e9
+    value = replica_gflops(prods, world, ms_per_step)
 
     # roofline of the dominant kernel (numeric step)
     peak, peak_src = measured_peak_hbm()
