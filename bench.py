@@ -480,6 +480,57 @@ def run_orderings(args, tsg, gen, ctx, reps=3):
     return out
 
 
+def run_rmat20(args, tsg, gen, ctx, budget=1.5e9):
+    """R-MAT scale 20 (edge factor 16, a,b,c,d = .57,.19,.19,.05, duplicates
+    merged, values U(-1,1)): C = A*A and C = A*A^T.  C (~9.5e9 nonzeros) does
+    not fit one GPU, so A goes in blocks of tile rows holding at most `budget`
+    scalar products each; every block is converted, multiplied (steps 1-3 on
+    the resident B) and its C freed.  GFLOP/s over the steps-1-3 time of all
+    blocks; wall time includes the block conversions."""
+    import torch
+    A = gen.rmat(20, 16, seed=1)
+    m, n, rp, ci, v = A
+    out = {"workload": "R-MAT scale 20, edge factor 16 (n=1,048,576), FP64 U(-1,1); A in row blocks of <= %.1e "
+                       "products" % budget}
+    for label, B in (("A*A", A), ("A*A^T", gen.transpose(A))):
+        TB = tsg.csr_host_to_tiled(ctx, B, tsg.TSG_TILED_CSC_VIEW)
+        blen = np.diff(B[2]).astype(np.int64)
+        rowprod = np.zeros(m, np.int64)
+        nz = np.diff(rp) > 0
+        rowprod[nz] = np.add.reduceat(blen[ci], rp[:-1][nz])
+        tileprod = np.add.reduceat(rowprod, np.arange(0, m, 16))
+        bounds, acc = [0], 0
+        for t, pt in enumerate(tileprod):
+            if acc > 0 and acc + pt > budget:
+                bounds.append(t)
+                acc = 0
+            acc += int(pt)
+        bounds.append(len(tileprod))
+        ctx.set_timing(True)
+        steps_ms, prods, nnz, tiles = 0.0, 0, 0, 0
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for b0, b1 in zip(bounds[:-1], bounds[1:]):
+            r0, r1 = b0 * 16, min(b1 * 16, m)
+            blk = (r1 - r0, n, (rp[r0:r1 + 1] - rp[r0]).astype(np.int32), ci[rp[r0]:rp[r1]], v[rp[r0]:rp[r1]])
+            TA = tsg.csr_host_to_tiled(ctx, blk, tsg.TSG_TILED_PACKED_COL)
+            C, info = tsg.spgemm(ctx, TA, TB)
+            steps_ms += info["ms_total"]
+            nnz += info["nnz_C"]
+            tiles += info["numtile_C"]
+            C.free()
+            TA.free()
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        ctx.set_timing(False)
+        prods = int(rowprod.sum())
+        TB.free()
+        out[label] = {"products": prods, "nnz_C": int(nnz), "tiles_C": int(tiles), "blocks": len(bounds) - 1,
+                      "ms_steps_1_3": round(steps_ms, 1), "gflops": round(2.0 * prods / (steps_ms * 1e-3) / 1e9, 2),
+                      "wall_s": round(wall, 2)}
+    return out
+
+
 def res_name(sel, idx):
     o, a = sel.CONFIGS[idx]
     return f"{o}/{a[0]}-{a[1]}-{a[2]}"
@@ -588,6 +639,7 @@ def run_ours(args, tsg, gen, world, rank, local):
                                  half_capacity=False)
     selector = run_selector(args, tsg, gen, ctx) if "selector" in args.sections else None
     orderings = run_orderings(args, tsg, gen, ctx) if "orderings" in args.sections else None
+    rmat20 = run_rmat20(args, tsg, gen, ctx) if "rmat20" in args.sections else None
     out = {
         "metric": METRIC, "value": round(value, 3), "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,
@@ -624,6 +676,8 @@ def run_ours(args, tsg, gen, world, rank, local):
         out["selector"] = selector
     if orderings:
         out["orderings"] = orderings
+    if rmat20:
+        out["rmat20"] = rmat20
     if rank == 0:
         print(json.dumps(out), flush=True)
     ctx.close()

@@ -759,12 +759,14 @@ struct SpaStage
 struct SpaSmem
 {
     double acc[SPA_CAP];
-    unsigned cm[TSG_BS * SPA_SEGT]; // [row][tile]: (row's first slot << 16) | C row mask
+    unsigned cm[TSG_BS * SPA_SEGT]; // [row][tile]: (entries of the row in earlier tiles << 16) | C row mask
+    int rstart[TSG_BS];             // first accumulator slot of each row's private, column-sorted run
     unsigned short map[SPA_WIN];    // tile column - J0 -> segment tile, 0xFFFF none
     SpaStage stage[SPA_WARPS];
 };
 
-__device__ __forceinline__ void spa_add(SpaSmem &S, int r, int J0, int J1, bool full, int col, double a, double b)
+__device__ __forceinline__ void spa_add(SpaSmem &S, int r, int rs, int J0, int J1, bool full, int col, double a,
+                                        double b)
 {
     const int J = col >> 4;
     if (!full && (J < J0 || J >= J1 || J - J0 >= SPA_WIN))
@@ -773,7 +775,7 @@ __device__ __forceinline__ void spa_add(SpaSmem &S, int r, int J0, int J1, bool 
     if (slot >= SPA_SEGT)
         return;
     const unsigned cmw = S.cm[r * SPA_SEGT + slot];
-    const int pos = (int)(cmw >> 16) + __popc((cmw & 0xFFFFu) >> (16 - (col & 15)));
+    const int pos = rs + (int)(cmw >> 16) + __popc((cmw & 0xFFFFu) >> (16 - (col & 15)));
     if (pos < SPA_CAP)
         S.acc[pos] = __dadd_rn(S.acc[pos], __dmul_rn(a, b));
 }
@@ -798,9 +800,7 @@ __device__ __forceinline__ void step3_spa_segment(const ProdView &P, SpaSmem &S,
     for (int u = tid; u < nt * TSG_BS; u += SPA_THREADS)
     {
         const int jl = u >> 4, rr = u & 15;
-        const long long tt = (long long)(t0 + jl) * TSG_BS + rr;
-        const unsigned b = (unsigned)(P.C_tnnz[t0 + jl] - base0 + P.C_Ptr[tt]);
-        S.cm[rr * SPA_SEGT + jl] = (b << 16) | P.C_mask[tt];
+        S.cm[rr * SPA_SEGT + jl] = P.C_mask[(long long)(t0 + jl) * TSG_BS + rr];
         if (rr == 0)
         {
             const int w = P.C_col[t0 + jl] - J0;
@@ -809,6 +809,44 @@ __device__ __forceinline__ void step3_spa_segment(const ProdView &P, SpaSmem &S,
         }
     }
     __syncthreads();
+    // each row accumulates in a private run sorted by column (the entries
+    // of one B row then hit nearly consecutive slots: few bank conflicts);
+    // warp r: entries of row r in earlier tiles of the segment
+    {
+        int run = 0;
+        for (int s0 = 0; s0 < nt; s0 += 32)
+        {
+            const int sl = s0 + lane;
+            const unsigned m = sl < nt ? S.cm[r * SPA_SEGT + sl] : 0u;
+            const int c = __popc(m);
+            int incl = c;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1)
+            {
+                const int o = __shfl_up_sync(TSG_FULL_MASK, incl, d);
+                if (lane >= d)
+                    incl += o;
+            }
+            if (sl < nt)
+                S.cm[r * SPA_SEGT + sl] = ((unsigned)(run + incl - c) << 16) | m;
+            run += __shfl_sync(TSG_FULL_MASK, incl, 31);
+        }
+        if (lane == 0)
+            S.rstart[r] = run;
+    }
+    __syncthreads();
+    if (tid == 0)
+    {
+        int acc0 = 0;
+        for (int q = 0; q < TSG_BS; q++)
+        {
+            const int n = S.rstart[q];
+            S.rstart[q] = acc0;
+            acc0 += n;
+        }
+    }
+    __syncthreads();
+    const int rs = S.rstart[r];
     SpaStage &G = S.stage[r];
     const int pa_beg = P.A_ptr[I], pa_end = P.A_ptr[I + 1];
     for (int g = pa_beg; g < pa_end; g += 32)
@@ -885,9 +923,9 @@ __device__ __forceinline__ void step3_spa_segment(const ProdView &P, SpaSmem &S,
                 }
                 const double a = G.a[i];
                 if (c_cur >= 0)
-                    spa_add(S, r, J0, J1, full, c_cur, a, v_cur);
+                    spa_add(S, r, rs, J0, J1, full, c_cur, a, v_cur);
                 for (int e = G.bs[i] + 32 + lane; e < G.be[i]; e += 32)
-                    spa_add(S, r, J0, J1, full, P.B_rcol[e], a, P.B_rval[e]);
+                    spa_add(S, r, rs, J0, J1, full, P.B_rcol[e], a, P.B_rval[e]);
                 __syncwarp();
                 c_cur = c_nxt;
                 v_cur = v_nxt;
@@ -895,17 +933,25 @@ __device__ __forceinline__ void step3_spa_segment(const ProdView &P, SpaSmem &S,
         }
     }
     __syncthreads();
-    for (int q = tid; q < cn; q += SPA_THREADS)
-        P.C_Val[base0 + q] = S.acc[q];
+    // out to C's tiled layout: tile row (jl, rr) starts at the tile's value
+    // offset + its row offset; its values are the row's run from its prefix
     for (int u = tid; u < nt * TSG_BS; u += SPA_THREADS)
     {
-        const unsigned cmw = S.cm[(u & 15) * SPA_SEGT + (u >> 4)];
+        const int jl = u >> 4, rr = u & 15;
+        const unsigned cmw = S.cm[rr * SPA_SEGT + jl];
         unsigned mk = cmw & 0xFFFFu;
-        int p = base0 + (int)(cmw >> 16);
+        if (!mk)
+            continue;
+        const long long tt = (long long)(t0 + jl) * TSG_BS + rr;
+        int p = P.C_tnnz[t0 + jl] + P.C_Ptr[tt];
+        int q = S.rstart[rr] + (int)(cmw >> 16);
         while (mk)
         {
             const int bit = 31 - __clz(mk);
-            P.C_Colb[p++] = (unsigned char)(15 - bit);
+            P.C_Colb[p] = (unsigned char)(15 - bit);
+            P.C_Val[p] = q < SPA_CAP ? S.acc[q] : 0.0;
+            p++;
+            q++;
             mk ^= 1u << bit;
         }
     }
