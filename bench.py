@@ -695,7 +695,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--sched", default="spa", choices=["rows", "tiles", "elems", "spa"])
-    ap.add_argument("--sections", default="plain,batched,served,orderings",
+    ap.add_argument("--sections", default="plain,batched,served,orderings,rmat20",
                     help="comma list: plain (always), batched, served, selector")
     ap.add_argument("--batch-count", type=int, default=512)
     ap.add_argument("--selector-samples", type=int, default=5000)
