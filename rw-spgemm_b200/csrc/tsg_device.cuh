@@ -1157,7 +1157,7 @@ __device__ __forceinline__ void step3_spa_block(const ProdView &P, SpaSmem &S, i
 __device__ __forceinline__ void step2_spa_block(const ProdView &P, Spa2Smem &S, int tb, int te,
                                                 const int *__restrict__ wide, int *s_bins)
 {
-    spa_block_pieces<SP2_SEGT>(P, tb, te, [&](int I, int ps, int pe) {
+    spa_block_pieces<SPA_BLK>(P, tb, te, [&](int I, int ps, int pe) {
         if (!wide[I])
             return;
         for (int t0 = ps; t0 < pe;)
