@@ -257,3 +257,27 @@ def test_two_phase_end_to_end_into_caller_buffers(tsg, ctx, oracle, gen):
         np.testing.assert_array_equal(C[2], G[2])
         np.testing.assert_array_equal(C[3], G[3])
         assert_values(C[4], G[4])
+
+
+def test_row_blocks_of_a_give_the_whole_product(tsg, ctx, gen):
+    """C computed from blocks of A's tile rows (the large-product driver)
+    equals C computed at once, bit for bit."""
+    import torch
+    A = gen.rmat(12, 8, seed=21)
+    B = gen.transpose(A)
+    m, n, rp, ci, v = A
+    TB = tsg.csr_host_to_tiled(ctx, B, tsg.TSG_TILED_CSC_VIEW)
+    TA = tsg.csr_host_to_tiled(ctx, A, tsg.TSG_TILED_PACKED_COL)
+    C, _ = tsg.spgemm(ctx, TA, TB)
+    whole = [x.cpu().numpy() for x in tsg.tiled_to_csr(ctx, C)]
+    parts = []
+    for r0 in range(0, m, 16 * 37):  # blocks of 37 tile rows
+        r1 = min(r0 + 16 * 37, m)
+        blk = (r1 - r0, n, (rp[r0:r1 + 1] - rp[r0]).astype(np.int32), ci[rp[r0]:rp[r1]], v[rp[r0]:rp[r1]])
+        Tb = tsg.csr_host_to_tiled(ctx, blk, tsg.TSG_TILED_PACKED_COL)
+        Cb, _ = tsg.spgemm(ctx, Tb, TB)
+        parts.append([x.cpu().numpy() for x in tsg.tiled_to_csr(ctx, Cb)])
+    rp_all = np.concatenate([[0]] + [p[0][1:] + sum(q[0][-1] for q in parts[:i]) for i, p in enumerate(parts)])
+    np.testing.assert_array_equal(rp_all, whole[0])
+    np.testing.assert_array_equal(np.concatenate([p[1] for p in parts]), whole[1])
+    assert np.array_equal(np.concatenate([p[2] for p in parts]).view(np.uint64), whole[2].view(np.uint64))
