@@ -752,7 +752,7 @@ __device__ __forceinline__ void step3_rows_item(const ProdView &P, long long ite
 
 struct SpaStage
 {
-    int bs[SPA_STAGE], be[SPA_STAGE]; // B row bounds
+    int2 bl[SPA_STAGE]; // B row: first entry, length
     double a[SPA_STAGE];
 };
 
@@ -765,8 +765,8 @@ struct SpaSmem
     SpaStage stage[SPA_WARPS];
 };
 
-__device__ __forceinline__ void spa_add(SpaSmem &S, int r, int rs, int J0, int J1, bool full, int col, double a,
-                                        double b)
+__device__ __forceinline__ void spa_add(SpaSmem &S, const unsigned *cmr, int rs, int J0, int J1, bool full, int col,
+                                        double a, double b)
 {
     const int J = col >> 4;
     if (!full && (J < J0 || J >= J1 || J - J0 >= SPA_WIN))
@@ -774,7 +774,7 @@ __device__ __forceinline__ void spa_add(SpaSmem &S, int r, int rs, int J0, int J
     const int slot = S.map[J - J0];
     if (slot >= SPA_SEGT)
         return;
-    const unsigned cmw = S.cm[r * SPA_SEGT + slot];
+    const unsigned cmw = cmr[slot];
     const int pos = rs + (int)(cmw >> 16) + __popc((cmw & 0xFFFFu) >> (16 - (col & 15)));
     if (pos < SPA_CAP)
         S.acc[pos] = __dadd_rn(S.acc[pos], __dmul_rn(a, b));
@@ -847,6 +847,7 @@ __device__ __forceinline__ void step3_spa_segment(const ProdView &P, SpaSmem &S,
     }
     __syncthreads();
     const int rs = S.rstart[r];
+    const unsigned *cmr = S.cm + r * SPA_SEGT;
     SpaStage &G = S.stage[r];
     const int pa_beg = P.A_ptr[I], pa_end = P.A_ptr[I + 1];
     for (int g = pa_beg; g < pa_end; g += 32)
@@ -891,41 +892,40 @@ __device__ __forceinline__ void step3_spa_segment(const ProdView &P, SpaSmem &S,
                         b0 += lower_bound_int(P.B_rcol + b0, b1 - b0, J0 * TSG_BS);
                         b1 = b0 + lower_bound_int(P.B_rcol + b0, b1 - b0, J1 * TSG_BS);
                     }
-                    G.bs[e] = b0;
-                    G.be[e] = b1;
+                    G.bl[e] = make_int2(b0, b1 - b0);
                     G.a[e] = P.A_Val[st + x];
                 }
             }
             __syncwarp();
             const int ne = min(SPA_STAGE, total - base);
+            int2 nb = G.bl[0];
             int c_cur = -1;
             double v_cur = 0.0;
+            if (lane < nb.y)
             {
-                const int e = G.bs[0] + lane;
-                if (e < G.be[0])
-                {
-                    c_cur = P.B_rcol[e];
-                    v_cur = P.B_rval[e];
-                }
+                c_cur = P.B_rcol[nb.x + lane];
+                v_cur = P.B_rval[nb.x + lane];
             }
             for (int i = 0; i < ne; i++)
             {
+                const int2 cb = nb;
                 int c_nxt = -1;
                 double v_nxt = 0.0;
                 if (i + 1 < ne)
                 {
-                    const int e = G.bs[i + 1] + lane;
-                    if (e < G.be[i + 1])
+                    nb = G.bl[i + 1];
+                    if (lane < nb.y)
                     {
-                        c_nxt = P.B_rcol[e];
-                        v_nxt = P.B_rval[e];
+                        c_nxt = P.B_rcol[nb.x + lane];
+                        v_nxt = P.B_rval[nb.x + lane];
                     }
                 }
                 const double a = G.a[i];
                 if (c_cur >= 0)
-                    spa_add(S, r, rs, J0, J1, full, c_cur, a, v_cur);
-                for (int e = G.bs[i] + 32 + lane; e < G.be[i]; e += 32)
-                    spa_add(S, r, rs, J0, J1, full, P.B_rcol[e], a, P.B_rval[e]);
+                    spa_add(S, cmr, rs, J0, J1, full, c_cur, a, v_cur);
+                if (cb.y > 32) // B rows longer than a warp
+                    for (int e = cb.x + 32 + lane; e < cb.x + cb.y; e += 32)
+                        spa_add(S, cmr, rs, J0, J1, full, P.B_rcol[e], a, P.B_rval[e]);
                 __syncwarp();
                 c_cur = c_nxt;
                 v_cur = v_nxt;

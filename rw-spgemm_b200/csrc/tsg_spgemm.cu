@@ -168,7 +168,7 @@ __global__ void __launch_bounds__(128) k_step3_rows(ProdView P)
 }
 
 // persistent: CTAs take blocks of C tiles from a device counter
-__global__ void __launch_bounds__(SPA_THREADS) k_step3_spa(ProdView P, unsigned *__restrict__ ctr)
+__global__ void __launch_bounds__(SPA_THREADS, 3) k_step3_spa(ProdView P, unsigned *__restrict__ ctr)
 {
     extern __shared__ __align__(16) unsigned char s_raw[];
     SpaSmem &S = *reinterpret_cast<SpaSmem *>(s_raw);
