@@ -399,7 +399,7 @@ def run_served(args, tsg, gen, device, deliver="device", n_jobs=None, half_capac
 
 
 # ---------------------------------------------------------------------------
-# learned selector: trained on method-generated timings, judged by exhaustive
+# learned selector: trained on method-generated timings, measured against exhaustive
 # search on held-out matrices
 # ---------------------------------------------------------------------------
 def run_selector(args, tsg, gen, ctx):
