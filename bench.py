@@ -531,6 +531,37 @@ def run_rmat20(args, tsg, gen, ctx, budget=1.5e9):
     return out
 
 
+def run_cusparse(args, mat, prods, reps=5):
+    """The same product, C = A*A for the stencil, by cuSPARSE's FP64 SpGEMM
+    (through torch's CUDA CSR matmul), inputs resident, CUDA-event timed: a
+    library reference on the same GPU, not part of this library's path."""
+    import warnings
+
+    import torch
+    m, n, rp, ci, v = mat
+    dev = torch.device("cuda", torch.cuda.current_device())
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        A = torch.sparse_csr_tensor(torch.from_numpy(rp.astype(np.int64)).to(dev),
+                                    torch.from_numpy(ci.astype(np.int64)).to(dev),
+                                    torch.from_numpy(v).to(dev), size=(m, n))
+        C = torch.sparse.mm(A, A)
+        nnz = int(C._nnz())
+        del C
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        best = float("inf")
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            ev[0].record()
+            C = torch.sparse.mm(A, A)
+            ev[1].record()
+            ev[1].synchronize()
+            best = min(best, ev[0].elapsed_time(ev[1]))
+            del C
+    return {"what": "cuSPARSE SpGEMM (torch.sparse.mm, CSR, FP64, int64 indices), same product", "ms": round(best, 3),
+            "gflops": round(2.0 * prods / (best * 1e-3) / 1e9, 2), "nnz_C": nnz}
+
+
 def res_name(sel, idx):
     o, a = sel.CONFIGS[idx]
     return f"{o}/{a[0]}-{a[1]}-{a[2]}"
@@ -625,6 +656,9 @@ def run_ours(args, tsg, gen, world, rank, local):
         e2e_t = float(np.mean(e2e_ms))
         h2d = rp.nbytes + ci.nbytes + v.nbytes
         d2h = Cc[2].nbytes + Cc[3].nbytes + Cc[4].nbytes
+    cusparse = None
+    if world == 1 and "cusparse" in args.sections:
+        cusparse = run_cusparse(args, mat, prods)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = run_cpu_reference(argparse.Namespace(warmup=0, steps=1), gen, 1, 0)
@@ -678,6 +712,8 @@ def run_ours(args, tsg, gen, world, rank, local):
         out["orderings"] = orderings
     if rmat20:
         out["rmat20"] = rmat20
+    if cusparse:
+        out["library_reference"] = cusparse
     if rank == 0:
         print(json.dumps(out), flush=True)
     ctx.close()
@@ -695,7 +731,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--sched", default="spa", choices=["rows", "tiles", "elems", "spa"])
-    ap.add_argument("--sections", default="plain,batched,served,orderings,rmat20",
+    ap.add_argument("--sections", default="plain,cusparse,batched,served,orderings,rmat20",
                     help="comma list: plain (always), batched, served, selector")
     ap.add_argument("--batch-count", type=int, default=512)
     ap.add_argument("--selector-samples", type=int, default=5000)
