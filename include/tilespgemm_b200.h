@@ -474,6 +474,11 @@ int tsg_batch_sync(tsg_batch *b, long long *total_tiles, long long *total_nnz);
  * destroy; tsg_tiled_free on it only clears the struct). */
 int tsg_batch_product(tsg_batch *b, int p, tsg_tiled *C);
 int tsg_batch_info(tsg_batch *b, int *graph, int *grid, size_t *arena_bytes, long long *launches);
+/* Duration (ms, GPU global timer) of each of the seven phases of the last
+ * finished run: step-1 counts, C row-pointer scans, work-item prefixes,
+ * step-1 emit + fused step 2, step 2 of the remaining tiles, tile-count scans,
+ * numeric step. */
+int tsg_batch_phase_ms(tsg_batch *b, double *ms);
 int tsg_batch_destroy(tsg_batch *b);
 
 /* ------------------------------------------------------------------------ */

@@ -637,6 +637,7 @@ def _declare_batch(L):
     L.tsg_batch_info.argtypes = [vp, ctypes.POINTER(ip), ctypes.POINTER(ip), ctypes.POINTER(ctypes.c_size_t),
                                  ctypes.POINTER(ctypes.c_longlong)]
     L.tsg_batch_destroy.argtypes = [vp]
+    L.tsg_batch_phase_ms.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
     L.tsg_product_bounds.argtypes = [vp, ctypes.POINTER(TsgTiled), ctypes.POINTER(TsgTiled),
                                      ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]
 
@@ -675,6 +676,14 @@ class Batch:
 
     def run(self):
         check(lib().tsg_batch_run(self.handle))
+
+    def phase_ms(self):
+        """Per-phase GPU time (ms) of the last finished run (see
+        tsg_batch_phase_ms)."""
+        out = (ctypes.c_double * 7)()
+        check(lib().tsg_batch_phase_ms(self.handle, out))
+        names = ["step1_counts", "row_scans", "item_prefix", "step1_emit_step2", "step2_rest", "tile_scans", "step3"]
+        return {k: round(v, 4) for k, v in zip(names, out)}
 
     def sync(self):
         t, z = ctypes.c_longlong(0), ctypes.c_longlong(0)

@@ -154,6 +154,19 @@ __device__ long long block_scan_inplace(int *a, int n, long long *s_tmp)
     return run;
 }
 
+// GPU global timer (ns); block 0 stamps the end of each phase into
+// stamp[1..6] and every block raises stamp[7] as it leaves.
+__device__ __forceinline__ unsigned long long gtimer()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+#define BATCH_STAMP(k)                                                  \
+    if (blockIdx.x == 0 && threadIdx.x == 0)                           \
+        stamp[k] = gtimer();
+
 template <int SCHED, int W, int CAP, int NT>
 __global__ void __launch_bounds__(NT)
     k_batch(BatchProd *prods, int count, const long long *__restrict__ rowoff, long long *itemoff, unsigned *bar,
@@ -169,6 +182,8 @@ __global__ void __launch_bounds__(NT)
     const long long nwarps = (long long)gridDim.x * (NT / 32);
     const long long nhw = (long long)gridDim.x * (NT / 16);
     const long long total_rows = rowoff[count];
+    unsigned long long *stamp = reinterpret_cast<unsigned long long *>(itemoff + 2 * ((long long)count + 1));
+    BATCH_STAMP(0)
 
     // phase 1: step-1 counts
     {
@@ -185,6 +200,7 @@ __global__ void __launch_bounds__(NT)
     }
     if (!grid_barrier(bar, err))
         return;
+    BATCH_STAMP(1)
     // phase 2: per-product scan of C tile counts
     for (int p = blockIdx.x; p < count; p += gridDim.x)
     {
@@ -207,6 +223,7 @@ __global__ void __launch_bounds__(NT)
     }
     if (!grid_barrier(bar, err))
         return;
+    BATCH_STAMP(2)
     // phase 3: item prefix over products (block 0)
     if (blockIdx.x == 0)
     {
@@ -237,6 +254,7 @@ __global__ void __launch_bounds__(NT)
     }
     if (!grid_barrier(bar, err))
         return;
+    BATCH_STAMP(3)
     // phase 4: step-1 emit (fused with step 2 for narrow rows unless the
     // row schedule runs its own step 2)
     if (threadIdx.x < 4)
@@ -269,6 +287,7 @@ __global__ void __launch_bounds__(NT)
     }
     if (!grid_barrier(bar, err))
         return;
+    BATCH_STAMP(4)
     // phase 5: step 2 (all tiles for the row schedule, tiles of wide rows otherwise)
     if (SCHED == 3)
     {
@@ -311,6 +330,7 @@ __global__ void __launch_bounds__(NT)
         atomicAdd(&bins[threadIdx.x], s_bins[threadIdx.x]);
     if (!grid_barrier(bar, err))
         return;
+    BATCH_STAMP(5)
     // phase 6: per-product scan of tile nnz
     for (int p = blockIdx.x; p < count; p += gridDim.x)
     {
@@ -329,6 +349,7 @@ __global__ void __launch_bounds__(NT)
     }
     if (!grid_barrier(bar, err))
         return;
+    BATCH_STAMP(6)
     // phase 7: step 3
     if (SCHED == 3)
     {
@@ -405,6 +426,9 @@ __global__ void __launch_bounds__(NT)
                 step3_tile(P, (int)item, hmask, lane, tacc);
         }
     }
+    __syncthreads();
+    if (threadIdx.x == 0)
+        atomicMax(&stamp[7], gtimer());
 }
 
 // ---------------------------------------------------------------------------
@@ -550,6 +574,8 @@ static int record_run(tsg_batch *b, cudaStream_t st)
     batch_kernel_t kern = pick_kernel(b->params, &smem, &threads);
     TSG_CUDA(cudaMemsetAsync(b->d_err, 0, sizeof(int), st));
     TSG_CUDA(cudaMemsetAsync(b->d_bar, 0, sizeof(unsigned), st));
+    // phase stamps (after the two item prefixes): [7] is a running maximum
+    TSG_CUDA(cudaMemsetAsync(b->d_itemoff + 2 * ((size_t)b->count + 1), 0, 8 * sizeof(long long), st));
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)b->grid);
     cfg.blockDim = dim3(threads);
@@ -703,7 +729,7 @@ extern "C" int tsg_batch_create(tsg_context *ctx, int count, const tsg_tiled *A,
         P.numC = 0;
     }
     if ((st = tsg_alloc(ctx, &b->d_prod, (size_t)count)) != TSG_OK || (st = tsg_alloc(ctx, &b->d_rowoff, (size_t)count + 1)) ||
-        (st = tsg_alloc(ctx, &b->d_itemoff, 2 * ((size_t)count + 1))) || (st = tsg_alloc(ctx, &b->d_bar, 4)) ||
+        (st = tsg_alloc(ctx, &b->d_itemoff, 2 * ((size_t)count + 1) + 8)) || (st = tsg_alloc(ctx, &b->d_bar, 4)) ||
         (st = tsg_alloc(ctx, &b->d_err, 1)) || (st = tsg_alloc(ctx, &b->d_bins, 4)))
     {
         tsg_batch_destroy(b);
@@ -822,6 +848,20 @@ extern "C" int tsg_batch_product(tsg_batch *b, int p, tsg_tiled *C)
     C->tile_csr_Col = h.P.C_Colb;
     C->tile_csr_Value = h.P.C_Val;
     C->_alloc = (void *)b; // borrowed view into the batch arena
+    return TSG_OK;
+}
+
+extern "C" int tsg_batch_phase_ms(tsg_batch *b, double *ms)
+{
+    if (!b || !ms)
+        return tsg_set_error(TSG_ERR_INVALID, "null argument");
+    unsigned long long t[8];
+    tsg_context *ctx = b->ctx;
+    TSG_CUDA(cudaMemcpyAsync(t, b->d_itemoff + 2 * ((size_t)b->count + 1), sizeof(t), cudaMemcpyDeviceToHost,
+                             ctx->stream));
+    TSG_CUDA(cudaStreamSynchronize(ctx->stream));
+    for (int k = 0; k < 7; k++)
+        ms[k] = t[k + 1] >= t[k] ? (double)(t[k + 1] - t[k]) * 1e-6 : 0.0;
     return TSG_OK;
 }
 

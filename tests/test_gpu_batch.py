@@ -81,3 +81,15 @@ def test_product_bounds_bound_the_result(tsg, ctx, oracle, gen):
         assert prods == oracle.count_products(a, b)
         C, info = tsg.spgemm(ctx, A, B)
         assert info["nnz_C"] <= prods and info["numtile_C"] <= pairs
+
+
+def test_batch_phase_times(tsg, ctx, gen):
+    mats = _pairs(gen)[:6]
+    pairs = [(_tiled(tsg, ctx, a, 1), _tiled(tsg, ctx, b, 2)) for a, b in mats]
+    batch = tsg.Batch(ctx, pairs)
+    batch.run()
+    batch.sync()
+    ph = batch.phase_ms()
+    assert len(ph) == 7 and all(v >= 0.0 for v in ph.values())
+    assert 0.0 < sum(ph.values()) < 10_000.0
+    batch.close()
