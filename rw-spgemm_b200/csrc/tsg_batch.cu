@@ -154,6 +154,101 @@ __device__ long long block_scan_inplace(int *a, int n, long long *s_tmp)
     return run;
 }
 
+// Block-wide sum of a[0..n) (NT threads).
+template <int NT>
+__device__ long long block_sum(const int *a, int n, long long *s_tmp)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    long long v = 0;
+    for (int i = threadIdx.x; i < n; i += NT)
+        v += a[i];
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1)
+        v += __shfl_xor_sync(TSG_FULL_MASK, v, d);
+    if (lane == 0)
+        s_tmp[warp] = v;
+    __syncthreads();
+    long long tot = 0;
+#pragma unroll
+    for (int w = 0; w < NT / 32; w++)
+        tot += s_tmp[w];
+    __syncthreads();
+    return tot;
+}
+
+// Block-wide exclusive scan of a[0..n) in place, offset by off (NT threads).
+template <int NT>
+__device__ void block_scan_offset(int *a, int n, long long off, long long *s_tmp)
+{
+    long long run = off;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int base = 0; base < n; base += NT)
+    {
+        const int i = base + threadIdx.x;
+        const long long v = i < n ? a[i] : 0;
+        long long incl = v;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1)
+        {
+            const long long o = __shfl_up_sync(TSG_FULL_MASK, incl, d);
+            if (lane >= d)
+                incl += o;
+        }
+        if (lane == 31)
+            s_tmp[warp] = incl;
+        __syncthreads();
+        long long woff = 0, tot = 0;
+#pragma unroll
+        for (int w = 0; w < NT / 32; w++)
+        {
+            woff += w < warp ? s_tmp[w] : 0;
+            tot += s_tmp[w];
+        }
+        if (i < n)
+            a[i] = (int)(run + woff + incl - v);
+        run += tot;
+        __syncthreads();
+    }
+}
+
+// Exclusive scan of v[0..n) in place (long long) by one block; returns the total.
+template <int NT>
+__device__ long long block_scan_ll(long long *v, int n, long long *s_tmp)
+{
+    long long run = 0;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int base = 0; base < n; base += NT)
+    {
+        const int i = base + threadIdx.x;
+        const long long x = i < n ? v[i] : 0;
+        long long incl = x;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1)
+        {
+            const long long o = __shfl_up_sync(TSG_FULL_MASK, incl, d);
+            if (lane >= d)
+                incl += o;
+        }
+        if (lane == 31)
+            s_tmp[warp] = incl;
+        __syncthreads();
+        long long woff = 0, tot = 0;
+#pragma unroll
+        for (int w = 0; w < NT / 32; w++)
+        {
+            woff += w < warp ? s_tmp[w] : 0;
+            tot += s_tmp[w];
+        }
+        if (i < n)
+            v[i] = run + woff + incl - x;
+        run += tot;
+        __syncthreads();
+    }
+    return run;
+}
+
+#define SCAN_CHUNK 4096 // C tiles per chunk of the tile-count scan
+
 // GPU global timer (ns); block 0 stamps the end of each phase into
 // stamp[1..6] and every block raises stamp[7] as it leaves.
 __device__ __forceinline__ unsigned long long gtimer()
@@ -173,7 +268,7 @@ __global__ void __launch_bounds__(NT)
             int *err, int *bins)
 {
     extern __shared__ __align__(16) unsigned char s_raw[];
-    __shared__ long long s_tmp[NT / 32];
+    __shared__ long long s_tmp[NT / 32 + 1];
     __shared__ int s_row;
     __shared__ int s_bins[4];
     const int lane32 = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -246,6 +341,15 @@ __global__ void __launch_bounds__(NT)
                 run += ((long long)prods[p].numC + SPA_BLK - 1) / SPA_BLK;
             }
             blkoff[count] = run;
+            // tile-count scan chunks per product, prefix after the stamps
+            long long *chunkoff = itemoff + 2 * ((long long)count + 1) + 8;
+            run = 0;
+            for (int p = 0; p < count; p++)
+            {
+                chunkoff[p] = run;
+                run += ((long long)prods[p].numC + SCAN_CHUNK - 1) / SCAN_CHUNK;
+            }
+            chunkoff[count] = run;
             bar[2] = 0;
             bar[3] = 0;
         }
@@ -331,20 +435,53 @@ __global__ void __launch_bounds__(NT)
     if (!grid_barrier(bar, err))
         return;
     BATCH_STAMP(5)
-    // phase 6: per-product scan of tile nnz
-    for (int p = blockIdx.x; p < count; p += gridDim.x)
+    // phase 6: per-product exclusive scan of the tile counts, in chunks of
+    // SCAN_CHUNK tiles spread over all blocks: chunk sums, a scan of each
+    // product's chunk sums, then every chunk scanned with its offset
     {
-        BatchProd &bp = prods[p];
-        const long long tot = block_scan_inplace<NT>(bp.P.C_tnnz, bp.numC, s_tmp);
-        if (threadIdx.x == 0)
+        const long long *chunkoff = itemoff + 2 * ((long long)count + 1) + 8;
+        long long *csum = const_cast<long long *>(chunkoff) + count + 1;
+        const long long nch = chunkoff[count];
+        for (long long c = blockIdx.x; c < nch; c += gridDim.x)
         {
-            if (tot > bp.capN)
+            const int p = find_product(chunkoff, count, c);
+            const BatchProd &bp = prods[p];
+            const long long t0 = (c - chunkoff[p]) * SCAN_CHUNK;
+            const int n = (int)min((long long)SCAN_CHUNK, (long long)bp.numC - t0);
+            const long long tot = bp.status ? 0 : block_sum<NT>(bp.P.C_tnnz + t0, n, s_tmp);
+            if (threadIdx.x == 0)
+                csum[c] = tot;
+        }
+        if (!grid_barrier(bar, err))
+            return;
+        for (int p = blockIdx.x; p < count; p += gridDim.x)
+        {
+            BatchProd &bp = prods[p];
+            const long long tot =
+                block_scan_ll<NT>(csum + chunkoff[p], (int)(chunkoff[p + 1] - chunkoff[p]), s_tmp);
+            if (threadIdx.x == 0 && !bp.status)
             {
-                bp.status = 2;
-                bp.nnzC = 0;
+                if (tot > bp.capN)
+                {
+                    bp.status = 2;
+                    bp.nnzC = 0;
+                }
+                else
+                    bp.nnzC = (int)tot;
+                bp.P.C_tnnz[bp.numC] = (int)(tot > bp.capN ? 0 : tot);
             }
-            else
-                bp.nnzC = (int)tot;
+        }
+        if (!grid_barrier(bar, err))
+            return;
+        for (long long c = blockIdx.x; c < nch; c += gridDim.x)
+        {
+            const int p = find_product(chunkoff, count, c);
+            const BatchProd &bp = prods[p];
+            if (bp.status)
+                continue;
+            const long long t0 = (c - chunkoff[p]) * SCAN_CHUNK;
+            const int n = (int)min((long long)SCAN_CHUNK, (long long)bp.numC - t0);
+            block_scan_offset<NT>(bp.P.C_tnnz + t0, n, csum[c], s_tmp);
         }
     }
     if (!grid_barrier(bar, err))
@@ -635,7 +772,7 @@ extern "C" int tsg_batch_create(tsg_context *ctx, int count, const tsg_tiled *A,
     // bounds and arena layout
     size_t bytes = 0;
     std::vector<size_t> off(count);
-    long long run = 0;
+    long long run = 0, chunk_cap = 0;
     for (int p = 0; p < count; p++)
     {
         long long prods = 0, pairs = 0;
@@ -664,6 +801,7 @@ extern "C" int tsg_batch_create(tsg_context *ctx, int count, const tsg_tiled *A,
         memset(&h, 0, sizeof(h));
         h.capT = capT;
         h.capN = capN;
+        chunk_cap += (capT + SCAN_CHUNK - 1) / SCAN_CHUNK;
         h.tilemA = A[p].tilem;
         b->rowoff[p] = run;
         run += A[p].tilem;
@@ -729,7 +867,7 @@ extern "C" int tsg_batch_create(tsg_context *ctx, int count, const tsg_tiled *A,
         P.numC = 0;
     }
     if ((st = tsg_alloc(ctx, &b->d_prod, (size_t)count)) != TSG_OK || (st = tsg_alloc(ctx, &b->d_rowoff, (size_t)count + 1)) ||
-        (st = tsg_alloc(ctx, &b->d_itemoff, 2 * ((size_t)count + 1) + 8)) || (st = tsg_alloc(ctx, &b->d_bar, 4)) ||
+        (st = tsg_alloc(ctx, &b->d_itemoff, 3 * ((size_t)count + 1) + 8 + (size_t)chunk_cap)) || (st = tsg_alloc(ctx, &b->d_bar, 4)) ||
         (st = tsg_alloc(ctx, &b->d_err, 1)) || (st = tsg_alloc(ctx, &b->d_bins, 4)))
     {
         tsg_batch_destroy(b);
