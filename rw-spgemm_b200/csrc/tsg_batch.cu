@@ -53,6 +53,7 @@ struct tsg_batch
     size_t arena_bytes;
     int grid, block;
     size_t smem;
+    int grid3; // persistent grid of k_batch_spa3 (SPA schedule)
     cudaGraph_t graph;
     cudaGraphExec_t exec;
     int graph_ok;
@@ -487,48 +488,11 @@ __global__ void __launch_bounds__(NT)
     if (!grid_barrier(bar, err))
         return;
     BATCH_STAMP(6)
-    // phase 7: step 3
+    // phase 7: step 3 (the SPA schedule runs it as two kernels after this one:
+    // k_batch_spa3 and k_batch_dense3, each at its own occupancy)
     if (SCHED == 3)
-    {
-        // CTAs take blocks of C tiles from a counter (products with sparse
-        // C tiles); a block goes in row parts and SPA-limited segments
-        SpaSmem &S = *reinterpret_cast<SpaSmem *>(s_raw);
-        const long long *blkoff = itemoff + count + 1;
-        for (;;)
-        {
-            __syncthreads();
-            if (threadIdx.x == 0)
-                s_row = (int)atomicAdd(&bar[2], 1u);
-            __syncthreads();
-            const long long blk = s_row;
-            if (blk >= blkoff[count])
-                break;
-            const int p = find_product(blkoff, count, blk);
-            if (prods[p].status || prods[p].nnzC >= (long long)SPA_DENSE * prods[p].numC)
-                continue;
-            const ProdView &P = prods[p].P;
-            const long long tb = (blk - blkoff[p]) * SPA_BLK;
-            step3_spa_block(P, S, (int)tb, (int)min((long long)P.numC, tb + SPA_BLK));
-        }
-    }
-    if (SCHED == 3)
-    {
-        // products with dense C tiles: tile kernel, half-warp per C tile
-        __syncthreads();
-        double *tacc = reinterpret_cast<double *>(s_raw) + hw * (TSG_BS * S3T_STRIDE);
-        for (int q = lane; q < TSG_BS * S3T_STRIDE; q += 16)
-            tacc[q] = 0.0;
-        __syncwarp(hmask);
-        const long long total_items = itemoff[count];
-        for (long long h = (long long)blockIdx.x * (NT / 16) + hw; h < total_items; h += nhw)
-        {
-            const int p = find_product(itemoff, count, h);
-            if (prods[p].status || prods[p].nnzC < (long long)SPA_DENSE * prods[p].numC)
-                continue;
-            step3_tile(prods[p].P, (int)(h - itemoff[p]), hmask, lane, tacc);
-        }
-    }
-    else if (SCHED == 2)
+        return;
+    if (SCHED == 2)
     {
         int2 *pairs = reinterpret_cast<int2 *>(s_raw) + warp * S3E_PAIRS;
         const long long total_items = itemoff[count];
@@ -566,6 +530,68 @@ __global__ void __launch_bounds__(NT)
     __syncthreads();
     if (threadIdx.x == 0)
         atomicMax(&stamp[7], gtimer());
+}
+
+// Step 3 of the SPA schedule over a batch, after k_batch: products with
+// sparse C tiles, CTAs taking blocks of SPA_BLK C tiles (all products) from a
+// device counter.  Raises stamp[7] on exit.
+__global__ void __launch_bounds__(SPA_THREADS, 3)
+    k_batch_spa3(BatchProd *prods, int count, const long long *__restrict__ itemoff, unsigned *bar)
+{
+    extern __shared__ __align__(16) unsigned char s_raw[];
+    __shared__ int s_blk;
+    SpaSmem &S = *reinterpret_cast<SpaSmem *>(s_raw);
+    const long long *blkoff = itemoff + count + 1;
+    for (;;)
+    {
+        __syncthreads();
+        if (threadIdx.x == 0)
+            s_blk = (int)atomicAdd(&bar[2], 1u);
+        __syncthreads();
+        const long long blk = s_blk;
+        if (blk >= blkoff[count])
+            break;
+        const int p = find_product(blkoff, count, blk);
+        if (prods[p].status || prods[p].nnzC >= (long long)SPA_DENSE * prods[p].numC)
+            continue;
+        const ProdView &P = prods[p].P;
+        const long long tb = (blk - blkoff[p]) * SPA_BLK;
+        step3_spa_block(P, S, (int)tb, (int)min((long long)P.numC, tb + SPA_BLK));
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+        atomicMax(reinterpret_cast<unsigned long long *>(const_cast<long long *>(itemoff)) + 2 * ((long long)count + 1) +
+                      7,
+                  gtimer());
+}
+
+// ... and products with dense C tiles (>= SPA_DENSE values per tile on
+// average): the tile kernel, a half-warp per C tile.
+#define DENSE3_THREADS 256
+__global__ void __launch_bounds__(DENSE3_THREADS)
+    k_batch_dense3(BatchProd *prods, int count, const long long *__restrict__ itemoff)
+{
+    __shared__ double s_acc[DENSE3_THREADS / 16][TSG_BS * S3T_STRIDE];
+    const int lane = threadIdx.x & 15, hw = threadIdx.x >> 4;
+    const unsigned hmask = TSG_HW_MASK(threadIdx.x);
+    double *tacc = s_acc[hw];
+    for (int q = lane; q < TSG_BS * S3T_STRIDE; q += 16)
+        tacc[q] = 0.0;
+    __syncwarp(hmask);
+    const long long total_items = itemoff[count];
+    const long long nhw = (long long)gridDim.x * (DENSE3_THREADS / 16);
+    for (long long h = (long long)blockIdx.x * (DENSE3_THREADS / 16) + hw; h < total_items; h += nhw)
+    {
+        const int p = find_product(itemoff, count, h);
+        if (prods[p].status || prods[p].nnzC < (long long)SPA_DENSE * prods[p].numC)
+            continue;
+        step3_tile(prods[p].P, (int)(h - itemoff[p]), hmask, lane, tacc);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+        atomicMax(reinterpret_cast<unsigned long long *>(const_cast<long long *>(itemoff)) + 2 * ((long long)count + 1) +
+                      7,
+                  gtimer());
 }
 
 // ---------------------------------------------------------------------------
@@ -672,8 +698,7 @@ static batch_kernel_t pick_kernel(const tsg_batch_params &p, size_t *smem, int *
         const size_t t1a = (size_t)(SPA_THREADS / 32) * S1_WORDS * 4;
         const size_t t12 = (size_t)(SPA_THREADS / 32) * sizeof(S12Smem);
         const size_t t1 = t1a > t12 ? t1a : t12;
-        const size_t t3 = sizeof(SpaSmem) > sizeof(Spa2Smem) ? sizeof(SpaSmem) : sizeof(Spa2Smem);
-        *smem = t1 > t3 ? t1 : t3;
+        *smem = t1 > sizeof(Spa2Smem) ? t1 : sizeof(Spa2Smem);
         return k_batch<3, 8, 256, SPA_THREADS>;
     }
     if (p.schedule == TSG_SCHED_ELEMS)
@@ -725,6 +750,13 @@ static int record_run(tsg_batch *b, cudaStream_t st)
     cfg.numAttrs = 1;
     TSG_CUDA(cudaLaunchKernelEx(&cfg, kern, b->d_prod, b->count, (const long long *)b->d_rowoff, b->d_itemoff,
                                 b->d_bar, b->d_err, b->d_bins));
+    if (b->params.schedule == TSG_SCHED_SPA)
+    {
+        k_batch_spa3<<<b->grid3, SPA_THREADS, sizeof(SpaSmem), st>>>(b->d_prod, b->count, b->d_itemoff, b->d_bar);
+        TSG_CUDA(cudaGetLastError());
+        k_batch_dense3<<<b->ctx->num_sms * 8, DENSE3_THREADS, 0, st>>>(b->d_prod, b->count, b->d_itemoff);
+        TSG_CUDA(cudaGetLastError());
+    }
     return TSG_OK;
 }
 
@@ -892,6 +924,21 @@ extern "C" int tsg_batch_create(tsg_context *ctx, int count, const tsg_tiled *A,
         return tsg_set_error(TSG_ERR_CUDA, "batch kernel cannot be resident");
     }
     b->grid = per_sm * ctx->num_sms;
+    b->grid3 = 0;
+    if (prm.schedule == TSG_SCHED_SPA)
+    {
+        int per3 = 0;
+        if (cudaFuncSetAttribute(k_batch_spa3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SpaSmem)) !=
+                cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per3, k_batch_spa3, SPA_THREADS, sizeof(SpaSmem)) !=
+                cudaSuccess ||
+            per3 < 1)
+        {
+            tsg_batch_destroy(b);
+            return tsg_set_error(TSG_ERR_CUDA, "batch numeric kernel cannot be resident");
+        }
+        b->grid3 = per3 * ctx->num_sms;
+    }
     b->block = threads;
     b->smem = smem;
     b->graph_ok = 0;
