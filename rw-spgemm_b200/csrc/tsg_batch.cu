@@ -29,11 +29,12 @@ int tsg_count_c_tiles(tsg_context *ctx, const tsg_tiled *A, const tsg_tiled *B, 
 struct BatchProd
 {
     ProdView P;
-    int *wide; // per A tile row: 1 when step 2 runs per tile (fused pass declined)
+    int *wide; // per A tile row: 1 when step 2 runs per tile (fused pass declined), 2 hypersparse
     long long capT, capN;
     int tilemA;
     int status; // 0 ok, 1 tile capacity, 2 value capacity
     int numC, nnzC;
+    int spa_blk; // C tiles per SPA work block (set with the block prefix)
 };
 
 struct tsg_batch
@@ -333,13 +334,15 @@ __global__ void __launch_bounds__(NT)
                 run += SCHED == 1 ? (nc + W - 1) / W : nc;
             }
             itemoff[count] = run;
-            // SPA: blocks of SPA_BLK C tiles per product, prefix after itemoff
+            // SPA: blocks of spa_blk C tiles per product, prefix after itemoff
             long long *blkoff = itemoff + count + 1;
             run = 0;
             for (int p = 0; p < count; p++)
             {
                 blkoff[p] = run;
-                run += ((long long)prods[p].numC + SPA_BLK - 1) / SPA_BLK;
+                const int blk = spa_block_tiles(prods[p].numC, prods[p].tilemA);
+                prods[p].spa_blk = blk;
+                run += ((long long)prods[p].numC + blk - 1) / blk;
             }
             blkoff[count] = run;
             // tile-count scan chunks per product, prefix after the stamps
@@ -379,13 +382,15 @@ __global__ void __launch_bounds__(NT)
             else
             {
                 const int done = step12_row(prods[p].P, i, *s12, lane32, s_bins);
+                int kind = 0;
                 if (!done)
                 {
                     __syncwarp();
                     step1_row<true>(prods[p].P, i, reinterpret_cast<unsigned *>(s12), lane32, nullptr);
+                    kind = SCHED == 3 ? wide_kind(prods[p].P, i, lane32) : 1;
                 }
                 if (lane32 == 0)
-                    prods[p].wide[i] = done ? 0 : 1;
+                    prods[p].wide[i] = kind;
                 __syncwarp();
             }
         }
@@ -412,8 +417,9 @@ __global__ void __launch_bounds__(NT)
             if (prods[p].status)
                 continue;
             const ProdView &P = prods[p].P;
-            const long long tb = (blk - blkoff[p]) * SPA_BLK;
-            step2_spa_block(P, S2, (int)tb, (int)min((long long)P.numC, tb + SPA_BLK), prods[p].wide, s_bins);
+            const int nb = prods[p].spa_blk;
+            const long long tb = (blk - blkoff[p]) * nb;
+            step2_spa_block(P, S2, (int)tb, (int)min((long long)P.numC, tb + nb), nb, prods[p].wide, s_bins);
         }
     }
     else
@@ -533,7 +539,7 @@ __global__ void __launch_bounds__(NT)
 }
 
 // Step 3 of the SPA schedule over a batch, after k_batch: products with
-// sparse C tiles, CTAs taking blocks of SPA_BLK C tiles (all products) from a
+// sparse C tiles, CTAs taking blocks of C tiles (spa_blk, all products) from a
 // device counter.  Raises stamp[7] on exit.
 __global__ void __launch_bounds__(SPA_THREADS, 3)
     k_batch_spa3(BatchProd *prods, int count, const long long *__restrict__ itemoff, unsigned *bar)
@@ -555,8 +561,9 @@ __global__ void __launch_bounds__(SPA_THREADS, 3)
         if (prods[p].status || prods[p].nnzC >= (long long)SPA_DENSE * prods[p].numC)
             continue;
         const ProdView &P = prods[p].P;
-        const long long tb = (blk - blkoff[p]) * SPA_BLK;
-        step3_spa_block(P, S, (int)tb, (int)min((long long)P.numC, tb + SPA_BLK));
+        const int nb = prods[p].spa_blk;
+        const long long tb = (blk - blkoff[p]) * nb;
+        step3_spa_block(P, S, (int)tb, (int)min((long long)P.numC, tb + nb), nb, prods[p].wide);
     }
     __syncthreads();
     if (threadIdx.x == 0)

@@ -1098,19 +1098,376 @@ __device__ __forceinline__ void step2_spa_segment(const ProdView &P, Spa2Smem &S
         step2_store(P, t0 + jl, hmask, tid & 15, S.m[(tid & 15) * SP2_SEGT + jl], s_bins);
 }
 
-// Work item of the SPA steps: a block of SPA_BLK consecutive C tiles (global
-// tile order).  Ownership: a row of at most SPA_BLK tiles belongs, whole, to
-// the block holding its first tile; a longer row is cut into SPA_BLK-tile
-// chunks from its start, each belonging to the block holding the chunk's
-// first tile.  So every tile is done once, short rows are never cut, and a
-// long row is spread over many blocks (and CTAs).  The CTA cuts each piece
-// further into segments within the SPA limits.
+// ---------------------------------------------------------------------------
+// Hypersparse tile rows.  With very sparse, unstructured operands step 1's
+// tile structure of a C tile row holds nearly every tile column while the
+// row's scalar products reach only a few of those tiles (n = 65,536 with 8
+// entries per row of A and B: ~4,000 C tiles and ~1,000 products per tile
+// row).  The SPA segments would spend their time on empty tiles, segment
+// after segment, each re-walking A's row.  A wide row whose estimated
+// products are below HYP_RATIO per C tile is therefore done whole by one CTA:
+//  - step 2 zero-fills the row's masks, row offsets and tile counts with
+//    16-byte stores, ORs every product's bit into C's mask word in global
+//    memory (two rows' 16-bit masks share a 32-bit word), notes the tiles
+//    hit in a shared bitmap and finishes only those tiles (step2_store);
+//  - step 3 zero-fills the row's values and adds every product into its
+//    value slot -- the tile's value offset + the row offset + the popcount
+//    of the row mask left of the column -- in global memory.  Warp r takes
+//    row r's products in generation order (A's entries in column order, each
+//    with its B row), 32 at a time; lanes of one batch that meet the same
+//    slot are summed by the lowest of them in lane order, and batches follow
+//    one another behind warp barriers, so every C entry sums its products in
+//    k order, each product rounded before the add, as the reference does.
+// The tile column -> tile map covers HYP_WIN tile columns; a row spanning
+// more is done in window passes, each taking the products that fall in it.
+// ---------------------------------------------------------------------------
+#define HYP_WIN 8192
+#define HYP_RATIO 4
+
+struct HypStage
+{
+    int2 bl[SPA_STAGE];      // B row: first entry, length
+    int off[SPA_STAGE + 1];  // first product of each staged entry
+    double a[SPA_STAGE];     // A value of each staged entry
+    double prod[32];         // products of the current batch, by lane
+};
+
+struct HypSmem
+{
+    unsigned short map[HYP_WIN]; // tile column - W0 -> tile - s0 (only C's columns are read);
+                                 // step 2 then lists the window's hit tiles here
+    unsigned hit[HYP_WIN / 32];  // tiles of the window that received a product (step 2)
+    int wsum[SPA_WARPS];
+    int win_end;
+    HypStage stage[SPA_WARPS];
+};
+
+// Exclusive scan of v over the CTA (SPA_THREADS threads); total = the sum.
+__device__ __forceinline__ int hyp_cta_scan(int v, int *wsum, int &total)
+{
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int incl = v;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1)
+    {
+        const int o = __shfl_up_sync(TSG_FULL_MASK, incl, d);
+        if (lane >= d)
+            incl += o;
+    }
+    if (lane == 31)
+        wsum[w] = incl;
+    __syncthreads();
+    int off = 0, tot = 0;
+#pragma unroll
+    for (int q = 0; q < SPA_WARPS; q++)
+    {
+        const int x = wsum[q];
+        off += q < w ? x : 0;
+        tot += x;
+    }
+    total = tot;
+    __syncthreads();
+    return off + incl - v;
+}
+
+// 2 when the wide A tile row i is hypersparse (estimated scalar products
+// below HYP_RATIO per C tile of the row) and B has a row view, else 1.  The
+// estimate takes each A tile's nonzeros times the mean length of the B rows
+// of its tile column: sum(nnz(A tile) * nnz(B tile row)) / 16.  Warp-uniform;
+// every lane calls it; C's row pointer must be final.
+__device__ __forceinline__ int wide_kind(const ProdView &P, int i, int lane)
+{
+    if (!P.B_rptr)
+        return 1;
+    const int a0 = P.A_ptr[i], a1 = P.A_ptr[i + 1];
+    long long est = 0;
+    for (int pa = a0 + lane; pa < a1; pa += 32)
+    {
+        const int k = P.A_col[pa];
+        const long long nb = P.B_tnnz[P.B_ptr[k + 1]] - P.B_tnnz[P.B_ptr[k]];
+        est += (long long)(P.A_tnnz[pa + 1] - P.A_tnnz[pa]) * nb;
+    }
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1)
+        est += __shfl_xor_sync(TSG_FULL_MASK, est, d);
+    const long long nt = P.C_ptr[i + 1] - P.C_ptr[i];
+    return est < (long long)HYP_RATIO * TSG_BS * nt ? 2 : 1;
+}
+
+// Warp r enumerates the products of C row 16 I + r: A's entries of the row in
+// column order, each with its B row (row view), flattened 32 products at a
+// time.  f(valid, e, bi) is called with the whole warp converged; e is the
+// staged entry (G.a[e] its A value when VAL), bi the product's index in B's
+// row view.  Lane order within a batch, and batch order, follow k.
+template <bool VAL, typename F>
+__device__ __forceinline__ void hyp_walk(const ProdView &P, HypStage &G, int I, int r, int lane, F f)
+{
+    const int pa_beg = P.A_ptr[I], pa_end = P.A_ptr[I + 1];
+    for (int g = pa_beg; g < pa_end; g += 32)
+    {
+        const int pa = g + lane;
+        unsigned mr = 0;
+        int st = 0, kb = 0;
+        if (pa < pa_end)
+        {
+            mr = P.A_mask[(long long)pa * TSG_BS + r];
+            if (mr)
+            {
+                kb = P.A_col[pa] * TSG_BS;
+                if (VAL)
+                    st = P.A_tnnz[pa] + P.A_Ptr[(long long)pa * TSG_BS + r];
+            }
+        }
+        const int cnt = __popc(mr);
+        int incl = cnt;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1)
+        {
+            const int o = __shfl_up_sync(TSG_FULL_MASK, incl, d);
+            if (lane >= d)
+                incl += o;
+        }
+        const int total = __shfl_sync(TSG_FULL_MASK, incl, 31);
+        for (int base = 0; base < total; base += SPA_STAGE)
+        {
+            __syncwarp();
+            unsigned bits = mr;
+            for (int x = 0; x < cnt; x++)
+            {
+                const int bit = 31 - __clz(bits);
+                bits ^= 1u << bit;
+                const int e = incl - cnt + x - base;
+                if (e >= 0 && e < SPA_STAGE)
+                {
+                    const int k = kb + (15 - bit);
+                    const int b0 = P.B_rptr[k];
+                    G.bl[e] = make_int2(b0, P.B_rptr[k + 1] - b0);
+                    if (VAL)
+                        G.a[e] = P.A_Val[st + x];
+                }
+            }
+            __syncwarp();
+            const int ne = min(SPA_STAGE, total - base);
+            {
+                const int l0 = lane < ne ? G.bl[lane].y : 0;
+                const int l1 = lane + 32 < ne ? G.bl[lane + 32].y : 0;
+                int i0 = l0, i1 = l1;
+#pragma unroll
+                for (int d = 1; d < 32; d <<= 1)
+                {
+                    const int o0 = __shfl_up_sync(TSG_FULL_MASK, i0, d);
+                    const int o1 = __shfl_up_sync(TSG_FULL_MASK, i1, d);
+                    if (lane >= d)
+                    {
+                        i0 += o0;
+                        i1 += o1;
+                    }
+                }
+                const int t0s = __shfl_sync(TSG_FULL_MASK, i0, 31);
+                if (lane < ne)
+                    G.off[lane] = i0 - l0;
+                if (lane + 32 < ne)
+                    G.off[lane + 32] = t0s + i1 - l1;
+                if (lane == 31)
+                    G.off[ne] = t0s + i1;
+            }
+            __syncwarp();
+            const int ni = G.off[ne];
+            int ent = 0;
+            for (int ib = 0; ib < ni; ib += 32)
+            {
+                const int item = ib + lane;
+                const bool valid = item < ni;
+                if (valid)
+                    while (G.off[ent + 1] <= item)
+                        ent++;
+                f(valid, ent, valid ? G.bl[ent].x + (item - G.off[ent]) : 0);
+            }
+        }
+    }
+}
+
+// First tile of the window starting at tile s0 of a row ending at re: tiles
+// [s0, end) have tile columns below C_col[s0] + HYP_WIN.  Fills the map.
+__device__ __forceinline__ int hyp_window(const ProdView &P, HypSmem &S, int s0, int re, int W0)
+{
+    if (threadIdx.x == 0)
+        S.win_end = s0 + lower_bound_int(P.C_col + s0, re - s0, W0 + HYP_WIN);
+    __syncthreads();
+    const int s1 = S.win_end;
+    for (int q = threadIdx.x; q < s1 - s0; q += SPA_THREADS)
+        S.map[P.C_col[s0 + q] - W0] = (unsigned short)q;
+    __syncthreads();
+    return s1;
+}
+
+// Step 2 of hypersparse tile row I by the CTA (SPA_THREADS threads).
+__device__ __forceinline__ void step2_hyper_row(const ProdView &P, HypSmem &S, int I, int *s_bins)
+{
+    const int tid = threadIdx.x, lane = tid & 31, r = tid >> 5;
+    const int rs = P.C_ptr[I], re = P.C_ptr[I + 1];
+    __syncthreads();
+    {
+        const uint4 z = make_uint4(0u, 0u, 0u, 0u);
+        uint4 *mk = reinterpret_cast<uint4 *>(P.C_mask + (long long)rs * TSG_BS);
+        uint4 *pt = reinterpret_cast<uint4 *>(P.C_Ptr + (long long)rs * TSG_BS);
+        for (int q = tid; q < 2 * (re - rs); q += SPA_THREADS)
+            mk[q] = z;
+        for (int q = tid; q < re - rs; q += SPA_THREADS)
+        {
+            pt[q] = z;
+            P.C_tnnz[rs + q] = 0;
+        }
+    }
+    __threadfence_block();
+    for (int s0 = rs; s0 < re;)
+    {
+        __syncthreads();
+        const int W0 = P.C_col[s0];
+        for (int q = tid; q < HYP_WIN / 32; q += SPA_THREADS)
+            S.hit[q] = 0u;
+        const int s1 = hyp_window(P, S, s0, re, W0);
+        const int nw = s1 - s0;
+        hyp_walk<false>(P, S.stage[r], I, r, lane, [&](bool valid, int, int bi) {
+            if (!valid)
+                return;
+            const int col = P.B_rcol[bi];
+            const int w = (col >> 4) - W0;
+            if (w < 0 || w >= HYP_WIN)
+                return; // another window's product
+            const int sl = S.map[w];
+            if (sl >= nw)
+                return;
+            const long long t = (long long)s0 + sl;
+            unsigned *word = reinterpret_cast<unsigned *>(P.C_mask + t * TSG_BS + (r & ~1));
+            atomicOr(word, 1u << ((15 - (col & 15)) + ((r & 1) << 4)));
+            const unsigned hb = 1u << (sl & 31);
+            if (!(S.hit[sl >> 5] & hb))
+                atomicOr(&S.hit[sl >> 5], hb);
+        });
+        __threadfence_block();
+        __syncthreads();
+        // list the tiles that received a product (over the map), then a
+        // thread per listed tile: its 16 row masks (two 16-byte loads from
+        // L2), row offsets, count and bin
+        const unsigned hw = tid < ((nw + 31) >> 5) ? S.hit[tid] : 0u;
+        int nh;
+        int at = hyp_cta_scan(__popc(hw), S.wsum, nh);
+        for (unsigned b = hw; b; b &= b - 1)
+            S.map[at++] = (unsigned short)(tid * 32 + __ffs(b) - 1);
+        __syncthreads();
+        for (int j = tid; j < nh; j += SPA_THREADS)
+        {
+            const long long t = (long long)s0 + S.map[j];
+            const uint4 *mp = reinterpret_cast<const uint4 *>(P.C_mask + t * TSG_BS);
+            const uint4 m0 = __ldcg(mp), m1 = __ldcg(mp + 1);
+            const unsigned w2[8] = {m0.x, m0.y, m0.z, m0.w, m1.x, m1.y, m1.z, m1.w};
+            unsigned pk[4] = {0u, 0u, 0u, 0u};
+            int run = 0;
+#pragma unroll
+            for (int rr = 0; rr < TSG_BS; rr++)
+            {
+                pk[rr >> 2] |= (unsigned)run << ((rr & 3) * 8);
+                run += __popc((w2[rr >> 1] >> ((rr & 1) * 16)) & 0xFFFFu);
+            }
+            *reinterpret_cast<uint4 *>(P.C_Ptr + t * TSG_BS) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+            P.C_tnnz[t] = run;
+            if (s_bins)
+                atomicAdd(&s_bins[nnz_bin(run)], 1);
+        }
+        s0 = s1;
+    }
+}
+
+// Step 3 of hypersparse tile row I by the CTA.
+__device__ __forceinline__ void step3_hyper_row(const ProdView &P, HypSmem &S, int I)
+{
+    const int tid = threadIdx.x, lane = tid & 31, r = tid >> 5;
+    const int rs = P.C_ptr[I], re = P.C_ptr[I + 1];
+    __syncthreads();
+    {
+        const int v1 = P.C_tnnz[re];
+        for (int q = P.C_tnnz[rs] + tid; q < v1; q += SPA_THREADS)
+            P.C_Val[q] = 0.0;
+    }
+    __threadfence_block();
+    HypStage &G = S.stage[r];
+    for (int s0 = rs; s0 < re;)
+    {
+        __syncthreads();
+        const int W0 = P.C_col[s0];
+        const int s1 = hyp_window(P, S, s0, re, W0);
+        const int nw = s1 - s0;
+        hyp_walk<true>(P, G, I, r, lane, [&](bool valid, int e, int bi) {
+            int pos = -1 - lane; // distinct keys for lanes without a slot
+            double prod = 0.0;
+            if (valid)
+            {
+                const int col = P.B_rcol[bi];
+                const int w = (col >> 4) - W0;
+                if (w >= 0 && w < HYP_WIN)
+                {
+                    const int sl = S.map[w];
+                    if (sl < nw)
+                    {
+                        const long long t = (long long)s0 + sl;
+                        const unsigned m = P.C_mask[t * TSG_BS + r];
+                        const int cc = col & 15;
+                        if ((m >> (15 - cc)) & 1u)
+                        {
+                            pos = P.C_tnnz[t] + P.C_Ptr[t * TSG_BS + r] + __popc(m >> (16 - cc));
+                            prod = __dmul_rn(G.a[e], P.B_rval[bi]);
+                            P.C_Colb[pos] = (unsigned char)cc;
+                        }
+                    }
+                }
+            }
+            const unsigned grp = __match_any_sync(TSG_FULL_MASK, pos);
+            G.prod[lane] = prod;
+            __syncwarp();
+            if (pos >= 0 && lane == __ffs(grp) - 1)
+            {
+                double acc = __ldcg(P.C_Val + pos);
+                unsigned gl = grp;
+                while (gl)
+                {
+                    const int l = __ffs(gl) - 1;
+                    gl &= gl - 1;
+                    acc = __dadd_rn(acc, G.prod[l]);
+                }
+                P.C_Val[pos] = acc;
+            }
+            __syncwarp();
+        });
+        s0 = s1;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Work item of the SPA steps: a block of blk consecutive C tiles (global
+// tile order).  Ownership: a row of at most blk tiles belongs, whole, to the
+// block holding its first tile; a longer row is cut into blk-tile chunks from
+// its start, each belonging to the block holding the chunk's first tile.  So
+// every tile is done once, short rows are never cut, and a long row is spread
+// over many blocks (and CTAs).  The CTA cuts each piece further into segments
+// within the SPA limits.  blk is SPA_BLK, doubled (up to 16 SPA_BLK) while
+// the product's mean C tile row holds at least two blocks: products whose
+// rows are all long then take fewer blocks from the shared counter.
 #define SPA_BLK 256
+
+__host__ __device__ __forceinline__ int spa_block_tiles(long long numC, int tilem)
+{
+    const long long mean = tilem > 0 ? numC / tilem : 0;
+    int blk = SPA_BLK;
+    while (blk < 16 * SPA_BLK && mean >= 2LL * blk)
+        blk <<= 1;
+    return blk;
+}
 
 // calls piece(I, t0, t1) for the pieces [t0, t1) owned by block [tb, te),
 // rows longer than CH tiles being cut into CH-tile chunks
-template <int CH, typename F>
-__device__ __forceinline__ void spa_block_pieces(const ProdView &P, int tb, int te, F piece)
+template <typename F>
+__device__ __forceinline__ void spa_block_pieces(const ProdView &P, int tb, int te, int CH, F piece)
 {
     int t = tb;
     {
@@ -1137,9 +1494,20 @@ __device__ __forceinline__ void spa_block_pieces(const ProdView &P, int tb, int 
     }
 }
 
-__device__ __forceinline__ void step3_spa_block(const ProdView &P, SpaSmem &S, int tb, int te)
+// Hypersparse rows (kind[I] == 2, kind may be null) are done whole by the
+// block owning their first tile.
+static_assert(sizeof(HypSmem) <= sizeof(SpaSmem) && sizeof(HypSmem) <= sizeof(Spa2Smem), "hyper scratch");
+
+__device__ __forceinline__ void step3_spa_block(const ProdView &P, SpaSmem &S, int tb, int te, int blk,
+                                                const int *__restrict__ kind)
 {
-    spa_block_pieces<SPA_BLK>(P, tb, te, [&](int I, int ps, int pe) {
+    spa_block_pieces(P, tb, te, blk, [&](int I, int ps, int pe) {
+        if (kind && kind[I] == 2)
+        {
+            if (ps == P.C_ptr[I])
+                step3_hyper_row(P, reinterpret_cast<HypSmem &>(S), I);
+            return;
+        }
         for (int t0 = ps; t0 < pe;)
         {
             const int cand = t0 + 1 + (int)threadIdx.x;
@@ -1153,13 +1521,21 @@ __device__ __forceinline__ void step3_spa_block(const ProdView &P, SpaSmem &S, i
     });
 }
 
-// Symbolic counterpart, for the pieces of wide rows only (wide[I] != 0).
-__device__ __forceinline__ void step2_spa_block(const ProdView &P, Spa2Smem &S, int tb, int te,
+// Symbolic counterpart, for the pieces of wide rows only (wide[I] != 0;
+// 2 marks a hypersparse row).
+__device__ __forceinline__ void step2_spa_block(const ProdView &P, Spa2Smem &S, int tb, int te, int blk,
                                                 const int *__restrict__ wide, int *s_bins)
 {
-    spa_block_pieces<SPA_BLK>(P, tb, te, [&](int I, int ps, int pe) {
-        if (!wide[I])
+    spa_block_pieces(P, tb, te, blk, [&](int I, int ps, int pe) {
+        const int kind = wide[I];
+        if (!kind)
             return;
+        if (kind == 2)
+        {
+            if (ps == P.C_ptr[I])
+                step2_hyper_row(P, reinterpret_cast<HypSmem &>(S), I, s_bins);
+            return;
+        }
         for (int t0 = ps; t0 < pe;)
         {
             const int cand = t0 + 1 + (int)threadIdx.x;

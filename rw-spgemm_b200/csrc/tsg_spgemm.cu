@@ -29,7 +29,7 @@ __global__ void __launch_bounds__(S1_WARPS * 32) k_step1(ProdView P, int *__rest
 }
 
 // fused step-1 emit + step 2 (warp per A tile row); wide rows are emitted by
-// step1_row and flagged for k_step2_wide
+// step1_row and flagged for the wide-row step 2 (1, or 2 when hypersparse)
 __global__ void __launch_bounds__(256) k_step12(ProdView P, int *__restrict__ wide, int *__restrict__ bins)
 {
     __shared__ S12Smem sm[8];
@@ -42,16 +42,18 @@ __global__ void __launch_bounds__(256) k_step12(ProdView P, int *__restrict__ wi
     if (i < P.tilemA)
     {
         const int done = step12_row(P, i, sm[warp], lane, s_bins);
+        int kind = 0;
         if (!done)
         {
             static_assert(sizeof(S12Smem) >= S1_WORDS * sizeof(unsigned), "bitmap scratch");
             __syncwarp();
             step1_row<true>(P, i, reinterpret_cast<unsigned *>(&sm[warp]), lane, nullptr);
+            kind = wide_kind(P, i, lane);
         }
         if (lane == 0)
         {
-            wide[i] = done ? 0 : 1;
-            if (!done)
+            wide[i] = kind;
+            if (kind)
                 atomicAdd(&wide[P.tilemA], 1); // count of wide rows
         }
     }
@@ -77,7 +79,7 @@ __global__ void __launch_bounds__(256) k_step2_wide(ProdView P, const int *__res
 
 // scalar step 2 for the wide rows k_step12 left: CTAs take blocks of C tiles
 // from a device counter and run the wide rows' parts
-__global__ void __launch_bounds__(SPA_THREADS) k_step2_spa(ProdView P, const int *__restrict__ wide,
+__global__ void __launch_bounds__(SPA_THREADS) k_step2_spa(ProdView P, const int *__restrict__ wide, int blk,
                                                            unsigned *__restrict__ ctr, int *__restrict__ bins)
 {
     extern __shared__ __align__(16) unsigned char s_raw[];
@@ -94,10 +96,10 @@ __global__ void __launch_bounds__(SPA_THREADS) k_step2_spa(ProdView P, const int
         if (threadIdx.x == 0)
             s_blk = (int)atomicAdd(ctr, 1u);
         __syncthreads();
-        const long long tb = (long long)s_blk * SPA_BLK;
+        const long long tb = (long long)s_blk * blk;
         if (tb >= P.numC)
             break;
-        step2_spa_block(P, S, (int)tb, (int)min((long long)P.numC, tb + SPA_BLK), wide, s_bins);
+        step2_spa_block(P, S, (int)tb, (int)min((long long)P.numC, tb + blk), blk, wide, s_bins);
     }
     __syncthreads();
     if (threadIdx.x < 4 && s_bins[threadIdx.x])
@@ -167,8 +169,10 @@ __global__ void __launch_bounds__(128) k_step3_rows(ProdView P)
     step3_rows_item<W, CAP>(P, item, TSG_HW_MASK(threadIdx.x), threadIdx.x & 15, sm[threadIdx.x >> 4]);
 }
 
-// persistent: CTAs take blocks of C tiles from a device counter
-__global__ void __launch_bounds__(SPA_THREADS, 3) k_step3_spa(ProdView P, unsigned *__restrict__ ctr)
+// persistent: CTAs take blocks of C tiles from a device counter; kind (may
+// be null) marks the hypersparse rows (2), each done whole
+__global__ void __launch_bounds__(SPA_THREADS, 3) k_step3_spa(ProdView P, const int *__restrict__ kind, int blk,
+                                                              unsigned *__restrict__ ctr)
 {
     extern __shared__ __align__(16) unsigned char s_raw[];
     SpaSmem &S = *reinterpret_cast<SpaSmem *>(s_raw);
@@ -179,10 +183,10 @@ __global__ void __launch_bounds__(SPA_THREADS, 3) k_step3_spa(ProdView P, unsign
         if (threadIdx.x == 0)
             s_blk = (int)atomicAdd(ctr, 1u);
         __syncthreads();
-        const long long tb = (long long)s_blk * SPA_BLK;
+        const long long tb = (long long)s_blk * blk;
         if (tb >= P.numC)
             break;
-        step3_spa_block(P, S, (int)tb, (int)min((long long)P.numC, tb + SPA_BLK));
+        step3_spa_block(P, S, (int)tb, (int)min((long long)P.numC, tb + blk), blk, kind);
     }
 }
 
@@ -302,31 +306,34 @@ static int launch_step2_spa(tsg_context *ctx, const ProdView &P, const int *d_wi
     TSG_TRY(spa_grid(ctx, k_step2_spa, smem, &grid));
     TSG_TRY(tsg_alloc(ctx, &ctr, 1));
     TSG_CUDA(cudaMemsetAsync(ctr, 0, sizeof(unsigned), ctx->stream));
-    k_step2_spa<<<grid, SPA_THREADS, smem, ctx->stream>>>(P, d_wide, ctr, d_bins);
+    k_step2_spa<<<grid, SPA_THREADS, smem, ctx->stream>>>(P, d_wide, spa_block_tiles(P.numC, P.tilemA), ctr,
+                                                          d_bins);
     TSG_LAUNCH_CHECK();
     tsg_release(ctx, ctr);
     return TSG_OK;
 }
 
-static int launch_step3_spa(tsg_context *ctx, const ProdView &P)
+static int launch_step3_spa(tsg_context *ctx, const ProdView &P, const int *d_kind)
 {
     unsigned *ctr = nullptr, grid = 0;
     const int smem = (int)sizeof(SpaSmem);
     TSG_TRY(spa_grid(ctx, k_step3_spa, smem, &grid));
     TSG_TRY(tsg_alloc(ctx, &ctr, 1));
     TSG_CUDA(cudaMemsetAsync(ctr, 0, sizeof(unsigned), ctx->stream));
-    k_step3_spa<<<grid, SPA_THREADS, smem, ctx->stream>>>(P, ctr);
+    k_step3_spa<<<grid, SPA_THREADS, smem, ctx->stream>>>(P, d_kind, spa_block_tiles(P.numC, P.tilemA), ctr);
     TSG_LAUNCH_CHECK();
     tsg_release(ctx, ctr);
     return TSG_OK;
 }
 
-static int launch_step3(tsg_context *ctx, const ProdView &P, long long nnzC)
+// d_kind: the row kinds of the fused step 1/2 pass (0 narrow, 1 wide,
+// 2 hypersparse), or null
+static int launch_step3(tsg_context *ctx, const ProdView &P, long long nnzC, const int *d_kind)
 {
     // SPA: products whose C tiles are dense on average (>= SPA_DENSE values)
     // and B without a row view (borrowed foreign buffers) take the tile kernel
     if (ctx->sched == TSG_SCHED_SPA && P.B_rptr && nnzC < (long long)SPA_DENSE * P.numC)
-        return launch_step3_spa(ctx, P);
+        return launch_step3_spa(ctx, P, d_kind);
     if (ctx->sched == TSG_SCHED_ROWS)
     {
         const int W = ctx->seg_tiles, cap = ctx->acc_cap;
@@ -431,7 +438,6 @@ extern "C" int tsg_spgemm(tsg_context *ctx, const tsg_tiled *A, const tsg_tiled 
     }
     else
         TSG_CUDA(cudaMemsetAsync(C->tile_nnz, 0, sizeof(int), st));
-    tsg_release(ctx, d_wide);
     C->nnz = (int)nnzC;
     if (timing)
         TSG_CUDA(cudaEventRecord(ctx->ev[2], st));
@@ -440,7 +446,8 @@ extern "C" int tsg_spgemm(tsg_context *ctx, const tsg_tiled *A, const tsg_tiled 
     TSG_TRY(tsg_alloc(ctx, &C->tile_csr_Col, (size_t)nnzC));
     TSG_TRY(tsg_alloc(ctx, &C->tile_csr_Value, (size_t)nnzC));
     if (nnzC > 0)
-        TSG_TRY(launch_step3(ctx, make_view(A, B, C), nnzC));
+        TSG_TRY(launch_step3(ctx, make_view(A, B, C), nnzC, d_wide));
+    tsg_release(ctx, d_wide);
     if (timing)
         TSG_CUDA(cudaEventRecord(ctx->ev[3], st));
 

@@ -33,6 +33,9 @@ def _pairs(gen):
     mats.append((gen.laplacian_2d(30), gen.laplacian_2d(30)))
     mats.append(((5, 6, np.zeros(6, np.int32), np.zeros(0, np.int32), np.zeros(0)),
                  gen.random_poisson(6, 9, 2.0, seed=9)))                    # empty A
+    # hypersparse: wide C tile rows with few products (whole-row path)
+    mats.append((gen.random_poisson(8192, 8192, 4.0, seed=10), gen.random_poisson(8192, 8192, 4.0, seed=11)))
+    mats.append((gen.random_poisson(3000, 4000, 2.0, seed=12), gen.random_poisson(4000, 9000, 3.0, seed=13)))
     return mats
 
 
