@@ -34,7 +34,6 @@ struct BatchProd
     int tilemA;
     int status; // 0 ok, 1 tile capacity, 2 value capacity
     int numC, nnzC;
-    int spa_blk; // C tiles per SPA work block (set with the block prefix)
 };
 
 struct tsg_batch
@@ -114,6 +113,13 @@ __device__ __forceinline__ int find_product(const long long *__restrict__ off, i
             hi = mid - 1;
     }
     return lo;
+}
+
+// The same for x at or after off[p] (a CTA's claims from a counter only grow):
+// usually x is still in product p.
+__device__ __forceinline__ int find_product_from(const long long *__restrict__ off, int count, long long x, int p)
+{
+    return off[p + 1] > x ? p : find_product(off, count, x);
 }
 
 // Block-wide exclusive scan of a[0..n) in place, a[n] = total (NT threads;
@@ -334,15 +340,13 @@ __global__ void __launch_bounds__(NT)
                 run += SCHED == 1 ? (nc + W - 1) / W : nc;
             }
             itemoff[count] = run;
-            // SPA: blocks of spa_blk C tiles per product, prefix after itemoff
+            // SPA: blocks of SPA_BLK C tiles per product, prefix after itemoff
             long long *blkoff = itemoff + count + 1;
             run = 0;
             for (int p = 0; p < count; p++)
             {
                 blkoff[p] = run;
-                const int blk = spa_block_tiles(prods[p].numC, prods[p].tilemA);
-                prods[p].spa_blk = blk;
-                run += ((long long)prods[p].numC + blk - 1) / blk;
+                run += ((long long)prods[p].numC + SPA_BLK - 1) / SPA_BLK;
             }
             blkoff[count] = run;
             // tile-count scan chunks per product, prefix after the stamps
@@ -387,6 +391,7 @@ __global__ void __launch_bounds__(NT)
                 {
                     __syncwarp();
                     step1_row<true>(prods[p].P, i, reinterpret_cast<unsigned *>(s12), lane32, nullptr);
+                    __syncwarp(); // the row's C columns, emitted by all lanes
                     kind = SCHED == 3 ? wide_kind(prods[p].P, i, lane32) : 1;
                 }
                 if (lane32 == 0)
@@ -404,22 +409,30 @@ __global__ void __launch_bounds__(NT)
         // wide rows through B's row view; CTAs take blocks of C tiles
         Spa2Smem &S2 = *reinterpret_cast<Spa2Smem *>(s_raw);
         const long long *blkoff = itemoff + count + 1;
+        unsigned nxt = 0; // thread 0: the next block, claimed one block ahead
+        if (threadIdx.x == 0)
+            nxt = atomicAdd(&bar[3], 1u);
+        int p = 0;
         for (;;)
         {
             __syncthreads();
             if (threadIdx.x == 0)
-                s_row = (int)atomicAdd(&bar[3], 1u);
+            {
+                s_row = (int)nxt;
+                nxt = atomicAdd(&bar[3], 1u);
+            }
             __syncthreads();
             const long long blk = s_row;
             if (blk >= blkoff[count])
                 break;
-            const int p = find_product(blkoff, count, blk);
+            p = find_product_from(blkoff, count, blk, p);
             if (prods[p].status)
                 continue;
             const ProdView &P = prods[p].P;
-            const int nb = prods[p].spa_blk;
-            const long long tb = (blk - blkoff[p]) * nb;
-            step2_spa_block(P, S2, (int)tb, (int)min((long long)P.numC, tb + nb), nb, prods[p].wide, s_bins);
+            const long long tb = (blk - blkoff[p]) * SPA_BLK;
+            if (threadIdx.x == 0)
+                spa_skip_hyper(P, prods[p].wide, (int)tb, &bar[3], blkoff[p]);
+            step2_spa_block(P, S2, (int)tb, (int)min((long long)P.numC, tb + SPA_BLK), prods[p].wide, s_bins);
         }
     }
     else
@@ -539,7 +552,7 @@ __global__ void __launch_bounds__(NT)
 }
 
 // Step 3 of the SPA schedule over a batch, after k_batch: products with
-// sparse C tiles, CTAs taking blocks of C tiles (spa_blk, all products) from a
+// sparse C tiles, CTAs taking blocks of SPA_BLK C tiles (all products) from a
 // device counter.  Raises stamp[7] on exit.
 __global__ void __launch_bounds__(SPA_THREADS, 3)
     k_batch_spa3(BatchProd *prods, int count, const long long *__restrict__ itemoff, unsigned *bar)
@@ -548,22 +561,30 @@ __global__ void __launch_bounds__(SPA_THREADS, 3)
     __shared__ int s_blk;
     SpaSmem &S = *reinterpret_cast<SpaSmem *>(s_raw);
     const long long *blkoff = itemoff + count + 1;
+    unsigned nxt = 0; // thread 0: the next block, claimed one block ahead
+    if (threadIdx.x == 0)
+        nxt = atomicAdd(&bar[2], 1u);
+    int p = 0;
     for (;;)
     {
         __syncthreads();
         if (threadIdx.x == 0)
-            s_blk = (int)atomicAdd(&bar[2], 1u);
+        {
+            s_blk = (int)nxt;
+            nxt = atomicAdd(&bar[2], 1u);
+        }
         __syncthreads();
         const long long blk = s_blk;
         if (blk >= blkoff[count])
             break;
-        const int p = find_product(blkoff, count, blk);
+        p = find_product_from(blkoff, count, blk, p);
         if (prods[p].status || prods[p].nnzC >= (long long)SPA_DENSE * prods[p].numC)
             continue;
         const ProdView &P = prods[p].P;
-        const int nb = prods[p].spa_blk;
-        const long long tb = (blk - blkoff[p]) * nb;
-        step3_spa_block(P, S, (int)tb, (int)min((long long)P.numC, tb + nb), nb, prods[p].wide);
+        const long long tb = (blk - blkoff[p]) * SPA_BLK;
+        if (threadIdx.x == 0)
+            spa_skip_hyper(P, prods[p].wide, (int)tb, &bar[2], blkoff[p]);
+        step3_spa_block(P, S, (int)tb, (int)min((long long)P.numC, tb + SPA_BLK), prods[p].wide);
     }
     __syncthreads();
     if (threadIdx.x == 0)

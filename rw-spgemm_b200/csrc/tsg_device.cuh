@@ -1118,11 +1118,14 @@ __device__ __forceinline__ void step2_spa_segment(const ProdView &P, Spa2Smem &S
 //    slot are summed by the lowest of them in lane order, and batches follow
 //    one another behind warp barriers, so every C entry sums its products in
 //    k order, each product rounded before the add, as the reference does.
-// The tile column -> tile map covers HYP_WIN tile columns; a row spanning
-// more is done in window passes, each taking the products that fall in it.
+// The tile column -> tile map covers HYP_WIN tile columns.  Rows are marked
+// hypersparse only when their C tiles span less than that (each further
+// window would repeat the walk of the row's products); the routines still
+// take any row, window by window, each pass adding the products in it.
 // ---------------------------------------------------------------------------
-#define HYP_WIN 8192
+#define HYP_WIN 16384
 #define HYP_RATIO 4
+static_assert(HYP_WIN / 32 <= SPA_THREADS, "one hit-bitmap word per thread");
 
 struct HypStage
 {
@@ -1170,28 +1173,43 @@ __device__ __forceinline__ int hyp_cta_scan(int v, int *wsum, int &total)
     return off + incl - v;
 }
 
-// 2 when the wide A tile row i is hypersparse (estimated scalar products
-// below HYP_RATIO per C tile of the row) and B has a row view, else 1.  The
-// estimate takes each A tile's nonzeros times the mean length of the B rows
-// of its tile column: sum(nnz(A tile) * nnz(B tile row)) / 16.  Warp-uniform;
-// every lane calls it; C's row pointer must be final.
+// 2 when the wide A tile row i is hypersparse, else 1: B has a row view,
+// the row's C tiles span less than one map window (HYP_WIN tile columns), and
+// the row's scalar products -- counted exactly, sum over A's entries of the
+// length of B's row -- are below HYP_RATIO per C tile.  The count stops at
+// that limit.  Warp-uniform; every lane calls it, after the row's C columns
+// are emitted (and visible to the warp).
 __device__ __forceinline__ int wide_kind(const ProdView &P, int i, int lane)
 {
     if (!P.B_rptr)
         return 1;
+    const int rs = P.C_ptr[i], re = P.C_ptr[i + 1];
+    if (re == rs || P.C_col[re - 1] - P.C_col[rs] >= HYP_WIN)
+        return 1;
+    const long long lim = (long long)HYP_RATIO * (re - rs);
     const int a0 = P.A_ptr[i], a1 = P.A_ptr[i + 1];
-    long long est = 0;
-    for (int pa = a0 + lane; pa < a1; pa += 32)
+    long long np = 0;
+    for (int g = a0; g < a1; g += 32)
     {
-        const int k = P.A_col[pa];
-        const long long nb = P.B_tnnz[P.B_ptr[k + 1]] - P.B_tnnz[P.B_ptr[k]];
-        est += (long long)(P.A_tnnz[pa + 1] - P.A_tnnz[pa]) * nb;
-    }
+        const int pa = g + lane; // lane per A tile: its entries' B row lengths
+        if (pa < a1)
+        {
+            const int kb = P.A_col[pa] * TSG_BS;
+            const int e1 = P.A_tnnz[pa + 1];
+            for (int e = P.A_tnnz[pa]; e < e1; e++)
+            {
+                const int k = kb + (P.A_Colb[e] & 15);
+                np += P.B_rptr[k + 1] - P.B_rptr[k];
+            }
+        }
 #pragma unroll
-    for (int d = 16; d > 0; d >>= 1)
-        est += __shfl_xor_sync(TSG_FULL_MASK, est, d);
-    const long long nt = P.C_ptr[i + 1] - P.C_ptr[i];
-    return est < (long long)HYP_RATIO * TSG_BS * nt ? 2 : 1;
+        for (int d = 16; d > 0; d >>= 1)
+            np += __shfl_xor_sync(TSG_FULL_MASK, np, d);
+        if (np >= lim)
+            return 1;
+        np = lane == 0 ? np : 0; // keep the running total in one lane
+    }
+    return 2;
 }
 
 // Warp r enumerates the products of C row 16 I + r: A's entries of the row in
@@ -1444,30 +1462,20 @@ __device__ __forceinline__ void step3_hyper_row(const ProdView &P, HypSmem &S, i
 }
 
 // ---------------------------------------------------------------------------
-// Work item of the SPA steps: a block of blk consecutive C tiles (global
-// tile order).  Ownership: a row of at most blk tiles belongs, whole, to the
-// block holding its first tile; a longer row is cut into blk-tile chunks from
-// its start, each belonging to the block holding the chunk's first tile.  So
-// every tile is done once, short rows are never cut, and a long row is spread
-// over many blocks (and CTAs).  The CTA cuts each piece further into segments
-// within the SPA limits.  blk is SPA_BLK, doubled (up to 16 SPA_BLK) while
-// the product's mean C tile row holds at least two blocks: products whose
-// rows are all long then take fewer blocks from the shared counter.
+// Work item of the SPA steps: a block of SPA_BLK consecutive C tiles (global
+// tile order).  Ownership: a row of at most SPA_BLK tiles belongs, whole, to
+// the block holding its first tile; a longer row is cut into SPA_BLK-tile
+// chunks from its start, each belonging to the block holding the chunk's
+// first tile.  So every tile is done once, short rows are never cut, and a
+// long row is spread over many blocks (and CTAs).  The CTA cuts each piece
+// further into segments within the SPA limits.  A hypersparse row belongs
+// whole to the block holding its first tile.
 #define SPA_BLK 256
-
-__host__ __device__ __forceinline__ int spa_block_tiles(long long numC, int tilem)
-{
-    const long long mean = tilem > 0 ? numC / tilem : 0;
-    int blk = SPA_BLK;
-    while (blk < 16 * SPA_BLK && mean >= 2LL * blk)
-        blk <<= 1;
-    return blk;
-}
 
 // calls piece(I, t0, t1) for the pieces [t0, t1) owned by block [tb, te),
 // rows longer than CH tiles being cut into CH-tile chunks
-template <typename F>
-__device__ __forceinline__ void spa_block_pieces(const ProdView &P, int tb, int te, int CH, F piece)
+template <int CH, typename F>
+__device__ __forceinline__ void spa_block_pieces(const ProdView &P, int tb, int te, F piece)
 {
     int t = tb;
     {
@@ -1494,14 +1502,31 @@ __device__ __forceinline__ void spa_block_pieces(const ProdView &P, int tb, int 
     }
 }
 
+// A block lying inside a hypersparse row (kind[I] == 2) that an earlier block
+// owns has no work, nor have the row's following blocks before the one
+// holding the row's end: the claiming thread raises the block counter ctr
+// (blocks of this product numbered from base) past them.
+__device__ __forceinline__ void spa_skip_hyper(const ProdView &P, const int *__restrict__ kind, int tb,
+                                               unsigned *ctr, long long base)
+{
+    if (!kind)
+        return;
+    const int I = P.C_row[tb];
+    if (kind[I] != 2 || P.C_ptr[I] >= tb)
+        return;
+    const long long next = base + P.C_ptr[I + 1] / SPA_BLK;
+    if (next > base + tb / SPA_BLK + 1)
+        atomicMax(ctr, (unsigned)next);
+}
+
 // Hypersparse rows (kind[I] == 2, kind may be null) are done whole by the
 // block owning their first tile.
 static_assert(sizeof(HypSmem) <= sizeof(SpaSmem) && sizeof(HypSmem) <= sizeof(Spa2Smem), "hyper scratch");
 
-__device__ __forceinline__ void step3_spa_block(const ProdView &P, SpaSmem &S, int tb, int te, int blk,
+__device__ __forceinline__ void step3_spa_block(const ProdView &P, SpaSmem &S, int tb, int te,
                                                 const int *__restrict__ kind)
 {
-    spa_block_pieces(P, tb, te, blk, [&](int I, int ps, int pe) {
+    spa_block_pieces<SPA_BLK>(P, tb, te, [&](int I, int ps, int pe) {
         if (kind && kind[I] == 2)
         {
             if (ps == P.C_ptr[I])
@@ -1522,11 +1547,13 @@ __device__ __forceinline__ void step3_spa_block(const ProdView &P, SpaSmem &S, i
 }
 
 // Symbolic counterpart, for the pieces of wide rows only (wide[I] != 0;
-// 2 marks a hypersparse row).
-__device__ __forceinline__ void step2_spa_block(const ProdView &P, Spa2Smem &S, int tb, int te, int blk,
+// 2 marks a hypersparse row).  Long rows go in chunks of SP2_SEGT tiles, one
+// segment's worth: each segment walks A's whole row, so shorter chunks would
+// repeat that walk.
+__device__ __forceinline__ void step2_spa_block(const ProdView &P, Spa2Smem &S, int tb, int te,
                                                 const int *__restrict__ wide, int *s_bins)
 {
-    spa_block_pieces(P, tb, te, blk, [&](int I, int ps, int pe) {
+    spa_block_pieces<SP2_SEGT>(P, tb, te, [&](int I, int ps, int pe) {
         const int kind = wide[I];
         if (!kind)
             return;

@@ -48,6 +48,7 @@ __global__ void __launch_bounds__(256) k_step12(ProdView P, int *__restrict__ wi
             static_assert(sizeof(S12Smem) >= S1_WORDS * sizeof(unsigned), "bitmap scratch");
             __syncwarp();
             step1_row<true>(P, i, reinterpret_cast<unsigned *>(&sm[warp]), lane, nullptr);
+            __syncwarp(); // the row's C columns, emitted by all lanes
             kind = wide_kind(P, i, lane);
         }
         if (lane == 0)
@@ -79,7 +80,7 @@ __global__ void __launch_bounds__(256) k_step2_wide(ProdView P, const int *__res
 
 // scalar step 2 for the wide rows k_step12 left: CTAs take blocks of C tiles
 // from a device counter and run the wide rows' parts
-__global__ void __launch_bounds__(SPA_THREADS) k_step2_spa(ProdView P, const int *__restrict__ wide, int blk,
+__global__ void __launch_bounds__(SPA_THREADS) k_step2_spa(ProdView P, const int *__restrict__ wide,
                                                            unsigned *__restrict__ ctr, int *__restrict__ bins)
 {
     extern __shared__ __align__(16) unsigned char s_raw[];
@@ -90,16 +91,24 @@ __global__ void __launch_bounds__(SPA_THREADS) k_step2_spa(ProdView P, const int
         return;
     if (threadIdx.x < 4)
         s_bins[threadIdx.x] = 0;
+    unsigned nxt = 0; // thread 0: the next block, claimed one block ahead
+    if (threadIdx.x == 0)
+        nxt = atomicAdd(ctr, 1u);
     for (;;)
     {
         __syncthreads();
         if (threadIdx.x == 0)
-            s_blk = (int)atomicAdd(ctr, 1u);
+        {
+            s_blk = (int)nxt;
+            nxt = atomicAdd(ctr, 1u);
+        }
         __syncthreads();
-        const long long tb = (long long)s_blk * blk;
+        const long long tb = (long long)s_blk * SPA_BLK;
         if (tb >= P.numC)
             break;
-        step2_spa_block(P, S, (int)tb, (int)min((long long)P.numC, tb + blk), blk, wide, s_bins);
+        if (threadIdx.x == 0)
+            spa_skip_hyper(P, wide, (int)tb, ctr, 0);
+        step2_spa_block(P, S, (int)tb, (int)min((long long)P.numC, tb + SPA_BLK), wide, s_bins);
     }
     __syncthreads();
     if (threadIdx.x < 4 && s_bins[threadIdx.x])
@@ -171,22 +180,30 @@ __global__ void __launch_bounds__(128) k_step3_rows(ProdView P)
 
 // persistent: CTAs take blocks of C tiles from a device counter; kind (may
 // be null) marks the hypersparse rows (2), each done whole
-__global__ void __launch_bounds__(SPA_THREADS, 3) k_step3_spa(ProdView P, const int *__restrict__ kind, int blk,
+__global__ void __launch_bounds__(SPA_THREADS, 3) k_step3_spa(ProdView P, const int *__restrict__ kind,
                                                               unsigned *__restrict__ ctr)
 {
     extern __shared__ __align__(16) unsigned char s_raw[];
     SpaSmem &S = *reinterpret_cast<SpaSmem *>(s_raw);
     __shared__ int s_blk;
+    unsigned nxt = 0; // thread 0: the next block, claimed one block ahead
+    if (threadIdx.x == 0)
+        nxt = atomicAdd(ctr, 1u);
     for (;;)
     {
         __syncthreads();
         if (threadIdx.x == 0)
-            s_blk = (int)atomicAdd(ctr, 1u);
+        {
+            s_blk = (int)nxt;
+            nxt = atomicAdd(ctr, 1u);
+        }
         __syncthreads();
-        const long long tb = (long long)s_blk * blk;
+        const long long tb = (long long)s_blk * SPA_BLK;
         if (tb >= P.numC)
             break;
-        step3_spa_block(P, S, (int)tb, (int)min((long long)P.numC, tb + blk), blk, kind);
+        if (threadIdx.x == 0)
+            spa_skip_hyper(P, kind, (int)tb, ctr, 0);
+        step3_spa_block(P, S, (int)tb, (int)min((long long)P.numC, tb + SPA_BLK), kind);
     }
 }
 
@@ -306,8 +323,7 @@ static int launch_step2_spa(tsg_context *ctx, const ProdView &P, const int *d_wi
     TSG_TRY(spa_grid(ctx, k_step2_spa, smem, &grid));
     TSG_TRY(tsg_alloc(ctx, &ctr, 1));
     TSG_CUDA(cudaMemsetAsync(ctr, 0, sizeof(unsigned), ctx->stream));
-    k_step2_spa<<<grid, SPA_THREADS, smem, ctx->stream>>>(P, d_wide, spa_block_tiles(P.numC, P.tilemA), ctr,
-                                                          d_bins);
+    k_step2_spa<<<grid, SPA_THREADS, smem, ctx->stream>>>(P, d_wide, ctr, d_bins);
     TSG_LAUNCH_CHECK();
     tsg_release(ctx, ctr);
     return TSG_OK;
@@ -320,7 +336,7 @@ static int launch_step3_spa(tsg_context *ctx, const ProdView &P, const int *d_ki
     TSG_TRY(spa_grid(ctx, k_step3_spa, smem, &grid));
     TSG_TRY(tsg_alloc(ctx, &ctr, 1));
     TSG_CUDA(cudaMemsetAsync(ctr, 0, sizeof(unsigned), ctx->stream));
-    k_step3_spa<<<grid, SPA_THREADS, smem, ctx->stream>>>(P, d_kind, spa_block_tiles(P.numC, P.tilemA), ctr);
+    k_step3_spa<<<grid, SPA_THREADS, smem, ctx->stream>>>(P, d_kind, ctr);
     TSG_LAUNCH_CHECK();
     tsg_release(ctx, ctr);
     return TSG_OK;

@@ -171,41 +171,41 @@ def test_many_pairs_per_c_tile(tsg, ctx, sched, oracle, gen):
     assert np.array_equal(v.view(np.uint64), G[4].view(np.uint64))
 
 
-def _hyper_estimate(matA, matB, tile_ptr_C):
-    """Per A tile row: (estimated scalar products, C tiles), the estimate being
-    sum over A tiles of nnz(A tile) * nnz(B tile row) / 16 -- the figure the
-    fused step 1/2 pass compares with 4 products per C tile."""
+def _hyper_rows(matA, matB, Co):
+    """Per A tile row: True where the fused step 1/2 pass marks it
+    hypersparse -- more than 128 C tiles, C tile columns spanning less than
+    16,384, and exact scalar products (sum over A's entries of B's row
+    length) below 4 per C tile."""
     m, _, rpA, ciA, _ = matA
-    k, _, rpB, _, _ = matB
-    tilem, tilek = (m + 15) // 16, (k + 15) // 16
+    tilem = (m + 15) // 16
     rowsA = np.repeat(np.arange(m), np.diff(rpA)) // 16
-    nnz_tile = np.zeros((tilem, tilek), np.int64)
-    np.add.at(nnz_tile, (rowsA, ciA // 16), 1)
-    brow = np.add.reduceat(np.diff(rpB), np.arange(0, k, 16)) if k else np.zeros(0, np.int64)
-    est = (nnz_tile * brow[None, :]).sum(axis=1) / 16.0
-    return est, np.diff(np.asarray(tile_ptr_C))
+    prods = np.bincount(rowsA, weights=np.diff(matB[2])[ciA], minlength=tilem)
+    tp, col = np.asarray(Co["tile_ptr"]), np.asarray(Co["tile_columnidx"])
+    nt = np.diff(tp)
+    span = np.zeros(tilem, np.int64)
+    has = nt > 0
+    span[has] = col[tp[1:][has] - 1] - col[tp[:-1][has]]
+    return (nt > 128) & (span < 16384) & (prods < 4 * nt)
 
 
 def test_hypersparse_rows(tsg, ctx, sched, oracle, gen):
     """Random operands so sparse that nearly every tile column of a C tile row
     exists while few of those tiles receive a product: the whole-row
     hypersparse path (masks ORed in global memory, values summed in k order
-    in place).  Covers rectangular shapes, empty rows of A and B, and C rows
-    spanning more than one 8192-tile-column window (n = 150,000)."""
-    cases = [(gen.random_poisson(8192, 8192, 4.0, seed=31), gen.random_poisson(8192, 8192, 4.0, seed=32)),
-             (gen.random_poisson(6000, 5000, 0.4, seed=33), gen.random_poisson(5000, 7000, 6.0, seed=34)),
-             (gen.random_poisson(4096, 8192, 3.0, seed=35), gen.random_poisson(8192, 150000, 3.0, seed=36))]
-    for matA, matB in cases:
+    in place).  Covers rectangular shapes, empty rows of A and B and rows
+    spanning ~12,000 tile columns (n = 200,000); the last case's C rows span
+    more than 16,384 tile columns (n = 300,000) and take the segment path
+    instead."""
+    cases = [(gen.random_poisson(8192, 8192, 4.0, seed=31), gen.random_poisson(8192, 8192, 4.0, seed=32), True),
+             (gen.random_poisson(6000, 5000, 0.4, seed=33), gen.random_poisson(5000, 7000, 6.0, seed=34), True),
+             (gen.random_poisson(2048, 4096, 3.0, seed=37), gen.random_poisson(4096, 200000, 3.0, seed=38), True),
+             (gen.random_poisson(4096, 8192, 3.0, seed=35), gen.random_poisson(8192, 300000, 3.0, seed=36), False)]
+    for matA, matB, hyper in cases:
         A_, B_, C, info = _handle_product(tsg, ctx, matA, matB)
         Co = oracle.spgemm_tiled(oracle.csr2tile_row_major(matA), oracle.csr2tile_col_major(matB))
         assert_tiles(C.download(), Co, C_KEYS + ["tile_csr_Value"])
-        est, nt = _hyper_estimate(matA, matB, Co["tile_ptr"])
-        wide = nt > 128
-        assert (est[wide] < 4 * nt[wide]).mean() > 0.9  # the inputs do reach the hypersparse path
-    # the last case: C tile rows spanning more than one window of tile columns
-    tp, col = np.asarray(Co["tile_ptr"]), np.asarray(Co["tile_columnidx"])
-    rows = np.flatnonzero(np.diff(tp) > 0)
-    assert int((col[tp[rows + 1] - 1] - col[tp[rows]]).max()) >= 8192
+        frac = _hyper_rows(matA, matB, Co).mean()
+        assert (frac > 0.9) if hyper else (frac < 0.1)
 
 
 _ORACLE_CACHE = {}
@@ -230,8 +230,7 @@ def test_long_rows_in_large_blocks(tsg, ctx, sched, oracle, gen):
     assert_tiles(C.download(), Co, C_KEYS + ["tile_csr_Value"])
     nt = np.diff(np.asarray(Co["tile_ptr"]))
     assert Co["numtile"] // len(nt) >= 2048 and nt.max() > 2048
-    est, _ = _hyper_estimate(matA, matB, Co["tile_ptr"])
-    assert (est[nt > 0] >= 4 * nt[nt > 0]).all()  # SPA rows, not hypersparse
+    assert not _hyper_rows(matA, matB, Co).any()  # SPA rows, not hypersparse
 
 
 def test_laplacian_256_known_answers(tsg, ctx, sched, oracle, gen):
