@@ -584,7 +584,7 @@ __global__ void __launch_bounds__(SPA_THREADS, 3)
         const long long tb = (blk - blkoff[p]) * SPA_BLK;
         if (threadIdx.x == 0)
             spa_skip_hyper(P, prods[p].wide, (int)tb, &bar[2], blkoff[p]);
-        step3_spa_block(P, S, (int)tb, (int)min((long long)P.numC, tb + SPA_BLK), prods[p].wide);
+        step3_spa_block<true>(P, S, (int)tb, (int)min((long long)P.numC, tb + SPA_BLK), prods[p].wide);
     }
     __syncthreads();
     if (threadIdx.x == 0)
@@ -914,6 +914,7 @@ extern "C" int tsg_batch_create(tsg_context *ctx, int count, const tsg_tiled *A,
         P.B_rptr = B[p].row_ptr;
         P.B_rcol = B[p].row_col;
         P.B_rval = B[p].row_val;
+        P.browB = B[p].m > 0 ? (int)(B[p].nnz / B[p].m) : 0;
         P.tilenB = B[p].tilen;
         P.C_ptr = (int *)take(((size_t)A[p].tilem + 1) * 4);
         h.wide = (int *)take((size_t)A[p].tilem * 4);

@@ -34,6 +34,7 @@ struct ProdView
     const unsigned short *B_maskT;
     const int *B_rptr, *B_rcol; // row view of B (scalar CSR), may be null
     const double *B_rval;
+    int browB; // mean entries per row of B (rounded down)
     int tilenB;
     int *C_ptr, *C_col, *C_row, *C_tnnz;
     unsigned short *C_mask;
@@ -749,6 +750,7 @@ __device__ __forceinline__ void step3_rows_item(const ProdView &P, long long ite
 #define SPA_WIN 2048
 #define SPA_STAGE 64
 #define SPA_DENSE 64 // C values per tile from which the tile kernel is faster
+#define SPA_FLAT 16  // B rows averaging fewer entries (inside a segment) have their products flattened
 
 struct SpaStage
 {
@@ -765,6 +767,21 @@ struct SpaSmem
     SpaStage stage[SPA_WARPS];
 };
 
+// accumulator slot of column col in the row (cmr, rs), -1 outside the segment
+__device__ __forceinline__ int spa_slot(const SpaSmem &S, const unsigned *cmr, int rs, int J0, int J1, bool full,
+                                        int col)
+{
+    const int J = col >> 4;
+    if (!full && (J < J0 || J >= J1 || J - J0 >= SPA_WIN))
+        return -1;
+    const int slot = S.map[J - J0];
+    if (slot >= SPA_SEGT)
+        return -1;
+    const unsigned cmw = cmr[slot];
+    const int pos = rs + (int)(cmw >> 16) + __popc((cmw & 0xFFFFu) >> (16 - (col & 15)));
+    return pos < SPA_CAP ? pos : -1;
+}
+
 __device__ __forceinline__ void spa_add(SpaSmem &S, const unsigned *cmr, int rs, int J0, int J1, bool full, int col,
                                         double a, double b)
 {
@@ -780,7 +797,25 @@ __device__ __forceinline__ void spa_add(SpaSmem &S, const unsigned *cmr, int rs,
         S.acc[pos] = __dadd_rn(S.acc[pos], __dmul_rn(a, b));
 }
 
-// The CTA computes C tiles [t0, t1) (one tile row, limits as above).
+// True when a product may meet short B rows in the numeric SPA step -- B's
+// rows are short on average, or the mean C tile row is cut into several
+// segments (B rows restricted to a segment's columns) -- so that it runs the
+// FLAT form of step3_spa_segment.  The other form keeps the per-entry loop
+// alone (and its registers).
+__host__ __device__ __forceinline__ bool spa_wants_flat(int browB, long long numC, long long nnzC, int tilem)
+{
+    return browB < SPA_FLAT || numC > (long long)SPA_SEGT * tilem || nnzC > (long long)SPA_CAP * tilem;
+}
+
+// The CTA computes C tiles [t0, t1) (one tile row, limits as above).  FLAT:
+// a stage of A entries whose B rows (inside the segment) hold fewer than
+// SPA_FLAT entries on average has its products flattened -- 32 per batch in
+// k order (A's entries in column order, each with its B row); lanes of a
+// batch meeting the same slot are folded by the lowest of them in lane
+// order, and batches follow one another behind warp barriers, so every slot
+// still sums its products in k order.  Short B rows would otherwise leave
+// most lanes idle, one A entry at a time.
+template <bool FLAT>
 __device__ __forceinline__ void step3_spa_segment(const ProdView &P, SpaSmem &S, int t0, int t1)
 {
     const int tid = threadIdx.x, lane = tid & 31, r = tid >> 5;
@@ -898,6 +933,71 @@ __device__ __forceinline__ void step3_spa_segment(const ProdView &P, SpaSmem &S,
             }
             __syncwarp();
             const int ne = min(SPA_STAGE, total - base);
+            if (FLAT)
+            {
+                const int l0 = lane < ne ? G.bl[lane].y : 0;
+                const int l1 = lane + 32 < ne ? G.bl[lane + 32].y : 0;
+                int i0 = l0, i1 = l1;
+#pragma unroll
+                for (int d = 1; d < 32; d <<= 1)
+                {
+                    const int o0 = __shfl_up_sync(TSG_FULL_MASK, i0, d);
+                    const int o1 = __shfl_up_sync(TSG_FULL_MASK, i1, d);
+                    if (lane >= d)
+                    {
+                        i0 += o0;
+                        i1 += o1;
+                    }
+                }
+                const int h0 = __shfl_sync(TSG_FULL_MASK, i0, 31);
+                const int ni = h0 + __shfl_sync(TSG_FULL_MASK, i1, 31);
+                if (ni < SPA_FLAT * ne)
+                {
+                    // entry e becomes (its first B index - its first item, its first item)
+                    if (lane < ne)
+                        G.bl[lane] = make_int2(G.bl[lane].x - (i0 - l0), i0 - l0);
+                    if (lane + 32 < ne)
+                        G.bl[lane + 32] = make_int2(G.bl[lane + 32].x - (h0 + i1 - l1), h0 + i1 - l1);
+                    __syncwarp();
+                    int ent = 0;
+                    for (int ib = 0; ib < ni; ib += 32)
+                    {
+                        const int item = ib + lane;
+                        int pos = -1 - lane; // distinct keys for lanes without a slot
+                        double prod = 0.0;
+                        if (item < ni)
+                        {
+                            while (ent + 1 < ne && G.bl[ent + 1].y <= item)
+                                ent++;
+                            const int bi = G.bl[ent].x + item;
+                            const int p = spa_slot(S, cmr, rs, J0, J1, full, P.B_rcol[bi]);
+                            if (p >= 0)
+                            {
+                                pos = p;
+                                prod = __dmul_rn(G.a[ent], P.B_rval[bi]);
+                            }
+                        }
+                        const unsigned grp = __match_any_sync(TSG_FULL_MASK, pos);
+                        const bool lead = pos >= 0 && lane == __ffs(grp) - 1;
+                        const int rounds = __reduce_max_sync(TSG_FULL_MASK, pos >= 0 ? __popc(grp) : 0);
+                        double acc = lead ? S.acc[pos] : 0.0;
+                        unsigned gl = grp;
+                        for (int q = 0; q < rounds; q++)
+                        {
+                            const double v = __shfl_sync(TSG_FULL_MASK, prod, gl ? __ffs(gl) - 1 : lane);
+                            if (gl)
+                            {
+                                acc = __dadd_rn(acc, v);
+                                gl &= gl - 1;
+                            }
+                        }
+                        if (lead)
+                            S.acc[pos] = acc;
+                        __syncwarp();
+                    }
+                    continue;
+                }
+            }
             int2 nb = G.bl[0];
             int c_cur = -1;
             double v_cur = 0.0;
@@ -1523,6 +1623,7 @@ __device__ __forceinline__ void spa_skip_hyper(const ProdView &P, const int *__r
 // block owning their first tile.
 static_assert(sizeof(HypSmem) <= sizeof(SpaSmem) && sizeof(HypSmem) <= sizeof(Spa2Smem), "hyper scratch");
 
+template <bool FLAT>
 __device__ __forceinline__ void step3_spa_block(const ProdView &P, SpaSmem &S, int tb, int te,
                                                 const int *__restrict__ kind)
 {
@@ -1540,7 +1641,7 @@ __device__ __forceinline__ void step3_spa_block(const ProdView &P, SpaSmem &S, i
                             P.C_col[cand - 1] - P.C_col[t0] < SPA_WIN;
             const int n = __syncthreads_count(ok);
             const int t1 = t0 + (n > 0 ? n : 1);
-            step3_spa_segment(P, S, t0, t1);
+            step3_spa_segment<FLAT>(P, S, t0, t1);
             t0 = t1;
         }
     });

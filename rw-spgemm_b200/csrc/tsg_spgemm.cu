@@ -180,6 +180,7 @@ __global__ void __launch_bounds__(128) k_step3_rows(ProdView P)
 
 // persistent: CTAs take blocks of C tiles from a device counter; kind (may
 // be null) marks the hypersparse rows (2), each done whole
+template <bool FLAT>
 __global__ void __launch_bounds__(SPA_THREADS, 3) k_step3_spa(ProdView P, const int *__restrict__ kind,
                                                               unsigned *__restrict__ ctr)
 {
@@ -203,7 +204,7 @@ __global__ void __launch_bounds__(SPA_THREADS, 3) k_step3_spa(ProdView P, const 
             break;
         if (threadIdx.x == 0)
             spa_skip_hyper(P, kind, (int)tb, ctr, 0);
-        step3_spa_block(P, S, (int)tb, (int)min((long long)P.numC, tb + SPA_BLK), kind);
+        step3_spa_block<FLAT>(P, S, (int)tb, (int)min((long long)P.numC, tb + SPA_BLK), kind);
     }
 }
 
@@ -256,6 +257,7 @@ static ProdView make_view(const tsg_tiled *A, const tsg_tiled *B, tsg_tiled *C)
     P.B_rptr = B->row_ptr;
     P.B_rcol = B->row_col;
     P.B_rval = B->row_val;
+    P.browB = B->m > 0 ? (int)(B->nnz / B->m) : 0;
     P.tilenB = B->tilen;
     P.C_ptr = C->tile_ptr;
     P.C_col = C->tile_columnidx;
@@ -329,14 +331,15 @@ static int launch_step2_spa(tsg_context *ctx, const ProdView &P, const int *d_wi
     return TSG_OK;
 }
 
+template <bool FLAT>
 static int launch_step3_spa(tsg_context *ctx, const ProdView &P, const int *d_kind)
 {
     unsigned *ctr = nullptr, grid = 0;
     const int smem = (int)sizeof(SpaSmem);
-    TSG_TRY(spa_grid(ctx, k_step3_spa, smem, &grid));
+    TSG_TRY(spa_grid(ctx, k_step3_spa<FLAT>, smem, &grid));
     TSG_TRY(tsg_alloc(ctx, &ctr, 1));
     TSG_CUDA(cudaMemsetAsync(ctr, 0, sizeof(unsigned), ctx->stream));
-    k_step3_spa<<<grid, SPA_THREADS, smem, ctx->stream>>>(P, d_kind, ctr);
+    k_step3_spa<FLAT><<<grid, SPA_THREADS, smem, ctx->stream>>>(P, d_kind, ctr);
     TSG_LAUNCH_CHECK();
     tsg_release(ctx, ctr);
     return TSG_OK;
@@ -349,7 +352,8 @@ static int launch_step3(tsg_context *ctx, const ProdView &P, long long nnzC, con
     // SPA: products whose C tiles are dense on average (>= SPA_DENSE values)
     // and B without a row view (borrowed foreign buffers) take the tile kernel
     if (ctx->sched == TSG_SCHED_SPA && P.B_rptr && nnzC < (long long)SPA_DENSE * P.numC)
-        return launch_step3_spa(ctx, P, d_kind);
+        return spa_wants_flat(P.browB, P.numC, nnzC, P.tilemA) ? launch_step3_spa<true>(ctx, P, d_kind)
+                                                               : launch_step3_spa<false>(ctx, P, d_kind);
     if (ctx->sched == TSG_SCHED_ROWS)
     {
         const int W = ctx->seg_tiles, cap = ctx->acc_cap;
