@@ -480,6 +480,33 @@ def run_orderings(args, tsg, gen, ctx, reps=3):
     return out
 
 
+def run_hyper(args, tsg, gen, ctx, reps=3):
+    """The largest random product of the batched configuration: A and B
+    65,536 x 65,536 with Poisson(8) nonzeros per row, C = A*B.  Step 1 lists
+    nearly every tile column of each C tile row (16.4 M C tiles for 4.2 M
+    values), so steps 2 and 3 run the hypersparse whole-row path.  Steps 1-3
+    (min of reps, CUDA events)."""
+    A = gen.random_poisson(65536, None, 8.0, seed=7)
+    B = gen.random_poisson(65536, None, 8.0, seed=8)
+    TA = tsg.csr_host_to_tiled(ctx, A, tsg.TSG_TILED_PACKED_COL)
+    TB = tsg.csr_host_to_tiled(ctx, B, tsg.TSG_TILED_CSC_VIEW)
+    prods = tsg.product_bounds(ctx, TA, TB)[0]
+    ctx.set_timing(True)
+    best, info = float("inf"), None
+    for _ in range(reps):
+        C, inf = tsg.spgemm(ctx, TA, TB)
+        if inf["ms_total"] < best:
+            best, info = inf["ms_total"], inf
+        C.free()
+    ctx.set_timing(False)
+    TA.free()
+    TB.free()
+    return {"workload": "C = A*B, A and B 65,536 x 65,536 random with Poisson(8) nonzeros per row, FP64 U(-1,1)",
+            "products": int(prods), "tiles_C": int(info["numtile_C"]), "nnz_C": int(info["nnz_C"]),
+            "step_ms": {k: round(info[k], 4) for k in ("ms_step1", "ms_step2", "ms_step3")},
+            "ms_steps_1_3": round(best, 4), "gflops": round(2.0 * prods / (best * 1e-3) / 1e9, 2)}
+
+
 def run_rmat20(args, tsg, gen, ctx, budget=1.5e9):
     """R-MAT scale 20 (edge factor 16, a,b,c,d = .57,.19,.19,.05, duplicates
     merged, values U(-1,1)): C = A*A and C = A*A^T.  C (~9.5e9 nonzeros) does
@@ -673,6 +700,7 @@ def run_ours(args, tsg, gen, world, rank, local):
                                  half_capacity=False)
     selector = run_selector(args, tsg, gen, ctx) if "selector" in args.sections else None
     orderings = run_orderings(args, tsg, gen, ctx) if "orderings" in args.sections else None
+    hyper = run_hyper(args, tsg, gen, ctx) if "hyper" in args.sections else None
     rmat20 = run_rmat20(args, tsg, gen, ctx) if "rmat20" in args.sections else None
     out = {
         "metric": METRIC, "value": round(value, 3), "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
@@ -710,6 +738,8 @@ def run_ours(args, tsg, gen, world, rank, local):
         out["selector"] = selector
     if orderings:
         out["orderings"] = orderings
+    if hyper:
+        out["hypersparse"] = hyper
     if rmat20:
         out["rmat20"] = rmat20
     if cusparse:
@@ -731,8 +761,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--sched", default="spa", choices=["rows", "tiles", "elems", "spa"])
-    ap.add_argument("--sections", default="plain,cusparse,batched,served,orderings,rmat20",
-                    help="comma list: plain (always), batched, served, selector")
+    ap.add_argument("--sections", default="plain,cusparse,batched,served,orderings,hyper,rmat20",
+                    help="comma list: plain (always), cusparse, batched, served, orderings, hyper, rmat20, selector")
     ap.add_argument("--batch-count", type=int, default=512)
     ap.add_argument("--selector-samples", type=int, default=5000)
     ap.add_argument("--served-jobs", type=int, default=2000)
