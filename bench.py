@@ -665,19 +665,20 @@ def run_ours(args, tsg, gen, world, rank, local):
     comp = compulsory_bytes(A, A, numC, nnzC)
 
     # end to end through the C ABI with host buffers: pinned inputs, results
-    # copied into reused pinned output buffers (two-phase call)
+    # written into reused pinned output buffers by one call whose copy of C
+    # overlaps the numeric step (tsg_spgemm_csr_host_into)
     e2e_t, h2d, d2h = float("nan"), 0, 0
     if not args.no_e2e:
         pin = lambda x: torch.from_numpy(x).pin_memory().numpy()  # noqa: E731
         hmat = (m, n, pin(rp), pin(ci), pin(v))
         outbuf = tsg.HostResultBuffers(m, nnzC)
-        tsg.spgemm_csr_host_into(ctx, hmat, None, outbuf)
+        tsg.spgemm_csr_host_overlap(ctx, hmat, None, outbuf)
         e2e_ms = []
         for _ in range(max(2, min(args.steps, 5))):
             flush.zero_()
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            Cc, _ = tsg.spgemm_csr_host_into(ctx, hmat, None, outbuf)
+            Cc, _ = tsg.spgemm_csr_host_overlap(ctx, hmat, None, outbuf)
             torch.cuda.synchronize()
             e2e_ms.append((time.perf_counter() - t0) * 1e3)
         e2e_t = float(np.mean(e2e_ms))
@@ -722,7 +723,8 @@ def run_ours(args, tsg, gen, world, rank, local):
                      "algorithmic_bytes": alg3, "traffic": profiled_traffic("stencil27_64", args.sched)},
         "e2e": {"value": round(2.0 * prods / (e2e_t * 1e-3) / 1e9, 3), "unit": "GFLOP/s", "ms": round(e2e_t, 3),
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-                "path": "tsg_spgemm_csr_host_start + tsg_result_copy (host CSR in -> host CSR out, pinned buffers)"},
+                "path": "tsg_spgemm_csr_host_into (host CSR in -> host CSR out into the caller's pinned buffers; "
+                        "the copy of C overlaps the numeric step)"},
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
     }

@@ -430,6 +430,25 @@ int tsg_spgemm_csr_host_start(tsg_context *ctx,
 int tsg_result_copy(tsg_result *res, int *rowptr, int *colidx, double *val);
 int tsg_result_free(tsg_result *res);
 
+/* One end-to-end call into caller-owned host buffers: C = A*B (B may alias
+ * A's arrays) lands in c_rowptr[m+1], c_colidx[nnz_cap], c_val[nnz_cap],
+ * with the device-to-host copy overlapping the numeric step -- C's row
+ * pointer is final after the symbolic steps and goes out first; then the
+ * tile rows of C are computed and converted in chunks on the context's
+ * stream while earlier chunks are copied out on a second stream.  The
+ * buffers should be page-locked (pageable memory is correct but the copies
+ * then serialise).  When nnz(C) > nnz_cap nothing but *nnzC is written and
+ * TSG_ERR_OVERFLOW is returned: grow the buffers (tsg_product_bounds gives
+ * an upper bound) and call again.  Synchronous.  No reference counterpart:
+ * the reference returns C through tilespgemm (src/tilespgemm-cuda.h:2610)
+ * and tile2csr (src/tile2csr.h:71), in sequence. */
+int tsg_spgemm_csr_host_into(tsg_context *ctx,
+                             int m, int k, int n,
+                             int nnzA, const int *a_rowptr, const int *a_colidx, const double *a_val,
+                             int nnzB, const int *b_rowptr, const int *b_colidx, const double *b_val,
+                             int *c_rowptr, int *c_colidx, double *c_val, long long nnz_cap,
+                             int *nnzC, tsg_spgemm_info *info);
+
 /* Host CSR -> device tiles in one call (copies through pooled device memory;
  * the host arrays may be pageable or pinned). */
 int tsg_csr_host_to_tiled(tsg_context *ctx, int m, int n, int nnz,

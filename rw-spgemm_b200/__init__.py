@@ -756,6 +756,8 @@ def _declare_result(L):
                                             ctypes.POINTER(ip), ctypes.POINTER(TsgInfo)]
     L.tsg_result_copy.argtypes = [vp, vp, vp, vp]
     L.tsg_result_free.argtypes = [vp]
+    L.tsg_spgemm_csr_host_into.argtypes = [vp, ip, ip, ip, ip, vp, vp, vp, ip, vp, vp, vp, vp, vp, vp,
+                                           ctypes.c_longlong, ctypes.POINTER(ip), ctypes.POINTER(TsgInfo)]
 
 
 _declare_prev3 = _declare
@@ -785,6 +787,37 @@ class HostResultBuffers:
             self.rp = np.empty(m + 1, np.int32)
             self.ci = np.empty(max(nnz_cap, 1), np.int32)
             self.v = np.empty(max(nnz_cap, 1), np.float64)
+
+
+TSG_ERR_OVERFLOW = -5
+
+
+def spgemm_csr_host_overlap(ctx: Context, matA, matB, out: HostResultBuffers):
+    """End to end in one C call (tsg_spgemm_csr_host_into): the result is
+    written into out while it is computed, C's CSR copied to the host chunk
+    by chunk during the numeric step.  out is grown (and the product run
+    again) when C has more nonzeros than it holds.  Returns (m, n, rowptr,
+    colidx, val) views into out, and the info dict."""
+    hA = HostCSR(matA)
+    hB = hA if matB is None else HostCSR(matB)
+    m, k, n = hA.sm.m, hA.sm.n, hB.sm.n
+    for _ in range(2):
+        if out.m != m:
+            out.resize(m, out.cap)
+        nnzC = ctypes.c_int(0)
+        info = TsgInfo()
+        st = lib().tsg_spgemm_csr_host_into(
+            ctx.handle, m, k, n, hA.sm.nnz, hA.rp.ctypes.data, hA.ci.ctypes.data, hA.v.ctypes.data,
+            hB.sm.nnz, hB.rp.ctypes.data, hB.ci.ctypes.data, hB.v.ctypes.data,
+            out.rp.ctypes.data, out.ci.ctypes.data, out.v.ctypes.data, out.cap, ctypes.byref(nnzC),
+            ctypes.byref(info))
+        if st == TSG_ERR_OVERFLOW and nnzC.value > out.cap:
+            out.resize(m, nnzC.value)
+            continue
+        check(st)
+        nz = nnzC.value
+        return (m, n, out.rp, out.ci[:nz], out.v[:nz]), info.as_dict()
+    raise TsgError(TSG_ERR_OVERFLOW, "result buffers could not be sized")
 
 
 def spgemm_csr_host_into(ctx: Context, matA, matB, out: HostResultBuffers):

@@ -83,6 +83,12 @@ extern "C" int tsg_context_destroy(tsg_context *ctx)
     cudaStreamSynchronize(ctx->stream);
     for (int i = 0; i < 8; i++)
         cudaEventDestroy(ctx->ev[i]);
+    if (ctx->copy_stream)
+    {
+        cudaStreamSynchronize(ctx->copy_stream);
+        cudaStreamDestroy(ctx->copy_stream);
+        cudaEventDestroy(ctx->copy_ev);
+    }
     if (ctx->own_stream)
         cudaStreamDestroy(ctx->stream);
     cudaFreeHost(ctx->h_pinned);
@@ -763,6 +769,45 @@ extern "C" int tsg_spgemm_csr_host_start(tsg_context *ctx, int m, int k, int n, 
     *nnzC = r->nnz;
     *res = r;
     return TSG_OK;
+}
+
+int tsg_copy_stream(tsg_context *ctx)
+{
+    if (ctx->copy_stream)
+        return TSG_OK;
+    TSG_CUDA(cudaEventCreateWithFlags(&ctx->copy_ev, cudaEventDisableTiming));
+    cudaError_t e = cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess)
+    {
+        cudaEventDestroy(ctx->copy_ev);
+        ctx->copy_stream = nullptr;
+        return tsg_set_error(TSG_ERR_CUDA, "copy stream creation failed: %s", cudaGetErrorString(e));
+    }
+    return TSG_OK;
+}
+
+extern "C" int tsg_spgemm_csr_host_into(tsg_context *ctx, int m, int k, int n, int nnzA, const int *a_rowptr,
+                                        const int *a_colidx, const double *a_val, int nnzB, const int *b_rowptr,
+                                        const int *b_colidx, const double *b_val, int *c_rowptr, int *c_colidx,
+                                        double *c_val, long long nnz_cap, int *nnzC, tsg_spgemm_info *info)
+{
+    if (!ctx || !nnzC || !a_rowptr || !b_rowptr || !c_rowptr || (nnz_cap > 0 && (!c_colidx || !c_val)) ||
+        nnz_cap < 0)
+        return tsg_set_error(TSG_ERR_INVALID, "null argument");
+    *nnzC = 0;
+    const bool alias = (a_rowptr == b_rowptr && a_colidx == b_colidx && a_val == b_val && m == k && k == n);
+    tsg_tiled A, B;
+    memset(&A, 0, sizeof(A));
+    memset(&B, 0, sizeof(B));
+    int st = alias ? tsg_csr_host_to_tiled(ctx, m, k, nnzA, a_rowptr, a_colidx, a_val, TSG_TILED_CSC_VIEW, &A)
+                   : tsg_csr_host_to_tiled(ctx, m, k, nnzA, a_rowptr, a_colidx, a_val, TSG_TILED_PACKED_COL, &A);
+    if (st == TSG_OK && !alias)
+        st = tsg_csr_host_to_tiled(ctx, k, n, nnzB, b_rowptr, b_colidx, b_val, TSG_TILED_CSC_VIEW, &B);
+    if (st == TSG_OK)
+        st = tsg_spgemm_to_host(ctx, &A, alias ? &A : &B, c_rowptr, c_colidx, c_val, nnz_cap, nnzC, info);
+    tsg_tiled_free(ctx, &A);
+    tsg_tiled_free(ctx, &B);
+    return st;
 }
 
 extern "C" int tsg_result_copy(tsg_result *r, int *rowptr, int *colidx, double *val)

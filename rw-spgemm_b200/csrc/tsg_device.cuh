@@ -1573,7 +1573,9 @@ __device__ __forceinline__ void step3_hyper_row(const ProdView &P, HypSmem &S, i
 #define SPA_BLK 256
 
 // calls piece(I, t0, t1) for the pieces [t0, t1) owned by block [tb, te),
-// rows longer than CH tiles being cut into CH-tile chunks
+// rows longer than CH tiles being cut into CH-tile chunks.  [tb, te) may be a
+// block clamped to a range of whole tile rows: it then yields the block's
+// pieces of those rows only.
 template <int CH, typename F>
 __device__ __forceinline__ void spa_block_pieces(const ProdView &P, int tb, int te, F piece)
 {

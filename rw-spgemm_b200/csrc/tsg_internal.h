@@ -24,7 +24,23 @@ struct tsg_context
     int seg_tiles;       // row schedule: C tiles per work item (8 or 16)
     int acc_cap;         // row schedule: FP64 accumulator slots per half-warp
     int fuse12;          // step-1 emit fused with step 2 for narrow tile rows
+    cudaStream_t copy_stream; // device-to-host copies overlapping compute (created on first use)
+    cudaEvent_t copy_ev;      // orders a chunk's copy after its fill
 };
+
+// C tile rows are copied to the host in at most TSG_MAX_CHUNKS chunks of at
+// least TSG_CHUNK_NNZ nonzeros (tsg_spgemm_to_host).
+#define TSG_MAX_CHUNKS 8
+#define TSG_CHUNK_NNZ (1LL << 20)
+
+// Creates the context's copy stream and event if needed.
+int tsg_copy_stream(tsg_context *ctx);
+
+// C = A*B (device operands) into host CSR buffers of nnz_cap entries, the
+// copy overlapping the numeric step; TSG_ERR_OVERFLOW (with *nnzC set) when
+// nnz(C) > nnz_cap.  Synchronous.
+int tsg_spgemm_to_host(tsg_context *ctx, const tsg_tiled *A, const tsg_tiled *B, int *h_rowptr, int *h_colidx,
+                       double *h_val, long long nnz_cap, int *nnzC, tsg_spgemm_info *info);
 
 // Records a formatted message as the thread's last error and returns code.
 int tsg_set_error(int code, const char *fmt, ...);

@@ -10,6 +10,8 @@
 // the tile schedule (half-warp per C tile, A-row x B-column intersection, as
 // the reference decomposes the work) or the row-segment schedule (half-warp
 // per run of C tiles in one tile row, tile-level Gustavson, no intersection).
+#include <algorithm>
+
 #include "tsg_device.cuh"
 
 #define S1_WARPS 8
@@ -179,10 +181,13 @@ __global__ void __launch_bounds__(128) k_step3_rows(ProdView P)
 }
 
 // persistent: CTAs take blocks of C tiles from a device counter; kind (may
-// be null) marks the hypersparse rows (2), each done whole
-template <bool FLAT>
-__global__ void __launch_bounds__(SPA_THREADS, 3) k_step3_spa(ProdView P, const int *__restrict__ kind,
-                                                              unsigned *__restrict__ ctr)
+// be null) marks the hypersparse rows (2), each done whole.  RANGED: only
+// the tile rows [row0, row1) are done -- the blocks holding their tiles, each
+// clamped to those tiles (a separate instantiation keeps the whole-product
+// form's registers).
+template <bool FLAT, bool RANGED>
+__global__ void __launch_bounds__(SPA_THREADS, 3) k_step3_spa(ProdView P, const int *__restrict__ kind, int row0,
+                                                              int row1, unsigned *__restrict__ ctr)
 {
     extern __shared__ __align__(16) unsigned char s_raw[];
     SpaSmem &S = *reinterpret_cast<SpaSmem *>(s_raw);
@@ -190,6 +195,8 @@ __global__ void __launch_bounds__(SPA_THREADS, 3) k_step3_spa(ProdView P, const 
     unsigned nxt = 0; // thread 0: the next block, claimed one block ahead
     if (threadIdx.x == 0)
         nxt = atomicAdd(ctr, 1u);
+    const int t_beg = RANGED ? P.C_ptr[row0] : 0, t_end = RANGED ? P.C_ptr[row1] : P.numC;
+    const long long blk0 = t_beg / SPA_BLK;
     for (;;)
     {
         __syncthreads();
@@ -199,12 +206,13 @@ __global__ void __launch_bounds__(SPA_THREADS, 3) k_step3_spa(ProdView P, const 
             nxt = atomicAdd(ctr, 1u);
         }
         __syncthreads();
-        const long long tb = (long long)s_blk * SPA_BLK;
-        if (tb >= P.numC)
+        const long long tb = (blk0 + s_blk) * SPA_BLK;
+        if (tb >= t_end)
             break;
         if (threadIdx.x == 0)
-            spa_skip_hyper(P, kind, (int)tb, ctr, 0);
-        step3_spa_block<FLAT>(P, S, (int)tb, (int)min((long long)P.numC, tb + SPA_BLK), kind);
+            spa_skip_hyper(P, kind, (int)tb, ctr, -blk0);
+        // the block, clamped to the tiles of rows [row0, row1)
+        step3_spa_block<FLAT>(P, S, max((int)tb, t_beg), (int)min((long long)t_end, tb + SPA_BLK), kind);
     }
 }
 
@@ -331,29 +339,46 @@ static int launch_step2_spa(tsg_context *ctx, const ProdView &P, const int *d_wi
     return TSG_OK;
 }
 
-template <bool FLAT>
-static int launch_step3_spa(tsg_context *ctx, const ProdView &P, const int *d_kind)
+template <bool FLAT, bool RANGED>
+static int launch_step3_spa(tsg_context *ctx, const ProdView &P, const int *d_kind, int row0, int row1)
 {
     unsigned *ctr = nullptr, grid = 0;
     const int smem = (int)sizeof(SpaSmem);
-    TSG_TRY(spa_grid(ctx, k_step3_spa<FLAT>, smem, &grid));
+    TSG_TRY(spa_grid(ctx, k_step3_spa<FLAT, RANGED>, smem, &grid));
     TSG_TRY(tsg_alloc(ctx, &ctr, 1));
     TSG_CUDA(cudaMemsetAsync(ctr, 0, sizeof(unsigned), ctx->stream));
-    k_step3_spa<FLAT><<<grid, SPA_THREADS, smem, ctx->stream>>>(P, d_kind, ctr);
+    k_step3_spa<FLAT, RANGED><<<grid, SPA_THREADS, smem, ctx->stream>>>(P, d_kind, row0, row1, ctr);
     TSG_LAUNCH_CHECK();
     tsg_release(ctx, ctr);
     return TSG_OK;
+}
+
+// step 3 by the SPA kernel: the default schedule, except for products whose
+// C tiles are dense on average (>= SPA_DENSE values) and B without a row view
+// (borrowed foreign buffers), which take the tile kernel
+static bool step3_by_spa(const tsg_context *ctx, const ProdView &P, long long nnzC)
+{
+    return ctx->sched == TSG_SCHED_SPA && P.B_rptr && nnzC < (long long)SPA_DENSE * P.numC;
+}
+
+// the SPA numeric step for tile rows [row0, row1)
+static int launch_step3_spa_rows(tsg_context *ctx, const ProdView &P, long long nnzC, const int *d_kind, int row0,
+                                 int row1)
+{
+    const bool flat = spa_wants_flat(P.browB, P.numC, nnzC, P.tilemA);
+    if (row0 == 0 && row1 == P.tilemA)
+        return flat ? launch_step3_spa<true, false>(ctx, P, d_kind, 0, 0)
+                    : launch_step3_spa<false, false>(ctx, P, d_kind, 0, 0);
+    return flat ? launch_step3_spa<true, true>(ctx, P, d_kind, row0, row1)
+                : launch_step3_spa<false, true>(ctx, P, d_kind, row0, row1);
 }
 
 // d_kind: the row kinds of the fused step 1/2 pass (0 narrow, 1 wide,
 // 2 hypersparse), or null
 static int launch_step3(tsg_context *ctx, const ProdView &P, long long nnzC, const int *d_kind)
 {
-    // SPA: products whose C tiles are dense on average (>= SPA_DENSE values)
-    // and B without a row view (borrowed foreign buffers) take the tile kernel
-    if (ctx->sched == TSG_SCHED_SPA && P.B_rptr && nnzC < (long long)SPA_DENSE * P.numC)
-        return spa_wants_flat(P.browB, P.numC, nnzC, P.tilemA) ? launch_step3_spa<true>(ctx, P, d_kind)
-                                                               : launch_step3_spa<false>(ctx, P, d_kind);
+    if (step3_by_spa(ctx, P, nnzC))
+        return launch_step3_spa_rows(ctx, P, nnzC, d_kind, 0, P.tilemA);
     if (ctx->sched == TSG_SCHED_ROWS)
     {
         const int W = ctx->seg_tiles, cap = ctx->acc_cap;
@@ -377,12 +402,21 @@ static int launch_step3(tsg_context *ctx, const ProdView &P, long long nnzC, con
     return TSG_OK;
 }
 
-extern "C" int tsg_spgemm(tsg_context *ctx, const tsg_tiled *A, const tsg_tiled *B, tsg_tiled *C,
-                          tsg_spgemm_info *info)
+// What steps 1-2 leave for step 3 and the statistics.
+struct SpgemmRun
 {
-    if (!ctx || !C)
-        return tsg_set_error(TSG_ERR_INVALID, "null argument");
-    TSG_TRY(validate_operands(A, B));
+    unsigned long long *d_pairs;
+    int *d_bins;
+    int *d_wide; // row kinds of the fused pass, or null
+    long long numC, nnzC;
+};
+
+// Steps 1 and 2 of C = A*B: on return C's tile structure, masks, row offsets
+// and tile value offsets are final, nnz(C) is known on the host and C's value
+// arrays are allocated.  Records ev[0..2] when timing.
+static int spgemm_structure(tsg_context *ctx, const tsg_tiled *A, const tsg_tiled *B, tsg_tiled *C, SpgemmRun &R)
+{
+    memset(&R, 0, sizeof(R));
     memset(C, 0, sizeof(*C));
     C->m = A->m;
     C->n = B->n;
@@ -396,24 +430,23 @@ extern "C" int tsg_spgemm(tsg_context *ctx, const tsg_tiled *A, const tsg_tiled 
         TSG_CUDA(cudaEventRecord(ctx->ev[0], st));
 
     // step 1: structure
-    unsigned long long *d_pairs;
-    int *d_bins;
-    TSG_TRY(tsg_alloc(ctx, &d_pairs, 1));
-    TSG_TRY(tsg_alloc(ctx, &d_bins, 4));
-    TSG_CUDA(cudaMemsetAsync(d_pairs, 0, sizeof(unsigned long long), st));
-    TSG_CUDA(cudaMemsetAsync(d_bins, 0, 4 * sizeof(int), st));
+    TSG_TRY(tsg_alloc(ctx, &R.d_pairs, 1));
+    TSG_TRY(tsg_alloc(ctx, &R.d_bins, 4));
+    TSG_CUDA(cudaMemsetAsync(R.d_pairs, 0, sizeof(unsigned long long), st));
+    TSG_CUDA(cudaMemsetAsync(R.d_bins, 0, 4 * sizeof(int), st));
     TSG_TRY(tsg_alloc(ctx, &C->tile_ptr, (size_t)tilem + 1));
     long long numC = 0;
     if (tilem > 0)
     {
         ProdView P = make_view(A, B, C);
-        k_step1<false><<<tsg_blocks(tilem, S1_WARPS), S1_WARPS * 32, 0, st>>>(P, C->tile_ptr, d_pairs);
+        k_step1<false><<<tsg_blocks(tilem, S1_WARPS), S1_WARPS * 32, 0, st>>>(P, C->tile_ptr, R.d_pairs);
         TSG_LAUNCH_CHECK();
         TSG_TRY(tsg_scan_counts(ctx, C->tile_ptr, C->tile_ptr, tilem, &numC));
     }
     else
         TSG_CUDA(cudaMemsetAsync(C->tile_ptr, 0, sizeof(int), st));
     C->numtile = (int)numC;
+    R.numC = numC;
     TSG_TRY(tsg_alloc(ctx, &C->tile_columnidx, (size_t)numC));
     TSG_TRY(tsg_alloc(ctx, &C->tile_rowidx, (size_t)numC));
     TSG_TRY(tsg_alloc(ctx, &C->mask, (size_t)numC * TSG_BS));
@@ -421,15 +454,14 @@ extern "C" int tsg_spgemm(tsg_context *ctx, const tsg_tiled *A, const tsg_tiled 
     TSG_TRY(tsg_alloc(ctx, &C->tile_nnz, (size_t)numC + 1));
     long long nnzC = 0;
     const bool fused = ctx->fuse12 && ctx->sched != TSG_SCHED_ROWS;
-    int *d_wide = nullptr;
     if (numC > 0)
     {
         ProdView P = make_view(A, B, C);
         if (fused)
         {
-            TSG_TRY(tsg_alloc(ctx, &d_wide, (size_t)tilem + 1));
-            TSG_CUDA(cudaMemsetAsync(d_wide + tilem, 0, sizeof(int), st));
-            k_step12<<<tsg_blocks(tilem, 8), 256, 0, st>>>(P, d_wide, d_bins);
+            TSG_TRY(tsg_alloc(ctx, &R.d_wide, (size_t)tilem + 1));
+            TSG_CUDA(cudaMemsetAsync(R.d_wide + tilem, 0, sizeof(int), st));
+            k_step12<<<tsg_blocks(tilem, 8), 256, 0, st>>>(P, R.d_wide, R.d_bins);
             TSG_LAUNCH_CHECK();
         }
         else
@@ -446,14 +478,14 @@ extern "C" int tsg_spgemm(tsg_context *ctx, const tsg_tiled *A, const tsg_tiled 
     {
         ProdView P = make_view(A, B, C);
         if (fused && P.B_rptr)
-            TSG_TRY(launch_step2_spa(ctx, P, d_wide, d_bins));
+            TSG_TRY(launch_step2_spa(ctx, P, R.d_wide, R.d_bins));
         else if (fused)
         {
-            k_step2_wide<<<tsg_blocks(numC * 16, 256), 256, 0, st>>>(P, d_wide, d_bins);
+            k_step2_wide<<<tsg_blocks(numC * 16, 256), 256, 0, st>>>(P, R.d_wide, R.d_bins);
             TSG_LAUNCH_CHECK();
         }
         else
-            TSG_TRY(launch_step2(ctx, P, d_bins));
+            TSG_TRY(launch_step2(ctx, P, R.d_bins));
         TSG_TRY(tsg_scan_counts(ctx, C->tile_nnz, C->tile_nnz, numC, &nnzC));
     }
     else
@@ -462,27 +494,32 @@ extern "C" int tsg_spgemm(tsg_context *ctx, const tsg_tiled *A, const tsg_tiled 
     if (timing)
         TSG_CUDA(cudaEventRecord(ctx->ev[2], st));
 
-    // step 3: numeric
+    R.nnzC = nnzC;
+    // C's value arrays
     TSG_TRY(tsg_alloc(ctx, &C->tile_csr_Col, (size_t)nnzC));
     TSG_TRY(tsg_alloc(ctx, &C->tile_csr_Value, (size_t)nnzC));
-    if (nnzC > 0)
-        TSG_TRY(launch_step3(ctx, make_view(A, B, C), nnzC, d_wide));
-    tsg_release(ctx, d_wide);
-    if (timing)
-        TSG_CUDA(cudaEventRecord(ctx->ev[3], st));
+    return TSG_OK;
+}
 
+// Statistics of a product (tile pairs, bins, step times from ev[0..3]) and
+// the release of the steps' scratch.
+static int spgemm_finish(tsg_context *ctx, SpgemmRun &R, tsg_spgemm_info *info)
+{
+    cudaStream_t st = ctx->stream;
+    tsg_release(ctx, R.d_wide);
+    R.d_wide = nullptr;
     if (info)
     {
         memset(info, 0, sizeof(*info));
-        info->numtile_C = numC;
-        info->nnz_C = nnzC;
+        info->numtile_C = R.numC;
+        info->nnz_C = R.nnzC;
         long long *h = ctx->h_pinned;
-        TSG_CUDA(cudaMemcpyAsync(h, d_pairs, sizeof(long long), cudaMemcpyDeviceToHost, st));
-        TSG_CUDA(cudaMemcpyAsync(h + 1, d_bins, 4 * sizeof(int), cudaMemcpyDeviceToHost, st));
+        TSG_CUDA(cudaMemcpyAsync(h, R.d_pairs, sizeof(long long), cudaMemcpyDeviceToHost, st));
+        TSG_CUDA(cudaMemcpyAsync(h + 1, R.d_bins, 4 * sizeof(int), cudaMemcpyDeviceToHost, st));
         TSG_CUDA(cudaStreamSynchronize(st));
         info->tile_pairs = h[0];
         memcpy(info->bins, h + 1, 4 * sizeof(int));
-        if (timing)
+        if (ctx->timing)
         {
             info->ms_step1 = ev_ms(ctx->ev[0], ctx->ev[1]);
             info->ms_step2 = ev_ms(ctx->ev[1], ctx->ev[2]);
@@ -490,9 +527,152 @@ extern "C" int tsg_spgemm(tsg_context *ctx, const tsg_tiled *A, const tsg_tiled 
             info->ms_total = ev_ms(ctx->ev[0], ctx->ev[3]);
         }
     }
-    tsg_release(ctx, d_pairs);
-    tsg_release(ctx, d_bins);
+    tsg_release(ctx, R.d_pairs);
+    tsg_release(ctx, R.d_bins);
     return TSG_OK;
+}
+
+extern "C" int tsg_spgemm(tsg_context *ctx, const tsg_tiled *A, const tsg_tiled *B, tsg_tiled *C,
+                          tsg_spgemm_info *info)
+{
+    if (!ctx || !C)
+        return tsg_set_error(TSG_ERR_INVALID, "null argument");
+    TSG_TRY(validate_operands(A, B));
+    SpgemmRun R;
+    TSG_TRY(spgemm_structure(ctx, A, B, C, R));
+    // step 3: numeric
+    if (R.nnzC > 0)
+        TSG_TRY(launch_step3(ctx, make_view(A, B, C), R.nnzC, R.d_wide));
+    if (ctx->timing)
+        TSG_CUDA(cudaEventRecord(ctx->ev[3], ctx->stream));
+    return spgemm_finish(ctx, R, info);
+}
+
+__global__ void k_t2c_rowlen(int m, int tilem, const int *__restrict__ tile_ptr, const int *__restrict__ tnnz,
+                             const unsigned char *__restrict__ Ptr, int *__restrict__ rowlen);
+__global__ void k_t2c_fill(int m, int tilem, const int *__restrict__ tile_ptr, const int *__restrict__ tile_col,
+                           const int *__restrict__ tnnz, const unsigned char *__restrict__ Ptr,
+                           const unsigned char *__restrict__ Col, const double *__restrict__ Val,
+                           const int *__restrict__ rowptr, int *__restrict__ ccol, double *__restrict__ cval);
+
+// C = A*B straight into host CSR buffers, the copy overlapping the numeric
+// step.  After step 2 the row pointer of C is final: it is computed and
+// copied first, so the host knows where every tile row's entries go.  Then
+// the tile rows of C are taken in chunks of about equal nonzeros: a chunk's
+// numeric step (the SPA kernel over its rows) and its CSR fill run on the
+// context's stream while the previous chunks' column indices and values are
+// copied out on the copy stream.  Products whose step 3 is not the SPA
+// kernel run it whole first; their fill and copy are still chunked.
+int tsg_spgemm_to_host(tsg_context *ctx, const tsg_tiled *A, const tsg_tiled *B, int *h_rowptr, int *h_colidx,
+                       double *h_val, long long nnz_cap, int *nnzC_out, tsg_spgemm_info *info)
+{
+    TSG_TRY(validate_operands(A, B));
+    tsg_tiled C;
+    SpgemmRun R;
+    int status = spgemm_structure(ctx, A, B, &C, R);
+    int *d_rp = nullptr, *d_ci = nullptr;
+    double *d_v = nullptr;
+    cudaStream_t st = ctx->stream;
+    const int m = C.m, tilem = C.tilem;
+    if (status == TSG_OK)
+    {
+        *nnzC_out = (int)R.nnzC;
+        if (R.nnzC > nnz_cap)
+            status = tsg_set_error(TSG_ERR_OVERFLOW, "C has %lld nonzeros; the output buffers hold %lld", R.nnzC,
+                                   nnz_cap);
+    }
+    if (status == TSG_OK)
+        status = tsg_alloc(ctx, &d_rp, (size_t)m + 1);
+    if (status == TSG_OK)
+        status = tsg_alloc(ctx, &d_ci, (size_t)R.nnzC);
+    if (status == TSG_OK)
+        status = tsg_alloc(ctx, &d_v, (size_t)R.nnzC);
+    if (status == TSG_OK)
+        status = ([&]() -> int {
+            // row pointer, to the host first
+            if (m > 0)
+            {
+                k_t2c_rowlen<<<tsg_blocks((long long)tilem * 16, 256), 256, 0, st>>>(m, tilem, C.tile_ptr, C.tile_nnz,
+                                                                                   C.tile_csr_Ptr, d_rp);
+                TSG_LAUNCH_CHECK();
+                TSG_TRY(tsg_scan_counts(ctx, d_rp, d_rp, m, nullptr));
+            }
+            else
+                TSG_CUDA(cudaMemsetAsync(d_rp, 0, sizeof(int), st));
+            TSG_CUDA(cudaMemcpyAsync(h_rowptr, d_rp, ((size_t)m + 1) * sizeof(int), cudaMemcpyDeviceToHost, st));
+            TSG_CUDA(cudaStreamSynchronize(st));
+            if (R.nnzC == 0 || tilem == 0)
+                return TSG_OK;
+            TSG_TRY(tsg_copy_stream(ctx));
+            const ProdView P = make_view(A, B, &C);
+            const bool spa = step3_by_spa(ctx, P, R.nnzC);
+            if (!spa)
+                TSG_TRY(launch_step3(ctx, P, R.nnzC, R.d_wide));
+            // chunks of about equal nonzeros (>= TSG_CHUNK_NNZ each, at most TSG_MAX_CHUNKS)
+            const long long nch = std::max(1LL, std::min((long long)TSG_MAX_CHUNKS, R.nnzC / TSG_CHUNK_NNZ));
+            int r0 = 0;
+            for (long long c = 1; c <= nch; c++)
+            {
+                int r1 = tilem;
+                if (c < nch)
+                {
+                    // first tile row whose entries start at or after c / nch of C's
+                    const long long want = R.nnzC * c / nch;
+                    int lo = r0 + 1, hi = tilem;
+                    while (lo < hi)
+                    {
+                        const int mid = (lo + hi) >> 1;
+                        if ((long long)h_rowptr[(long long)mid * TSG_BS] >= want)
+                            hi = mid;
+                        else
+                            lo = mid + 1;
+                    }
+                    r1 = lo;
+                }
+                if (r1 <= r0)
+                    continue;
+                if (spa)
+                    TSG_TRY(launch_step3_spa_rows(ctx, P, R.nnzC, R.d_wide, r0, r1));
+                const int rows = std::min(m, r1 * TSG_BS) - r0 * TSG_BS;
+                k_t2c_fill<<<tsg_blocks((long long)(r1 - r0) * 16, 256), 256, 0, st>>>(
+                    rows, r1 - r0, C.tile_ptr + r0, C.tile_columnidx, C.tile_nnz, C.tile_csr_Ptr, C.tile_csr_Col,
+                    C.tile_csr_Value, d_rp + (long long)r0 * TSG_BS, d_ci, d_v);
+                TSG_LAUNCH_CHECK();
+                TSG_CUDA(cudaEventRecord(ctx->copy_ev, st));
+                TSG_CUDA(cudaStreamWaitEvent(ctx->copy_stream, ctx->copy_ev, 0));
+                const long long e0 = h_rowptr[(long long)r0 * TSG_BS], e1 = h_rowptr[r1 * TSG_BS < m ? r1 * TSG_BS : m];
+                if (e1 > e0)
+                {
+                    TSG_CUDA(cudaMemcpyAsync(h_colidx + e0, d_ci + e0, (size_t)(e1 - e0) * sizeof(int),
+                                             cudaMemcpyDeviceToHost, ctx->copy_stream));
+                    TSG_CUDA(cudaMemcpyAsync(h_val + e0, d_v + e0, (size_t)(e1 - e0) * sizeof(double),
+                                             cudaMemcpyDeviceToHost, ctx->copy_stream));
+                }
+                r0 = r1;
+            }
+            return TSG_OK;
+        })();
+    // the copies end before the buffers are released on the context's stream
+    if (ctx->copy_stream)
+        cudaStreamSynchronize(ctx->copy_stream);
+    if (status == TSG_OK && ctx->timing)
+        status = cudaEventRecord(ctx->ev[3], st) == cudaSuccess ? TSG_OK
+                                                                 : tsg_set_error(TSG_ERR_CUDA, "cudaEventRecord");
+    tsg_release(ctx, d_rp);
+    tsg_release(ctx, d_ci);
+    tsg_release(ctx, d_v);
+    if (status == TSG_OK)
+        status = spgemm_finish(ctx, R, info);
+    else
+    {
+        tsg_release(ctx, R.d_wide);
+        tsg_release(ctx, R.d_pairs);
+        tsg_release(ctx, R.d_bins);
+    }
+    tsg_tiled_free(ctx, &C);
+    if (status == TSG_OK)
+        TSG_CUDA(cudaStreamSynchronize(st));
+    return status;
 }
 
 // Number of C tiles of A*B (step 1's count pass only); A and B need their
