@@ -756,6 +756,7 @@ struct SpaStage
 {
     int2 bl[SPA_STAGE]; // B row: first entry, length
     double a[SPA_STAGE];
+    int tpre[32];       // FLAT staging: first entry of each lane's A tile
 };
 
 struct SpaSmem
@@ -906,29 +907,72 @@ __device__ __forceinline__ void step3_spa_segment(const ProdView &P, SpaSmem &S,
                 incl += o;
         }
         const int total = __shfl_sync(TSG_FULL_MASK, incl, 31);
+        if (FLAT)
+        {
+            __syncwarp();
+            G.tpre[lane] = incl - cnt;
+        }
         for (int base = 0; base < total; base += SPA_STAGE)
         {
             __syncwarp();
             // stage A(r, k) entries [base, base + SPA_STAGE) of this group in
             // column order: B row bounds and the A value
-            unsigned bits = mr;
-            for (int x = 0; x < cnt; x++)
+            if (FLAT)
             {
-                const int bit = 31 - __clz(bits);
-                bits ^= 1u << bit;
-                const int e = incl - cnt + x - base;
-                if (e >= 0 && e < SPA_STAGE)
+                // a lane per entry (A tiles holding many entries of the row
+                // would otherwise stage them one by one on a few lanes): the
+                // entry's tile is the last lane whose first entry is at or
+                // before it, its column the x-th set column of that tile's row
+                for (int h = 0; h < SPA_STAGE; h += 32)
                 {
-                    const int k = kb + (15 - bit);
-                    int b0 = P.B_rptr[k], b1 = P.B_rptr[k + 1];
-                    if (!full)
+                    const int e = base + h + lane;
+                    int t = 0;
+#pragma unroll
+                    for (int sz = 16; sz > 0; sz >>= 1)
+                        if (t + sz < 32 && G.tpre[t + sz] <= e)
+                            t += sz;
+                    const unsigned tm = __shfl_sync(TSG_FULL_MASK, mr, t);
+                    const int tkb = __shfl_sync(TSG_FULL_MASK, kb, t);
+                    const int tst = __shfl_sync(TSG_FULL_MASK, st, t);
+                    if (e < total)
                     {
-                        // only B's entries inside this segment's columns
-                        b0 += lower_bound_int(P.B_rcol + b0, b1 - b0, J0 * TSG_BS);
-                        b1 = b0 + lower_bound_int(P.B_rcol + b0, b1 - b0, J1 * TSG_BS);
+                        const int x = e - G.tpre[t];
+                        unsigned cols = __brev(tm) >> 16; // bit c: column c of the tile's row
+                        for (int q = 0; q < x; q++)
+                            cols &= cols - 1;
+                        const int k = tkb + __ffs(cols) - 1;
+                        int b0 = P.B_rptr[k], b1 = P.B_rptr[k + 1];
+                        if (!full)
+                        {
+                            b0 += lower_bound_int(P.B_rcol + b0, b1 - b0, J0 * TSG_BS);
+                            b1 = b0 + lower_bound_int(P.B_rcol + b0, b1 - b0, J1 * TSG_BS);
+                        }
+                        G.bl[h + lane] = make_int2(b0, b1 - b0);
+                        G.a[h + lane] = P.A_Val[tst + x];
                     }
-                    G.bl[e] = make_int2(b0, b1 - b0);
-                    G.a[e] = P.A_Val[st + x];
+                }
+            }
+            else
+            {
+                unsigned bits = mr;
+                for (int x = 0; x < cnt; x++)
+                {
+                    const int bit = 31 - __clz(bits);
+                    bits ^= 1u << bit;
+                    const int e = incl - cnt + x - base;
+                    if (e >= 0 && e < SPA_STAGE)
+                    {
+                        const int k = kb + (15 - bit);
+                        int b0 = P.B_rptr[k], b1 = P.B_rptr[k + 1];
+                        if (!full)
+                        {
+                            // only B's entries inside this segment's columns
+                            b0 += lower_bound_int(P.B_rcol + b0, b1 - b0, J0 * TSG_BS);
+                            b1 = b0 + lower_bound_int(P.B_rcol + b0, b1 - b0, J1 * TSG_BS);
+                        }
+                        G.bl[e] = make_int2(b0, b1 - b0);
+                        G.a[e] = P.A_Val[st + x];
+                    }
                 }
             }
             __syncwarp();
