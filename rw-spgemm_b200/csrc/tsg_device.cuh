@@ -1117,6 +1117,7 @@ struct Spa2Stage
 {
     int bs[SPA_STAGE];
     int off[SPA_STAGE + 1];
+    int tpre[32]; // first entry of each lane's A tile
 };
 
 struct Spa2Smem
@@ -1170,26 +1171,39 @@ __device__ __forceinline__ void step2_spa_segment(const ProdView &P, Spa2Smem &S
                 incl += o;
         }
         const int total = __shfl_sync(TSG_FULL_MASK, incl, 31);
+        __syncwarp();
+        G.tpre[lane] = incl - cnt;
         for (int base = 0; base < total; base += SPA_STAGE)
         {
             __syncwarp();
-            unsigned bits = mr;
-            for (int x = 0; x < cnt; x++)
+            // a lane per entry: the entry's tile is the last lane whose first
+            // entry is at or before it, its column the x-th set column of that
+            // tile's row (A tiles holding many entries of the row would
+            // otherwise stage them one by one on a few lanes)
+            for (int h = 0; h < SPA_STAGE; h += 32)
             {
-                const int bit = 31 - __clz(bits);
-                bits ^= 1u << bit;
-                const int e = incl - cnt + x - base;
-                if (e >= 0 && e < SPA_STAGE)
+                const int e = base + h + lane;
+                int t = 0;
+#pragma unroll
+                for (int sz = 16; sz > 0; sz >>= 1)
+                    if (t + sz < 32 && G.tpre[t + sz] <= e)
+                        t += sz;
+                const unsigned tm = __shfl_sync(TSG_FULL_MASK, mr, t);
+                const int tkb = __shfl_sync(TSG_FULL_MASK, kb, t);
+                if (e < total)
                 {
-                    const int k = kb + (15 - bit);
+                    unsigned cols = __brev(tm) >> 16; // bit c: column c of the tile's row
+                    for (int q = e - G.tpre[t]; q > 0; q--)
+                        cols &= cols - 1;
+                    const int k = tkb + __ffs(cols) - 1;
                     int b0 = P.B_rptr[k], b1 = P.B_rptr[k + 1];
                     if (!full)
                     {
                         b0 += lower_bound_int(P.B_rcol + b0, b1 - b0, J0 * TSG_BS);
                         b1 = b0 + lower_bound_int(P.B_rcol + b0, b1 - b0, J1 * TSG_BS);
                     }
-                    G.bs[e] = b0;
-                    G.off[e] = b1 - b0;
+                    G.bs[h + lane] = b0;
+                    G.off[h + lane] = b1 - b0;
                 }
             }
             __syncwarp();
