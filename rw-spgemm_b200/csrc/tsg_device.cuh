@@ -1262,12 +1262,14 @@ __device__ __forceinline__ void step2_spa_segment(const ProdView &P, Spa2Smem &S
 // row's scalar products reach only a few of those tiles (n = 65,536 with 8
 // entries per row of A and B: ~4,000 C tiles and ~1,000 products per tile
 // row).  The SPA segments would spend their time on empty tiles, segment
-// after segment, each re-walking A's row.  A wide row whose estimated
-// products are below HYP_RATIO per C tile is therefore done whole by one CTA:
+// after segment, each re-walking A's row.  A wide row whose scalar products
+// (counted by the fused step-1/2 pass, wide_kind) are below HYP_RATIO per C
+// tile is therefore done whole by one CTA:
 //  - step 2 zero-fills the row's masks, row offsets and tile counts with
 //    16-byte stores, ORs every product's bit into C's mask word in global
 //    memory (two rows' 16-bit masks share a 32-bit word), notes the tiles
-//    hit in a shared bitmap and finishes only those tiles (step2_store);
+//    hit in a shared bitmap and finishes only those tiles, a thread per tile
+//    (row offsets, count and bin from its 16 masks);
 //  - step 3 zero-fills the row's values and adds every product into its
 //    value slot -- the tile's value offset + the row offset + the popcount
 //    of the row mask left of the column -- in global memory.  Warp r takes
