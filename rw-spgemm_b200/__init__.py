@@ -775,8 +775,11 @@ class HostResultBuffers:
     def __init__(self, m: int, nnz_cap: int, pinned: bool = True):
         self.resize(m, nnz_cap, pinned)
 
-    def resize(self, m, nnz_cap, pinned=True):
-        self.m, self.cap = m, nnz_cap
+    def resize(self, m, nnz_cap, pinned=None):
+        """Reallocates for m rows and nnz_cap entries; page-locked or not as
+        before unless pinned says otherwise."""
+        pinned = getattr(self, "pinned", True) if pinned is None else pinned
+        self.m, self.cap, self.pinned = m, nnz_cap, pinned
         if pinned:
             import torch
             self._t = [torch.empty(m + 1, dtype=torch.int32).pin_memory(),

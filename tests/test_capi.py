@@ -4,6 +4,8 @@ import ctypes
 import re
 from pathlib import Path
 
+import numpy as np
+
 ROOT = Path(__file__).resolve().parents[1]
 
 
@@ -43,3 +45,33 @@ def test_cli_binary_prints_usage_without_gpu():
     out = subprocess.run([str(ROOT / "rw-spgemm_b200" / "bin" / "test"), "-d", "0"], capture_output=True, text=True,
                          timeout=60)
     assert out.returncode == 0 and "Run the code by './test -d 0 -aat 0 matrixA.mtx" in out.stdout
+
+
+def test_overlap_wrapper_grows_buffers_and_retries(tsg, monkeypatch):
+    """spgemm_csr_host_overlap: a first call whose buffers are too small gets
+    TSG_ERR_OVERFLOW with nnz(C); the wrapper grows the buffers (keeping them
+    pageable) and calls again (host logic only, through a stand-in library)."""
+    calls = []
+
+    class FakeLib:
+        def tsg_spgemm_csr_host_into(self, ctx, m, k, n, nnzA, arp, aci, av, nnzB, brp, bci, bv, crp, cci, cv, cap,
+                                     p_nnz, p_info):
+            calls.append(cap)
+            p_nnz._obj.value = 5
+            if cap < 5:
+                return tsg.TSG_ERR_OVERFLOW
+            (ctypes.c_int * (m + 1)).from_address(crp)[:] = [0, 2, 3, 5]
+            (ctypes.c_int * 5).from_address(cci)[:] = [0, 2, 1, 0, 2]
+            (ctypes.c_double * 5).from_address(cv)[:] = [1.0, 2.0, 3.0, 4.0, 5.0]
+            return 0
+
+    monkeypatch.setattr(tsg, "lib", lambda: FakeLib())
+
+    class Ctx:
+        handle = None
+
+    mat = (3, 3, np.array([0, 1, 2, 3], np.int32), np.array([0, 1, 2], np.int32), np.ones(3))
+    out = tsg.HostResultBuffers(3, 2, pinned=False)
+    (m, n, rp, ci, v), info = tsg.spgemm_csr_host_overlap(Ctx(), mat, None, out)
+    assert calls == [2, 5] and out.cap == 5 and out.pinned is False
+    assert list(rp) == [0, 2, 3, 5] and list(ci) == [0, 2, 1, 0, 2] and list(v) == [1.0, 2.0, 3.0, 4.0, 5.0]
