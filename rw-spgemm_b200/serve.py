@@ -80,6 +80,10 @@ class OperandCache:
         self.bytes += self.tiled_bytes(t)
         return t
 
+    def size_of(self, key):
+        """Device bytes of a resident operand."""
+        return self.tiled_bytes(self.tiles[key])
+
     def evict_until(self, limit, pinned_keys):
         for key in list(self.tiles.keys()):
             if self.bytes <= limit:
@@ -221,20 +225,27 @@ class SpGEMMServer:
             job = self.queue[0]
             A = self.cache.get(job.a_key, self.matrices[job.a_key])
             B = self.cache.get(job.b_key, self.matrices[job.b_key])
-            pinned.update((job.a_key, job.b_key))
             job.pred_bytes, job.pred_prods = self._predict(A, B)
             if jobs and work + job.pred_prods > self.batch_products:
                 break  # the batch holds its share of work; this job opens the next
-            if job.pred_bytes > self.mem_cap:
+            # its operands stay resident while it runs: a job needing more
+            # than the cap with them could never be admitted
+            need = job.pred_bytes + self.cache.size_of(job.a_key) + (
+                self.cache.size_of(job.b_key) if job.b_key != job.a_key else 0)
+            if need > self.mem_cap:
                 self.queue.popleft()
                 self.rejected += 1
-                job.future.set_exception(MemoryError(f"job {job.jid} needs {job.pred_bytes} bytes, cap {self.mem_cap}"))
+                job.future.set_exception(MemoryError(f"job {job.jid} needs {need} bytes with its operands, "
+                                                     f"cap {self.mem_cap}"))
                 continue
             if self._in_use() + pred + job.pred_bytes > self.mem_cap:
+                # evict operands of nobody running or admitted (this job's own kept)
                 self.cache.evict_until(self.mem_cap - pred - job.pred_bytes -
-                                       sum(s.arena for s in self.slots if s.batch is not None), pinned)
+                                       sum(s.arena for s in self.slots if s.batch is not None),
+                                       pinned | {job.a_key, job.b_key})
                 if self._in_use() + pred + job.pred_bytes > self.mem_cap:
                     break  # wait for memory to free up (arrival order kept)
+            pinned.update((job.a_key, job.b_key))
             self.queue.popleft()
             jobs.append(job)
             pairs.append((A, B))
