@@ -752,6 +752,29 @@ __device__ __forceinline__ void step3_rows_item(const ProdView &P, long long ite
 #define SPA_DENSE 64 // C values per tile from which the tile kernel is faster
 #define SPA_FLAT 16  // B rows averaging fewer entries (inside a segment) have their products flattened
 
+// Staging a lane per A entry.  A warp's row entries are numbered across its
+// lanes' A tiles (lane order, then column order inside a tile); tpre[l] is
+// the first entry of lane l's tile, mr / kb that tile's row mask and first
+// column.  For entry e: the tile's lane t (the last lane whose first entry is
+// at or before e), the entry's index x inside the tile and its A column.
+// Every lane calls it (shuffles); lanes at or past total (the row's entries)
+// get t's values but must not use them.
+__device__ __forceinline__ int stage_entry(const int *tpre, unsigned mr, int kb, int e, int total, int &t, int &x)
+{
+    t = 0;
+#pragma unroll
+    for (int sz = 16; sz > 0; sz >>= 1)
+        if (t + sz < 32 && tpre[t + sz] <= e)
+            t += sz;
+    const unsigned tm = __shfl_sync(TSG_FULL_MASK, mr, t);
+    const int tkb = __shfl_sync(TSG_FULL_MASK, kb, t);
+    x = e - tpre[t];
+    unsigned cols = __brev(tm) >> 16; // bit c: column c of the tile's row
+    for (int q = e < total ? x : 0; q > 0; q--)
+        cols &= cols - 1;
+    return tkb + __ffs(cols) - 1;
+}
+
 struct SpaStage
 {
     int2 bl[SPA_STAGE]; // B row: first entry, length
@@ -926,21 +949,11 @@ __device__ __forceinline__ void step3_spa_segment(const ProdView &P, SpaSmem &S,
                 for (int h = 0; h < SPA_STAGE; h += 32)
                 {
                     const int e = base + h + lane;
-                    int t = 0;
-#pragma unroll
-                    for (int sz = 16; sz > 0; sz >>= 1)
-                        if (t + sz < 32 && G.tpre[t + sz] <= e)
-                            t += sz;
-                    const unsigned tm = __shfl_sync(TSG_FULL_MASK, mr, t);
-                    const int tkb = __shfl_sync(TSG_FULL_MASK, kb, t);
+                    int t, x;
+                    const int k = stage_entry(G.tpre, mr, kb, e, total, t, x);
                     const int tst = __shfl_sync(TSG_FULL_MASK, st, t);
                     if (e < total)
                     {
-                        const int x = e - G.tpre[t];
-                        unsigned cols = __brev(tm) >> 16; // bit c: column c of the tile's row
-                        for (int q = 0; q < x; q++)
-                            cols &= cols - 1;
-                        const int k = tkb + __ffs(cols) - 1;
                         int b0 = P.B_rptr[k], b1 = P.B_rptr[k + 1];
                         if (!full)
                         {
@@ -1183,19 +1196,10 @@ __device__ __forceinline__ void step2_spa_segment(const ProdView &P, Spa2Smem &S
             for (int h = 0; h < SPA_STAGE; h += 32)
             {
                 const int e = base + h + lane;
-                int t = 0;
-#pragma unroll
-                for (int sz = 16; sz > 0; sz >>= 1)
-                    if (t + sz < 32 && G.tpre[t + sz] <= e)
-                        t += sz;
-                const unsigned tm = __shfl_sync(TSG_FULL_MASK, mr, t);
-                const int tkb = __shfl_sync(TSG_FULL_MASK, kb, t);
+                int t, x;
+                const int k = stage_entry(G.tpre, mr, kb, e, total, t, x);
                 if (e < total)
                 {
-                    unsigned cols = __brev(tm) >> 16; // bit c: column c of the tile's row
-                    for (int q = e - G.tpre[t]; q > 0; q--)
-                        cols &= cols - 1;
-                    const int k = tkb + __ffs(cols) - 1;
                     int b0 = P.B_rptr[k], b1 = P.B_rptr[k + 1];
                     if (!full)
                     {
