@@ -75,3 +75,24 @@ def test_overlap_wrapper_grows_buffers_and_retries(tsg, monkeypatch):
     (m, n, rp, ci, v), info = tsg.spgemm_csr_host_overlap(Ctx(), mat, None, out)
     assert calls == [2, 5] and out.cap == 5 and out.pinned is False
     assert list(rp) == [0, 2, 3, 5] and list(ci) == [0, 2, 1, 0, 2] and list(v) == [1.0, 2.0, 3.0, 4.0, 5.0]
+
+
+def test_bench_byte_accounting_matches_the_documented_figures():
+    """The roofline's byte counts: compulsory bytes (tiled A and B read, tiled
+    C written) and the numeric step's algorithmic bytes, from the tile and
+    nonzero counts of the stencil 64^3 product (the bench line's 528,497,108
+    and 505,262,028) and of the 5-point Laplacian 256^2 product (18.99 MB)."""
+    import importlib.util
+    from types import SimpleNamespace as NS
+    spec = importlib.util.spec_from_file_location("bench_for_bytes", ROOT / "bench.py")
+    b = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(b)
+
+    def tiled(tilem, tilen, T, nnz):
+        return NS(s=NS(tilem=tilem, tilen=tilen), numtile=T, nnz=nnz)
+
+    A = tiled(16384, 16384, 361_000, 6_859_000)
+    assert b.compulsory_bytes(A, A, 1_380_344, 30_959_144) == 528_497_108
+    assert b.step3_algorithmic_bytes(A, A, 1_380_344, 30_959_144) == 505_262_028
+    L = tiled(4096, 4096, 19_936, 326_656)
+    assert b.compulsory_bytes(L, L, 50_532, 846_852) == 18_991_280
