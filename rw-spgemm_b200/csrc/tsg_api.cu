@@ -54,6 +54,10 @@ extern "C" int tsg_context_create(int device, tsg_context **out)
         e = cudaMallocHost((void **)&ctx->h_pinned, 64 * sizeof(long long));
     for (int i = 0; i < 8 && e == cudaSuccess; i++)
         e = cudaEventCreate(&ctx->ev[i]);
+    if (e == cudaSuccess)
+        e = cudaMalloc((void **)&ctx->d_status, sizeof(int));
+    if (e == cudaSuccess)
+        e = cudaMemset(ctx->d_status, 0, sizeof(int));
     if (e != cudaSuccess)
     {
         free(ctx);
@@ -92,8 +96,25 @@ extern "C" int tsg_context_destroy(tsg_context *ctx)
     if (ctx->own_stream)
         cudaStreamDestroy(ctx->stream);
     cudaFreeHost(ctx->h_pinned);
+    cudaFree(ctx->d_status);
     free(ctx);
     return TSG_OK;
+}
+
+int tsg_take_device_status(tsg_context *ctx)
+{
+    int *h = (int *)(ctx->h_pinned + 63);
+    TSG_CUDA(cudaMemcpyAsync(h, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    TSG_CUDA(cudaStreamSynchronize(ctx->stream));
+    const int code = *h;
+    if (code == TSG_OK)
+        return TSG_OK;
+    TSG_CUDA(cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->stream));
+    if (code == TSG_ERR_TIMEOUT)
+        return tsg_set_error(code, "a kernel's bounded wait ran out (numeric step pipeline)");
+    if (code == TSG_ERR_OVERFLOW)
+        return tsg_set_error(code, "a numeric step's accumulator slot fell outside its segment");
+    return tsg_set_error(code, "a kernel recorded error %d", code);
 }
 
 extern "C" int tsg_context_set_stream(tsg_context *ctx, void *stream)
@@ -164,7 +185,7 @@ extern "C" int tsg_context_synchronize(tsg_context *ctx)
     if (!ctx)
         return tsg_set_error(TSG_ERR_INVALID, "null context");
     TSG_CUDA(cudaStreamSynchronize(ctx->stream));
-    return TSG_OK;
+    return tsg_take_device_status(ctx);
 }
 
 extern "C" long long tsg_context_launches(tsg_context *ctx) { return ctx ? ctx->launches : 0; }

@@ -41,6 +41,7 @@ struct ProdView
     unsigned char *C_Ptr, *C_Colb;
     double *C_Val;
     int numC;
+    int padded; // every array allocated by tsg_alloc (16-byte aligned, 16 bytes of slack at the end)
 };
 
 // ---------------------------------------------------------------------------
@@ -1689,11 +1690,15 @@ __device__ __forceinline__ void spa_skip_hyper(const ProdView &P, const int *__r
 // block owning their first tile.
 static_assert(sizeof(HypSmem) <= sizeof(SpaSmem) && sizeof(HypSmem) <= sizeof(Spa2Smem), "hyper scratch");
 
+// only (may be null): only the tile rows I with only[I] != 0 (the rows the
+// staged numeric step left).
 template <bool FLAT>
 __device__ __forceinline__ void step3_spa_block(const ProdView &P, SpaSmem &S, int tb, int te,
-                                                const int *__restrict__ kind)
+                                                const int *__restrict__ kind, const int *__restrict__ only = nullptr)
 {
     spa_block_pieces<SPA_BLK>(P, tb, te, [&](int I, int ps, int pe) {
+        if (only && !only[I])
+            return;
         if (kind && kind[I] == 2)
         {
             if (ps == P.C_ptr[I])

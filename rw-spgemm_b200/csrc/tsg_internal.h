@@ -26,7 +26,12 @@ struct tsg_context
     int fuse12;          // step-1 emit fused with step 2 for narrow tile rows
     cudaStream_t copy_stream; // device-to-host copies overlapping compute (created on first use)
     cudaEvent_t copy_ev;      // orders a chunk's copy after its fill
+    int *d_status;            // device error word kernels set (TSG_ERR_TIMEOUT, TSG_ERR_OVERFLOW), 0 when clear
 };
+
+// Reads and clears the context's device error word (synchronises the
+// context's stream); returns TSG_OK or the code a kernel recorded.
+int tsg_take_device_status(tsg_context *ctx);
 
 // C tile rows are copied to the host in at most TSG_MAX_CHUNKS chunks of at
 // least TSG_CHUNK_NNZ nonzeros (tsg_spgemm_to_host).
@@ -70,18 +75,22 @@ int tsg_set_error(int code, const char *fmt, ...);
         TSG_CUDA(cudaGetLastError()); \
     } while (0)
 
+// Device allocation on the context's stream.  Every allocation is rounded
+// up to 16 bytes and given 16 bytes of slack, so kernels may copy a range
+// with its end rounded up to a 16-byte boundary (bulk copies) without
+// leaving the allocation.
 template <typename T>
 static inline int tsg_alloc(tsg_context *ctx, T **p, size_t count)
 {
     *p = nullptr;
     if (count == 0)
         count = 1;
-    cudaError_t e = cudaMallocAsync((void **)p, count * sizeof(T), ctx->stream);
+    const size_t bytes = ((count * sizeof(T) + 15) & ~(size_t)15) + 16;
+    cudaError_t e = cudaMallocAsync((void **)p, bytes, ctx->stream);
     if (e != cudaSuccess)
     {
         *p = nullptr;
-        return tsg_set_error(TSG_ERR_OOM, "device allocation of %zu bytes failed: %s",
-                             count * sizeof(T), cudaGetErrorString(e));
+        return tsg_set_error(TSG_ERR_OOM, "device allocation of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
     }
     return TSG_OK;
 }

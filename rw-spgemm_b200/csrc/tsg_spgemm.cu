@@ -13,6 +13,7 @@
 #include <algorithm>
 
 #include "tsg_device.cuh"
+#include "tsg_staged.cuh"
 
 #define S1_WARPS 8
 
@@ -58,6 +59,8 @@ __global__ void __launch_bounds__(256) k_step12(ProdView P, int *__restrict__ wi
             wide[i] = kind;
             if (kind)
                 atomicAdd(&wide[P.tilemA], 1); // count of wide rows
+            if (kind == 2)
+                atomicAdd(&wide[P.tilemA + 1], 1); // count of hypersparse rows
         }
     }
     __syncthreads();
@@ -216,6 +219,42 @@ __global__ void __launch_bounds__(SPA_THREADS, 3) k_step3_spa(ProdView P, const 
     }
 }
 
+// The tile rows the staged numeric step left (left[I] != 0: its stage would
+// not fit, or the row is hypersparse), by the SPA kernel; nothing unless it
+// left some (left[tilemA]).
+template <bool RANGED>
+__global__ void __launch_bounds__(SPA_THREADS, 2) k_step3_rest(ProdView P, const int *__restrict__ kind,
+                                                               const int *__restrict__ left, int row0, int row1,
+                                                               unsigned *__restrict__ ctr)
+{
+    extern __shared__ __align__(16) unsigned char s_raw[];
+    SpaSmem &S = *reinterpret_cast<SpaSmem *>(s_raw);
+    __shared__ int s_blk;
+    if (left[P.tilemA] == 0)
+        return;
+    unsigned nxt = 0;
+    if (threadIdx.x == 0)
+        nxt = atomicAdd(ctr, 1u);
+    const int t_beg = RANGED ? P.C_ptr[row0] : 0, t_end = RANGED ? P.C_ptr[row1] : P.numC;
+    const long long blk0 = t_beg / SPA_BLK;
+    for (;;)
+    {
+        __syncthreads();
+        if (threadIdx.x == 0)
+        {
+            s_blk = (int)nxt;
+            nxt = atomicAdd(ctr, 1u);
+        }
+        __syncthreads();
+        const long long tb = (blk0 + s_blk) * SPA_BLK;
+        if (tb >= t_end)
+            break;
+        if (threadIdx.x == 0)
+            spa_skip_hyper(P, kind, (int)tb, ctr, -blk0);
+        step3_spa_block<false>(P, S, max((int)tb, t_beg), (int)min((long long)t_end, tb + SPA_BLK), kind, left);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Host orchestration.
 // ---------------------------------------------------------------------------
@@ -276,6 +315,14 @@ static ProdView make_view(const tsg_tiled *A, const tsg_tiled *B, tsg_tiled *C)
     P.C_Colb = C->tile_csr_Col;
     P.C_Val = C->tile_csr_Value;
     P.numC = C->numtile;
+    // the staged numeric step copies ranges rounded out to 16-byte
+    // boundaries: library allocations only (tsg_alloc's slack), 16-byte aligned
+    const void *bases[] = {P.A_mask, P.A_Ptr, P.A_tnnz, P.A_col, P.A_Val, P.B_rcol, P.B_rval,
+                           P.C_mask, P.C_Ptr, P.C_tnnz, P.C_col};
+    bool aligned = true;
+    for (const void *p : bases)
+        aligned = aligned && ((uintptr_t)p & 15) == 0;
+    P.padded = !A->_alloc && !B->_alloc && !C->_alloc && aligned;
     return P;
 }
 
@@ -353,6 +400,35 @@ static int launch_step3_spa(tsg_context *ctx, const ProdView &P, const int *d_ki
     return TSG_OK;
 }
 
+// the staged numeric step for tile rows [row0, row1), then the SPA kernel
+// for the rows it left
+template <bool RANGED>
+static int launch_step3_stg(tsg_context *ctx, const ProdView &P, const int *d_kind, int row0, int row1)
+{
+    unsigned *ctr = nullptr, grid = 0;
+    int *left = nullptr;
+    const int smem = (int)sizeof(StgSmem);
+    TSG_CUDA(cudaFuncSetAttribute(k_step3_stg<RANGED>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    int per_sm = 0;
+    TSG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step3_stg<RANGED>, STG_THREADS, smem));
+    if (per_sm < 1)
+        return tsg_set_error(TSG_ERR_CUDA, "the staged numeric step does not fit an SM");
+    TSG_TRY(tsg_alloc(ctx, &ctr, 2));
+    TSG_TRY(tsg_alloc(ctx, &left, (size_t)P.tilemA + 1));
+    TSG_CUDA(cudaMemsetAsync(ctr, 0, 2 * sizeof(unsigned), ctx->stream));
+    TSG_CUDA(cudaMemsetAsync(left, 0, ((size_t)P.tilemA + 1) * sizeof(int), ctx->stream));
+    k_step3_stg<RANGED><<<ctx->num_sms * per_sm, STG_THREADS, smem, ctx->stream>>>(P, d_kind, row0, row1, ctr, left,
+                                                                                 ctx->d_status);
+    TSG_LAUNCH_CHECK();
+    const int rsmem = (int)sizeof(SpaSmem);
+    TSG_TRY(spa_grid(ctx, k_step3_rest<RANGED>, rsmem, &grid));
+    k_step3_rest<RANGED><<<grid, SPA_THREADS, rsmem, ctx->stream>>>(P, d_kind, left, row0, row1, ctr + 1);
+    TSG_LAUNCH_CHECK();
+    tsg_release(ctx, ctr);
+    tsg_release(ctx, left);
+    return TSG_OK;
+}
+
 // step 3 by the SPA kernel: the default schedule, except for products whose
 // C tiles are dense on average (>= SPA_DENSE values) and B without a row view
 // (borrowed foreign buffers), which take the tile kernel
@@ -366,11 +442,15 @@ static int launch_step3_spa_rows(tsg_context *ctx, const ProdView &P, long long 
                                  int row1)
 {
     const bool flat = spa_wants_flat(P.browB, P.numC, nnzC, P.tilemA);
-    if (row0 == 0 && row1 == P.tilemA)
-        return flat ? launch_step3_spa<true, false>(ctx, P, d_kind, 0, 0)
-                    : launch_step3_spa<false, false>(ctx, P, d_kind, 0, 0);
-    return flat ? launch_step3_spa<true, true>(ctx, P, d_kind, row0, row1)
-                : launch_step3_spa<false, true>(ctx, P, d_kind, row0, row1);
+    const bool whole = row0 == 0 && row1 == P.tilemA;
+    if (flat)
+        return whole ? launch_step3_spa<true, false>(ctx, P, d_kind, 0, 0)
+                     : launch_step3_spa<true, true>(ctx, P, d_kind, row0, row1);
+    if (P.padded)
+        return whole ? launch_step3_stg<false>(ctx, P, d_kind, 0, 0) : launch_step3_stg<true>(ctx, P, d_kind, row0, row1);
+    // operands viewing a batch arena: not padded for the bulk copies' rounding
+    return whole ? launch_step3_spa<false, false>(ctx, P, d_kind, 0, 0)
+                 : launch_step3_spa<false, true>(ctx, P, d_kind, row0, row1);
 }
 
 // d_kind: the row kinds of the fused step 1/2 pass (0 narrow, 1 wide,
@@ -459,8 +539,8 @@ static int spgemm_structure(tsg_context *ctx, const tsg_tiled *A, const tsg_tile
         ProdView P = make_view(A, B, C);
         if (fused)
         {
-            TSG_TRY(tsg_alloc(ctx, &R.d_wide, (size_t)tilem + 1));
-            TSG_CUDA(cudaMemsetAsync(R.d_wide + tilem, 0, sizeof(int), st));
+            TSG_TRY(tsg_alloc(ctx, &R.d_wide, (size_t)tilem + 2));
+            TSG_CUDA(cudaMemsetAsync(R.d_wide + tilem, 0, 2 * sizeof(int), st));
             k_step12<<<tsg_blocks(tilem, 8), 256, 0, st>>>(P, R.d_wide, R.d_bins);
             TSG_LAUNCH_CHECK();
         }
@@ -508,6 +588,15 @@ static int spgemm_finish(tsg_context *ctx, SpgemmRun &R, tsg_spgemm_info *info)
     cudaStream_t st = ctx->stream;
     tsg_release(ctx, R.d_wide);
     R.d_wide = nullptr;
+    {
+        const int dev = tsg_take_device_status(ctx);
+        if (dev != TSG_OK)
+        {
+            tsg_release(ctx, R.d_pairs);
+            tsg_release(ctx, R.d_bins);
+            return dev;
+        }
+    }
     if (info)
     {
         memset(info, 0, sizeof(*info));
