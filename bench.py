@@ -302,22 +302,6 @@ def run_batched(args, tsg, gen, ctx, steps):
 # ---------------------------------------------------------------------------
 # served: Poisson arrivals into the continuous-batching server
 # ---------------------------------------------------------------------------
-def served_pool(gen, seed=0):
-    """Fixed mix: 40 small matrices from the batched generators (n 1k-16k),
-    R-MAT scale 14 (edge factor 8, 16), 15 (8, 16) and 16 (8)."""
-    rng = np.random.default_rng(seed)
-    small = []
-    for i in range(40):
-        n = int(round(np.exp(rng.uniform(np.log(1024), np.log(16384)))))
-        s = int(rng.integers(0, 2**31 - 1))
-        small.append(gen.banded(n, int(rng.integers(8, 65)), seed=s) if rng.random() < 0.5
-                     else gen.random_poisson(n, None, 8.0, seed=s))
-    rmat = {14: [gen.rmat(14, 8, seed=1), gen.rmat(14, 16, seed=2)],
-            15: [gen.rmat(15, 8, seed=3), gen.rmat(15, 16, seed=4)],
-            16: [gen.rmat(16, 8, seed=5)]}
-    return small, rmat
-
-
 def _served_stream(srv, jobs, rate, rng):
     """Submits jobs with Poisson arrivals at `rate` jobs/s; returns the
     server's statistics and the wall time of the stream."""
@@ -345,31 +329,16 @@ def run_served(args, tsg, gen, device, deliver="device", n_jobs=None, half_capac
     service alone); "host": as numpy arrays in page-locked memory (every
     result crosses the bus)."""
     srv_mod = _load("rw_spgemm_b200.serve", PKG_DIR / "serve.py")
-    small, rmat = served_pool(gen)
+    pool = gen.served_pool()
     srv = srv_mod.SpGEMMServer(device, mem_cap=40 << 30, slots=2, max_batch=64, schedule=tuple(args.served_schedule),
                                deliver=deliver)
-    keys = []
-    for i, m in enumerate(small):
-        srv.register(f"s{i}", m)
-        keys.append(("small", f"s{i}", m))
-    for sc, lst in rmat.items():
-        for i, m in enumerate(lst):
-            srv.register(f"r{sc}_{i}", m)
-            keys.append((sc, f"r{sc}_{i}", m))
+    for key, m in pool.items():
+        srv.register(key, m)
     rng = np.random.default_rng(1)
     jobs = []
-    by_kind = {"small": [k for k in keys if k[0] == "small"], 14: [k for k in keys if k[0] == 14],
-               15: [k for k in keys if k[0] == 15], 16: [k for k in keys if k[0] == 16]}
-    for _ in range(n_jobs or args.served_jobs):
-        u = rng.random()
-        cls = "small" if u < 0.85 else 14 if u < 0.95 else 15 if u < 0.99 else 16
-        _, key, mat = by_kind[cls][int(rng.integers(0, len(by_kind[cls])))]
-        if rng.random() < 0.5:
-            jobs.append(("AAT", key, None, gen.products(mat, gen.transpose(mat))))
-        else:
-            same = [k for k in by_kind[cls] if k[2][0] == mat[1]] or [(None, key, mat)]
-            _, bkey, bmat = same[int(rng.integers(0, len(same)))]
-            jobs.append(("AB", key, bkey, gen.products(mat, bmat)))
+    for kind, a, b in gen.served_jobs(pool, n_jobs or args.served_jobs, seed=1):
+        B = gen.transpose(pool[a]) if kind == "AAT" else pool[b]
+        jobs.append((kind, a, b, gen.products(pool[a], B)))
     # warm the operand cache and the kernels with one pass of distinct jobs
     srv.start()
     for f in [srv.submit(k, a, b) for k, a, b, _ in jobs[:64]]:
@@ -515,32 +484,21 @@ def run_rmat20(args, tsg, gen, ctx, budget=1.5e9):
     the resident B) and its C freed.  GFLOP/s over the steps-1-3 time of all
     blocks; wall time includes the block conversions."""
     import torch
+    blocks_mod = _load("rw_spgemm_b200.blocks", PKG_DIR / "blocks.py")
     A = gen.rmat(20, 16, seed=1)
     m, n, rp, ci, v = A
     out = {"workload": "R-MAT scale 20, edge factor 16 (n=1,048,576), FP64 U(-1,1); A in row blocks of <= %.1e "
                        "products" % budget}
     for label, B in (("A*A", A), ("A*A^T", gen.transpose(A))):
         TB = tsg.csr_host_to_tiled(ctx, B, tsg.TSG_TILED_CSC_VIEW)
-        blen = np.diff(B[2]).astype(np.int64)
-        rowprod = np.zeros(m, np.int64)
-        nz = np.diff(rp) > 0
-        rowprod[nz] = np.add.reduceat(blen[ci], rp[:-1][nz])
-        tileprod = np.add.reduceat(rowprod, np.arange(0, m, 16))
-        bounds, acc = [0], 0
-        for t, pt in enumerate(tileprod):
-            if acc > 0 and acc + pt > budget:
-                bounds.append(t)
-                acc = 0
-            acc += int(pt)
-        bounds.append(len(tileprod))
+        tileprod = blocks_mod.tile_row_products(A, B)
+        blocks = blocks_mod.row_blocks(tileprod, budget)
         ctx.set_timing(True)
         steps_ms, prods, nnz, tiles = 0.0, 0, 0, 0
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        for b0, b1 in zip(bounds[:-1], bounds[1:]):
-            r0, r1 = b0 * 16, min(b1 * 16, m)
-            blk = (r1 - r0, n, (rp[r0:r1 + 1] - rp[r0]).astype(np.int32), ci[rp[r0]:rp[r1]], v[rp[r0]:rp[r1]])
-            TA = tsg.csr_host_to_tiled(ctx, blk, tsg.TSG_TILED_PACKED_COL)
+        for b0, b1 in blocks:
+            TA = tsg.csr_host_to_tiled(ctx, blocks_mod.block_rows(A, b0, b1), tsg.TSG_TILED_PACKED_COL)
             C, info = tsg.spgemm(ctx, TA, TB)
             steps_ms += info["ms_total"]
             nnz += info["nnz_C"]
@@ -550,9 +508,9 @@ def run_rmat20(args, tsg, gen, ctx, budget=1.5e9):
         torch.cuda.synchronize()
         wall = time.perf_counter() - t0
         ctx.set_timing(False)
-        prods = int(rowprod.sum())
+        prods = int(tileprod.sum())
         TB.free()
-        out[label] = {"products": prods, "nnz_C": int(nnz), "tiles_C": int(tiles), "blocks": len(bounds) - 1,
+        out[label] = {"products": prods, "nnz_C": int(nnz), "tiles_C": int(tiles), "blocks": len(blocks),
                       "ms_steps_1_3": round(steps_ms, 1), "gflops": round(2.0 * prods / (steps_ms * 1e-3) / 1e9, 2),
                       "wall_s": round(wall, 2)}
     return out

@@ -56,6 +56,8 @@ def olib():
         _o.tsgo_count_products.argtypes = [ctypes.c_int, vp, vp]
         _o.tsgo_gustavson_symbolic.restype = ctypes.c_longlong
         _o.tsgo_gustavson_symbolic.argtypes = [ctypes.c_int, ctypes.c_int, vp, vp, vp, vp, vp, ctypes.c_int]
+        _o.tsgo_gustavson_row_nnz.restype = ctypes.c_longlong
+        _o.tsgo_gustavson_row_nnz.argtypes = [ctypes.c_int, ctypes.c_int, vp, vp, vp, vp, vp, ctypes.c_int]
         _o.tsgo_gustavson_numeric.argtypes = [ctypes.c_int, ctypes.c_int, vp, vp, vp, vp, vp, vp, vp, vp, vp,
                                               ctypes.c_int]
         _o.tsgo_order_degree.argtypes = [ctypes.c_int, vp, vp]
@@ -194,6 +196,17 @@ def gustavson(matA, matB, nthreads=1):
                                   ciB.ctypes.data, vB.ctypes.data, rpC.ctypes.data, ciC.ctypes.data,
                                   vC.ctypes.data, nthreads)
     return mA, nB, rpC, ciC[:nnz], vC[:nnz]
+
+
+def gustavson_row_nnz(matA, matB, nthreads=1):
+    """nnz of every row of C = A*B (int32 per row) and the 64-bit total."""
+    mA, nA, rpA, ciA, _ = matA
+    mB, nB, rpB, ciB, _ = matB
+    rpA, ciA, rpB, ciB = (np.ascontiguousarray(x, dtype=np.int32) for x in (rpA, ciA, rpB, ciB))
+    counts = np.zeros(max(mA, 1), dtype=np.int32)
+    total = olib().tsgo_gustavson_row_nnz(mA, nB, rpA.ctypes.data, ciA.ctypes.data, rpB.ctypes.data,
+                                          ciB.ctypes.data, counts.ctypes.data, nthreads)
+    return counts[:mA], int(total)
 
 
 def order(kind, mat, seed=1):

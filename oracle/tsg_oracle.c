@@ -597,6 +597,47 @@ long long tsgo_gustavson_symbolic(int m, int n,
     return s;
 }
 
+/* Per-row nnz of C = A*B (structure only, element level), as the symbolic
+ * pass above but without a 32-bit row pointer: counts[i] = nnz(C row i),
+ * returns the total as 64 bits (products of more than 2^31 nonzeros). */
+long long tsgo_gustavson_row_nnz(int m, int n,
+                                 const int *a_rowptr, const int *a_col,
+                                 const int *b_rowptr, const int *b_col,
+                                 int *counts, int nthreads)
+{
+    if (nthreads <= 0)
+        nthreads = 1;
+    long long total = 0;
+#pragma omp parallel num_threads(nthreads) reduction(+ : total)
+    {
+        int *mark = (int *)xmalloc((size_t)(n ? n : 1) * sizeof(int));
+        for (int j = 0; j < n; j++)
+            mark[j] = -1;
+#pragma omp for schedule(dynamic, 64)
+        for (int i = 0; i < m; i++)
+        {
+            int cnt = 0;
+            for (int p = a_rowptr[i]; p < a_rowptr[i + 1]; p++)
+            {
+                int k = a_col[p];
+                for (int q = b_rowptr[k]; q < b_rowptr[k + 1]; q++)
+                {
+                    int j = b_col[q];
+                    if (mark[j] != i)
+                    {
+                        mark[j] = i;
+                        cnt++;
+                    }
+                }
+            }
+            counts[i] = cnt;
+            total += cnt;
+        }
+        free(mark);
+    }
+    return total;
+}
+
 void tsgo_gustavson_numeric(int m, int n,
                             const int *a_rowptr, const int *a_col, const double *a_val,
                             const int *b_rowptr, const int *b_col, const double *b_val,

@@ -61,6 +61,10 @@ long long tsgo_gustavson_symbolic(int m, int n,
                                   const int *a_rowptr, const int *a_col,
                                   const int *b_rowptr, const int *b_col,
                                   int *c_rowptr, int nthreads);
+long long tsgo_gustavson_row_nnz(int m, int n,
+                                 const int *a_rowptr, const int *a_col,
+                                 const int *b_rowptr, const int *b_col,
+                                 int *counts, int nthreads);
 void tsgo_gustavson_numeric(int m, int n,
                             const int *a_rowptr, const int *a_col, const double *a_val,
                             const int *b_rowptr, const int *b_col, const double *b_val,

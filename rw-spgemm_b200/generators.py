@@ -166,3 +166,42 @@ def batched_products(count: int = 512, seed: int = 0, n_min: int = 1024, n_max: 
                 mats.append(random_poisson(n, None, lam, seed=s))
         out.append((mats[0], mats[1]))
     return out
+
+
+def served_pool(seed: int = 0):
+    """The served mix's matrices, by key: 40 small ones from the batched
+    generators ("s0".."s39", n 1k-16k, banded or Poisson(8)) and R-MAT scale
+    14 (edge factor 8, 16), 15 (8, 16) and 16 (8) ("r14_0", ...)."""
+    rng = np.random.default_rng(seed)
+    pool = {}
+    for i in range(40):
+        n = int(round(np.exp(rng.uniform(np.log(1024), np.log(16384)))))
+        s = int(rng.integers(0, 2**31 - 1))
+        pool[f"s{i}"] = (banded(n, int(rng.integers(8, 65)), seed=s) if rng.random() < 0.5
+                         else random_poisson(n, None, 8.0, seed=s))
+    for sc, efs in ((14, (8, 16)), (15, (8, 16)), (16, (8,))):
+        for i, ef in enumerate(efs):
+            pool[f"r{sc}_{i}"] = rmat(sc, ef, seed=2 * (sc - 14) + i + 1)
+    return pool
+
+
+def served_jobs(pool, count: int, seed: int = 1):
+    """`count` jobs (kind, a_key, b_key) over served_pool(): 85% small
+    matrices, 10% R-MAT scale 14, 4% scale 15, 1% scale 16; half A*A^T (b_key
+    None), half A*B with B a same-class matrix of matching size (A itself
+    when there is none)."""
+    rng = np.random.default_rng(seed)
+    classes = {"small": [k for k in pool if k[0] == "s"]}
+    for sc in (14, 15, 16):
+        classes[sc] = [k for k in pool if k.startswith(f"r{sc}_")]
+    jobs = []
+    for _ in range(count):
+        u = rng.random()
+        cls = "small" if u < 0.85 else 14 if u < 0.95 else 15 if u < 0.99 else 16
+        a = classes[cls][int(rng.integers(0, len(classes[cls])))]
+        if rng.random() < 0.5:
+            jobs.append(("AAT", a, None))
+        else:
+            same = [k for k in classes[cls] if pool[k][0] == pool[a][1]] or [a]
+            jobs.append(("AB", a, same[int(rng.integers(0, len(same)))]))
+    return jobs
