@@ -181,8 +181,8 @@ int build_original_reorder_plan(ReorderProblemKind kind,
  * computed from matrixA / matrixB in memory); ordergen_ms receives the GPU
  * ordering time.  AA/AAT apply A's order to all three axes; AB uses A's order
  * for rows and inner axis and B's order for the column axis.  Returns 0, or
- * -42 for an algorithm this library does not provide (the reference's
- * missing-dependency exit code). */
+ * -20 for an algorithm this library does not provide (the reference's return
+ * for an order generator that did not run, src/external_reorder.h:133). */
 int build_external_reorder_plan(ReorderProblemKind kind,
                                 const char *algorithm,
                                 const char *matrix_path_A,
@@ -308,10 +308,16 @@ int tsg_context_set_fusion(tsg_context *ctx, int fuse_step12);
 /* 0 when all work queued on the context's stream has finished, 1 while
  * some is pending, a negative status on error (non-blocking). */
 int tsg_context_query(tsg_context *ctx);
-/* Blocks until all work queued on the context's stream has finished. */
+/* Blocks until all work queued on the context's stream has finished; returns
+ * an error a kernel recorded in the context's device status word since the
+ * last check (TSG_ERR_TIMEOUT: a bounded wait gave up; TSG_ERR_OVERFLOW: an
+ * accumulator bound was exceeded) and clears it. */
 int tsg_context_synchronize(tsg_context *ctx);
 /* Number of this library's kernels launched on the context so far. */
 long long tsg_context_launches(tsg_context *ctx);
+/* Number of device allocations the library made on the context so far (its
+ * stream-ordered pool requests; no reference counterpart). */
+long long tsg_context_allocations(tsg_context *ctx);
 /* Record per-step CUDA-event timings into tsg_spgemm_info. */
 int tsg_context_set_timing(tsg_context *ctx, int enabled);
 
@@ -354,9 +360,9 @@ int tsg_tiled_to_csr(tsg_context *ctx, const tsg_tiled *C,
  *   - The scratch is one per device, shared by all contexts, streams and
  *     threads: calls that may overlap on one device race on it; order them
  *     (same stream, or an event between them).
- *   - The first call on a device looks up the scratch address
- *     (cudaGetSymbolAddress, with that device current); make that first call
- *     before any stream capture. */
+ *   - The scratch address is looked up (cudaGetSymbolAddress) when a context
+ *     is created on the device, so the call itself makes no runtime call but
+ *     its launches; after a cudaDeviceReset create a new context. */
 int tsg_tiled_to_csr_noalloc(tsg_context *ctx, const tsg_tiled *C,
                              int *d_rowptr, int *d_colidx, double *d_val);
 
@@ -498,6 +504,13 @@ int tsg_batch_info(tsg_batch *b, int *graph, int *grid, size_t *arena_bytes, lon
  * step-1 emit + fused step 2, step 2 of the remaining tiles, tile-count scans,
  * numeric step. */
 int tsg_batch_phase_ms(tsg_batch *b, double *ms);
+/* Sets how long (seconds) a block of the batch kernel waits at its grid
+ * barrier before it gives up, sets TSG_ERR_TIMEOUT for tsg_batch_sync and
+ * leaves (the batch stays usable: the next run starts clean).  The default
+ * is 2 s plus 10 ns per scalar product of the whole batch.  A graph captured
+ * at creation reads the limit from device memory, so it applies to it too.
+ * No reference counterpart (the reference has no batched path). */
+int tsg_batch_set_wait_limit(tsg_batch *b, double seconds);
 int tsg_batch_destroy(tsg_batch *b);
 
 /* ------------------------------------------------------------------------ */

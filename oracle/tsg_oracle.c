@@ -809,7 +809,7 @@ void tsgo_order_rcm(int n, const int *rowptr, const int *col, int *order)
 {
     int *gptr, *adj;
     symmetric_graph(n, rowptr, col, &gptr, &adj);
-    Key3 *seeds = (Key3 *)xmalloc((size_t)(n ? n : 1) * sizeof(Key3));
+    Key3 *seeds = (Key3 *)xmalloc((size_t)(n > 0 ? n : 1) * sizeof(Key3));
     for (int i = 0; i < n; i++)
     {
         seeds[i].k0 = gptr[i + 1] - gptr[i];

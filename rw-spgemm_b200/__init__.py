@@ -111,6 +111,8 @@ def _declare(L):
     L.tsg_context_set_stream.argtypes = [vp, vp]
     L.tsg_context_set_timing.argtypes = [vp, ip]
     L.tsg_context_launches.argtypes = [vp]
+    L.tsg_context_allocations.argtypes = [vp]
+    L.tsg_context_allocations.restype = ctypes.c_longlong
     L.tsg_context_synchronize.argtypes = [vp]
     L.tsg_context_query.argtypes = [vp]
     L.tsg_context_set_fusion.argtypes = [vp, ip]
@@ -308,6 +310,10 @@ class Context:
 
     def launches(self) -> int:
         return int(lib().tsg_context_launches(self.handle))
+
+    def allocations(self) -> int:
+        """Device allocations the library made on this context so far."""
+        return int(lib().tsg_context_allocations(self.handle))
 
     def close(self):
         if self.handle:
@@ -638,6 +644,7 @@ def _declare_batch(L):
                                  ctypes.POINTER(ctypes.c_longlong)]
     L.tsg_batch_destroy.argtypes = [vp]
     L.tsg_batch_phase_ms.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
+    L.tsg_batch_set_wait_limit.argtypes = [vp, ctypes.c_double]
     L.tsg_product_bounds.argtypes = [vp, ctypes.POINTER(TsgTiled), ctypes.POINTER(TsgTiled),
                                      ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]
 
@@ -684,6 +691,10 @@ class Batch:
         check(lib().tsg_batch_phase_ms(self.handle, out))
         names = ["step1_counts", "row_scans", "item_prefix", "step1_emit_step2", "step2_rest", "tile_scans", "step3"]
         return {k: round(v, 4) for k, v in zip(names, out)}
+
+    def set_wait_limit(self, seconds: float):
+        """Grid-barrier wait bound in seconds (tsg_batch_set_wait_limit)."""
+        check(lib().tsg_batch_set_wait_limit(self.handle, float(seconds)))
 
     def sync(self):
         t, z = ctypes.c_longlong(0), ctypes.c_longlong(0)

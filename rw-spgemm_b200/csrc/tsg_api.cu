@@ -58,6 +58,8 @@ extern "C" int tsg_context_create(int device, tsg_context **out)
         e = cudaMalloc((void **)&ctx->d_status, sizeof(int));
     if (e == cudaSuccess)
         e = cudaMemset(ctx->d_status, 0, sizeof(int));
+    if (e == cudaSuccess && tsg_noalloc_prepare(device) != TSG_OK)
+        e = cudaErrorUnknown;
     if (e != cudaSuccess)
     {
         free(ctx);
@@ -189,6 +191,8 @@ extern "C" int tsg_context_synchronize(tsg_context *ctx)
 }
 
 extern "C" long long tsg_context_launches(tsg_context *ctx) { return ctx ? ctx->launches : 0; }
+
+extern "C" long long tsg_context_allocations(tsg_context *ctx) { return ctx ? ctx->allocs : 0; }
 
 extern "C" int tsg_context_set_timing(tsg_context *ctx, int enabled)
 {
@@ -423,7 +427,8 @@ extern "C" int tsg_spgemm_csr_host_ex(tsg_context *ctx, int m, int k, int n, int
 {
     if (!ctx || !a_rowptr || !b_rowptr || !nnzC || !c_rowptr || !c_colidx || !c_val)
         return tsg_set_error(TSG_ERR_INVALID, "null argument");
-    const bool alias = (a_rowptr == b_rowptr && a_colidx == b_colidx && a_val == b_val && m == k && k == n);
+    const bool alias =
+        (a_rowptr == b_rowptr && a_colidx == b_colidx && a_val == b_val && m == k && k == n && nnzA == nnzB);
     int *dA_rp, *dA_ci, *dB_rp = nullptr, *dB_ci = nullptr;
     double *dA_v, *dB_v = nullptr;
     TSG_TRY(h2d(ctx, &dA_rp, a_rowptr, (size_t)m + 1));
@@ -752,7 +757,8 @@ extern "C" int tsg_spgemm_csr_host_start(tsg_context *ctx, int m, int k, int n, 
     if (!ctx || !res || !nnzC || !a_rowptr || !b_rowptr)
         return tsg_set_error(TSG_ERR_INVALID, "null argument");
     *res = nullptr;
-    const bool alias = (a_rowptr == b_rowptr && a_colidx == b_colidx && a_val == b_val && m == k && k == n);
+    const bool alias =
+        (a_rowptr == b_rowptr && a_colidx == b_colidx && a_val == b_val && m == k && k == n && nnzA == nnzB);
     tsg_tiled A, B, C;
     memset(&A, 0, sizeof(A));
     memset(&B, 0, sizeof(B));
@@ -816,7 +822,8 @@ extern "C" int tsg_spgemm_csr_host_into(tsg_context *ctx, int m, int k, int n, i
         nnz_cap < 0)
         return tsg_set_error(TSG_ERR_INVALID, "null argument");
     *nnzC = 0;
-    const bool alias = (a_rowptr == b_rowptr && a_colidx == b_colidx && a_val == b_val && m == k && k == n);
+    const bool alias =
+        (a_rowptr == b_rowptr && a_colidx == b_colidx && a_val == b_val && m == k && k == n && nnzA == nnzB);
     tsg_tiled A, B;
     memset(&A, 0, sizeof(A));
     memset(&B, 0, sizeof(B));

@@ -15,8 +15,10 @@
 // Memory: one arena per batch, sized at creation from per-product upper
 // bounds computed on the device (C tiles <= matched tile pairs, C nonzeros <=
 // scalar products), so a run needs no host round trip.  The grid barrier is
-// bounded: a wait that exceeds its iteration limit sets an error flag that
-// tsg_batch_sync reports, and every block leaves.
+// bounded in time (%globaltimer): a wait longer than the batch's limit --
+// BATCH_WAIT_FLOOR_NS plus BATCH_WAIT_NS_PER_PRODUCT per scalar product of
+// the whole batch, or tsg_batch_set_wait_limit's -- sets TSG_ERR_TIMEOUT in
+// the error word that tsg_batch_sync reports, and every block leaves.
 #include <cooperative_groups.h>
 #include <stdlib.h>
 
@@ -46,7 +48,8 @@ struct tsg_batch
     BatchProd *d_prod;
     long long *d_rowoff;
     long long *d_itemoff;
-    unsigned *d_bar; // [0] arrivals, [1] generation, [2] / [3] next tile block (SPA steps 3 / 2)
+    unsigned *d_bar; // [0] arrivals, [1] generation, [2] / [3] next tile block (SPA steps 3 / 2),
+                     // [4..5] the barrier's wait limit in ns (64-bit)
     int *d_err;
     int *d_bins;
     void *arena;
@@ -59,10 +62,21 @@ struct tsg_batch
     int graph_ok;
     std::vector<int> m, n, tilen; // per product C dimensions
     long long launches;
+    unsigned long long wait_ns; // the grid barrier's wait limit
 };
 
 #define BATCH_THREADS 128
-#define BATCH_BAR_LIMIT 4000000LL
+// a barrier wait gives up after this floor plus a share of the batch's work
+// (a B200 does well over 10 scalar products per ns, so the bound is loose)
+#define BATCH_WAIT_FLOOR_NS 2000000000ULL
+#define BATCH_WAIT_NS_PER_PRODUCT 10ULL
+
+__device__ __forceinline__ unsigned long long batch_clock_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
 
 // ---------------------------------------------------------------------------
 // bounded grid barrier (all blocks co-resident: cooperative launch)
@@ -84,12 +98,13 @@ __device__ __forceinline__ bool grid_barrier(unsigned *bar, int *err)
         }
         else
         {
-            long long spins = 0;
+            const unsigned long long limit = *(volatile unsigned long long *)(bar + 4);
+            const unsigned long long t0 = batch_clock_ns();
             while (*vgen == gen)
             {
-                if (++spins > BATCH_BAR_LIMIT || *(volatile int *)err)
+                if (*(volatile int *)err || batch_clock_ns() - t0 > limit)
                 {
-                    atomicOr(err, 1);
+                    atomicCAS(err, 0, TSG_ERR_TIMEOUT);
                     break;
                 }
                 __nanosleep(100);
@@ -259,12 +274,7 @@ __device__ long long block_scan_ll(long long *v, int n, long long *s_tmp)
 
 // GPU global timer (ns); block 0 stamps the end of each phase into
 // stamp[1..6] and every block raises stamp[7] as it leaves.
-__device__ __forceinline__ unsigned long long gtimer()
-{
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
+__device__ __forceinline__ unsigned long long gtimer() { return batch_clock_ns(); }
 
 #define BATCH_STAMP(k)                                                  \
     if (blockIdx.x == 0 && threadIdx.x == 0)                           \
@@ -553,10 +563,13 @@ __global__ void __launch_bounds__(NT)
 
 // Step 3 of the SPA schedule over a batch, after k_batch: products with
 // sparse C tiles, CTAs taking blocks of SPA_BLK C tiles (all products) from a
-// device counter.  Raises stamp[7] on exit.
+// device counter.  Raises stamp[7] on exit.  Does nothing when k_batch left
+// with an error (its later phases did not run).
 __global__ void __launch_bounds__(SPA_THREADS, 3)
-    k_batch_spa3(BatchProd *prods, int count, const long long *__restrict__ itemoff, unsigned *bar)
+    k_batch_spa3(BatchProd *prods, int count, const long long *__restrict__ itemoff, unsigned *bar, const int *err)
 {
+    if (*(volatile const int *)err)
+        return;
     extern __shared__ __align__(16) unsigned char s_raw[];
     __shared__ int s_blk;
     SpaSmem &S = *reinterpret_cast<SpaSmem *>(s_raw);
@@ -597,8 +610,10 @@ __global__ void __launch_bounds__(SPA_THREADS, 3)
 // average): the tile kernel, a half-warp per C tile.
 #define DENSE3_THREADS 256
 __global__ void __launch_bounds__(DENSE3_THREADS)
-    k_batch_dense3(BatchProd *prods, int count, const long long *__restrict__ itemoff)
+    k_batch_dense3(BatchProd *prods, int count, const long long *__restrict__ itemoff, const int *err)
 {
+    if (*(volatile const int *)err)
+        return;
     __shared__ double s_acc[DENSE3_THREADS / 16][TSG_BS * S3T_STRIDE];
     const int lane = threadIdx.x & 15, hw = threadIdx.x >> 4;
     const unsigned hmask = TSG_HW_MASK(threadIdx.x);
@@ -780,9 +795,10 @@ static int record_run(tsg_batch *b, cudaStream_t st)
                                 b->d_bar, b->d_err, b->d_bins));
     if (b->params.schedule == TSG_SCHED_SPA)
     {
-        k_batch_spa3<<<b->grid3, SPA_THREADS, sizeof(SpaSmem), st>>>(b->d_prod, b->count, b->d_itemoff, b->d_bar);
+        k_batch_spa3<<<b->grid3, SPA_THREADS, sizeof(SpaSmem), st>>>(b->d_prod, b->count, b->d_itemoff, b->d_bar,
+                                                                     b->d_err);
         TSG_CUDA(cudaGetLastError());
-        k_batch_dense3<<<b->ctx->num_sms * 8, DENSE3_THREADS, 0, st>>>(b->d_prod, b->count, b->d_itemoff);
+        k_batch_dense3<<<b->ctx->num_sms * 8, DENSE3_THREADS, 0, st>>>(b->d_prod, b->count, b->d_itemoff, b->d_err);
         TSG_CUDA(cudaGetLastError());
     }
     return TSG_OK;
@@ -832,7 +848,7 @@ extern "C" int tsg_batch_create(tsg_context *ctx, int count, const tsg_tiled *A,
     // bounds and arena layout
     size_t bytes = 0;
     std::vector<size_t> off(count);
-    long long run = 0, chunk_cap = 0;
+    long long run = 0, chunk_cap = 0, total_prods = 0;
     for (int p = 0; p < count; p++)
     {
         long long prods = 0, pairs = 0;
@@ -851,6 +867,7 @@ extern "C" int tsg_batch_create(tsg_context *ctx, int count, const tsg_tiled *A,
             return st;
         }
         (void)pairs;
+        total_prods += prods;
         long long capN = prods < 256 * capT ? prods : 256 * capT;
         if (capN > 2147483647LL || capT > 2147483647LL / 16)
         {
@@ -926,19 +943,26 @@ extern "C" int tsg_batch_create(tsg_context *ctx, int count, const tsg_tiled *A,
         P.C_Colb = (unsigned char *)take((size_t)h.capN);
         P.C_Val = (double *)take((size_t)h.capN * 8);
         P.numC = 0;
+        P.padded = 0;
+        P.status = nullptr; // the batch's error word, set once it is allocated
     }
     if ((st = tsg_alloc(ctx, &b->d_prod, (size_t)count)) != TSG_OK || (st = tsg_alloc(ctx, &b->d_rowoff, (size_t)count + 1)) ||
-        (st = tsg_alloc(ctx, &b->d_itemoff, 3 * ((size_t)count + 1) + 8 + (size_t)chunk_cap)) || (st = tsg_alloc(ctx, &b->d_bar, 4)) ||
+        (st = tsg_alloc(ctx, &b->d_itemoff, 3 * ((size_t)count + 1) + 8 + (size_t)chunk_cap)) || (st = tsg_alloc(ctx, &b->d_bar, 8)) ||
         (st = tsg_alloc(ctx, &b->d_err, 1)) || (st = tsg_alloc(ctx, &b->d_bins, 4)))
     {
         tsg_batch_destroy(b);
         return st;
     }
     cudaStream_t s = ctx->stream;
+    // an in-kernel error (a numeric accumulator overflow) goes to the batch's error word
+    for (BatchProd &h : b->host)
+        h.P.status = b->d_err;
     cudaMemcpyAsync(b->d_prod, b->host.data(), sizeof(BatchProd) * count, cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(b->d_rowoff, b->rowoff.data(), sizeof(long long) * (count + 1), cudaMemcpyHostToDevice, s);
-    cudaMemsetAsync(b->d_bar, 0, 4 * sizeof(unsigned), s);
+    cudaMemsetAsync(b->d_bar, 0, 8 * sizeof(unsigned), s);
     cudaMemsetAsync(b->d_err, 0, sizeof(int), s);
+    b->wait_ns = BATCH_WAIT_FLOOR_NS + BATCH_WAIT_NS_PER_PRODUCT * (unsigned long long)total_prods;
+    cudaMemcpyAsync(b->d_bar + 4, &b->wait_ns, sizeof(unsigned long long), cudaMemcpyHostToDevice, s);
     // co-resident grid
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
     {
@@ -1024,8 +1048,10 @@ extern "C" int tsg_batch_sync(tsg_batch *b, long long *total_tiles, long long *t
                              ctx->stream));
     TSG_CUDA(cudaMemcpyAsync(&err, b->d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     TSG_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (err == TSG_ERR_OVERFLOW)
+        return tsg_set_error(TSG_ERR_OVERFLOW, "a numeric accumulator of the batch overflowed");
     if (err)
-        return tsg_set_error(TSG_ERR_TIMEOUT, "batch grid barrier gave up waiting");
+        return tsg_set_error(TSG_ERR_TIMEOUT, "batch grid barrier gave up waiting (bound %.3f s)", b->wait_ns * 1e-9);
     long long tt = 0, tn = 0;
     for (int p = 0; p < b->count; p++)
     {
@@ -1038,6 +1064,18 @@ extern "C" int tsg_batch_sync(tsg_batch *b, long long *total_tiles, long long *t
         *total_tiles = tt;
     if (total_nnz)
         *total_nnz = tn;
+    return TSG_OK;
+}
+
+extern "C" int tsg_batch_set_wait_limit(tsg_batch *b, double seconds)
+{
+    if (!b || !(seconds >= 0.0) || seconds > 1e6)
+        return tsg_set_error(TSG_ERR_INVALID, "bad batch wait limit");
+    tsg_context *ctx = b->ctx;
+    b->wait_ns = (unsigned long long)(seconds * 1e9);
+    TSG_CUDA(cudaMemcpyAsync(b->d_bar + 4, &b->wait_ns, sizeof(unsigned long long), cudaMemcpyHostToDevice,
+                             ctx->stream));
+    TSG_CUDA(cudaStreamSynchronize(ctx->stream));
     return TSG_OK;
 }
 

@@ -41,7 +41,8 @@ struct ProdView
     unsigned char *C_Ptr, *C_Colb;
     double *C_Val;
     int numC;
-    int padded; // every array allocated by tsg_alloc (16-byte aligned, 16 bytes of slack at the end)
+    int padded;  // every array allocated by tsg_alloc (16-byte aligned, 16 bytes of slack at the end)
+    int *status; // device status word for errors found inside a kernel (or null)
 };
 
 // ---------------------------------------------------------------------------
@@ -1103,15 +1104,23 @@ __device__ __forceinline__ void step3_spa_segment(const ProdView &P, SpaSmem &S,
         const long long tt = (long long)(t0 + jl) * TSG_BS + rr;
         int p = P.C_tnnz[t0 + jl] + P.C_Ptr[tt];
         int q = S.rstart[rr] + (int)(cmw >> 16);
+        bool over = false;
         while (mk)
         {
             const int bit = 31 - __clz(mk);
             P.C_Colb[p] = (unsigned char)(15 - bit);
-            P.C_Val[p] = q < SPA_CAP ? S.acc[q] : 0.0;
+            if (q < SPA_CAP)
+                P.C_Val[p] = S.acc[q];
+            else
+                over = true;
             p++;
             q++;
             mk ^= 1u << bit;
         }
+        // segments are cut to hold at most SPA_CAP values; a value past the
+        // accumulator is reported, not written as a silent zero
+        if (over && P.status)
+            atomicExch(P.status, TSG_ERR_OVERFLOW);
     }
 }
 

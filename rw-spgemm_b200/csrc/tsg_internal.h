@@ -27,7 +27,12 @@ struct tsg_context
     cudaStream_t copy_stream; // device-to-host copies overlapping compute (created on first use)
     cudaEvent_t copy_ev;      // orders a chunk's copy after its fill
     int *d_status;            // device error word kernels set (TSG_ERR_TIMEOUT, TSG_ERR_OVERFLOW), 0 when clear
+    long long allocs;         // device allocations tsg_alloc made on the context
 };
+
+// Looks up the no-alloc conversion's scratch address on a device (that
+// device current); run at context creation.
+int tsg_noalloc_prepare(int device);
 
 // Reads and clears the context's device error word (synchronises the
 // context's stream); returns TSG_OK or the code a kernel recorded.
@@ -86,6 +91,7 @@ static inline int tsg_alloc(tsg_context *ctx, T **p, size_t count)
     if (count == 0)
         count = 1;
     const size_t bytes = ((count * sizeof(T) + 15) & ~(size_t)15) + 16;
+    ctx->allocs++;
     cudaError_t e = cudaMallocAsync((void **)p, bytes, ctx->stream);
     if (e != cudaSuccess)
     {

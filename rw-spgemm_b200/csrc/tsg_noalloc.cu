@@ -19,9 +19,10 @@
 //    thread of the process: two calls that can run at the same time on one
 //    device (different streams without an event between them, or different
 //    host threads) race on it and must be serialised by the caller;
-//  - the first call on a device looks up the scratch's address with
-//    cudaGetSymbolAddress (once per device, with that device current); make
-//    that first call before any stream capture.
+//  - the scratch's address is looked up with cudaGetSymbolAddress (with the
+//    device current) when a context is created on the device
+//    (tsg_noalloc_prepare), so the conversion itself makes no runtime call
+//    but its launches and may be captured in a graph.
 #include <mutex>
 
 #include "tsg_internal.h"
@@ -144,16 +145,18 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_na_apply(int *rowptr, int m, c
     }
 }
 
-// Scratch address per device, looked up once with that device current.
+// Scratch address per device, looked up with that device current: at every
+// context creation (refresh: a cudaDeviceReset since the last lookup moves
+// it), and on a conversion only if no context ever looked it up.
 static std::mutex g_na_mutex;
 static long long *g_na_scratch[NA_MAX_DEVICES];
 
-static int na_scratch(int device, long long **out)
+static int na_lookup(int device, bool refresh)
 {
     if (device < 0 || device >= NA_MAX_DEVICES)
         return tsg_set_error(TSG_ERR_INVALID, "tsg_tiled_to_csr_noalloc: device %d out of range", device);
     std::lock_guard<std::mutex> lock(g_na_mutex);
-    if (!g_na_scratch[device])
+    if (refresh || !g_na_scratch[device])
     {
         int cur = -1;
         TSG_CUDA(cudaGetDevice(&cur));
@@ -168,6 +171,14 @@ static int na_scratch(int device, long long **out)
                                  cudaGetErrorString(e));
         g_na_scratch[device] = ptr;
     }
+    return TSG_OK;
+}
+
+int tsg_noalloc_prepare(int device) { return na_lookup(device, true); }
+
+static int na_scratch(int device, long long **out)
+{
+    TSG_TRY(na_lookup(device, false));
     *out = g_na_scratch[device];
     return TSG_OK;
 }

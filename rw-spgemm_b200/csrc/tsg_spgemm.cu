@@ -323,6 +323,7 @@ static ProdView make_view(const tsg_tiled *A, const tsg_tiled *B, tsg_tiled *C)
     for (const void *p : bases)
         aligned = aligned && ((uintptr_t)p & 15) == 0;
     P.padded = !A->_alloc && !B->_alloc && !C->_alloc && aligned;
+    P.status = nullptr;
     return P;
 }
 
@@ -387,8 +388,10 @@ static int launch_step2_spa(tsg_context *ctx, const ProdView &P, const int *d_wi
 }
 
 template <bool FLAT, bool RANGED>
-static int launch_step3_spa(tsg_context *ctx, const ProdView &P, const int *d_kind, int row0, int row1)
+static int launch_step3_spa(tsg_context *ctx, const ProdView &P0, const int *d_kind, int row0, int row1)
 {
+    ProdView P = P0;
+    P.status = ctx->d_status;
     unsigned *ctr = nullptr, grid = 0;
     const int smem = (int)sizeof(SpaSmem);
     TSG_TRY(spa_grid(ctx, k_step3_spa<FLAT, RANGED>, smem, &grid));
@@ -403,8 +406,10 @@ static int launch_step3_spa(tsg_context *ctx, const ProdView &P, const int *d_ki
 // the staged numeric step for tile rows [row0, row1), then the SPA kernel
 // for the rows it left
 template <bool RANGED>
-static int launch_step3_stg(tsg_context *ctx, const ProdView &P, const int *d_kind, int row0, int row1)
+static int launch_step3_stg(tsg_context *ctx, const ProdView &P0, const int *d_kind, int row0, int row1)
 {
+    ProdView P = P0;
+    P.status = ctx->d_status;
     unsigned *ctr = nullptr, grid = 0;
     int *left = nullptr;
     const int smem = (int)sizeof(StgSmem);
@@ -665,7 +670,7 @@ int tsg_spgemm_to_host(tsg_context *ctx, const tsg_tiled *A, const tsg_tiled *B,
     const int m = C.m, tilem = C.tilem;
     if (status == TSG_OK)
     {
-        *nnzC_out = (int)R.nnzC;
+        *nnzC_out = R.nnzC > INT_MAX ? INT_MAX : (int)R.nnzC; // the scan rejects more than 32-bit offsets
         if (R.nnzC > nnz_cap)
             status = tsg_set_error(TSG_ERR_OVERFLOW, "C has %lld nonzeros; the output buffers hold %lld", R.nnzC,
                                    nnz_cap);

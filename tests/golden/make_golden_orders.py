@@ -3,7 +3,8 @@
 native_degree, native_rcm), run in this container on small Matrix Market files
 written from the library's generators.
 
-Run where the reference tree exists:  python tests/golden/make_golden_orders.py
+Run where the reference tree exists:
+    python tests/golden/make_golden_orders.py <reference tree>
 """
 from __future__ import annotations
 
@@ -15,7 +16,11 @@ from pathlib import Path
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
-REF_UTILS = Path("/root/reference/reorder_algorithm/common/order_utils.py")
+if len(sys.argv) != 2:
+    sys.exit("usage: make_golden_orders.py <reference tree (holds reorder_algorithm/common/order_utils.py)>")
+REF_UTILS = Path(sys.argv[1]) / "reorder_algorithm" / "common" / "order_utils.py"
+if not REF_UTILS.is_file():
+    sys.exit(f"{REF_UTILS} not found")
 sys.path.insert(0, str(HERE.parent))
 from conftest import load_package  # noqa: E402
 

@@ -96,3 +96,30 @@ def test_batch_phase_times(tsg, ctx, gen):
     assert len(ph) == 7 and all(v >= 0.0 for v in ph.values())
     assert 0.0 < sum(ph.values()) < 10_000.0
     batch.close()
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_batch_barrier_bound_gives_up_and_the_batch_recovers(tsg, ctx, oracle, gen, graph):
+    """A grid-barrier wait bound of zero makes the waiting blocks give up: the
+    run reports TSG_ERR_TIMEOUT through sync (no GPU fault, the context stays
+    usable), and the same batch with a normal bound then computes every
+    product exactly."""
+    mats = _pairs(gen)[:8]
+    pairs = [(_tiled(tsg, ctx, a, tsg.TSG_TILED_PACKED_COL), _tiled(tsg, ctx, b, tsg.TSG_TILED_CSC_VIEW))
+             for a, b in mats]
+    batch = tsg.Batch(ctx, pairs, "spa", 8, 512, graph=graph)
+    batch.set_wait_limit(0.0)
+    batch.run()
+    with pytest.raises(tsg.TsgError) as ei:
+        batch.sync()
+    assert ei.value.status == -7  # TSG_ERR_TIMEOUT
+    batch.set_wait_limit(10.0)
+    batch.run()
+    batch.sync()
+    for p, (a, b) in enumerate(mats):
+        got = batch.product(p).download()
+        want = oracle.spgemm_tiled(oracle.csr2tile_row_major(a), oracle.csr2tile_col_major(b))
+        for k in C_KEYS:
+            np.testing.assert_array_equal(np.asarray(got[k]).view(np.uint8), np.asarray(want[k]).view(np.uint8),
+                                          err_msg=f"product {p} {k}")
+    batch.close()

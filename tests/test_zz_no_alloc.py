@@ -1,9 +1,10 @@
 """tsg_tiled_to_csr_noalloc: tiles -> CSR with its scan scratch in a fixed
 device array (no allocation), called through the C ABI.  Its output must
 equal tsg_tiled_to_csr's on the same tiled C, on two calls in a row (the
-second reuses the scratch the first wrote), and a C larger than the scratch
-covers must be rejected before any work.  The file name keeps it last in
-collection; it also passes run alone."""
+second reuses the scratch the first wrote), the context's allocation count
+must not move across a call, an empty C must give rowptr = [0], and a C
+larger than the scratch covers must be rejected before any work.  The file
+name keeps it last in collection; it also passes run alone."""
 import ctypes
 
 import numpy as np
@@ -19,8 +20,8 @@ def _noalloc(tsg, ctx, C, rp, ci, v):
     f = L.tsg_tiled_to_csr_noalloc
     f.argtypes = [ctypes.c_void_p, ctypes.POINTER(tsg.TsgTiled), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
     f.restype = ctypes.c_int
-    return f(ctx.handle, ctypes.byref(C.s), ctypes.c_void_p(rp.data_ptr()), ctypes.c_void_p(ci.data_ptr()),
-             ctypes.c_void_p(v.data_ptr()))
+    ptr = lambda t: ctypes.c_void_p(t.data_ptr() if t is not None else None)  # noqa: E731
+    return f(ctx.handle, ctypes.byref(C.s), ptr(rp), ptr(ci), ptr(v))
 
 
 def _product(tsg, ctx, gen, case):
@@ -28,6 +29,8 @@ def _product(tsg, ctx, gen, case):
         A = gen.random_poisson(3000, None, 6.0, seed=11)
     elif case == "stencil_multi_block":
         A = gen.stencil_27pt_3d(40)  # 64,000 rows: 8 scan blocks
+    elif case == "million_rows":
+        A = gen.banded(1000000, 1, seed=6)  # 123 scan blocks: the partial scan spans several warps
     else:
         A = gen.banded(100003, 9, seed=4)  # ragged last block and tile row
     return _tiled_square(tsg, ctx, A)
@@ -44,7 +47,7 @@ def _tiled_square(tsg, ctx, A):
     return C
 
 
-@pytest.mark.parametrize("case", ["poisson_small", "stencil_multi_block", "banded_ragged"])
+@pytest.mark.parametrize("case", ["poisson_small", "stencil_multi_block", "banded_ragged", "million_rows"])
 def test_noalloc_matches_tiled_to_csr_twice(tsg, ctx, gen, case):
     import torch
     C = _product(tsg, ctx, gen, case)
@@ -55,7 +58,10 @@ def test_noalloc_matches_tiled_to_csr_twice(tsg, ctx, gen, case):
         rp = torch.full((m + 1,), -7, dtype=torch.int32, device=d)
         ci = torch.full((max(nnz, 1),), -7, dtype=torch.int32, device=d)
         v = torch.full((max(nnz, 1),), float("nan"), dtype=torch.float64, device=d)
+        torch.cuda.synchronize()
+        before = ctx.allocations()
         assert _noalloc(tsg, ctx, C, rp, ci, v) == 0, tsg.lib().tsg_last_error()
+        assert ctx.allocations() == before, "the no-alloc conversion allocated"
         ctx.synchronize()
         # integer structure bit-exact; values are copies (tolerance 0)
         assert torch.equal(rp, rp0), f"rowptr differs on call {call}"
@@ -77,3 +83,20 @@ def test_noalloc_rejects_more_rows_than_the_scratch_covers(tsg, ctx):
     st = _noalloc(tsg, ctx, C, rp, rp, rp)
     assert st == -1
     assert b"scratch" in tsg.lib().tsg_last_error()
+
+
+def test_noalloc_empty_c(tsg, ctx):
+    import torch
+    empty = tsg.TsgTiled()
+    empty.m = 0
+    empty.n = 5
+    empty.tilem = 0
+    empty.tilen = 1
+    d = torch.device("cuda", torch.cuda.current_device())
+    rp = torch.full((1,), -7, dtype=torch.int32, device=d)
+    C = type("T", (), {"s": empty})()
+    before = ctx.allocations()
+    assert _noalloc(tsg, ctx, C, rp, None, None) == 0, tsg.lib().tsg_last_error()
+    assert ctx.allocations() == before
+    ctx.synchronize()
+    assert int(rp[0]) == 0
