@@ -12,8 +12,13 @@ events.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Under torchrun each rank computes its own product (independent replicas: the
-product has no exchange step); value = products of all ranks / max rank time.
+Under torchrun each rank computes its own stencil product (independent
+replicas: the product has no exchange step); value = products of all ranks /
+max rank time.  The R-MAT scale-20 products (C ~ 9.7e9 nonzeros) run as one
+row-partitioned product over the ranks instead ("rmat20_sharded"): each rank
+owns a range of A's tile rows cut by predicted products, holds all of B, and
+computes its range in row blocks; one all-gather of (rows, nnz) places the
+pieces.
 """
 from __future__ import annotations
 
@@ -152,6 +157,17 @@ def max_over_ranks(value, dist=None, device=None):
     return float(t.item())
 
 
+def sum_over_ranks(value, dist=None, device=None):
+    """The sum of every rank's value; the value itself without a process
+    group."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
 def replica_gflops(products_per_rank, world, ms_per_step):
     """Whole-job GFLOP/s of `world` independent replicas, each computing
     products_per_rank scalar products per step (2 flops each)."""
@@ -185,9 +201,34 @@ def step3_algorithmic_bytes(tA, tB, numC, nnzC):
 
 
 # ---------------------------------------------------------------------------
-# CPU reference arm: the reference's own spgemm_cpu (serial, FP64) on a
-# bounded row sample of the same workload.
+# CPU reference arm: the reference's own CPU SpGEMM codes on a bounded row
+# sample of the same workload -- spgemm_cpu (serial, FP64 numeric, the
+# tiled method) and spgemm_spa (OpenMP over rows on all host threads, C's
+# structure by a bitmap accumulator) -- the faster of the two is the baseline.
 # ---------------------------------------------------------------------------
+def host_cpu():
+    """(logical CPUs usable here, CPU model)."""
+    try:
+        usable = len(os.sched_getaffinity(0))
+    except AttributeError:
+        usable = os.cpu_count() or 1
+    model = "unknown"
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return usable, model
+
+
+def time_spa_step(oracle, sample, mat):
+    t0 = time.perf_counter()
+    oracle.ref_spgemm_spa(sample, mat)
+    return time.perf_counter() - t0
+
+
 def row_sample(mat, frac_den):
     m, n, rp, ci, v = mat
     rows = max(16, (m // frac_den) // 16 * 16)
@@ -210,11 +251,20 @@ def run_cpu_reference(args, gen, world, rank):
     sample = row_sample(mat, 8)
     prods = int(oracle.count_products(sample, mat))
     kind = "reference" if oracle.ref_available() else "port"
+    usable, model = host_cpu()
+    spa = None
     if kind == "reference":
         B_tiles = oracle.ref_csr2tile_col_major(mat)
         step = lambda: cpu_reference_step(oracle, sample, B_tiles)  # noqa: E731
         cores = 1
         what = "reference spgemm_cpu (src/spgemm-cpu.h:369, serial FP64, unpacked A bytes)"
+        omp = int(oracle.rlib().ref_omp_max_threads())
+        time_spa_step(oracle, sample, mat)  # warm-up (thread pool, pages)
+        ts = [time_spa_step(oracle, sample, mat) for _ in range(max(1, args.steps))]
+        spa = {"seconds_per_step": float(np.mean(ts)), "threads": omp,
+               "gflops_equiv": 2.0 * prods / float(np.mean(ts)) / 1e9,
+               "what": "reference spgemm_spa (src/spgemm_serialref_spa_new.h:7), both passes (row counts, "
+                       "columns), OpenMP on %d threads; structure only, no values" % omp}
     else:
         nthreads = os.cpu_count() or 1
 
@@ -236,9 +286,23 @@ def run_cpu_reference(args, gen, world, rank):
         os.close(devnull)
     t = float(np.mean(times))
     gflops = 2.0 * prods / t / 1e9
-    return {"value": gflops, "unit": "GFLOP/s", "cores": cores, "kind": kind,
-            "sample": f"rows 0..{sample[0]} of the workload's A (1/8 of its rows) times the full A; "
-                      f"{prods} products; {what}", "seconds_per_step": t}
+    out = {"value": gflops, "unit": "GFLOP/s", "cores": cores, "kind": kind,
+           "sample": f"rows 0..{sample[0]} of the workload's A (1/8 of its rows) times the full A; "
+                     f"{prods} products; {what}", "seconds_per_step": t,
+           "host": {"nproc": usable, "cpu_model": model}}
+    if spa:
+        out["spgemm_cpu_serial"] = {"gflops": round(gflops, 4), "seconds_per_step": round(t, 4)}
+        out["spgemm_spa_all_cores"] = {"gflops_equiv": round(spa["gflops_equiv"], 4),
+                                       "seconds_per_step": round(spa["seconds_per_step"], 4),
+                                       "omp_threads": spa["threads"], "what": spa["what"]}
+        out["host"]["omp_max_threads"] = spa["threads"]
+        if spa["gflops_equiv"] > gflops:
+            # the faster reference code is the baseline (rate: 2 x scalar products / s)
+            out.update(value=spa["gflops_equiv"], cores=spa["threads"], seconds_per_step=spa["seconds_per_step"],
+                       sample=f"rows 0..{sample[0]} of the workload's A (1/8 of its rows) times the full A; "
+                              f"{prods} products; {spa['what']}; value = 2 x products / s (GFLOP/s-equivalent), "
+                              f"faster than the serial numeric spgemm_cpu ({gflops:.4f} GFLOP/s)")
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -249,30 +313,51 @@ def run_batched(args, tsg, gen, ctx, steps):
     import torch
     at = _load("rw_spgemm_b200.autotune", PKG_DIR / "autotune.py")
     mats = gen.batched_products(args.batch_count, seed=0)
+    classes = gen.batched_product_classes(args.batch_count, seed=0)
     pairs = [(tsg.csr_host_to_tiled(ctx, a, tsg.TSG_TILED_CSC_VIEW), tsg.csr_host_to_tiled(ctx, b, tsg.TSG_TILED_CSC_VIEW))
              for a, b in mats]
-    total_products = sum(tsg.product_bounds(ctx, A, B)[0] for A, B in pairs)
+    prods_each = [tsg.product_bounds(ctx, A, B)[0] for A, B in pairs]
+    total_products = sum(prods_each)
     del mats
     tuner = at.Autotuner()
     choice = tuner.tune_batch(ctx, pairs, reps=1, use_cache=False)
     tune_ms = at.summarize(tuner.last_timings)
-    batch = tsg.Batch(ctx, pairs, *choice, graph=True)
     stream = torch.cuda.current_stream()
-    batch.run()
-    batch.sync()
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
-    ctx.synchronize()
-    ev[0].record(stream)
-    for _ in range(steps):
-        batch.run()
-    ev[1].record(stream)
-    ev[1].synchronize()
-    ms_batched = ev[0].elapsed_time(ev[1]) / steps
+
+    def timed(sub):
+        """(ms per run of a graph-captured batch over sub, batch) -- batch
+        left open, its last run finished."""
+        b = at.make_batch(ctx, sub, choice, graph=True)
+        b.run()
+        b.sync()
+        ctx.synchronize()
+        ev[0].record(stream)
+        for _ in range(steps):
+            b.run()
+        ev[1].record(stream)
+        ev[1].synchronize()
+        return ev[0].elapsed_time(ev[1]) / steps, b
+
+    ms_batched, batch = timed(pairs)
     tiles, nnz = batch.sync()
     info = batch.info()
+    phases = batch.phase_ms()
     batch.close()
+    # the same batch split by product class, each class a batch of its own
+    per_class = {}
+    for cl in sorted(set(classes)):
+        idx = [i for i, c in enumerate(classes) if c == cl]
+        ms_c, b = timed([pairs[i] for i in idx])
+        b.sync()
+        ph = b.phase_ms()
+        b.close()
+        pc = sum(prods_each[i] for i in idx)
+        per_class[cl] = {"products": int(pc), "count": len(idx), "ms": round(ms_c, 3),
+                         "gflops": round(2.0 * pc / (ms_c * 1e-3) / 1e9, 2),
+                         "phase_ms": ph}
     # plain path: one tsg_spgemm per product (its own launches, read-backs and allocations)
-    ctx.set_schedule(*choice)
+    ctx.set_schedule(*at.normalize(choice))
     for A, B in pairs[:8]:
         C, _ = tsg.spgemm(ctx, A, B)
         C.free()
@@ -295,7 +380,8 @@ def run_batched(args, tsg, gen, ctx, steps):
             "products": int(total_products), "C_tiles": int(tiles), "C_nnz": int(nnz),
             "gflops_batched": round(gf_b, 2), "gflops_plain": round(gf_p, 2), "speedup_vs_plain": round(gf_b / gf_p, 3),
             "ms_batched": round(ms_batched, 3), "ms_plain": round(ms_plain, 3),
-            "schedule": list(choice), "autotune_ms": tune_ms, "graph": info["graph"], "grid": info["grid"],
+            "phase_ms": phases, "per_class": per_class,
+            "schedule": at.label(choice), "autotune_ms": tune_ms, "graph": info["graph"], "grid": info["grid"],
             "arena_gb": round(info["arena_bytes"] / 1e9, 3)}
 
 
@@ -330,7 +416,7 @@ def run_served(args, tsg, gen, device, deliver="device", n_jobs=None, half_capac
     result crosses the bus)."""
     srv_mod = _load("rw_spgemm_b200.serve", PKG_DIR / "serve.py")
     pool = gen.served_pool()
-    srv = srv_mod.SpGEMMServer(device, mem_cap=40 << 30, slots=2, max_batch=64, schedule=tuple(args.served_schedule),
+    srv = srv_mod.SpGEMMServer(device, mem_cap=40 << 30, slots=2, max_batch=64, schedule=args.served_schedule,
                                deliver=deliver)
     for key, m in pool.items():
         srv.register(key, m)
@@ -339,9 +425,10 @@ def run_served(args, tsg, gen, device, deliver="device", n_jobs=None, half_capac
     for kind, a, b in gen.served_jobs(pool, n_jobs or args.served_jobs, seed=1):
         B = gen.transpose(pool[a]) if kind == "AAT" else pool[b]
         jobs.append((kind, a, b, gen.products(pool[a], B)))
-    # warm the operand cache and the kernels with one pass of distinct jobs
+    # warm the operand cache, the kernels and the tuned schedules with a pass
+    # over the first jobs
     srv.start()
-    for f in [srv.submit(k, a, b) for k, a, b, _ in jobs[:64]]:
+    for f in [srv.submit(k, a, b) for k, a, b, _ in jobs[:256]]:
         f.result(timeout=600)
     st, wall = _served_stream(srv, jobs, args.served_rate, rng)
     prods = sum(j[3] for j in jobs)
@@ -351,8 +438,8 @@ def run_served(args, tsg, gen, device, deliver="device", n_jobs=None, half_capac
            "jobs": st["jobs"], "jobs_per_s": round(st["jobs_per_s"], 1), "p50_ms": round(st["p50_ms"], 3),
            "p99_ms": round(st["p99_ms"], 3), "gflops": round(2.0 * prods / wall / 1e9, 2),
            "batches": st["batches"], "mean_batch": round(st["mean_batch"], 2), "rejected": st["rejected"],
-           "operand_cache": st["operand_cache"], "schedule": list(args.served_schedule), "mem_cap_gb": 40,
-           "deliver": deliver}
+           "operand_cache": st["operand_cache"], "mem_cap_gb": 40, "deliver": deliver,
+           "schedule": st["tuned"] if args.served_schedule == "auto" else "-".join(map(str, args.served_schedule))}
     if not half_capacity:
         srv.close()
         return out
@@ -365,6 +452,50 @@ def run_served(args, tsg, gen, device, deliver="device", n_jobs=None, half_capac
                                "p99_ms": round(st2["p99_ms"], 3)}
     srv.close()
     return out
+
+
+def run_served_plain(args, tsg, gen, ctx, n_jobs=None):
+    """The served job stream run on the plain path instead: one tsg_spgemm
+    per job (its own launches, host read-backs and allocations) and its
+    conversion to device CSR, jobs back to back with operands resident --
+    the plain path's best throughput on the same mix (no arrival gaps)."""
+    import torch
+    pool = gen.served_pool()
+    jobs = gen.served_jobs(pool, n_jobs or args.served_jobs, seed=1)
+    tiles, prods = {}, 0
+
+    def operand(key, mat):
+        if key not in tiles:
+            tiles[key] = tsg.csr_host_to_tiled(ctx, mat, tsg.TSG_TILED_CSC_VIEW)
+        return tiles[key]
+
+    work = []
+    for kind, a, b in jobs:
+        Bkey = (a, "T") if kind == "AAT" else b
+        Bm = gen.transpose(pool[a]) if kind == "AAT" and Bkey not in tiles else pool.get(b)
+        A, B = operand(a, pool[a]), operand(Bkey, Bm)
+        prods += tsg.product_bounds(ctx, A, B)[0]
+        work.append((A, B))
+
+    def one(A, B):
+        C, _ = tsg.spgemm(ctx, A, B)
+        out = tsg.tiled_to_csr(ctx, C)
+        C.free()
+        return out
+
+    for A, B in work[:64]:
+        one(A, B)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for A, B in work:
+        one(A, B)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    for t in tiles.values():
+        t.free()
+    return {"what": "same job mix, one tsg_spgemm + tsg_tiled_to_csr per job, back to back, operands resident, "
+                    "results left on the device", "jobs": len(work), "jobs_per_s": round(len(work) / wall, 1),
+            "ms_per_job": round(wall * 1e3 / len(work), 3), "gflops": round(2.0 * prods / wall / 1e9, 2)}
 
 
 # ---------------------------------------------------------------------------
@@ -476,25 +607,35 @@ def run_hyper(args, tsg, gen, ctx, reps=3):
             "ms_steps_1_3": round(best, 4), "gflops": round(2.0 * prods / (best * 1e-3) / 1e9, 2)}
 
 
-def run_rmat20(args, tsg, gen, ctx, budget=1.5e9):
+def run_rmat20(args, tsg, gen, ctx, budget=1.5e9, rank=0, world=1, dist=None, device=None):
     """R-MAT scale 20 (edge factor 16, a,b,c,d = .57,.19,.19,.05, duplicates
-    merged, values U(-1,1)): C = A*A and C = A*A^T.  C (~9.5e9 nonzeros) does
+    merged, values U(-1,1)): C = A*A and C = A*A^T.  C (~9.7e9 nonzeros) does
     not fit one GPU, so A goes in blocks of tile rows holding at most `budget`
     scalar products each; every block is converted, multiplied (steps 1-3 on
-    the resident B) and its C freed.  GFLOP/s over the steps-1-3 time of all
-    blocks; wall time includes the block conversions."""
+    the resident B) and its C freed.  With world > 1 the product is
+    row-partitioned: this rank takes its tile-row range (shard.plan) and the
+    time is the slowest rank's.  GFLOP/s over the steps-1-3 time of all
+    blocks; wall time includes the block conversions; hbm_frac = compulsory
+    tile bytes of every block (A block and B read, C written) / time / the
+    measured copy bandwidth."""
     import torch
     blocks_mod = _load("rw_spgemm_b200.blocks", PKG_DIR / "blocks.py")
+    shard = _load("rw_spgemm_b200.shard", PKG_DIR / "shard.py")
+    peak, _ = measured_peak_hbm()
     A = gen.rmat(20, 16, seed=1)
     m, n, rp, ci, v = A
     out = {"workload": "R-MAT scale 20, edge factor 16 (n=1,048,576), FP64 U(-1,1); A in row blocks of <= %.1e "
                        "products" % budget}
+    if world > 1:
+        out["partition"] = (f"{world} ranks, consecutive tile-row ranges of A cut by predicted products, B "
+                            "replicated per rank; time = slowest rank")
     for label, B in (("A*A", A), ("A*A^T", gen.transpose(A))):
         TB = tsg.csr_host_to_tiled(ctx, B, tsg.TSG_TILED_CSC_VIEW)
-        tileprod = blocks_mod.tile_row_products(A, B)
-        blocks = blocks_mod.row_blocks(tileprod, budget)
+        tileprod, ranges = shard.plan(A, B, world)
+        r0, r1 = ranges[rank]
+        blocks = [(r0 + b0, r0 + b1) for b0, b1 in blocks_mod.row_blocks(tileprod[r0:r1], budget)]
         ctx.set_timing(True)
-        steps_ms, prods, nnz, tiles = 0.0, 0, 0, 0
+        steps_ms, nnz, tiles, comp = 0.0, 0, 0, 0
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for b0, b1 in blocks:
@@ -503,16 +644,32 @@ def run_rmat20(args, tsg, gen, ctx, budget=1.5e9):
             steps_ms += info["ms_total"]
             nnz += info["nnz_C"]
             tiles += info["numtile_C"]
+            comp += compulsory_bytes(TA, TB, info["numtile_C"], info["nnz_C"])
             C.free()
             TA.free()
         torch.cuda.synchronize()
         wall = time.perf_counter() - t0
         ctx.set_timing(False)
-        prods = int(tileprod.sum())
         TB.free()
-        out[label] = {"products": prods, "nnz_C": int(nnz), "tiles_C": int(tiles), "blocks": len(blocks),
-                      "ms_steps_1_3": round(steps_ms, 1), "gflops": round(2.0 * prods / (steps_ms * 1e-3) / 1e9, 2),
-                      "wall_s": round(wall, 2)}
+        rows = min(r1 * 16, m) - min(r0 * 16, m)
+        mine = {"tile_rows": [int(r0), int(r1)], "products": int(tileprod[r0:r1].sum()), "blocks": len(blocks),
+                "ms_steps_1_3": round(steps_ms, 1)}
+        if world > 1:
+            ms = max_over_ranks(steps_ms, dist, device)
+            wall = max_over_ranks(wall, dist, device)
+            comp = sum_over_ranks(float(comp), dist, device)
+            _, _, nnz_total, per = shard.global_offsets(rows, nnz, dist, device)
+        else:
+            ms, nnz_total, per = steps_ms, nnz, [(rows, nnz)]
+        prods = int(tileprod.sum())
+        out[label] = {"products": prods, "nnz_C": int(nnz_total), "tiles_C_this_rank": int(tiles),
+                      "blocks_this_rank": len(blocks), "ms_steps_1_3": round(ms, 1),
+                      "gflops": round(2.0 * prods / (ms * 1e-3) / 1e9, 2), "wall_s": round(wall, 2),
+                      "compulsory_bytes": int(comp),
+                      "hbm_frac": round(comp / (ms * 1e-3) / 1e9 / (peak * world), 4)}
+        if world > 1:
+            out[label]["this_rank"] = mine
+            out[label]["rows_nnz_per_rank"] = per
     return out
 
 
@@ -642,25 +799,32 @@ def run_ours(args, tsg, gen, world, rank, local):
         e2e_t = float(np.mean(e2e_ms))
         h2d = rp.nbytes + ci.nbytes + v.nbytes
         d2h = Cc[2].nbytes + Cc[3].nbytes + Cc[4].nbytes
+    # sections beyond the headline run on one GPU; with several ranks only the
+    # row-partitioned R-MAT product runs (the stencil line above is replicas)
+    sections = args.sections if world == 1 else args.sections & {"rmat20"}
     cusparse = None
-    if world == 1 and "cusparse" in args.sections:
+    if "cusparse" in sections:
         cusparse = run_cusparse(args, mat, prods)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = run_cpu_reference(argparse.Namespace(warmup=0, steps=1), gen, 1, 0)
     batched = served = None
     A.free()
-    if "batched" in args.sections:
+    if "batched" in sections:
         batched = run_batched(args, tsg, gen, ctx, max(2, min(args.steps, 5)))
     served_host = None
-    if "served" in args.sections:
+    if "served" in sections:
         served = run_served(args, tsg, gen, local, deliver="device")
+        plain = run_served_plain(args, tsg, gen, ctx)
+        served["plain_path"] = plain
+        served["served_vs_plain"] = round(served["jobs_per_s"] / plain["jobs_per_s"], 3)
         served_host = run_served(args, tsg, gen, local, deliver="host", n_jobs=min(args.served_jobs, 600),
                                  half_capacity=False)
-    selector = run_selector(args, tsg, gen, ctx) if "selector" in args.sections else None
-    orderings = run_orderings(args, tsg, gen, ctx) if "orderings" in args.sections else None
-    hyper = run_hyper(args, tsg, gen, ctx) if "hyper" in args.sections else None
-    rmat20 = run_rmat20(args, tsg, gen, ctx) if "rmat20" in args.sections else None
+    selector = run_selector(args, tsg, gen, ctx) if "selector" in sections else None
+    orderings = run_orderings(args, tsg, gen, ctx) if "orderings" in sections else None
+    hyper = run_hyper(args, tsg, gen, ctx) if "hyper" in sections else None
+    rmat20 = (run_rmat20(args, tsg, gen, ctx, rank=rank, world=world, dist=dist, device=dev)
+              if "rmat20" in sections else None)
     out = {
         "metric": METRIC, "value": round(value, 3), "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,
@@ -676,7 +840,7 @@ def run_ours(args, tsg, gen, world, rank, local):
         "hbm_frac": round(comp / (ms_per_step * 1e-3) / 1e9 / peak, 4),
         "compulsory_bytes": comp,
         "step_ms": {k: round(float(np.mean([i[k] for i in infos])), 4) for k in ("ms_step1", "ms_step2", "ms_step3")},
-        "roofline": {"bound": "hbm", "kernel": {"tiles": "k_step3", "elems": "k_step3_elems", "rows": "k_step3_rows", "spa": "k_step3_spa"}[args.sched] + " (numeric)", "achieved": round(achieved, 2),
+        "roofline": {"bound": "hbm", "kernel": infos[-1]["step3_name"] + " (numeric step)", "achieved": round(achieved, 2),
                      "peak": peak, "peak_source": peak_src, "unit": "GB/s", "frac": round(achieved / peak, 4),
                      "algorithmic_bytes": alg3, "traffic": profiled_traffic("stencil27_64", args.sched)},
         "e2e": {"value": round(2.0 * prods / (e2e_t * 1e-3) / 1e9, 3), "unit": "GFLOP/s", "ms": round(e2e_t, 3),
@@ -701,7 +865,13 @@ def run_ours(args, tsg, gen, world, rank, local):
     if hyper:
         out["hypersparse"] = hyper
     if rmat20:
-        out["rmat20"] = rmat20
+        out["rmat20_sharded" if world > 1 else "rmat20"] = rmat20
+        # the second benchmark configuration beside the headline
+        out["config2"] = {"workload": "R-MAT scale 20, edge factor 16: C = A*A and C = A*A^T in row blocks" +
+                                      (f", row-partitioned over {world} ranks" if world > 1 else ""),
+                          "gflops": {k: rmat20[k]["gflops"] for k in ("A*A", "A*A^T")},
+                          "hbm_frac": {k: rmat20[k]["hbm_frac"] for k in ("A*A", "A*A^T")},
+                          "scaling": "strong" if world > 1 else None}
     if cusparse:
         out["library_reference"] = cusparse
     if rank == 0:
@@ -721,18 +891,21 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--sched", default="spa", choices=["rows", "tiles", "elems", "spa"])
-    ap.add_argument("--sections", default="plain,cusparse,batched,served,orderings,hyper,rmat20",
+    ap.add_argument("--sections", default="plain,cusparse,batched,served,orderings,hyper,rmat20,selector",
                     help="comma list: plain (always), cusparse, batched, served, orderings, hyper, rmat20, selector")
     ap.add_argument("--batch-count", type=int, default=512)
     ap.add_argument("--selector-samples", type=int, default=5000)
     ap.add_argument("--served-jobs", type=int, default=2000)
     ap.add_argument("--served-rate", type=float, default=2000.0)
-    ap.add_argument("--served-schedule", nargs=3, default=["spa", "8", "512"])
+    ap.add_argument("--served-schedule", default="auto",
+                    help='"auto" (tuned per density class) or schedule,seg,cap[,dense], e.g. spa,8,512')
     ap.add_argument("--seg", type=int, default=16)
     ap.add_argument("--cap", type=int, default=1024)
     args = ap.parse_args()
     args.sections = set(args.sections.split(","))
-    args.served_schedule = (args.served_schedule[0], int(args.served_schedule[1]), int(args.served_schedule[2]))
+    if args.served_schedule != "auto":
+        f = args.served_schedule.split(",")
+        args.served_schedule = (f[0],) + tuple(int(x) for x in f[1:])
     world, rank, local = dist_setup()
     tsg = _load("rw_spgemm_b200", PKG_DIR / "__init__.py", PKG_DIR)
     gen = _load("rw_spgemm_b200.generators", PKG_DIR / "generators.py")

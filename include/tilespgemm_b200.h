@@ -267,7 +267,18 @@ typedef struct
     long long tile_pairs; /* matched (A tile, B tile) pairs                   */
     double ms_step1, ms_step2, ms_step3, ms_total;
     int bins[4];          /* C tiles by nnz: <=32, <=224, <256, ==256         */
+    int step3_kernel;     /* numeric step that ran: TSG_STEP3_*               */
 } tsg_spgemm_info;
+
+/* tsg_spgemm_info.step3_kernel */
+#define TSG_STEP3_NONE 0   /* C has no nonzeros                               */
+#define TSG_STEP3_TILES 1  /* k_step3: half-warp per C tile                   */
+#define TSG_STEP3_ELEMS 2  /* k_step3_elems: warp per C tile, per element     */
+#define TSG_STEP3_ROWS 3   /* k_step3_rows: half-warp per run of C tiles      */
+#define TSG_STEP3_FLAT 4   /* k_step3_spa<flat>: SPA, CTA per C tile block    */
+#define TSG_STEP3_SPA 5    /* k_step3_spa: SPA, CTA per tile-row segment      */
+#define TSG_STEP3_STAGED 6 /* k_step3_stg + k_step3_rest: SPA with operands
+                            * staged in shared memory by bulk copies          */
 
 const char *tsg_status_string(int status);
 /* Message describing the last failure on the calling thread. */
@@ -301,6 +312,11 @@ int tsg_context_set_stream(tsg_context *ctx, void *cuda_stream);
  *                  TSG_SCHED_TILES. */
 #define TSG_SCHED_SPA 3
 int tsg_context_set_schedule(tsg_context *ctx, int schedule, int seg_tiles, int acc_cap);
+/* TSG_SCHED_SPA: a product whose C tiles hold at least values_per_tile
+ * values on average (nnz(C) / tiles(C), known after step 2) runs the numeric
+ * step with the tile kernel instead of the sparse accumulator; 0 restores
+ * the default (64); 257 never switches.  Results are identical either way. */
+int tsg_context_set_dense_threshold(tsg_context *ctx, int values_per_tile);
 /* 1 (default): step-1 emit and step 2 run as one row-wise pass for tile rows
  * with at most 128 C tiles (others fall back to step 2 per tile); 0: separate
  * step 2 of the schedule.  Results are identical. */
@@ -333,6 +349,13 @@ int tsg_tiled_upload_rowmajor(tsg_context *ctx, const SMatrix *host, tsg_tiled *
 int tsg_tiled_upload_colmajor(tsg_context *ctx, const SMatrix *host, tsg_tiled *out);
 
 int tsg_tiled_free(tsg_context *ctx, tsg_tiled *mat);
+/* Device bytes the library holds for a tiled matrix: every array present,
+ * as allocated (16-byte rounding plus 16 bytes of slack each); 0 for a
+ * borrowed view.  For admission control (no reference counterpart). */
+long long tsg_tiled_device_bytes(const tsg_tiled *mat);
+/* Bytes in use in the device's default stream-ordered memory pool, from
+ * which the library allocates (cudaMemPoolAttrUsedMemCurrent). */
+int tsg_context_pool_used(tsg_context *ctx, unsigned long long *bytes);
 
 /* C = A*B on the device.  A needs col_packed tiles (row role), B needs the
  * column view.  C is allocated by the library (row-major, plain Col bytes,
@@ -387,8 +410,9 @@ int tsg_spgemm_csr_host(tsg_context *ctx,
  * TSG_ORDER_ORIGINAL identity; TSG_ORDER_RCM reverse Cuthill-McKee on the
  * symmetrised pattern with (degree, id) tie-break (square only);
  * TSG_ORDER_DEGREE by (-degree, id); TSG_ORDER_GRAY by (density group,
- * Gray-decoded column signature, id); TSG_ORDER_RANDOM by
- * (SplitMix64(seed, id), id).  Replaces the order_gen adapters of
+ * Gray-decoded column signature, id); TSG_ORDER_RANDOM the permutation of
+ * Python's random.Random(seed).shuffle(list(range(m))), bit for bit (made on
+ * the host: one sequential chain of draws).  Replaces the order_gen adapters of
  * reorder_algorithm/{original,rcm,degree,gray,random}/ (run through
  * src/external_reorder.h:100-141). */
 #define TSG_ORDER_ORIGINAL 0
@@ -398,6 +422,9 @@ int tsg_spgemm_csr_host(tsg_context *ctx,
 #define TSG_ORDER_RANDOM 4
 int tsg_order(tsg_context *ctx, int kind, int m, int n, int nnz,
               const int *d_rowptr, const int *d_col, unsigned long long seed, int *d_order);
+/* TSG_ORDER_RANDOM's permutation written to host memory (no device work):
+ * order[0..n) = random.Random(seed).shuffle(list(range(n))) of CPython. */
+int tsg_order_random_host(int n, unsigned long long seed, int *order);
 /* "original", "rcm", "degree", "gray", "random" -> TSG_ORDER_*, else -1. */
 int tsg_order_from_name(const char *name);
 
@@ -480,6 +507,8 @@ typedef struct
     int seg_tiles; /* row schedule: C tiles per work item                */
     int acc_cap;   /* row schedule: FP64 accumulator slots per half-warp */
     int use_graph; /* capture the launch in a CUDA graph                 */
+    int dense_threshold; /* TSG_SCHED_SPA: C values per tile from which a
+                          * product takes the tile kernel (0: 64)       */
 } tsg_batch_params;
 
 typedef struct tsg_batch tsg_batch;

@@ -65,8 +65,6 @@ def olib():
         _o.tsgo_order_rcm.argtypes = [ctypes.c_int, vp, vp, vp]
         _o.tsgo_order_gray.argtypes = [ctypes.c_int, ctypes.c_int, vp, vp, vp]
         _o.tsgo_apply_bipermutation.argtypes = [ctypes.c_int, vp, vp, vp, vp, vp, vp, vp, vp]
-        _o.tsgo_random_key.restype = ctypes.c_ulonglong
-        _o.tsgo_random_key.argtypes = [ctypes.c_ulonglong, ctypes.c_ulonglong]
     return _o
 
 

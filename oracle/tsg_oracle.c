@@ -717,38 +717,104 @@ void tsgo_order_degree(int n, const int *rowptr, int *order)
     free(k);
 }
 
-/* Counter-based SplitMix64 keys; order = ids sorted by (key, id). */
-unsigned long long tsgo_random_key(unsigned long long seed, unsigned long long id)
+/* The reference's random ordering, order_utils.py:70-75:
+ * random.Random(seed).shuffle(list(range(n))) of CPython, restated from its
+ * published algorithm.  The generator is MT19937 (Matsumoto & Nishimura,
+ * 1998) seeded by init_by_array with the seed's 32-bit words, low word
+ * first (one word for seeds below 2^32, at least one); the shuffle is
+ * Fisher-Yates from the last position down, position i swapped with
+ * j = randbelow(i + 1), where randbelow(m) draws k = bit_length(m) bits
+ * (the top k bits of one 32-bit output) until the value is below m. */
+#define MT_N 624
+#define MT_M 397
+
+typedef struct
 {
-    unsigned long long x = seed * 0x9E3779B97F4A7C15ULL + id + 1ULL;
-    x ^= x >> 30;
-    x *= 0xBF58476D1CE4E5B9ULL;
-    x ^= x >> 27;
-    x *= 0x94D049BB133111EBULL;
-    x ^= x >> 31;
-    return x;
+    unsigned int mt[MT_N];
+    int next;
+} Mt19937;
+
+static void mt_init(Mt19937 *g, unsigned int s)
+{
+    g->mt[0] = s;
+    for (int i = 1; i < MT_N; i++)
+        g->mt[i] = 1812433253u * (g->mt[i - 1] ^ (g->mt[i - 1] >> 30)) + (unsigned int)i;
+    g->next = MT_N;
 }
 
-static int cmp_u64id(const void *a, const void *b)
+static void mt_init_by_array(Mt19937 *g, const unsigned int *key, int len)
 {
-    const unsigned long long *x = (const unsigned long long *)a, *y = (const unsigned long long *)b;
-    if (x[0] != y[0])
-        return (x[0] > y[0]) - (x[0] < y[0]);
-    return (x[1] > y[1]) - (x[1] < y[1]);
+    mt_init(g, 19650218u);
+    int i = 1, j = 0;
+    for (int k = MT_N > len ? MT_N : len; k > 0; k--)
+    {
+        g->mt[i] = (g->mt[i] ^ ((g->mt[i - 1] ^ (g->mt[i - 1] >> 30)) * 1664525u)) + key[j] + (unsigned int)j;
+        i++;
+        j++;
+        if (i >= MT_N)
+        {
+            g->mt[0] = g->mt[MT_N - 1];
+            i = 1;
+        }
+        if (j >= len)
+            j = 0;
+    }
+    for (int k = MT_N - 1; k > 0; k--)
+    {
+        g->mt[i] = (g->mt[i] ^ ((g->mt[i - 1] ^ (g->mt[i - 1] >> 30)) * 1566083941u)) - (unsigned int)i;
+        i++;
+        if (i >= MT_N)
+        {
+            g->mt[0] = g->mt[MT_N - 1];
+            i = 1;
+        }
+    }
+    g->mt[0] = 0x80000000u;
+}
+
+static unsigned int mt_twist_word(unsigned int hi, unsigned int lo, unsigned int far)
+{
+    const unsigned int y = (hi & 0x80000000u) | (lo & 0x7fffffffu);
+    return far ^ (y >> 1) ^ ((y & 1u) ? 0x9908b0dfu : 0u);
+}
+
+static unsigned int mt_u32(Mt19937 *g)
+{
+    if (g->next >= MT_N)
+    {
+        for (int k = 0; k < MT_N; k++)
+            g->mt[k] = mt_twist_word(g->mt[k], g->mt[(k + 1) % MT_N], g->mt[(k + MT_M) % MT_N]);
+        g->next = 0;
+    }
+    unsigned int y = g->mt[g->next++];
+    y ^= y >> 11;
+    y ^= (y << 7) & 0x9d2c5680u;
+    y ^= (y << 15) & 0xefc60000u;
+    y ^= y >> 18;
+    return y;
 }
 
 void tsgo_order_random(int n, unsigned long long seed, int *order)
 {
-    unsigned long long *k = (unsigned long long *)xmalloc((size_t)(n ? n : 1) * 2 * sizeof(unsigned long long));
+    unsigned int key[2] = {(unsigned int)seed, (unsigned int)(seed >> 32)};
+    Mt19937 g;
+    mt_init_by_array(&g, key, key[1] ? 2 : 1);
     for (int i = 0; i < n; i++)
+        order[i] = i;
+    for (int i = n - 1; i > 0; i--)
     {
-        k[2 * i] = tsgo_random_key(seed, (unsigned long long)i);
-        k[2 * i + 1] = (unsigned long long)i;
+        const unsigned int m = (unsigned int)i + 1u;
+        int k = 0;
+        while ((m >> k) != 0u)
+            k++;
+        unsigned int r;
+        do
+            r = mt_u32(&g) >> (32 - k);
+        while (r >= m);
+        const int t = order[i];
+        order[i] = order[r];
+        order[r] = t;
     }
-    qsort(k, (size_t)n, 2 * sizeof(unsigned long long), cmp_u64id);
-    for (int i = 0; i < n; i++)
-        order[i] = (int)k[2 * i + 1];
-    free(k);
 }
 
 /* Symmetrised off-diagonal adjacency (pattern of A + A^T without the

@@ -82,7 +82,6 @@ void tsgo_apply_bipermutation(int m, const int *rowptr, const int *col, const do
                               const int *row_old, const int *col_new,
                               int *out_rowptr, int *out_col, double *out_val);
 
-unsigned long long tsgo_random_key(unsigned long long seed, unsigned long long id);
 
 #ifdef __cplusplus
 }

@@ -65,17 +65,22 @@ class TsgTiled(ctypes.Structure):
     ]
 
 
+STEP3_KERNELS = {0: "none", 1: "k_step3", 2: "k_step3_elems", 3: "k_step3_rows", 4: "k_step3_spa<flat>",
+                 5: "k_step3_spa", 6: "k_step3_stg + k_step3_rest"}
+
+
 class TsgInfo(ctypes.Structure):
     _fields_ = [
         ("numtile_C", ctypes.c_longlong), ("nnz_C", ctypes.c_longlong), ("nnzCub", ctypes.c_longlong),
         ("tile_pairs", ctypes.c_longlong),
         ("ms_step1", ctypes.c_double), ("ms_step2", ctypes.c_double), ("ms_step3", ctypes.c_double),
-        ("ms_total", ctypes.c_double), ("bins", ctypes.c_int * 4),
+        ("ms_total", ctypes.c_double), ("bins", ctypes.c_int * 4), ("step3_kernel", ctypes.c_int),
     ]
 
     def as_dict(self):
         d = {f: getattr(self, f) for f, _ in self._fields_ if f != "bins"}
         d["bins"] = list(self.bins)
+        d["step3_name"] = STEP3_KERNELS.get(self.step3_kernel, "?")
         return d
 
 
@@ -112,11 +117,15 @@ def _declare(L):
     L.tsg_context_set_timing.argtypes = [vp, ip]
     L.tsg_context_launches.argtypes = [vp]
     L.tsg_context_allocations.argtypes = [vp]
+    L.tsg_tiled_device_bytes.argtypes = [ctypes.c_void_p]
+    L.tsg_tiled_device_bytes.restype = ctypes.c_longlong
+    L.tsg_context_pool_used.argtypes = [vp, ctypes.POINTER(ctypes.c_ulonglong)]
     L.tsg_context_allocations.restype = ctypes.c_longlong
     L.tsg_context_synchronize.argtypes = [vp]
     L.tsg_context_query.argtypes = [vp]
     L.tsg_context_set_fusion.argtypes = [vp, ip]
     L.tsg_context_set_schedule.argtypes = [vp, ip, ip, ip]
+    L.tsg_context_set_dense_threshold.argtypes = [vp, ip]
     L.tsg_context_launches.restype = ctypes.c_longlong
     L.tsg_csr_to_tiled.argtypes = [vp, ip, ip, ip, vp, vp, vp, ip, ctypes.POINTER(TsgTiled)]
     L.tsg_tiled_free.argtypes = [vp, ctypes.POINTER(TsgTiled)]
@@ -296,11 +305,14 @@ class Context:
     def set_timing(self, on: bool):
         check(lib().tsg_context_set_timing(self.handle, 1 if on else 0))
 
-    def set_schedule(self, schedule: str = "spa", seg_tiles: int = 8, acc_cap: int = 512):
+    def set_schedule(self, schedule: str = "spa", seg_tiles: int = 8, acc_cap: int = 512, dense: int = 0):
         """'tiles' (half-warp per C tile, intersection) or 'rows' (half-warp per
-        run of seg_tiles C tiles of one tile row, acc_cap FP64 slots)."""
+        run of seg_tiles C tiles of one tile row, acc_cap FP64 slots); 'spa'
+        takes `dense`, the C values per tile from which a product runs the
+        tile kernel (0: the default 64)."""
         check(lib().tsg_context_set_schedule(self.handle, SCHEDULE_IDS[schedule], seg_tiles,
                                              acc_cap))
+        check(lib().tsg_context_set_dense_threshold(self.handle, int(dense)))
 
     def set_fusion(self, on: bool):
         check(lib().tsg_context_set_fusion(self.handle, 1 if on else 0))
@@ -314,6 +326,13 @@ class Context:
     def allocations(self) -> int:
         """Device allocations the library made on this context so far."""
         return int(lib().tsg_context_allocations(self.handle))
+
+    def pool_used(self) -> int:
+        """Bytes in use in the device's default memory pool (the library's
+        allocations)."""
+        out = ctypes.c_ulonglong(0)
+        check(lib().tsg_context_pool_used(self.handle, ctypes.byref(out)))
+        return int(out.value)
 
     def close(self):
         if self.handle:
@@ -341,6 +360,12 @@ class Tiled:
     @property
     def nnz(self):
         return self.s.nnz
+
+    @property
+    def device_bytes(self) -> int:
+        """Device bytes the library holds for this matrix (every array as
+        allocated; 0 for a borrowed view)."""
+        return int(lib().tsg_tiled_device_bytes(ctypes.byref(self.s)))
 
     def download(self, colmajor: bool = False) -> dict:
         sm = SMatrix()
@@ -630,7 +655,7 @@ def build_reorder_plan(kind: str, algorithm: str, matA, matB=None) -> dict:
 # ---------------------------------------------------------------------------
 class BatchParams(ctypes.Structure):
     _fields_ = [("schedule", ctypes.c_int), ("seg_tiles", ctypes.c_int), ("acc_cap", ctypes.c_int),
-                ("use_graph", ctypes.c_int)]
+                ("use_graph", ctypes.c_int), ("dense_threshold", ctypes.c_int)]
 
 
 def _declare_batch(L):
@@ -669,17 +694,19 @@ class Batch:
     """tsg_batch over device-resident (A, B) operand pairs."""
 
     def __init__(self, ctx: Context, pairs, schedule: str = "spa", seg_tiles: int = 8, acc_cap: int = 512,
-                 graph: bool = True):
+                 graph: bool = True, dense: int = 0):
+        """dense: the 'spa' schedule's C values per tile from which a product
+        runs the tile kernel (0: the default 64)."""
         self.ctx = ctx
         self.pairs = list(pairs)  # keep operands alive
         n = len(self.pairs)
         arrA = (TsgTiled * n)(*[a.s for a, _ in self.pairs])
         arrB = (TsgTiled * n)(*[b.s for _, b in self.pairs])
-        prm = BatchParams(SCHEDULE_IDS[schedule], seg_tiles, acc_cap, 1 if graph else 0)
+        prm = BatchParams(SCHEDULE_IDS[schedule], seg_tiles, acc_cap, 1 if graph else 0, int(dense))
         self.handle = ctypes.c_void_p()
         check(lib().tsg_batch_create(ctx.handle, n, arrA, arrB, ctypes.byref(prm), ctypes.byref(self.handle)))
         self.count = n
-        self.params = dict(schedule=schedule, seg_tiles=seg_tiles, acc_cap=acc_cap)
+        self.params = dict(schedule=schedule, seg_tiles=seg_tiles, acc_cap=acc_cap, dense=dense)
 
     def run(self):
         check(lib().tsg_batch_run(self.handle))

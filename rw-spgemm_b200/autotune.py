@@ -1,10 +1,14 @@
 """Autotuner for the batched and one-product tiled SpGEMM.
 
 For a batch (or one product) it times every candidate configuration -- work
-schedule of steps 2-3 (tile / element / row-segment), the row schedule's
-segment length (C tiles per work item) and its FP64 accumulator capacity,
-which together set the block schedule and the split between the compact
-sparse accumulator and register accumulation -- and keeps the fastest.
+schedule of steps 2-3 (sparse accumulator / tile / element / row-segment),
+the row schedule's segment length (C tiles per work item) and its FP64
+accumulator capacity, and the sparse accumulator's dense threshold (C values
+per tile from which a product's numeric step takes the tile kernel), which
+together set the block schedule and the sparse/dense accumulator split --
+and keeps the fastest.  A candidate is (schedule, seg_tiles, acc_cap,
+dense); dense 0 is the default threshold and is ignored by the other
+schedules.
 Winners are cached by a key of batch features (product count, total scalar
 products, mean nonzeros per C-tile bound), in memory and optionally in a
 JSON file, so a similar batch reuses the choice without timing.
@@ -24,7 +28,20 @@ import numpy as np
 
 from . import Batch, Context, product_bounds, spgemm
 
-CANDIDATES = [("spa", 8, 512), ("elems", 8, 512), ("tiles", 8, 512), ("rows", 16, 1024), ("rows", 8, 256), ("rows", 32, 2048)]
+CANDIDATES = [("spa", 8, 512, 0), ("spa", 8, 512, 32), ("spa", 8, 512, 128), ("spa", 8, 512, 257),
+              ("elems", 8, 512, 0), ("tiles", 8, 512, 0), ("rows", 16, 1024, 0), ("rows", 8, 256, 0),
+              ("rows", 32, 2048, 0)]
+
+
+def normalize(cand) -> tuple:
+    """(schedule, seg_tiles, acc_cap, dense) from a 3- or 4-entry candidate."""
+    c = tuple(cand)
+    return c + (0,) if len(c) == 3 else c
+
+
+def make_batch(ctx: Context, pairs, cand, graph: bool = True) -> Batch:
+    s, w, c, d = normalize(cand)
+    return Batch(ctx, pairs, s, w, c, graph=graph, dense=d)
 
 
 def batch_key(ctx: Context, pairs) -> str:
@@ -39,11 +56,11 @@ def batch_key(ctx: Context, pairs) -> str:
 
 class Autotuner:
     def __init__(self, cache_path: str | None = None, candidates=None):
-        self.candidates = list(candidates or CANDIDATES)
+        self.candidates = [normalize(c) for c in (candidates or CANDIDATES)]
         self.path = Path(cache_path) if cache_path else None
         self.cache = {}
         if self.path and self.path.exists():
-            self.cache = {k: tuple(v) for k, v in json.loads(self.path.read_text()).items()}
+            self.cache = {k: normalize(v) for k, v in json.loads(self.path.read_text()).items()}
         self.last_timings = {}
 
     def _save(self):
@@ -51,15 +68,15 @@ class Autotuner:
             self.path.write_text(json.dumps(self.cache, indent=1))
 
     def tune_batch(self, ctx: Context, pairs, reps: int = 2, use_cache: bool = True):
-        """Best (schedule, seg_tiles, acc_cap) for this batch; timings in
-        self.last_timings (ms per run)."""
+        """Best (schedule, seg_tiles, acc_cap, dense) for this batch; timings
+        in self.last_timings (ms per run)."""
         import torch
         key = "batch-" + batch_key(ctx, pairs)
         if use_cache and key in self.cache:
             return self.cache[key]
         timings = {}
         for cand in self.candidates:
-            b = Batch(ctx, pairs, *cand, graph=True)
+            b = make_batch(ctx, pairs, cand, graph=True)
             b.run()
             b.sync()
             ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
@@ -106,8 +123,13 @@ class Autotuner:
         return choice
 
 
+def label(cand) -> str:
+    s, w, c, d = normalize(cand)
+    return f"{s}-{w}-{c}" + (f"-d{d or 64}" if s == "spa" else "")
+
+
 def summarize(timings: dict) -> dict:
-    return {f"{s}-{w}-{c}": round(t, 4) for (s, w, c), t in timings.items()}
+    return {label(k): round(t, 4) for k, t in timings.items()}
 
 
-__all__ = ["Autotuner", "CANDIDATES", "batch_key", "summarize", "np"]
+__all__ = ["Autotuner", "CANDIDATES", "batch_key", "label", "make_batch", "normalize", "summarize", "np"]

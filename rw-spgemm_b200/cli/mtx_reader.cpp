@@ -131,26 +131,38 @@ int read_matrix_market(const char *path, MtxCSR *out, std::string *err)
             out->val[o] = vv[q];
         }
     }
-    // stable per-row sort by column
+    return 0;
+}
+
+long long canonicalize_rows(int m, int *rowptr, int *colidx, double *val)
+{
     std::vector<int> idx;
     std::vector<int> ctmp;
     std::vector<double> vtmp;
-    for (int r = 0; r < out->m; r++)
+    long long w = 0; // write position: rows are compacted as duplicates go
+    for (int r = 0; r < m; r++)
     {
-        int s = out->rowptr[r], e = out->rowptr[r + 1];
-        if (std::is_sorted(out->colidx.begin() + s, out->colidx.begin() + e))
-            continue;
+        const int s = rowptr[r], e = rowptr[r + 1];
         idx.resize((size_t)(e - s));
         std::iota(idx.begin(), idx.end(), 0);
-        std::stable_sort(idx.begin(), idx.end(),
-                         [&](int a, int b) { return out->colidx[s + a] < out->colidx[s + b]; });
-        ctmp.assign(out->colidx.begin() + s, out->colidx.begin() + e);
-        vtmp.assign(out->val.begin() + s, out->val.begin() + e);
+        std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return colidx[s + a] < colidx[s + b]; });
+        ctmp.assign(colidx + s, colidx + e);
+        vtmp.assign(val + s, val + e);
+        rowptr[r] = (int)w;
         for (int q = 0; q < e - s; q++)
         {
-            out->colidx[s + q] = ctmp[idx[q]];
-            out->val[s + q] = vtmp[idx[q]];
+            const int c = ctmp[idx[q]];
+            if (q > 0 && c == colidx[w - 1])
+                val[w - 1] += vtmp[idx[q]];
+            else
+            {
+                colidx[w] = c;
+                val[w] = vtmp[idx[q]];
+                w++;
+            }
         }
     }
-    return 0;
+    const long long removed = (long long)rowptr[m] - w;
+    rowptr[m] = (int)w;
+    return removed;
 }

@@ -1,10 +1,17 @@
 // Drop-in replacement of the reference CLI (src/main.cu:15-638):
 //
 //   ./test -d <dev> -aat <0|1> A.mtx [-b B.mtx] [-reorder 1] [-reorder_algo original|rcm|degree|gray|random]
+//          [-o C.mtx]
 //
-// Same flags, same value overwrite (value[i] = i % 10, src/main.cu:191-197),
-// same product modes (A*A, A*A^T, A*B) and the same stdout report lines, so
-// the reference's batch scripts (which only redirect stdout) keep working.
+// Same flags, same value overwrite (value[i] = i % 10, src/main.cu:191-197,
+// applied in the reference reader's CSR order: rows in file order, columns
+// unsorted, duplicates kept), same product modes (A*A, A*A^T, A*B) and the
+// same stdout report lines, so the reference's batch scripts (which only
+// redirect stdout) keep working.  After the overwrite each row is sorted and
+// duplicate entries summed (canonicalize_rows), the form the library takes;
+// the reported nnz and nnzCub are the reference's, counted with duplicates.
+// -o (not in the reference) writes C, restored to the input order, as a
+// Matrix Market file.
 // Everything runs through the library's C ABI (include/tilespgemm_b200.h).
 // The closing check compares the result with cuSPARSE in FP64 -- row
 // pointers, columns and values (relative 1e-12) -- where the reference ran
@@ -189,6 +196,34 @@ static void cusparse_check(const SMatrix *A, const SMatrix *B, const SMatrix *C,
     printf("---------------------------------------------------------------\n");
 }
 
+// Scalar products of A*B counted over the CSR as read (duplicates included),
+// the reference's nnzCub (src/main.cu:392-397); B given by its row lengths.
+static unsigned long long count_products(const SMatrix *A, const std::vector<long long> &brow)
+{
+    unsigned long long s = 0;
+    for (int i = 0; i < A->nnz; i++)
+        s += (unsigned long long)brow[A->columnindex[i]];
+    return s;
+}
+
+static void canonicalize(SMatrix *s)
+{
+    canonicalize_rows(s->m, s->rowpointer, s->columnindex, s->value);
+    s->nnz = s->rowpointer[s->m];
+}
+
+static int write_mtx(const char *path, const SMatrix *C)
+{
+    FILE *f = fopen(path, "w");
+    if (!f)
+        return -1;
+    fprintf(f, "%%%%MatrixMarket matrix coordinate real general\n%d %d %d\n", C->m, C->n, C->nnz);
+    for (int r = 0; r < C->m; r++)
+        for (int p = C->rowpointer[r]; p < C->rowpointer[r + 1]; p++)
+            fprintf(f, "%d %d %.17g\n", r + 1, C->columnindex[p] + 1, C->value[p]);
+    return fclose(f);
+}
+
 static const char *problem_name(ReorderProblemKind k)
 {
     return k == REORDER_PROBLEM_AA ? "AA" : k == REORDER_PROBLEM_AAT ? "AAT" : "AB";
@@ -220,10 +255,11 @@ int main(int argc, char **argv)
     if (strcmp(argv[argi++], "-aat") != 0)
         return 0;
     aat = atoi(argv[argi++]);
-    char *filename = NULL, *filename_b = NULL;
+    char *filename = NULL, *filename_b = NULL, *filename_c = NULL;
     while (argi < argc)
     {
-        if (!strcmp(argv[argi], "-reorder") || !strcmp(argv[argi], "-b") || !strcmp(argv[argi], "-reorder_algo"))
+        if (!strcmp(argv[argi], "-reorder") || !strcmp(argv[argi], "-b") || !strcmp(argv[argi], "-reorder_algo") ||
+            !strcmp(argv[argi], "-o"))
         {
             const char *flag = argv[argi++];
             if (argi >= argc)
@@ -235,6 +271,8 @@ int main(int argc, char **argv)
                 reorder = atoi(argv[argi]);
             else if (!strcmp(flag, "-b"))
                 filename_b = argv[argi];
+            else if (!strcmp(flag, "-o"))
+                filename_c = argv[argi];
             else
                 reorder_algo = argv[argi];
             argi++;
@@ -303,13 +341,32 @@ int main(int argc, char **argv)
         for (int i = 0; i < B0.nnz; i++)
             B0.value[i] = i % 10;
     }
+    else if (aat && A0.m == A0.n && A0.isSymmetric)
+    {
+        printf("matrix AAT does not do symmetric matrix. Exit.\n");
+        return 0;
+    }
+    // the reference's nnzCub, over the CSR as read (it does not change under
+    // the reorderings: a sum over A's entries of B's row lengths)
+    std::vector<long long> brow;
+    if (ab_mode)
+        for (int k = 0; k < B0.m; k++)
+            brow.push_back(B0.rowpointer[k + 1] - B0.rowpointer[k]);
     else if (aat)
     {
-        if (A0.m == A0.n && A0.isSymmetric)
-        {
-            printf("matrix AAT does not do symmetric matrix. Exit.\n");
-            return 0;
-        }
+        brow.assign((size_t)A0.n, 0); // rows of A^T: A's column counts
+        for (int i = 0; i < A0.nnz; i++)
+            brow[A0.columnindex[i]]++;
+    }
+    else
+        for (int k = 0; k < A0.m; k++)
+            brow.push_back(A0.rowpointer[k + 1] - A0.rowpointer[k]);
+    const unsigned long long nnzCub_read = count_products(&A0, brow);
+    canonicalize(&A0);
+    if (ab_mode)
+        canonicalize(&B0);
+    else if (aat)
+    {
         transpose_csr(&A0, &B0);
         kind = REORDER_PROBLEM_AAT;
     }
@@ -413,12 +470,7 @@ int main(int argc, char **argv)
         printf("estimated C tiles after reorder = %lld\n", info.estimated_c_tiles_after);
     }
 
-    unsigned long long nnzCub = 0;
-    for (int i = 0; i < A->nnz; i++)
-    {
-        int k = A->columnindex[i];
-        nnzCub += B->rowpointer[k + 1] - B->rowpointer[k];
-    }
+    const unsigned long long nnzCub = nnzCub_read;
     printf("SpGEMM nnzCub = %lld\n", nnzCub);
 
     // tile format: A row-major (packed bytes), B column-major (its own copy
@@ -453,6 +505,8 @@ int main(int argc, char **argv)
         }
         printf("restore reorder result uses %.2f ms\n", now_ms() - t1);
     }
+    if (filename_c && write_mtx(filename_c, &C) != 0)
+        printf("cannot write %s\n", filename_c);
     cusparse_check(&A0, &B0, &C, nnzCub);
     matrix_destroy(&At);
     matrix_destroy(&Bt);

@@ -70,6 +70,7 @@ extern "C" int tsg_context_create(int device, tsg_context **out)
     ctx->seg_tiles = 8;
     ctx->acc_cap = 512;
     ctx->fuse12 = 1;
+    ctx->spa_dense = TSG_SPA_DENSE_DEFAULT;
     // keep freed pool memory cached so repeated products do not return pages
     cudaMemPool_t pool;
     if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess)
@@ -162,6 +163,16 @@ extern "C" int tsg_context_set_schedule(tsg_context *ctx, int schedule, int seg_
     return TSG_OK;
 }
 
+extern "C" int tsg_context_set_dense_threshold(tsg_context *ctx, int values_per_tile)
+{
+    if (!ctx)
+        return tsg_set_error(TSG_ERR_INVALID, "null context");
+    if (values_per_tile < 0 || values_per_tile > 257)
+        return tsg_set_error(TSG_ERR_INVALID, "dense threshold %d outside [0, 257]", values_per_tile);
+    ctx->spa_dense = values_per_tile ? values_per_tile : TSG_SPA_DENSE_DEFAULT;
+    return TSG_OK;
+}
+
 extern "C" int tsg_context_set_fusion(tsg_context *ctx, int fuse_step12)
 {
     if (!ctx)
@@ -227,6 +238,38 @@ extern "C" int tsg_tiled_free(tsg_context *ctx, tsg_tiled *t)
     tsg_release(ctx, t->row_col);
     tsg_release(ctx, t->row_val);
     memset(t, 0, sizeof(*t));
+    return TSG_OK;
+}
+
+static long long padded_bytes(const void *p, long long bytes)
+{
+    return p ? ((bytes + 15) & ~15LL) + 16 : 0; // tsg_alloc's size for `bytes`
+}
+
+extern "C" long long tsg_tiled_device_bytes(const tsg_tiled *t)
+{
+    if (!t || t->_alloc)
+        return 0;
+    const long long T = t->numtile, nnz = t->nnz;
+    return padded_bytes(t->tile_ptr, 4 * ((long long)t->tilem + 1)) + padded_bytes(t->tile_columnidx, 4 * T) +
+           padded_bytes(t->tile_rowidx, 4 * T) + padded_bytes(t->tile_nnz, 4 * (T + 1)) +
+           padded_bytes(t->tile_csr_Ptr, TSG_BS * T) + padded_bytes(t->tile_csr_Col, nnz) +
+           padded_bytes(t->tile_csr_Value, 8 * nnz) + padded_bytes(t->mask, 2 * TSG_BS * T) +
+           padded_bytes(t->csc_tile_ptr, 4 * ((long long)t->tilen + 1)) + padded_bytes(t->csc_tile_rowidx, 4 * T) +
+           padded_bytes(t->csc_tile_pos, 4 * T) + padded_bytes(t->mask_t, 2 * TSG_BS * T) +
+           padded_bytes(t->row_ptr, 4 * ((long long)t->m + 1)) + padded_bytes(t->row_col, 4 * nnz) +
+           padded_bytes(t->row_val, 8 * nnz);
+}
+
+extern "C" int tsg_context_pool_used(tsg_context *ctx, unsigned long long *bytes)
+{
+    if (!ctx || !bytes)
+        return tsg_set_error(TSG_ERR_INVALID, "null argument");
+    cudaMemPool_t pool;
+    TSG_CUDA(cudaDeviceGetDefaultMemPool(&pool, ctx->device));
+    unsigned long long used = 0; // the attribute is a 64-bit unsigned integer
+    TSG_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used));
+    *bytes = (unsigned long long)used;
     return TSG_OK;
 }
 

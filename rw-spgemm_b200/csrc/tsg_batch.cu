@@ -63,6 +63,7 @@ struct tsg_batch
     std::vector<int> m, n, tilen; // per product C dimensions
     long long launches;
     unsigned long long wait_ns; // the grid barrier's wait limit
+    int dense;                  // SPA schedule: values per C tile from which a product takes the tile kernel
 };
 
 #define BATCH_THREADS 128
@@ -566,7 +567,8 @@ __global__ void __launch_bounds__(NT)
 // device counter.  Raises stamp[7] on exit.  Does nothing when k_batch left
 // with an error (its later phases did not run).
 __global__ void __launch_bounds__(SPA_THREADS, 3)
-    k_batch_spa3(BatchProd *prods, int count, const long long *__restrict__ itemoff, unsigned *bar, const int *err)
+    k_batch_spa3(BatchProd *prods, int count, const long long *__restrict__ itemoff, unsigned *bar, const int *err,
+                 int dense)
 {
     if (*(volatile const int *)err)
         return;
@@ -591,7 +593,7 @@ __global__ void __launch_bounds__(SPA_THREADS, 3)
         if (blk >= blkoff[count])
             break;
         p = find_product_from(blkoff, count, blk, p);
-        if (prods[p].status || prods[p].nnzC >= (long long)SPA_DENSE * prods[p].numC)
+        if (prods[p].status || prods[p].nnzC >= (long long)dense * prods[p].numC)
             continue;
         const ProdView &P = prods[p].P;
         const long long tb = (blk - blkoff[p]) * SPA_BLK;
@@ -606,11 +608,11 @@ __global__ void __launch_bounds__(SPA_THREADS, 3)
                   gtimer());
 }
 
-// ... and products with dense C tiles (>= SPA_DENSE values per tile on
+// ... and products with dense C tiles (>= `dense` values per tile on
 // average): the tile kernel, a half-warp per C tile.
 #define DENSE3_THREADS 256
 __global__ void __launch_bounds__(DENSE3_THREADS)
-    k_batch_dense3(BatchProd *prods, int count, const long long *__restrict__ itemoff, const int *err)
+    k_batch_dense3(BatchProd *prods, int count, const long long *__restrict__ itemoff, const int *err, int dense)
 {
     if (*(volatile const int *)err)
         return;
@@ -626,7 +628,7 @@ __global__ void __launch_bounds__(DENSE3_THREADS)
     for (long long h = (long long)blockIdx.x * (DENSE3_THREADS / 16) + hw; h < total_items; h += nhw)
     {
         const int p = find_product(itemoff, count, h);
-        if (prods[p].status || prods[p].nnzC < (long long)SPA_DENSE * prods[p].numC)
+        if (prods[p].status || prods[p].nnzC < (long long)dense * prods[p].numC)
             continue;
         step3_tile(prods[p].P, (int)(h - itemoff[p]), hmask, lane, tacc);
     }
@@ -796,9 +798,10 @@ static int record_run(tsg_batch *b, cudaStream_t st)
     if (b->params.schedule == TSG_SCHED_SPA)
     {
         k_batch_spa3<<<b->grid3, SPA_THREADS, sizeof(SpaSmem), st>>>(b->d_prod, b->count, b->d_itemoff, b->d_bar,
-                                                                     b->d_err);
+                                                                     b->d_err, b->dense);
         TSG_CUDA(cudaGetLastError());
-        k_batch_dense3<<<b->ctx->num_sms * 8, DENSE3_THREADS, 0, st>>>(b->d_prod, b->count, b->d_itemoff, b->d_err);
+        k_batch_dense3<<<b->ctx->num_sms * 8, DENSE3_THREADS, 0, st>>>(b->d_prod, b->count, b->d_itemoff, b->d_err,
+                                                                        b->dense);
         TSG_CUDA(cudaGetLastError());
     }
     return TSG_OK;
@@ -819,7 +822,10 @@ extern "C" int tsg_batch_create(tsg_context *ctx, int count, const tsg_tiled *A,
         prm.seg_tiles = 16;
         prm.acc_cap = 1024;
         prm.use_graph = 1;
+        prm.dense_threshold = 0;
     }
+    if (prm.dense_threshold < 0 || prm.dense_threshold > 257)
+        return tsg_set_error(TSG_ERR_INVALID, "dense threshold %d outside [0, 257]", prm.dense_threshold);
     size_t smem;
     int threads;
     batch_kernel_t kern = pick_kernel(prm, &smem, &threads);
@@ -839,6 +845,7 @@ extern "C" int tsg_batch_create(tsg_context *ctx, int count, const tsg_tiled *A,
     b->ctx = ctx;
     b->count = count;
     b->params = prm;
+    b->dense = prm.dense_threshold ? prm.dense_threshold : SPA_DENSE;
     b->host.resize(count);
     b->rowoff.resize(count + 1);
     b->m.resize(count);

@@ -751,7 +751,7 @@ __device__ __forceinline__ void step3_rows_item(const ProdView &P, long long ite
 #define SPA_SEGT 256
 #define SPA_WIN 2048
 #define SPA_STAGE 64
-#define SPA_DENSE 64 // C values per tile from which the tile kernel is faster
+#define SPA_DENSE TSG_SPA_DENSE_DEFAULT
 #define SPA_FLAT 16  // B rows averaging fewer entries (inside a segment) have their products flattened
 
 // Staging a lane per A entry.  A warp's row entries are numbered across its

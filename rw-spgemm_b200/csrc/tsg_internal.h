@@ -9,6 +9,9 @@
 #include "tilespgemm_b200.h"
 
 #define TSG_BS 16
+// SPA schedule: C values per tile (on average) from which the numeric step's
+// tile kernel is faster than the sparse accumulator (the default threshold)
+#define TSG_SPA_DENSE_DEFAULT 64
 
 struct tsg_context
 {
@@ -28,6 +31,8 @@ struct tsg_context
     cudaEvent_t copy_ev;      // orders a chunk's copy after its fill
     int *d_status;            // device error word kernels set (TSG_ERR_TIMEOUT, TSG_ERR_OVERFLOW), 0 when clear
     long long allocs;         // device allocations tsg_alloc made on the context
+    int spa_dense;            // SPA schedule: C values per tile from which a product takes the tile kernel
+    int last_step3;           // TSG_STEP3_* of the last numeric step launched
 };
 
 // Looks up the no-alloc conversion's scratch address on a device (that

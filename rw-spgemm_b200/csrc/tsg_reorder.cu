@@ -4,7 +4,10 @@
 // reorder_algorithm/README.md:6-12):
 //   original  identity                      (src/external_reorder.h:173-202)
 //   degree    sorted by (-degree, id)       (reorder_algorithm/common/order_utils.py:78-81)
-//   random    sorted by (SplitMix64(seed, id), id) -- a seeded GPU shuffle
+//   random    CPython's random.Random(seed).shuffle(list(range(n)))
+//             (order_utils.py:70-75), bit for bit, on the host: the shuffle
+//             is one sequential chain of draws; the permutation is copied to
+//             the device
 //   rcm       reverse Cuthill-McKee on the symmetrised off-diagonal pattern
 //             with the (degree, id) tie-break (the scheme of scipy's RCM used
 //             by order_utils.py:84-104; tie-break of src/reorder.h:1678-1722),
@@ -19,6 +22,8 @@
 // radix sort of (row, column) keys, like the reference's thrust::sort_by_key.
 #include <stdlib.h>
 #include <sys/time.h>
+
+#include <vector>
 
 #include "tsg_internal.h"
 
@@ -42,15 +47,106 @@ extern "C" int tsg_order_from_name(const char *name)
     return -1;
 }
 
-__device__ __forceinline__ unsigned long long splitmix_key(unsigned long long seed, unsigned long long id)
+// MT19937 (Matsumoto & Nishimura, 1998) as CPython's random module runs it:
+// seeded from an integer by init_by_array over the integer's 32-bit words,
+// low word first; outputs tempered 32-bit words; state refilled 624 words
+// at a time.
+class PyMersenne
 {
-    unsigned long long x = seed * 0x9E3779B97F4A7C15ULL + id + 1ULL;
-    x ^= x >> 30;
-    x *= 0xBF58476D1CE4E5B9ULL;
-    x ^= x >> 27;
-    x *= 0x94D049BB133111EBULL;
-    x ^= x >> 31;
-    return x;
+  public:
+    explicit PyMersenne(unsigned long long seed)
+    {
+        const unsigned key[2] = {(unsigned)seed, (unsigned)(seed >> 32)};
+        const int len = key[1] ? 2 : 1;
+        s_[0] = 19650218u;
+        for (int i = 1; i < N; i++)
+            s_[i] = 1812433253u * (s_[i - 1] ^ (s_[i - 1] >> 30)) + (unsigned)i;
+        int i = 1, j = 0;
+        for (int k = N > len ? N : len; k > 0; k--, i++, j = (j + 1) % len)
+        {
+            if (i >= N)
+            {
+                s_[0] = s_[N - 1];
+                i = 1;
+            }
+            s_[i] = (s_[i] ^ ((s_[i - 1] ^ (s_[i - 1] >> 30)) * 1664525u)) + key[j] + (unsigned)j;
+        }
+        for (int k = N - 1; k > 0; k--, i++)
+        {
+            if (i >= N)
+            {
+                s_[0] = s_[N - 1];
+                i = 1;
+            }
+            s_[i] = (s_[i] ^ ((s_[i - 1] ^ (s_[i - 1] >> 30)) * 1566083941u)) - (unsigned)i;
+        }
+        if (i >= N)
+            s_[0] = s_[N - 1];
+        s_[0] = 0x80000000u;
+        pos_ = N;
+    }
+
+    unsigned next()
+    {
+        if (pos_ == N)
+            refill();
+        unsigned y = s_[pos_++];
+        y ^= y >> 11;
+        y ^= (y << 7) & 0x9d2c5680u;
+        y ^= (y << 15) & 0xefc60000u;
+        return y ^ (y >> 18);
+    }
+
+    // random.Random._randbelow(m) for 2 <= m < 2^32: k = bit_length(m) top
+    // bits of one output, drawn again while >= m
+    unsigned below(unsigned m)
+    {
+        const int k = 32 - __builtin_clz(m);
+        unsigned r;
+        do
+            r = next() >> (32 - k);
+        while (r >= m);
+        return r;
+    }
+
+  private:
+    static constexpr int N = 624, M = 397;
+    unsigned s_[N];
+    int pos_;
+
+    void refill()
+    {
+        for (int k = 0; k < N; k++)
+        {
+            const unsigned y = (s_[k] & 0x80000000u) | (s_[k + 1 < N ? k + 1 : 0] & 0x7fffffffu);
+            s_[k] = s_[(k + M) % N] ^ (y >> 1) ^ (0u - (y & 1u) & 0x9908b0dfu);
+        }
+        pos_ = 0;
+    }
+};
+
+// random.Random(seed).shuffle(list(range(n))): Fisher-Yates from the last
+// position down
+static void python_shuffle(int n, unsigned long long seed, int *order)
+{
+    PyMersenne g(seed);
+    for (int i = 0; i < n; i++)
+        order[i] = i;
+    for (int i = n - 1; i > 0; i--)
+    {
+        const unsigned j = g.below((unsigned)i + 1u);
+        const int t = order[i];
+        order[i] = order[j];
+        order[j] = t;
+    }
+}
+
+extern "C" int tsg_order_random_host(int n, unsigned long long seed, int *order)
+{
+    if (n < 0 || (n > 0 && !order))
+        return tsg_set_error(TSG_ERR_INVALID, "bad arguments");
+    python_shuffle(n, seed, order);
+    return TSG_OK;
 }
 
 __global__ void k_iota(long long n, int *__restrict__ v)
@@ -75,11 +171,6 @@ __global__ void k_degree_keys(int n, const int *__restrict__ rowptr, int descend
     }
 }
 
-__global__ void k_random_keys(int n, unsigned long long seed, unsigned long long *__restrict__ keys)
-{
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        keys[i] = splitmix_key(seed, (unsigned long long)i);
-}
 
 __device__ __forceinline__ unsigned gray_decode32(unsigned g)
 {
@@ -439,14 +530,10 @@ extern "C" int tsg_order(tsg_context *ctx, int kind, int m, int n, int nnz, cons
     }
     case TSG_ORDER_RANDOM:
     {
-        unsigned long long *k;
-        TSG_TRY(tsg_alloc(ctx, &k, (size_t)m));
-        k_random_keys<<<g1, 256, 0, st>>>(m, seed, k);
-        TSG_LAUNCH_CHECK();
-        k_iota<<<g1, 256, 0, st>>>(m, d_order);
-        TSG_LAUNCH_CHECK();
-        TSG_TRY(tsg_sort_pairs_u64(ctx, k, d_order, m, 64));
-        tsg_release(ctx, k);
+        std::vector<int> h((size_t)m);
+        python_shuffle(m, seed, h.data());
+        TSG_CUDA(cudaMemcpyAsync(d_order, h.data(), (size_t)m * sizeof(int), cudaMemcpyHostToDevice, st));
+        TSG_CUDA(cudaStreamSynchronize(st)); // h is released on return
         return TSG_OK;
     }
     case TSG_ORDER_GRAY:
@@ -798,7 +885,11 @@ extern "C" int build_external_reorder_plan(ReorderProblemKind kind, const char *
     reorder_info_destroy(info);
     *ordergen_ms = 0.0;
     const int okind = tsg_order_from_name(algorithm);
-    if (okind < 0)
+    // the reference's random adapter refuses to run unless asked to
+    // (reorder_algorithm/random/order_gen: exit 42 without
+    // TASA_ENABLE_UNSAFE_RANDOM=1), which its plan reports as -20
+    const char *unsafe = getenv("TASA_ENABLE_UNSAFE_RANDOM");
+    if (okind < 0 || (okind == TSG_ORDER_RANDOM && !(unsafe && !strcmp(unsafe, "1"))))
     {
         printf("external reorder missing dependency: %s\n", algorithm ? algorithm : "(null)");
         return -20;

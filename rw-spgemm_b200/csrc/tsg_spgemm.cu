@@ -435,11 +435,12 @@ static int launch_step3_stg(tsg_context *ctx, const ProdView &P0, const int *d_k
 }
 
 // step 3 by the SPA kernel: the default schedule, except for products whose
-// C tiles are dense on average (>= SPA_DENSE values) and B without a row view
-// (borrowed foreign buffers), which take the tile kernel
+// C tiles are dense on average (>= ctx->spa_dense values, SPA_DENSE unless
+// set) and B without a row view (borrowed foreign buffers), which take the
+// tile kernel
 static bool step3_by_spa(const tsg_context *ctx, const ProdView &P, long long nnzC)
 {
-    return ctx->sched == TSG_SCHED_SPA && P.B_rptr && nnzC < (long long)SPA_DENSE * P.numC;
+    return ctx->sched == TSG_SCHED_SPA && P.B_rptr && nnzC < (long long)ctx->spa_dense * P.numC;
 }
 
 // the SPA numeric step for tile rows [row0, row1)
@@ -448,6 +449,7 @@ static int launch_step3_spa_rows(tsg_context *ctx, const ProdView &P, long long 
 {
     const bool flat = spa_wants_flat(P.browB, P.numC, nnzC, P.tilemA);
     const bool whole = row0 == 0 && row1 == P.tilemA;
+    ctx->last_step3 = flat ? TSG_STEP3_FLAT : P.padded ? TSG_STEP3_STAGED : TSG_STEP3_SPA;
     if (flat)
         return whole ? launch_step3_spa<true, false>(ctx, P, d_kind, 0, 0)
                      : launch_step3_spa<true, true>(ctx, P, d_kind, row0, row1);
@@ -467,6 +469,7 @@ static int launch_step3(tsg_context *ctx, const ProdView &P, long long nnzC, con
     if (ctx->sched == TSG_SCHED_ROWS)
     {
         const int W = ctx->seg_tiles, cap = ctx->acc_cap;
+        ctx->last_step3 = TSG_STEP3_ROWS;
 #define TSG_DISPATCH3(w, c)                    \
     if (W == w && cap == c)                    \
         return launch_step3_rows<w, c>(ctx, P);
@@ -478,10 +481,12 @@ static int launch_step3(tsg_context *ctx, const ProdView &P, long long nnzC, con
     {
         if (!P.B_maskT)
             return tsg_set_error(TSG_ERR_INVALID, "element schedule needs B's column masks (mask_t)");
+        ctx->last_step3 = TSG_STEP3_ELEMS;
         k_step3_elems<<<tsg_blocks((long long)P.numC * 32, 256), 256, 0, ctx->stream>>>(P);
         TSG_LAUNCH_CHECK();
         return TSG_OK;
     }
+    ctx->last_step3 = TSG_STEP3_TILES;
     k_step3<<<tsg_blocks((long long)P.numC * 16, S3_THREADS), S3_THREADS, 0, ctx->stream>>>(P);
     TSG_LAUNCH_CHECK();
     return TSG_OK;
@@ -613,6 +618,7 @@ static int spgemm_finish(tsg_context *ctx, SpgemmRun &R, tsg_spgemm_info *info)
         TSG_CUDA(cudaStreamSynchronize(st));
         info->tile_pairs = h[0];
         memcpy(info->bins, h + 1, 4 * sizeof(int));
+        info->step3_kernel = R.nnzC > 0 ? ctx->last_step3 : TSG_STEP3_NONE;
         if (ctx->timing)
         {
             info->ms_step1 = ev_ms(ctx->ev[0], ctx->ev[1]);

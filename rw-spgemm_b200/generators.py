@@ -153,18 +153,40 @@ def batched_products(count: int = 512, seed: int = 0, n_min: int = 1024, n_max: 
     [n_min, n_max]; each of A_i, B_i banded (half-bandwidth uniform in
     [hb_min, hb_max]) or random with Poisson(lam) nonzeros per row; values
     uniform(-1, 1); a fixed seed per product."""
-    rng = np.random.default_rng(seed)
     out = []
+    for n, sides in _batched_specs(count, seed, n_min, n_max, hb_min, hb_max):
+        out.append(tuple(banded(n, p, seed=s) if kind == "banded" else random_poisson(n, None, lam, seed=s)
+                         for kind, p, s in sides))
+    return out
+
+
+def _batched_specs(count, seed, n_min, n_max, hb_min, hb_max):
+    """(n, [(kind, half-bandwidth, seed) for A, B]) of every product of
+    batched_products, drawn from one generator in a fixed order."""
+    rng = np.random.default_rng(seed)
+    specs = []
     for i in range(count):
         n = int(round(np.exp(rng.uniform(np.log(n_min), np.log(n_max)))))
-        mats = []
+        sides = []
         for side in range(2):
             s = int(rng.integers(0, 2**31 - 1))
             if rng.random() < 0.5:
-                mats.append(banded(n, int(rng.integers(hb_min, hb_max + 1)), seed=s))
+                sides.append(("banded", int(rng.integers(hb_min, hb_max + 1)), s))
             else:
-                mats.append(random_poisson(n, None, lam, seed=s))
-        out.append((mats[0], mats[1]))
+                sides.append(("poisson", 0, s))
+        specs.append((n, sides))
+    return specs
+
+
+def batched_product_classes(count: int = 512, seed: int = 0, n_min: int = 1024, n_max: int = 65536,
+                            hb_min: int = 8, hb_max: int = 64):
+    """Class of each product of batched_products(count, seed, ...):
+    "banded*banded", "poisson*poisson" (sparse C tiles, hypersparse for large
+    n) or "mixed"."""
+    out = []
+    for _, sides in _batched_specs(count, seed, n_min, n_max, hb_min, hb_max):
+        kinds = {k for k, _, _ in sides}
+        out.append("mixed" if len(kinds) == 2 else f"{sides[0][0]}*{sides[0][0]}")
     return out
 
 

@@ -13,6 +13,9 @@ dispatcher thread
   * packs admitted jobs into a batch (tsg_batch: one persistent,
     graph-captured launch) on a free stream slot while earlier batches are
     still running on the other slots, so their work overlaps on the GPU,
+    with the batch schedule fixed or (schedule="auto") chosen by the
+    autotuner once per density class of batch (scalar products per C-tile
+    bound, in powers of two) and reused for every later batch of the class,
   * when a batch finishes, copies each result to host CSR and completes the
     job's future with its latency (submit -> result on the host).
 Results are bit-identical whether a job runs alone or inside any mix: each
@@ -22,6 +25,7 @@ from __future__ import annotations
 
 import collections
 import ctypes
+import math
 import threading
 import time
 from concurrent.futures import Future
@@ -33,7 +37,7 @@ from . import TSG_TILED_CSC_VIEW, Batch, Context, check, csr_host_to_tiled, lib,
 
 class Job:
     __slots__ = ("jid", "kind", "a_key", "b_key", "t_submit", "t_done", "future", "pred_bytes", "pred_prods",
-                 "result_nnz")
+                 "pred_tiles", "result_nnz")
 
     def __init__(self, jid, kind, a_key, b_key):
         self.jid, self.kind, self.a_key, self.b_key = jid, kind, a_key, b_key
@@ -42,6 +46,7 @@ class Job:
         self.future = Future()
         self.pred_bytes = 0
         self.pred_prods = 0
+        self.pred_tiles = 0
         self.result_nnz = 0
 
 
@@ -66,8 +71,9 @@ class OperandCache:
 
     @staticmethod
     def tiled_bytes(t):
-        s = t.s
-        return (s.tilem + 1) * 4 + s.numtile * (4 + 4 + 4 + 16 + 32 + 8) + s.nnz * 9 + (s.tilen + 1) * 4
+        """Device bytes of a resident operand, as the library allocated them:
+        tiles, column view, column masks and the row view of the B role."""
+        return t.device_bytes
 
     def get(self, key, host_mat):
         if key in self.tiles:
@@ -120,15 +126,17 @@ class SpGEMMServer:
               bounds): a batch closes once it holds this much work, so a few
               large jobs do not hold many small ones back (a single job
               above it still runs, alone)
-    schedule  (schedule, seg_tiles, acc_cap) of the batched kernel, e.g. the
-              autotuner's choice
+    schedule  (schedule, seg_tiles, acc_cap[, dense]) of the batched kernel,
+              or "auto": the autotuner (`tuner`, a fresh one if None)
+              times its candidates on the first batch of each density class
+              and the class keeps that choice
     deliver   "host": a job's result is (m, n, rowptr, colidx, val) as numpy
               arrays; "device": the same as torch tensors on the GPU (for a
               consumer that stays on the device; nothing crosses the bus)
     """
 
     def __init__(self, device=0, mem_cap=40 << 30, slots=2, max_batch=64, schedule=("spa", 8, 512),
-                 batch_products=2e8, deliver="host"):
+                 batch_products=2e8, deliver="host", tuner=None):
         if deliver not in ("host", "device"):
             raise ValueError(deliver)
         self.deliver = deliver
@@ -137,6 +145,11 @@ class SpGEMMServer:
         self.max_batch = max_batch
         self.batch_products = float(batch_products)
         self.schedule = schedule
+        self.tuner = tuner
+        self.tuned = {}  # density class -> chosen schedule ("auto")
+        if schedule == "auto" and self.tuner is None:
+            from .autotune import Autotuner
+            self.tuner = Autotuner()
         self.matrices = {}
         self.slots = [_Slot(device) for _ in range(slots)]
         self.stage_ctx = Context(device, own_stream=True)  # operand staging and bounds
@@ -208,14 +221,26 @@ class SpGEMMServer:
         return self.cache.bytes + sum(s.arena for s in self.slots if s.batch is not None)
 
     def _predict(self, A, B):
-        """(device bytes of the result arena, scalar products) from the step-1
-        bounds."""
+        """(device bytes of the result arena, scalar products, C-tile bound)
+        from the step-1 bounds; the arena's per-array 256-byte alignment
+        and per-tile-row flags included."""
         prods, pairs = product_bounds(self.cache.ctx, A, B)
-        tiles = pairs
-        full = A.s.tilem * B.s.tilen
-        tiles = min(tiles, full)
+        tiles = min(pairs, A.s.tilem * B.s.tilen)
         vals = min(prods, 256 * tiles)
-        return tiles * (4 * 3 + 4 + 32 + 16) + vals * 9 + (A.s.tilem + 1) * 4, prods
+        return (tiles * (4 * 3 + 4 + 32 + 16) + vals * 9 + (A.s.tilem + 1) * 4 + A.s.tilem * 4 + 8 * 256,
+                prods, tiles)
+
+    def _schedule_for(self, slot, pairs, jobs):
+        """The batch's (schedule, seg_tiles, acc_cap, dense)."""
+        if self.schedule != "auto":
+            s = tuple(self.schedule)
+            return s + (0,) if len(s) == 3 else s
+        prods = sum(j.pred_prods for j in jobs)
+        tiles = max(1, sum(j.pred_tiles for j in jobs))
+        key = int(math.log2(prods / tiles + 1))
+        if key not in self.tuned:
+            self.tuned[key] = self.tuner.tune_batch(slot.ctx, pairs, reps=1, use_cache=False)
+        return self.tuned[key]
 
     def _form_batch(self, slot):
         jobs, pairs, pred, work = [], [], 0, 0
@@ -225,7 +250,7 @@ class SpGEMMServer:
             job = self.queue[0]
             A = self.cache.get(job.a_key, self.matrices[job.a_key])
             B = self.cache.get(job.b_key, self.matrices[job.b_key])
-            job.pred_bytes, job.pred_prods = self._predict(A, B)
+            job.pred_bytes, job.pred_prods, job.pred_tiles = self._predict(A, B)
             if jobs and work + job.pred_prods > self.batch_products:
                 break  # the batch holds its share of work; this job opens the next
             # its operands stay resident while it runs: a job needing more
@@ -253,8 +278,8 @@ class SpGEMMServer:
             work += job.pred_prods
         if not jobs:
             return False
-        sch, seg, cap = self.schedule
-        slot.batch = Batch(slot.ctx, pairs, sch, seg, cap, graph=False)
+        sch, seg, cap, dense = self._schedule_for(slot, pairs, jobs)
+        slot.batch = Batch(slot.ctx, pairs, sch, seg, cap, graph=False, dense=dense)
         slot.arena = slot.batch.info()["arena_bytes"]
         slot.jobs = jobs
         slot.t_launch = time.perf_counter()
@@ -346,4 +371,5 @@ class SpGEMMServer:
             "mean_batch": len(self.done) / self.batches if self.batches else 0.0,
             "rejected": self.rejected,
             "operand_cache": {"hits": self.cache.hits, "misses": self.cache.misses, "bytes": self.cache.bytes},
+            "tuned": {f"d{k}": "-".join(str(x) for x in v) for k, v in sorted(self.tuned.items())},
         }

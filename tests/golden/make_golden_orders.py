@@ -1,7 +1,8 @@
 """Regenerates tests/golden/orders.npz from the REFERENCE's own ordering code
 (for-the-juan/RW-SpGEMM reorder_algorithm/common/order_utils.py: native_original,
-native_degree, native_rcm), run in this container on small Matrix Market files
-written from the library's generators.
+native_degree, native_rcm, and native_random under TASA_RANDOM_SEED 1 and 7),
+run in this container on small Matrix Market files written from the library's
+generators.
 
 Run where the reference tree exists:
     python tests/golden/make_golden_orders.py <reference tree>
@@ -9,6 +10,7 @@ Run where the reference tree exists:
 from __future__ import annotations
 
 import importlib.util
+import os
 import sys
 import tempfile
 from pathlib import Path
@@ -67,6 +69,12 @@ def main():
                 rc = ou.run_native(kind, ["order_gen", str(mtx), str(of)])
                 assert rc == 0, (name, kind, rc)
                 out[f"{name}/{kind}"] = np.loadtxt(of, dtype=np.int64).astype(np.int32).reshape(-1)
+            for seed in (1, 7):
+                os.environ["TASA_RANDOM_SEED"] = str(seed)
+                of = Path(td) / f"{name}.random{seed}"
+                rc = ou.run_native("random", ["order_gen", str(mtx), str(of)])
+                assert rc in (0, None), (name, "random", rc)
+                out[f"{name}/random{seed}"] = np.loadtxt(of, dtype=np.int64).astype(np.int32).reshape(-1)
     np.savez_compressed(HERE / "orders.npz", **out)
     print("wrote", HERE / "orders.npz", sorted({k.split('/')[0] for k in out}))
 

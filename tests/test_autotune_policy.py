@@ -29,8 +29,9 @@ class FakeCtx:
 
 
 def test_tune_single_picks_caches_and_persists(at, monkeypatch, tmp_path):
-    cost = {("spa", 8, 512): 3.0, ("elems", 8, 512): 5.0, ("tiles", 8, 512): 4.0, ("rows", 16, 1024): 1.5,
-            ("rows", 8, 256): 2.0, ("rows", 32, 2048): 9.0}
+    cost = {("spa", 8, 512, 0): 3.0, ("spa", 8, 512, 32): 3.5, ("spa", 8, 512, 128): 2.5, ("spa", 8, 512, 257): 2.9,
+            ("elems", 8, 512, 0): 5.0, ("tiles", 8, 512, 0): 4.0, ("rows", 16, 1024, 0): 1.5,
+            ("rows", 8, 256, 0): 2.0, ("rows", 32, 2048, 0): 9.0}
     runs = []
 
     def fake_spgemm(ctx, A, B):
@@ -43,7 +44,7 @@ def test_tune_single_picks_caches_and_persists(at, monkeypatch, tmp_path):
     tuner = at.Autotuner(str(path))
     ctx = FakeCtx()
     choice = tuner.tune_single(ctx, "A", "B", reps=1)
-    assert choice == ("rows", 16, 1024) and ctx.schedule == choice
+    assert choice == ("rows", 16, 1024, 0) and ctx.schedule == choice
     assert set(runs) == set(cost) and len(runs) == 2 * len(cost)          # reps + 1 runs per candidate
     assert tuner.last_timings == cost and ctx.timing is False
     # cached: no timing on the second call, and a fresh tuner reads the file
@@ -51,7 +52,8 @@ def test_tune_single_picks_caches_and_persists(at, monkeypatch, tmp_path):
     assert tuner.tune_single(ctx, "A", "B") == choice and not runs
     again = at.Autotuner(str(path))
     assert again.tune_single(FakeCtx(), "A", "B") == choice and not runs
-    assert at.summarize(cost)["rows-16-1024"] == 1.5
+    assert at.summarize(cost)["rows-16-1024"] == 1.5 and at.summarize(cost)["spa-8-512-d128"] == 2.5
+    assert at.normalize(("spa", 8, 512)) == ("spa", 8, 512, 0)
 
 
 def test_batch_key_separates_sizes(at, monkeypatch):

@@ -1,5 +1,8 @@
 """The drop-in CLI (rw-spgemm_b200/bin/test) with the reference's flags:
-reports the same lines and passes its FP64 cuSPARSE cross-check."""
+reports the same lines and passes its FP64 cuSPARSE cross-check; values are
+overwritten (i % 10) in the reference reader's order and duplicate entries
+computed as the reference computes them."""
+import os
 import re
 import subprocess
 from pathlib import Path
@@ -24,8 +27,9 @@ def write_mtx(path, mat, symmetric_lower=False):
             f.write(f"{r + 1} {c + 1} {x!r}\n")
 
 
-def run(args):
-    out = subprocess.run([str(BIN)] + args, capture_output=True, text=True, timeout=300)
+def run(args, env=None):
+    out = subprocess.run([str(BIN)] + args, capture_output=True, text=True, timeout=300,
+                         env=dict(os.environ, **(env or {})))
     assert out.returncode == 0, out.stderr
     return out.stdout
 
@@ -61,9 +65,107 @@ def test_cli_reorder(tmp_path, gen, oracle, algo):
     a = gen.permute_symmetric(base, gen.random_symmetric_permutation(512, 3))
     p = tmp_path / "st.mtx"
     write_mtx(p, a, symmetric_lower=True)
-    txt = run(["-d", "0", "-aat", "0", str(p), "-reorder", "1", "-reorder_algo", algo])
+    args = ["-d", "0", "-aat", "0", str(p), "-reorder", "1", "-reorder_algo", algo]
+    if algo == "random":
+        # as the reference's adapter: refused unless TASA_ENABLE_UNSAFE_RANDOM=1
+        txt = run(args, env={"TASA_ENABLE_UNSAFE_RANDOM": "0"})
+        assert "external reorder missing dependency: random" in txt
+        assert "external reorder failed, status = -20. Exit." in txt
+    txt = run(args, env={"TASA_ENABLE_UNSAFE_RANDOM": "1"})
     assert f"reorder algorithm = {algo}" in txt and "estimated C tiles after reorder" in txt
     expect_passed(txt, oracle.gustavson(a, a)[3].size)
+
+
+def write_scrambled(path, entries, m, n, symmetric=False):
+    with open(path, "w") as f:
+        f.write(f"%%MatrixMarket matrix coordinate real {'symmetric' if symmetric else 'general'}\n"
+                f"{m} {n} {len(entries)}\n")
+        for r, c in entries:
+            f.write(f"{r + 1} {c + 1} 0.5\n")
+
+
+def reference_read(entries, m, n, symmetric=False):
+    """The reference reader's CSR (src/mmio_highlevel.h:593-759: rows grouped
+    in file order, a mirrored entry placed when its original is read,
+    columns unsorted, duplicates kept) with the CLI's value[i] = i % 10
+    (src/main.cu:191-197), then each row sorted and duplicates summed --
+    the matrix the reference's product computes with."""
+    rows = [[] for _ in range(m)]
+    for r, c in entries:
+        rows[r].append(c)
+        if symmetric and r != c:
+            rows[c].append(r)
+    val, p = [], 0
+    out_rp, out_ci, out_v = [0], [], []
+    for r in range(m):
+        acc = {}
+        for c in rows[r]:
+            acc[c] = acc.get(c, 0.0) + float(p % 10)
+            p += 1
+        for c in sorted(acc):
+            out_ci.append(c)
+            out_v.append(acc[c])
+        out_rp.append(len(out_ci))
+    return (m, n, np.array(out_rp, np.int32), np.array(out_ci, np.int32), np.array(out_v)), p
+
+
+def read_c(path):
+    with open(path) as f:
+        f.readline()
+        m, n, nnz = (int(x) for x in f.readline().split())
+        a = np.loadtxt(f, ndmin=2) if nnz else np.zeros((0, 3))
+    rows = a[:, 0].astype(np.int64) - 1
+    rp = np.zeros(m + 1, np.int64)
+    np.add.at(rp, rows + 1, 1)
+    return np.cumsum(rp), a[:, 1].astype(np.int32) - 1, a[:, 2]
+
+
+def _scrambled_entries(rng, m, n, count, dups, lower=False):
+    ents = set()
+    while len(ents) < count:
+        r, c = int(rng.integers(0, m)), int(rng.integers(0, n))
+        if lower and c > r:
+            r, c = c, r
+        ents.add((r, c))
+    ents = sorted(ents)
+    ents += [ents[int(i)] for i in rng.integers(0, len(ents), dups)]   # duplicate entries
+    rng.shuffle(ents)                                                  # file order not sorted
+    return [tuple(e) for e in ents]
+
+
+@pytest.mark.parametrize("mode", ["AA", "AA-symmetric", "AAT", "AB", "AB-reorder", "AAT-reorder"])
+def test_cli_values_in_file_order_with_duplicates(tmp_path, oracle, mode):
+    rng = np.random.default_rng(sum(map(ord, mode)))
+    n = 300
+    sym = mode == "AA-symmetric"
+    ea = _scrambled_entries(rng, n, n, 1500, 40, lower=sym)
+    pa = tmp_path / "a.mtx"
+    write_scrambled(pa, ea, n, n, symmetric=sym)
+    A, nnz_read = reference_read(ea, n, n, symmetric=sym)
+    args = ["-d", "0", "-aat", "1" if mode.startswith("AAT") else "0", str(pa), "-o", str(tmp_path / "c.mtx")]
+    if mode.startswith("AB"):
+        eb = _scrambled_entries(rng, n, n, 1200, 30)
+        pb = tmp_path / "b.mtx"
+        write_scrambled(pb, eb, n, n)
+        B, _ = reference_read(eb, n, n)
+        args += ["-b", str(pb)]
+    elif mode.startswith("AAT"):
+        import scipy.sparse as sp
+        T = sp.csr_matrix((A[4], A[3], A[2]), shape=(n, n)).T.tocsr()
+        T.sort_indices()
+        B = (n, n, T.indptr.astype(np.int32), T.indices.astype(np.int32), T.data)
+    else:
+        B = A
+    if mode.endswith("reorder"):
+        args += ["-reorder", "1", "-reorder_algo", "rcm" if mode.startswith("AB") else "degree"]
+    txt = run(args)
+    assert f"nnz = {nnz_read}\n" in txt                     # counted as read, duplicates included
+    G = oracle.gustavson(A, B)
+    expect_passed(txt, G[3].size)
+    rp, ci, v = read_c(tmp_path / "c.mtx")
+    np.testing.assert_array_equal(rp, G[2])
+    np.testing.assert_array_equal(ci, G[3])
+    np.testing.assert_array_equal(v, G[4])                   # small integers: exact
 
 
 def test_cli_usage_and_tasa(tmp_path, gen):

@@ -48,6 +48,9 @@ def test_orderings_match_reference_order_utils(tsg, ctx):
         m, n = (int(x) for x in z[f"{nm}/m"])
         mat = (m, n, z[f"{nm}/rowptr"], z[f"{nm}/colidx"], z[f"{nm}/val"])
         rp, ci, _ = _dev(mat)
+        for seed in (1, 7):
+            got = tsg.order(ctx, "random", m, n, rp, ci, seed=seed).cpu().numpy()
+            np.testing.assert_array_equal(got, z[f"{nm}/random{seed}"], err_msg=f"random/{seed} on {nm}")
         for kind in ("original", "degree", "rcm"):
             got = tsg.order(ctx, kind, m, n, rp, ci).cpu().numpy()
             if kind == "rcm" and nm == "rmat7":
@@ -85,10 +88,11 @@ def test_dropin_apply_restore_round_trip(tsg, gen):
 
 
 @pytest.mark.parametrize("algo", ["original", "rcm", "degree", "gray", "random"])
-def test_reorder_plan_estimates_and_restored_product(tsg, ctx, oracle, gen, algo):
+def test_reorder_plan_estimates_and_restored_product(tsg, ctx, oracle, gen, algo, monkeypatch):
     """AA plan on a randomly permuted 3D stencil: the plan's C-tile counts equal
     the oracle's tile counts of the permuted product, and the product computed
     in the new order and restored equals the product of the original matrix."""
+    monkeypatch.setenv("TASA_ENABLE_UNSAFE_RANDOM", "1")
     base = gen.stencil_27pt_3d(10, seed=3)
     mat = gen.permute_symmetric(base, gen.random_symmetric_permutation(1000, 11))
     plan = tsg.build_reorder_plan("AA", algo, mat)
@@ -116,7 +120,64 @@ def test_reorder_plan_estimates_and_restored_product(tsg, ctx, oracle, gen, algo
     assert rel.max() <= 1e-12   # the inner index order changes with the ordering
 
 
-def test_unknown_ordering_reports_missing_dependency(tsg, gen):
+def test_unknown_ordering_reports_missing_dependency(tsg, gen, monkeypatch):
     with pytest.raises(tsg.TsgError) as e:
         tsg.build_reorder_plan("AA", "slashburn", gen.laplacian_2d(8))
     assert e.value.status == -20
+    # the reference's random adapter runs only when asked to (order_gen exits
+    # 42 without TASA_ENABLE_UNSAFE_RANDOM=1, reported as -20)
+    monkeypatch.delenv("TASA_ENABLE_UNSAFE_RANDOM", raising=False)
+    with pytest.raises(tsg.TsgError) as e:
+        tsg.build_reorder_plan("AA", "random", gen.laplacian_2d(8))
+    assert e.value.status == -20
+    monkeypatch.setenv("TASA_ENABLE_UNSAFE_RANDOM", "1")
+    monkeypatch.setenv("TASA_RANDOM_SEED", "7")
+    plan = tsg.build_reorder_plan("AA", "random", gen.laplacian_2d(8))
+    import random
+    want = list(range(64))
+    random.Random(7).shuffle(want)
+    np.testing.assert_array_equal(plan["row_perm"], want)
+
+
+def _inverse(p):
+    q = np.empty_like(p)
+    q[p] = np.arange(p.size)
+    return q
+
+
+@pytest.mark.parametrize("kind", ["AAT", "AB"])
+@pytest.mark.parametrize("algo", ["original", "rcm", "degree", "random"])
+def test_reorder_plan_ab_and_aat(tsg, ctx, oracle, gen, kind, algo, monkeypatch):
+    """A*A^T and A*B plans (src/external_reorder.h:204-321): rows and the inner
+    axis take A's order, columns B's (A's for A*A^T); the plan's tile counts
+    equal the oracle's on the permuted operands, and the product computed in
+    the new order and restored equals the product of the original operands."""
+    monkeypatch.setenv("TASA_ENABLE_UNSAFE_RANDOM", "1")
+    n = 700
+    base = gen.random_poisson(n, None, 5.0, seed=21)   # square, not symmetric
+    A = gen.permute_symmetric(base, gen.random_symmetric_permutation(n, 4))
+    B = gen.transpose(A) if kind == "AAT" else gen.permute_symmetric(gen.banded(n, 6, seed=2),
+                                                                        gen.random_symmetric_permutation(n, 9))
+    plan = tsg.build_reorder_plan(kind, algo, A, B)
+    rp, ip, cp = plan["row_perm"], plan["inner_perm"], plan["col_perm"]
+    np.testing.assert_array_equal(ip, rp)
+    if algo == "original":
+        assert np.array_equal(rp, np.arange(n)) and np.array_equal(cp, np.arange(n))
+    else:
+        np.testing.assert_array_equal(rp, oracle.order(algo, A, seed=1))
+        np.testing.assert_array_equal(cp, rp if kind == "AAT" else oracle.order(algo, B, seed=1))
+    assert plan["shared_symmetric_csr"] == 0
+    PA = oracle.apply_bipermutation(A, rp, _inverse(ip))
+    PB = oracle.apply_bipermutation(B, ip, _inverse(cp))
+    tiles = lambda X, Y: oracle.spgemm_tiled(oracle.csr2tile_row_major(X), oracle.csr2tile_col_major(Y))["numtile"]  # noqa: E731
+    assert plan["estimated_c_tiles_before"] == tiles(A, B)
+    assert plan["estimated_c_tiles_after"] == tiles(PA, PB)
+    assert plan["input_tiles_A_after"] == oracle.csr2tile_row_major(PA)["numtile"]
+    assert plan["input_tiles_B_after"] == oracle.csr2tile_row_major(PB)["numtile"]
+    Cp, _ = tsg.spgemm_csr_host(ctx, tsg.apply_bipermutation_csr(A, rp, ip), tsg.apply_bipermutation_csr(B, ip, cp))
+    C = tsg.restore_bipermutation_csr(Cp, rp, cp)
+    G = oracle.gustavson(A, B)
+    np.testing.assert_array_equal(C[2], G[2])
+    np.testing.assert_array_equal(C[3], G[3])
+    rel = np.abs(C[4] - G[4]) / np.maximum(np.abs(G[4]), 1e-300)
+    assert rel.max(initial=0.0) <= 1e-12   # the inner index order changes with the ordering

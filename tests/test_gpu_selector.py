@@ -63,20 +63,22 @@ def test_mlp_training_reduces_loss(ctx, sel):
 
 def test_selector_beats_fixed_choice_on_held_out(ctx, sel, gen):
     """Trains on method-generated timings of small matrices and checks the
-    model's regret against the exhaustive best on held-out matrices is no
-    worse than the method without the model (original order, default
-    accumulator)."""
-    mats = sel.training_matrices(gen, 36, seed=11)
+    model's mean regret against the exhaustive best on held-out matrices is
+    within 10% (the selector's target), and no worse than the method
+    without the model (original order, default accumulator)."""
+    mats = sel.training_matrices(gen, 80, seed=11)
     data = [sel.time_configs(ctx, m, repeats=2) for m in mats]
     feats = np.stack([d[0] for d in data])
     times = np.stack([d[1] for d in data])
-    tr, te = slice(0, 28), slice(28, 36)
+    tr, te = slice(0, 64), slice(64, 80)
     net = sel.MLP(ctx, seed=7)
-    net.fit(feats[tr], times[tr], epochs=200, lr=3e-3)
+    net.fit(feats[tr], times[tr], epochs=300, lr=2e-3)
     picks = np.argmin(net.predict(feats[te]), axis=1)
     r_model = sel.regret(times[te], picks)[0]
     r_plain = sel.regret(times[te], np.zeros(times[te].shape[0], dtype=int))[0]
-    assert r_model <= r_plain + 0.05
+    print(f"held-out mean regret: model {r_model:.4f}, without the model {r_plain:.4f}")
+    assert r_model <= 0.10
+    assert r_model <= r_plain
     ch = sel.choose(None, ctx, mats[0])
     assert ch.source == "exhaustive" and ch.config in sel.CONFIGS
     net.close()

@@ -134,3 +134,42 @@ def test_device_delivery_matches_host_delivery(srv_mod, gen):
         assert h[0] == d[0] and h[1] == d[1]
         for x, y in zip(h[2:], d[2:]):
             assert np.array_equal(np.asarray(x).view(np.uint8), y.cpu().numpy().view(np.uint8))
+
+
+def test_operand_bytes_match_the_pool(tsg, ctx, gen):
+    """The admission's operand size (tsg_tiled_device_bytes) is what the
+    library holds: the pool's bytes in use grow by it (within the pool's own
+    rounding) when a B-role operand -- tiles, column view, column masks, row
+    view -- is made resident; the tile-data-only count is far below it."""
+    import torch
+    mat = gen.rmat(17, 16, seed=4)
+    torch.cuda.synchronize()
+    ctx.synchronize()
+    before = ctx.pool_used()
+    T = tsg.csr_host_to_tiled(ctx, mat, tsg.TSG_TILED_CSC_VIEW)
+    ctx.synchronize()
+    grown = ctx.pool_used() - before
+    dev = T.device_bytes
+    tile_data_only = (T.s.tilem + 1) * 4 + T.numtile * 68 + T.nnz * 9 + (T.s.tilen + 1) * 4
+    print(f"pool grew {grown} bytes, device_bytes {dev}, tile data only {tile_data_only}")
+    assert abs(grown - dev) <= 0.02 * dev + (1 << 20)
+    assert tile_data_only < 0.75 * dev
+    T.free()
+    ctx.synchronize()
+
+
+def test_auto_schedule_server_matches_the_fixed_one(srv_mod, gen):
+    mats = _matrices(gen)
+    jobs = _jobs(mats, random.Random(3), 40)
+    fixed, _ = _run(srv_mod, mats, jobs, gap=0.0)
+    srv = srv_mod.SpGEMMServer(0, mem_cap=8 << 30, slots=2, max_batch=16, schedule="auto")
+    for k, m in mats.items():
+        srv.register(k, m)
+    srv.start()
+    res = [f.result(timeout=300) for f in [srv.submit(*j) for j in jobs]]
+    st = srv.stats()
+    srv.close()
+    assert st["tuned"], "no batch was tuned"
+    for a, b in zip(res, fixed):
+        for x, y in zip(a[2:], b[2:]):
+            assert np.array_equal(np.asarray(x).view(np.uint8), np.asarray(y).view(np.uint8))

@@ -124,11 +124,14 @@ def test_reference_spgemm_cpu_edge_overcount_is_a_reference_bug(oracle, gen):
 
 def test_oracle_orders_match_reference_order_utils(oracle):
     """Golden orders from the reference's reorder_algorithm/common/order_utils.py
-    (native_original, native_degree, native_rcm), tests/golden/orders.npz."""
+    (native_original, native_degree, native_rcm, native_random with seeds 1
+    and 7), tests/golden/orders.npz."""
     z = np.load(GOLD / "orders.npz")
     for nm in sorted({k.split("/")[0] for k in z.files}):
         m, n = (int(x) for x in z[f"{nm}/m"])
         mat = (m, n, z[f"{nm}/rowptr"], z[f"{nm}/colidx"], z[f"{nm}/val"])
+        for seed in (1, 7):
+            np.testing.assert_array_equal(oracle.order("random", mat, seed=seed), z[f"{nm}/random{seed}"])
         for kind in ("original", "degree", "rcm"):
             got = oracle.order(kind, mat)
             if kind == "rcm" and nm == "rmat7":
@@ -138,3 +141,24 @@ def test_oracle_orders_match_reference_order_utils(oracle):
                 assert np.array_equal(np.sort(got), np.arange(m))
                 continue
             np.testing.assert_array_equal(got, z[f"{nm}/{kind}"], err_msg=f"{kind} on {nm}")
+
+
+def test_random_order_is_pythons_shuffle(oracle, tsg):
+    """The random ordering, in the oracle and in the library's host
+    generator, is random.Random(seed).shuffle(list(range(n))) -- the
+    reference's order_utils.py:70-75 -- for sizes across the rejection
+    sampler's bit lengths and seeds of one and two 32-bit words."""
+    import ctypes
+    import random
+    L = tsg.lib()
+    L.tsg_order_random_host.argtypes = [ctypes.c_int, ctypes.c_ulonglong, ctypes.c_void_p]
+    for n in (0, 1, 2, 3, 17, 1000, 65537, 262144):
+        for seed in (0, 1, 7, 2**32 - 1, 2**32, 2**40 + 3):
+            want = list(range(n))
+            random.Random(seed).shuffle(want)
+            want = np.array(want, dtype=np.int32)
+            empty = (n, n, np.zeros(n + 1, np.int32), np.zeros(0, np.int32), None)
+            np.testing.assert_array_equal(oracle.order("random", empty, seed=seed), want)
+            got = np.zeros(max(n, 1), np.int32)
+            assert L.tsg_order_random_host(n, seed, got.ctypes.data) == 0
+            np.testing.assert_array_equal(got[:n], want)

@@ -47,8 +47,9 @@ class FakeCache:
 
 
 class FakeBatch:
-    def __init__(self, ctx, pairs, *sched, graph=False):
+    def __init__(self, ctx, pairs, *sched, graph=False, dense=0):
         self.pairs = list(pairs)
+        self.sched = tuple(sched) + (dense,)
 
     def info(self):
         return {"arena_bytes": 0}
@@ -71,6 +72,7 @@ def make_server(serve_mod, monkeypatch, mem_cap, budget, sizes, predict):
     srv = serve_mod.SpGEMMServer.__new__(serve_mod.SpGEMMServer)
     srv.deliver, srv.device, srv.mem_cap, srv.max_batch = "device", 0, mem_cap, 64
     srv.batch_products, srv.schedule = float(budget), ("spa", 8, 512)
+    srv.tuner, srv.tuned = None, {}
     srv.matrices = {k: None for k in sizes}
     srv.slots = [FakeSlot(), FakeSlot()]
     srv.cache = FakeCache(sizes)
@@ -78,7 +80,7 @@ def make_server(serve_mod, monkeypatch, mem_cap, budget, sizes, predict):
     srv.lock = threading.Condition()
     srv.running, srv.thread, srv.next_id = False, None, 0
     srv.done, srv.batches, srv.rejected = [], 0, 0
-    srv._predict = lambda A, B: predict[(A, B)]
+    srv._predict = lambda A, B: tuple(predict[(A, B)]) + (1,) * (3 - len(predict[(A, B)]))
     return srv
 
 
@@ -121,3 +123,35 @@ def test_memory_cap_defers_evicts_and_rejects(serve_mod, monkeypatch):
     s0.batch, s0.jobs, s0.arena = None, [], 0
     assert srv._form_batch(s1) and batch_jobs(s1) == [3]
     assert set(srv.cache.evicted) >= {"a", "b"} and srv.cache.bytes + 300 <= 1000
+
+
+class FakeTuner:
+    def __init__(self):
+        self.calls = []
+
+    def tune_batch(self, ctx, pairs, reps=2, use_cache=True):
+        self.calls.append(len(pairs))
+        return ("rows", 16, 1024, 0) if len(self.calls) == 1 else ("spa", 8, 512, 128)
+
+
+def test_auto_schedule_tunes_once_per_density_class(serve_mod, monkeypatch):
+    # (bytes, products, C-tile bound): densities 1 and 1 (class 1), then 100 (class 6)
+    predict = {("a", "b"): (10, 50, 50), ("c", "d"): (10, 40, 40), ("e", "f"): (10, 8000, 80)}
+    srv = make_server(serve_mod, monkeypatch, 10_000, 60, {k: 1 for k in "abcdef"}, predict)
+    srv.schedule, srv.tuner = "auto", FakeTuner()
+    s0, s1 = srv.slots
+    srv.submit("AB", "a", "b")
+    assert srv._form_batch(s0) and s0.batch.sched == ("rows", 16, 1024, 0)
+    s0.batch = None
+    srv.submit("AB", "c", "d")
+    assert srv._form_batch(s0) and s0.batch.sched == ("rows", 16, 1024, 0)   # same class: no new tuning
+    assert srv.tuner.calls == [1]
+    srv.submit("AB", "e", "f")
+    assert srv._form_batch(s1) and s1.batch.sched == ("spa", 8, 512, 128)    # new class: tuned
+    assert srv.tuner.calls == [1, 1] and set(srv.tuned) == {1, 6}
+
+
+def test_operand_bytes_are_the_librarys_allocation(serve_mod):
+    class T:
+        device_bytes = 12345
+    assert serve_mod.OperandCache.tiled_bytes(T()) == 12345
