@@ -87,7 +87,8 @@ struct StgSmem
     unsigned char stage[2][STG_BYTES];
     double acc[STG_CAP + 2];             // a segment's rows' runs, then the sink (and 16-byte padding)
     double outbuf[STG_CAP + 2];          // the segment's C values in C's order at their 16-byte phase
-    unsigned cm[TSG_BS][SPA_SEGT];       // per row and tile: (row's entries in earlier tiles << 16) | row mask
+    unsigned cm[TSG_BS][SPA_SEGT + 1];   // per row and tile: (row's entries in earlier tiles << 16) | row mask
+                                         // (rows padded by a word: a tile's 16 rows in 16 banks)
     unsigned char colbuf[STG_CAP + 16];  // the segment's C column bytes at their 16-byte phase
     int rtot[TSG_BS];                    // entries of each row in the segment
     int rbase[TSG_BS];                   // first slot of each row's run
