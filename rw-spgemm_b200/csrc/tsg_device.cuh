@@ -749,6 +749,7 @@ __device__ __forceinline__ void step3_rows_item(const ProdView &P, long long ite
 #define SPA_THREADS (SPA_WARPS * 32)
 #define SPA_CAP 4096
 #define SPA_SEGT 256
+#define SPA_CMS (SPA_SEGT + 1) // row stride of the [row][tile] words: a tile's 16 rows in 16 banks
 #define SPA_WIN 2048
 #define SPA_STAGE 64
 #define SPA_DENSE TSG_SPA_DENSE_DEFAULT
@@ -787,7 +788,7 @@ struct SpaStage
 struct SpaSmem
 {
     double acc[SPA_CAP];
-    unsigned cm[TSG_BS * SPA_SEGT]; // [row][tile]: (entries of the row in earlier tiles << 16) | C row mask
+    unsigned cm[TSG_BS * SPA_CMS];  // [row][tile]: (entries of the row in earlier tiles << 16) | C row mask
     int rstart[TSG_BS];             // first accumulator slot of each row's private, column-sorted run
     unsigned short map[SPA_WIN];    // tile column - J0 -> segment tile, 0xFFFF none
     SpaStage stage[SPA_WARPS];
@@ -861,7 +862,7 @@ __device__ __forceinline__ void step3_spa_segment(const ProdView &P, SpaSmem &S,
     for (int u = tid; u < nt * TSG_BS; u += SPA_THREADS)
     {
         const int jl = u >> 4, rr = u & 15;
-        S.cm[rr * SPA_SEGT + jl] = P.C_mask[(long long)(t0 + jl) * TSG_BS + rr];
+        S.cm[rr * SPA_CMS + jl] = P.C_mask[(long long)(t0 + jl) * TSG_BS + rr];
         if (rr == 0)
         {
             const int w = P.C_col[t0 + jl] - J0;
@@ -878,7 +879,7 @@ __device__ __forceinline__ void step3_spa_segment(const ProdView &P, SpaSmem &S,
         for (int s0 = 0; s0 < nt; s0 += 32)
         {
             const int sl = s0 + lane;
-            const unsigned m = sl < nt ? S.cm[r * SPA_SEGT + sl] : 0u;
+            const unsigned m = sl < nt ? S.cm[r * SPA_CMS + sl] : 0u;
             const int c = __popc(m);
             int incl = c;
 #pragma unroll
@@ -889,7 +890,7 @@ __device__ __forceinline__ void step3_spa_segment(const ProdView &P, SpaSmem &S,
                     incl += o;
             }
             if (sl < nt)
-                S.cm[r * SPA_SEGT + sl] = ((unsigned)(run + incl - c) << 16) | m;
+                S.cm[r * SPA_CMS + sl] = ((unsigned)(run + incl - c) << 16) | m;
             run += __shfl_sync(TSG_FULL_MASK, incl, 31);
         }
         if (lane == 0)
@@ -908,7 +909,7 @@ __device__ __forceinline__ void step3_spa_segment(const ProdView &P, SpaSmem &S,
     }
     __syncthreads();
     const int rs = S.rstart[r];
-    const unsigned *cmr = S.cm + r * SPA_SEGT;
+    const unsigned *cmr = S.cm + r * SPA_CMS;
     SpaStage &G = S.stage[r];
     const int pa_beg = P.A_ptr[I], pa_end = P.A_ptr[I + 1];
     for (int g = pa_beg; g < pa_end; g += 32)
@@ -1097,7 +1098,7 @@ __device__ __forceinline__ void step3_spa_segment(const ProdView &P, SpaSmem &S,
     for (int u = tid; u < nt * TSG_BS; u += SPA_THREADS)
     {
         const int jl = u >> 4, rr = u & 15;
-        const unsigned cmw = S.cm[rr * SPA_SEGT + jl];
+        const unsigned cmw = S.cm[rr * SPA_CMS + jl];
         unsigned mk = cmw & 0xFFFFu;
         if (!mk)
             continue;
@@ -1134,6 +1135,7 @@ __device__ __forceinline__ void step3_spa_segment(const ProdView &P, SpaSmem &S,
 // The masks then go out through step2_store like every other step-2 path.
 // ---------------------------------------------------------------------------
 #define SP2_SEGT 1024
+#define SP2_MS (SP2_SEGT + 1) // row stride of the [row][tile] mask words (a tile's rows in distinct banks)
 #define SP2_WIN 4096
 
 struct Spa2Stage
@@ -1145,7 +1147,7 @@ struct Spa2Stage
 
 struct Spa2Smem
 {
-    unsigned m[TSG_BS * SP2_SEGT]; // [row][tile] mask words
+    unsigned m[TSG_BS * SP2_MS]; // [row][tile] mask words
     unsigned short map[SP2_WIN];
     Spa2Stage stage[SPA_WARPS];
 };
@@ -1161,7 +1163,7 @@ __device__ __forceinline__ void step2_spa_segment(const ProdView &P, Spa2Smem &S
     const bool full = t0 == P.C_ptr[I] && t1 == P.C_ptr[I + 1];
     __syncthreads();
     for (int q = tid; q < nt * TSG_BS; q += SPA_THREADS)
-        S.m[(q & 15) * SP2_SEGT + (q >> 4)] = 0u;
+        S.m[(q & 15) * SP2_MS + (q >> 4)] = 0u;
     for (int q = tid; q < win; q += SPA_THREADS)
         S.map[q] = 0xFFFF;
     __syncthreads();
@@ -1259,7 +1261,7 @@ __device__ __forceinline__ void step2_spa_segment(const ProdView &P, Spa2Smem &S
                     continue;
                 const int slot = S.map[J - J0];
                 if (slot < nt)
-                    atomicOr(&S.m[r * SP2_SEGT + slot], 1u << (15 - (col & 15)));
+                    atomicOr(&S.m[r * SP2_MS + slot], 1u << (15 - (col & 15)));
             }
         }
     }
@@ -1267,7 +1269,7 @@ __device__ __forceinline__ void step2_spa_segment(const ProdView &P, Spa2Smem &S
     // half-warp per C tile: row offsets, masks, tile count, bin
     const unsigned hmask = TSG_HW_MASK(tid);
     for (int jl = tid >> 4; jl < nt; jl += SPA_THREADS / 16)
-        step2_store(P, t0 + jl, hmask, tid & 15, S.m[(tid & 15) * SP2_SEGT + jl], s_bins);
+        step2_store(P, t0 + jl, hmask, tid & 15, S.m[(tid & 15) * SP2_MS + jl], s_bins);
 }
 
 // ---------------------------------------------------------------------------
