@@ -607,6 +607,32 @@ def run_hyper(args, tsg, gen, ctx, reps=3):
             "ms_steps_1_3": round(best, 4), "gflops": round(2.0 * prods / (best * 1e-3) / 1e9, 2)}
 
 
+def run_rmat16(args, tsg, gen, ctx, reps=3):
+    """One R-MAT product small enough to hold whole: scale 16, edge factor 16,
+    C = A*A (the kind of work of one scale-20 row block: hub rows, C tile
+    rows thousands of tiles wide with few values per tile).  Steps 1-3, min
+    of reps, CUDA events."""
+    A = gen.rmat(16, 16, seed=1)
+    TA = tsg.csr_host_to_tiled(ctx, A, tsg.TSG_TILED_PACKED_COL)
+    TB = tsg.csr_host_to_tiled(ctx, A, tsg.TSG_TILED_CSC_VIEW)
+    prods = tsg.product_bounds(ctx, TA, TB)[0]
+    ctx.set_timing(True)
+    best = None
+    for _ in range(reps):
+        C, info = tsg.spgemm(ctx, TA, TB)
+        C.free()
+        if best is None or info["ms_total"] < best["ms_total"]:
+            best = info
+    ctx.set_timing(False)
+    TA.free()
+    TB.free()
+    return {"workload": "R-MAT scale 16, edge factor 16 (n=65,536), C = A*A, FP64 U(-1,1)", "products": int(prods),
+            "tiles_C": int(best["numtile_C"]), "nnz_C": int(best["nnz_C"]),
+            "step_ms": {k: round(best[k], 3) for k in ("ms_step1", "ms_step2", "ms_step3")},
+            "ms_steps_1_3": round(best["ms_total"], 3), "gflops": round(2.0 * prods / (best["ms_total"] * 1e-3) / 1e9, 2),
+            "numeric_kernel": best["step3_name"]}
+
+
 def run_rmat20(args, tsg, gen, ctx, budget=1.5e9, rank=0, world=1, dist=None, device=None):
     """R-MAT scale 20 (edge factor 16, a,b,c,d = .57,.19,.19,.05, duplicates
     merged, values U(-1,1)): C = A*A and C = A*A^T.  C (~9.7e9 nonzeros) does
@@ -823,6 +849,7 @@ def run_ours(args, tsg, gen, world, rank, local):
     selector = run_selector(args, tsg, gen, ctx) if "selector" in sections else None
     orderings = run_orderings(args, tsg, gen, ctx) if "orderings" in sections else None
     hyper = run_hyper(args, tsg, gen, ctx) if "hyper" in sections else None
+    rmat16 = run_rmat16(args, tsg, gen, ctx) if "rmat16" in sections else None
     rmat20 = (run_rmat20(args, tsg, gen, ctx, rank=rank, world=world, dist=dist, device=dev)
               if "rmat20" in sections else None)
     out = {
@@ -864,6 +891,8 @@ def run_ours(args, tsg, gen, world, rank, local):
         out["orderings"] = orderings
     if hyper:
         out["hypersparse"] = hyper
+    if rmat16:
+        out["rmat16"] = rmat16
     if rmat20:
         out["rmat20_sharded" if world > 1 else "rmat20"] = rmat20
         # the second benchmark configuration beside the headline
@@ -892,7 +921,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--sched", default="spa", choices=["rows", "tiles", "elems", "spa"])
     ap.add_argument("--sections", default="plain,cusparse,batched,served,orderings,hyper,rmat20,selector",
-                    help="comma list: plain (always), cusparse, batched, served, orderings, hyper, rmat20, selector")
+                    help="comma list: plain (always), cusparse, batched, served, orderings, hyper, rmat16, rmat20, "
+                         "selector")
     ap.add_argument("--batch-count", type=int, default=512)
     ap.add_argument("--selector-samples", type=int, default=5000)
     ap.add_argument("--served-jobs", type=int, default=2000)

@@ -88,12 +88,24 @@ void csr2tile_col_major(SMatrix *matrix);
 
 /* Tiled SpGEMM C = A*B.  A from csr2tile_row_major, B from
  * csr2tile_col_major.  Replaces tilespgemm, src/tilespgemm-cuda.h:2610-2624.
- * The intersection bitmaps and densities are accepted for ABI compatibility
- * and not needed by this implementation.  Runs the product REPEAT (5) times,
+ * The intersection bitmaps (tile_intersection_bitmaps below) and the
+ * densities are accepted for ABI compatibility and IGNORED: this
+ * implementation's steps read A's and B's tile columns, masks and column
+ * view directly instead of intersecting bitmaps.  Runs the product REPEAT (5) times,
  * reports the minimum time of the reference's window (C allocation through
  * the numeric step), and fills matrixC's host tile arrays (tile_ptr,
  * tile_columnidx, tile_rowidx, tile_nnz, tile_csr_Ptr, tile_csr_Col,
  * tile_csr_Value, mask, numtile, nnz, m, n, tilem, tilen). */
+/* The reference driver's intersection bitmaps (src/main.cu:430-465), built on
+ * the GPU: len = ceil(A->tilen / 32); A's tile row i sets bit (31 - j % 32) of
+ * word i * len + j / 32 for each of its tile columns j (tile_ptr,
+ * tile_columnidx of csr2tile_row_major); B's tile column i the same for each
+ * of its tile rows (csc_tile_ptr, csc_tile_rowidx of csr2tile_col_major).
+ * *bitmask_A (tilem x len words) and *bitmask_B (B->tilen x len) are
+ * malloc'd, the caller frees them.  Returns 0 or a TSG_ERR_* code. */
+int tile_intersection_bitmaps(const SMatrix *A, const SMatrix *B, unsigned int **bitmask_A,
+                              unsigned int **bitmask_B, int *bitmask_len);
+
 void tilespgemm(SMatrix *matrixA,
                 SMatrix *matrixB,
                 SMatrix *matrixC,
@@ -422,6 +434,16 @@ int tsg_spgemm_csr_host(tsg_context *ctx,
 #define TSG_ORDER_RANDOM 4
 int tsg_order(tsg_context *ctx, int kind, int m, int n, int nnz,
               const int *d_rowptr, const int *d_col, unsigned long long seed, int *d_order);
+/* A plan's tile-count estimates for the permutations already in info
+ * (row_perm, inner_perm, col_perm): input_tiles_{A,B}_{before,after},
+ * estimated_c_tiles_{before,after} and the two risk ratios, computed as the
+ * reference's plans compute them (src/external_reorder.h:143-171): sampled
+ * over 24 evenly strided tile rows and scaled (src/reorder.h:785-975), on the
+ * host.  build_original_reorder_plan and build_external_reorder_plan fill
+ * them the same way.  No reference counterpart as a public call (the
+ * reference's fill_reorder_estimates is file-local). */
+int tsg_reorder_estimates(ReorderProblemKind kind, const SMatrix *matrixA, const SMatrix *matrixB,
+                          ReorderInfo *info);
 /* TSG_ORDER_RANDOM's permutation written to host memory (no device work):
  * order[0..n) = random.Random(seed).shuffle(list(range(n))) of CPython. */
 int tsg_order_random_host(int n, unsigned long long seed, int *order);

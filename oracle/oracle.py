@@ -295,3 +295,182 @@ def ref_spgemm_spa(matA, matB):
     R.ref_spgemm_spa_cols(mA, nA, int(ciA.size), rpA.ctypes.data, ciA.ctypes.data, mB, nB, int(ciB.size),
                           rpB.ctypes.data, ciB.ctypes.data, rpC.ctypes.data, ciC.ctypes.data)
     return rpC[:mA + 1], ciC[:nnz]
+
+
+def intersection_bitmaps(tilesA, tilesB):
+    """The driver's intersection bitmaps, src/main.cu:430-465: len =
+    ceil(tilen_A / 32) words per A tile row (bit 31 - j % 32 of word j / 32
+    for each tile column j) and per B tile column (the same for each of its
+    tile rows)."""
+    n = (int(tilesA["tilen"]) + 31) // 32
+
+    def build(rows, ptr, idx):
+        out = np.zeros((rows, max(n, 1)), dtype=np.uint32)
+        for i in range(rows):
+            for j in np.asarray(idx[ptr[i]:ptr[i + 1]], dtype=np.int64):
+                out[i, j // 32] |= np.uint32(1 << (31 - (j % 32)))
+        return out
+
+    return (build(int(tilesA["tilem"]), tilesA["tile_ptr"], tilesA["tile_columnidx"]),
+            build(int(tilesB["tilen"]), tilesB["csc_tile_ptr"], tilesB["csc_tile_rowidx"]))
+
+
+# --- reorder-plan estimators -------------------------------------------------
+REF_REORDER_SO = HERE / "_ref" / "libtsgref_reorder.so"
+PLAN_SAMPLE_ROWS = 24  # GTSP_PROXY_SAMPLE_ROWS, src/reorder.h:23
+_rr = None
+
+
+class OAxis(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int), ("old_id", _ip), ("new_id", _ip)]
+
+
+class OReorderInfo(ctypes.Structure):
+    """ReorderInfo, src/reorder.h:33-63."""
+    _fields_ = [("enabled", ctypes.c_int), ("n", ctypes.c_int), ("row_perm", OAxis), ("inner_perm", OAxis),
+                ("col_perm", OAxis)] + \
+               [(f, ctypes.c_longlong) for f in ("input_tiles_A_before", "input_tiles_A_after", "input_tiles_B_before",
+                                                 "input_tiles_B_after", "estimated_c_tiles_before",
+                                                 "estimated_c_tiles_after")] + \
+               [(f, ctypes.c_double) for f in ("reorder_time_ms", "signature_time_ms", "tile_profile_time_ms",
+                                               "affinity_time_ms", "sort_time_ms", "local_refine_time_ms",
+                                               "proxy_time_ms", "permute_time_ms", "risk_input_tile_ratio",
+                                               "risk_c_tile_ratio")] + \
+               [(f, ctypes.c_int) for f in ("local_refine_window", "proxy_sample_rows", "guard_degraded_to_identity",
+                                            "structural_conservative", "shared_symmetric_csr")] + \
+               [("mode", ctypes.c_char * 64), ("risk_reason", ctypes.c_char * 128)]
+
+
+ESTIMATE_FIELDS = ("input_tiles_A_before", "input_tiles_A_after", "input_tiles_B_before", "input_tiles_B_after",
+                   "estimated_c_tiles_before", "estimated_c_tiles_after", "risk_input_tile_ratio",
+                   "risk_c_tile_ratio")
+
+
+def ref_reorder_available() -> bool:
+    return REF_REORDER_SO.exists()
+
+
+def rrlib():
+    global _rr
+    if _rr is None:
+        _rr = ctypes.CDLL(str(REF_REORDER_SO))
+        vp = ctypes.c_void_p
+        for f in ("ref_est_input_tiles",):
+            getattr(_rr, f).restype = ctypes.c_longlong
+            getattr(_rr, f).argtypes = [vp, vp, vp]
+        _rr.ref_est_c_tiles.restype = ctypes.c_longlong
+        _rr.ref_est_c_tiles.argtypes = [vp, vp, vp, vp]
+        _rr.ref_est_c_tiles_ab.restype = ctypes.c_longlong
+        _rr.ref_est_c_tiles_ab.argtypes = [vp, vp, vp, vp, vp]
+        _rr.ref_fill_reorder_estimates.argtypes = [ctypes.c_int, vp, vp, vp]
+        _rr.ref_build_original_reorder_plan.argtypes = [ctypes.c_int, vp, vp, vp]
+        _rr.ref_reorder_info_init.argtypes = [vp]
+    return _rr
+
+
+class _AxisHold:
+    """AxisPermutation of a new -> old permutation (None: identity -> NULL)."""
+
+    def __init__(self, old):
+        self.ax = None
+        if old is not None:
+            self.old = np.ascontiguousarray(old, dtype=np.int32)
+            self.new = np.empty_like(self.old)
+            self.new[self.old] = np.arange(self.old.size, dtype=np.int32)
+            self.ax = OAxis(int(self.old.size), self.old.ctypes.data_as(_ip), self.new.ctypes.data_as(_ip))
+
+    def ref(self):
+        return ctypes.byref(self.ax) if self.ax is not None else None
+
+
+def ref_reorder_estimates(kind, matA, matB, row_old, inner_old, col_old):
+    """The reference's fill_reorder_estimates (src/external_reorder.h:143-171)
+    for the plan's three axis permutations (new -> old); kind "AA"/"AAT"/"AB"."""
+    R = rrlib()
+    hA = _CSRHold(matA)
+    hB = _CSRHold(matB) if matB is not None else hA
+    info = OReorderInfo()
+    R.ref_reorder_info_init(ctypes.byref(info))
+    axes = [_AxisHold(p) for p in (row_old, inner_old, col_old)]
+    info.row_perm, info.inner_perm, info.col_perm = (a.ax for a in axes)
+    R.ref_fill_reorder_estimates({"AA": 0, "AAT": 1, "AB": 2}[kind], ctypes.byref(hA.om), ctypes.byref(hB.om),
+                                 ctypes.byref(info))
+    return {f: getattr(info, f) for f in ESTIMATE_FIELDS}
+
+
+def _samples(tiles):
+    sc = min(tiles, PLAN_SAMPLE_ROWS)
+    stride = (tiles + sc - 1) // sc if sc > 0 else 1
+    return [s * stride for s in range(sc) if s * stride < tiles]
+
+
+def _scaled(total, tiles, samples):
+    return int(float(total) * float(tiles) / float(samples)) if samples else 0
+
+
+def _tile_row_cols(mat, tile_row, row_old, col_new):
+    """Tile columns (new ids) of the new tile row's rows, src/reorder.h:837-858."""
+    m, _, rp, ci, _ = mat
+    cols = []
+    for new_row in range(tile_row * 16, min(tile_row * 16 + 16, m)):
+        old = int(row_old[new_row]) if row_old is not None else new_row
+        c = np.asarray(ci[rp[old]:rp[old + 1]], dtype=np.int64)
+        cols.append((col_new[c] if col_new is not None else c) // 16)
+    return np.unique(np.concatenate(cols)) if cols else np.zeros(0, np.int64)
+
+
+def _inv(old):
+    if old is None:
+        return None
+    new = np.empty(len(old), dtype=np.int64)
+    new[np.asarray(old)] = np.arange(len(old))
+    return new
+
+
+def est_input_tiles(mat, row_old=None, col_old=None):
+    """estimate_input_tile_count_biperm, src/reorder.h:785-829: distinct tile
+    columns of 24 evenly strided tile rows, scaled to all tile rows."""
+    tilem = (mat[0] + 15) // 16
+    col_new = _inv(col_old)
+    smp = _samples(tilem)
+    total = sum(int(_tile_row_cols(mat, t, row_old, col_new).size) for t in smp)
+    return _scaled(total, tilem, len(smp))
+
+
+def est_c_tiles(matA, matB, row_old=None, inner_old=None, col_old=None, ab=True):
+    """estimate_symbolic_c_tile_count(_ab), src/reorder.h:890-975: for 24
+    strided tile rows of A, the distinct tile columns of the B tile rows its
+    tile columns name, scaled.  ab=False is the one-matrix form (B = A, every
+    axis counted in A's tile rows)."""
+    rows = (matA[0] + 15) // 16
+    inner = (matA[1] + 15) // 16 if ab else rows
+    inner_new, col_new = _inv(inner_old), _inv(col_old)
+    smp = _samples(rows)
+    total = 0
+    for t in smp:
+        marked = set()
+        for it in _tile_row_cols(matA, t, row_old, inner_new):
+            if 0 <= it < inner:
+                marked.update(_tile_row_cols(matB, int(it), inner_old, col_new).tolist())
+        total += len(marked)
+    return _scaled(total, rows, len(smp))
+
+
+def reorder_estimates(kind, matA, matB, row_old, inner_old, col_old):
+    """The plan's estimate fields by the restatement above (the layout of
+    src/external_reorder.h:143-171)."""
+    if kind == "AA":
+        a0 = est_input_tiles(matA)
+        a1 = est_input_tiles(matA, row_old, inner_old)
+        b0, b1 = a0, a1
+        c0 = est_c_tiles(matA, matA, ab=False)
+        c1 = est_c_tiles(matA, matA, row_old, inner_old, col_old, ab=False)
+    else:
+        a0, a1 = est_input_tiles(matA), est_input_tiles(matA, row_old, inner_old)
+        b0, b1 = est_input_tiles(matB), est_input_tiles(matB, inner_old, col_old)
+        c0 = est_c_tiles(matA, matB)
+        c1 = est_c_tiles(matA, matB, row_old, inner_old, col_old)
+    ratio = lambda after, before: 1.0 if before <= 0 else after / before  # noqa: E731
+    return dict(input_tiles_A_before=a0, input_tiles_A_after=a1, input_tiles_B_before=b0, input_tiles_B_after=b1,
+                estimated_c_tiles_before=c0, estimated_c_tiles_after=c1,
+                risk_input_tile_ratio=max(ratio(a1, a0), ratio(b1, b0)), risk_c_tile_ratio=ratio(c1, c0))

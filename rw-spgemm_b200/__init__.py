@@ -34,6 +34,7 @@ _c_int_p = ctypes.POINTER(ctypes.c_int)
 _c_dbl_p = ctypes.POINTER(ctypes.c_double)
 _c_u8_p = ctypes.POINTER(ctypes.c_ubyte)
 _c_u16_p = ctypes.POINTER(ctypes.c_ushort)
+_c_u32_p = ctypes.POINTER(ctypes.c_uint)
 
 
 class SMatrix(ctypes.Structure):
@@ -251,6 +252,23 @@ def tile2csr(tiles: dict):
     ci = _np_from(sm.columnindex, sm.nnz, np.int32, True)
     v = _np_from(sm.value, sm.nnz, np.float64, True)
     return rp, ci, v
+
+
+def tile_intersection_bitmaps(tilesA: dict, tilesB: dict):
+    """The reference driver's intersection bitmaps (src/main.cu:430-465) on
+    the GPU: (bitmask_A [tilem x len], bitmask_B [tilen_B x len]) uint32."""
+    smA, holdA = smatrix_from_tiles(tilesA)
+    smB, holdB = smatrix_from_tiles(tilesB)
+    pa, pb, ln = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_int(0)
+    L = lib()
+    L.tile_intersection_bitmaps.argtypes = [ctypes.POINTER(SMatrix), ctypes.POINTER(SMatrix), ctypes.POINTER(ctypes.c_void_p),
+                                            ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_int)]
+    check(L.tile_intersection_bitmaps(ctypes.byref(smA), ctypes.byref(smB), ctypes.byref(pa), ctypes.byref(pb),
+                                      ctypes.byref(ln)))
+    n = ln.value
+    bmA = _np_from(ctypes.cast(pa, _c_u32_p), int(tilesA["tilem"]) * n, np.uint32, True).reshape(-1, max(n, 1))
+    bmB = _np_from(ctypes.cast(pb, _c_u32_p), int(tilesB["tilen"]) * n, np.uint32, True).reshape(-1, max(n, 1))
+    return bmA, bmB
 
 
 def tilespgemm(tilesA: dict, tilesB: dict, nnzCub: int = 0) -> tuple[dict, dict]:
@@ -576,6 +594,25 @@ class _Axis:
         self.new = np.empty_like(self.old)
         self.new[self.old] = np.arange(self.old.size, dtype=np.int32)
         self.s = AxisPermutation(int(self.old.size), self.old.ctypes.data_as(_c_int_p), self.new.ctypes.data_as(_c_int_p))
+
+
+PLAN_ESTIMATES = ("input_tiles_A_before", "input_tiles_A_after", "input_tiles_B_before", "input_tiles_B_after",
+                  "estimated_c_tiles_before", "estimated_c_tiles_after", "risk_input_tile_ratio", "risk_c_tile_ratio")
+
+
+def reorder_estimates(kind: str, matA, matB, row_old, inner_old, col_old) -> dict:
+    """tsg_reorder_estimates: a plan's sampled tile-count estimates for three
+    new -> old permutations (host computation, no device work)."""
+    hA = HostCSR(matA)
+    hB = HostCSR(matB) if matB is not None else hA
+    axes = [_Axis(p) for p in (row_old, inner_old, col_old)]
+    info = ReorderInfo()
+    info.row_perm, info.inner_perm, info.col_perm = (a.s for a in axes)
+    L = lib()
+    L.tsg_reorder_estimates.argtypes = [ctypes.c_int, ctypes.POINTER(SMatrix), ctypes.POINTER(SMatrix),
+                                        ctypes.POINTER(ReorderInfo)]
+    check(L.tsg_reorder_estimates(REORDER_PROBLEM[kind], ctypes.byref(hA.sm), ctypes.byref(hB.sm), ctypes.byref(info)))
+    return {f: getattr(info, f) for f in PLAN_ESTIMATES}
 
 
 def _csr_from_smatrix(sm: SMatrix, free=True):

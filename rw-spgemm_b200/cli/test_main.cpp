@@ -485,11 +485,25 @@ int main(int argc, char **argv)
     printf("tile space overhead = %.2f MB\n", tile_bytes / 1024 / 1024);
     csr2tile_col_major(&Bt);
 
+    // the driver's intersection bitmaps and densities (src/main.cu:430-465),
+    // handed to tilespgemm like the reference does (which ignores them)
+    unsigned int *bmA = NULL, *bmB = NULL;
+    int bmlen = 0;
+    if (tile_intersection_bitmaps(&At, &Bt, &bmA, &bmB, &bmlen) != 0)
+    {
+        printf("intersection bitmaps failed: %s. Exit.\n", tsg_last_error());
+        return 0;
+    }
+    const double densA = (double)At.numtile / ((double)At.tilem * (double)At.tilen);
+    const double densB = (double)Bt.numtile / ((double)Bt.tilem * (double)Bt.tilen);
     SMatrix C;
     memset(&C, 0, sizeof(C));
     unsigned long long nnzC = 0;
     double cr = 0, ttile = 0, gf = 0, s1 = 0, s2 = 0, s3 = 0, sm = 0;
-    tilespgemm(&At, &Bt, &C, NULL, NULL, 0, 0.0, 0.0, nnzCub, &nnzC, &cr, &ttile, &gf, filename, &s1, &s2, &s3, &sm);
+    tilespgemm(&At, &Bt, &C, bmA, bmB, bmlen, densA, densB, nnzCub, &nnzC, &cr, &ttile, &gf, filename, &s1, &s2,
+               &s3, &sm);
+    free(bmA);
+    free(bmB);
 
     printf("-------------------------------check----------------------------------------\n");
     tile2csr(&C);

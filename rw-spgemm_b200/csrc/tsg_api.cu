@@ -657,6 +657,81 @@ extern "C" void tile2csr(SMatrix *matrix)
     cudaStreamSynchronize(ctx->stream);
 }
 
+// ---------------------------------------------------------------------------
+// Intersection bitmaps of the reference's driver (src/main.cu:430-465): a
+// warp per tile row (A) or tile column (B), its lanes over the row's tiles,
+// each setting bit 31 - idx % 32 of word idx / 32 of the row's words.
+// ---------------------------------------------------------------------------
+__global__ void k_tile_bitmaps(int rows, int len, const int *__restrict__ ptr, const int *__restrict__ idx,
+                               unsigned *__restrict__ bits)
+{
+    const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= rows)
+        return;
+    unsigned *row = bits + w * (long long)len;
+    for (int j = ptr[w] + lane; j < ptr[w + 1]; j += 32)
+    {
+        const int c = idx[j];
+        if (c >= 0 && (c >> 5) < len) // validated on the host; kept inside the row regardless
+            atomicOr(&row[c >> 5], 1u << (31 - (c & 31)));
+    }
+}
+
+static int bitmaps_of(tsg_context *ctx, int rows, int len, const int *h_ptr, const int *h_idx, unsigned **out)
+{
+    *out = (unsigned *)calloc((size_t)rows * len > 0 ? (size_t)rows * len : 1, sizeof(unsigned));
+    if (!*out)
+        return tsg_set_error(TSG_ERR_OOM, "host allocation failed");
+    if (rows == 0 || len == 0)
+        return TSG_OK;
+    const int n = h_ptr[rows];
+    int *d_ptr, *d_idx;
+    unsigned *d_bits;
+    TSG_TRY(tsg_alloc(ctx, &d_ptr, (size_t)rows + 1));
+    TSG_TRY(tsg_alloc(ctx, &d_idx, (size_t)(n > 0 ? n : 1)));
+    TSG_TRY(tsg_alloc(ctx, &d_bits, (size_t)rows * len));
+    TSG_CUDA(cudaMemcpyAsync(d_ptr, h_ptr, ((size_t)rows + 1) * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    if (n > 0)
+        TSG_CUDA(cudaMemcpyAsync(d_idx, h_idx, (size_t)n * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    TSG_CUDA(cudaMemsetAsync(d_bits, 0, (size_t)rows * len * sizeof(unsigned), ctx->stream));
+    k_tile_bitmaps<<<tsg_blocks((long long)rows * 32, 256), 256, 0, ctx->stream>>>(rows, len, d_ptr, d_idx, d_bits);
+    TSG_LAUNCH_CHECK();
+    TSG_CUDA(cudaMemcpyAsync(*out, d_bits, (size_t)rows * len * sizeof(unsigned), cudaMemcpyDeviceToHost,
+                             ctx->stream));
+    TSG_CUDA(cudaStreamSynchronize(ctx->stream));
+    tsg_release(ctx, d_ptr);
+    tsg_release(ctx, d_idx);
+    tsg_release(ctx, d_bits);
+    return TSG_OK;
+}
+
+extern "C" int tile_intersection_bitmaps(const SMatrix *A, const SMatrix *B, unsigned **bitmask_A,
+                                         unsigned **bitmask_B, int *bitmask_len)
+{
+    if (!A || !B || !bitmask_A || !bitmask_B || !bitmask_len || !A->tile_ptr || !B->csc_tile_ptr ||
+        (A->numtile > 0 && !A->tile_columnidx) || (B->numtile > 0 && !B->csc_tile_rowidx))
+        return tsg_set_error(TSG_ERR_INVALID, "tile_intersection_bitmaps: A needs csr2tile_row_major's tiles, "
+                                              "B csr2tile_col_major's");
+    if (A->tilen != B->tilem)
+        return tsg_set_error(TSG_ERR_INVALID, "tile_intersection_bitmaps: A has %d tile columns, B %d tile rows",
+                             A->tilen, B->tilem);
+    *bitmask_A = *bitmask_B = nullptr;
+    const int len = (A->tilen + 31) / 32; // ceil(tilen_A / 32), as the reference's driver
+    *bitmask_len = len;
+    tsg_context *ctx = tsg_dropin_context();
+    int st = bitmaps_of(ctx, A->tilem, len, A->tile_ptr, A->tile_columnidx, bitmask_A);
+    if (st == TSG_OK)
+        st = bitmaps_of(ctx, B->tilen, len, B->csc_tile_ptr, B->csc_tile_rowidx, bitmask_B);
+    if (st != TSG_OK)
+    {
+        free(*bitmask_A);
+        free(*bitmask_B);
+        *bitmask_A = *bitmask_B = nullptr;
+    }
+    return st;
+}
+
 #define DROPIN_REPEAT 5
 
 extern "C" void tilespgemm(SMatrix *matrixA, SMatrix *matrixB, SMatrix *matrixC,

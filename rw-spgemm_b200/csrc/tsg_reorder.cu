@@ -28,7 +28,6 @@
 #include "tsg_internal.h"
 
 
-int tsg_count_c_tiles(tsg_context *ctx, const tsg_tiled *A, const tsg_tiled *B, long long *numC);
 
 extern "C" int tsg_order_from_name(const char *name)
 {
@@ -763,19 +762,112 @@ static int permute_dev(tsg_context *ctx, const DevCSR *in, const int *h_row_old,
     return TSG_OK;
 }
 
-// tiles of A, tiles of B and C tiles of A*B (exact, from the tile structure)
-static int structure_counts(tsg_context *ctx, const DevCSR *A, const DevCSR *B, long long *tA, long long *tB,
-                            long long *tC)
+// ---------------------------------------------------------------------------
+// Sampled tile counts of a reorder plan, as the reference reports them
+// (src/reorder.h:785-975, GTSP_PROXY_SAMPLE_ROWS = 24): a count over
+// PLAN_SAMPLE_ROWS tile rows taken at an even stride, scaled to all tile rows
+// (total * tile rows / samples in double, truncated).  Host code, like the
+// reference's: 24 tile rows and their B tile rows, no device work.
+// ---------------------------------------------------------------------------
+#define PLAN_SAMPLE_ROWS 24
+
+static int perm_old(const AxisPermutation *p, int id) { return p ? p->old_id[id] : id; }
+static int perm_new(const AxisPermutation *p, int id) { return p ? p->new_id[id] : id; }
+
+static long long scaled_estimate(long long total, int tiles, int samples)
 {
-    tsg_tiled ta, tb;
-    TSG_TRY(tsg_csr_to_tiled(ctx, A->m, A->n, A->nnz, A->rp, A->ci, A->v, 0, &ta));
-    TSG_TRY(tsg_csr_to_tiled(ctx, B->m, B->n, B->nnz, B->rp, B->ci, B->v, 0, &tb));
-    *tA = ta.numtile;
-    *tB = tb.numtile;
-    TSG_TRY(tsg_count_c_tiles(ctx, &ta, &tb, tC));
-    tsg_tiled_free(ctx, &ta);
-    tsg_tiled_free(ctx, &tb);
-    return TSG_OK;
+    return samples ? (long long)((double)total * (double)tiles / (double)samples) : 0;
+}
+
+// visits the new tile columns of the entries of new tile row tr of M (rows
+// through row_perm, columns through col_perm)
+template <typename F>
+static void tile_row_cols(const SMatrix *M, int tr, const AxisPermutation *row, const AxisPermutation *col, F f)
+{
+    const int r1 = tr * TSG_BS + TSG_BS < M->m ? tr * TSG_BS + TSG_BS : M->m;
+    for (int nr = tr * TSG_BS; nr < r1; nr++)
+    {
+        const int o = perm_old(row, nr);
+        for (int j = M->rowpointer[o]; j < M->rowpointer[o + 1]; j++)
+            f(perm_new(col, M->columnindex[j]) / TSG_BS);
+    }
+}
+
+static void plan_samples(int tiles, int *count, int *stride)
+{
+    *count = tiles < PLAN_SAMPLE_ROWS ? tiles : PLAN_SAMPLE_ROWS;
+    *stride = *count > 0 ? (tiles + *count - 1) / *count : 1;
+}
+
+// tile count of M under (row, col): distinct tile columns per sampled tile row
+static long long estimate_input_tiles(const SMatrix *M, const AxisPermutation *row, const AxisPermutation *col)
+{
+    const int tilem = (M->m + TSG_BS - 1) / TSG_BS, tilen = (M->n + TSG_BS - 1) / TSG_BS;
+    int count, stride, used = 0;
+    plan_samples(tilem, &count, &stride);
+    std::vector<int> seen((size_t)(tilen > 0 ? tilen : 1), -1);
+    long long total = 0;
+    for (int sm = 0; sm < count; sm++)
+    {
+        const int tr = sm * stride;
+        if (tr >= tilem)
+            continue;
+        tile_row_cols(M, tr, row, col, [&](int c) {
+            if (seen[c] != sm)
+            {
+                seen[c] = sm;
+                total++;
+            }
+        });
+        used++;
+    }
+    return scaled_estimate(total, tilem, used);
+}
+
+// C tile count of A*B under (row, inner, col): for a sampled tile row of A,
+// the distinct tile columns of the B tile rows its tile columns name.  one:
+// the reference's one-matrix form for A*A (every axis counted in A's tile
+// rows, B = A).
+static long long estimate_c_tiles(const SMatrix *A, const SMatrix *B, const AxisPermutation *row,
+                                  const AxisPermutation *inner, const AxisPermutation *col, bool one)
+{
+    const int rows = (A->m + TSG_BS - 1) / TSG_BS;
+    const int inner_tiles = one ? rows : (A->n + TSG_BS - 1) / TSG_BS;
+    const int cols = one ? rows : (B->n + TSG_BS - 1) / TSG_BS;
+    const int inner_span = (A->n + TSG_BS - 1) / TSG_BS; // tile columns A's entries can name
+    int count, stride, used = 0;
+    plan_samples(rows, &count, &stride);
+    std::vector<int> a_seen((size_t)(inner_span > 0 ? inner_span : 1), -1), c_seen((size_t)(cols > 0 ? cols : 1), -1);
+    std::vector<int> a_tiles;
+    long long total = 0;
+    for (int sm = 0; sm < count; sm++)
+    {
+        const int tr = sm * stride;
+        if (tr >= rows)
+            continue;
+        a_tiles.clear();
+        tile_row_cols(A, tr, row, inner, [&](int c) {
+            if (a_seen[c] != sm)
+            {
+                a_seen[c] = sm;
+                a_tiles.push_back(c);
+            }
+        });
+        for (int it : a_tiles)
+        {
+            if (it < 0 || it >= inner_tiles)
+                continue;
+            tile_row_cols(B, it, inner, col, [&](int c) {
+                if (c < cols && c_seen[c] != sm)
+                {
+                    c_seen[c] = sm;
+                    total++;
+                }
+            });
+        }
+        used++;
+    }
+    return scaled_estimate(total, rows, used);
 }
 
 static double safe_ratio(long long after, long long before)
@@ -783,27 +875,40 @@ static double safe_ratio(long long after, long long before)
     return before <= 0 ? 1.0 : (double)after / (double)before;
 }
 
-// before/after tile counts (src/external_reorder.h:148-171, exact instead of sampled)
-static int fill_estimates(tsg_context *ctx, const SMatrix *A, const SMatrix *B, ReorderInfo *info)
+// before/after tile counts of a plan (src/external_reorder.h:143-171)
+static void fill_estimates(ReorderProblemKind kind, const SMatrix *A, const SMatrix *B, ReorderInfo *info)
 {
-    DevCSR dA, dB, pA, pB;
-    TSG_TRY(upload_csr(ctx, A, &dA));
-    TSG_TRY(upload_csr(ctx, B, &dB));
-    TSG_TRY(structure_counts(ctx, &dA, &dB, &info->input_tiles_A_before, &info->input_tiles_B_before,
-                             &info->estimated_c_tiles_before));
-    TSG_TRY(permute_dev(ctx, &dA, info->row_perm.old_id, info->inner_perm.new_id, &pA));
-    TSG_TRY(permute_dev(ctx, &dB, info->inner_perm.old_id, info->col_perm.new_id, &pB));
-    TSG_TRY(structure_counts(ctx, &pA, &pB, &info->input_tiles_A_after, &info->input_tiles_B_after,
-                             &info->estimated_c_tiles_after));
-    free_csr(ctx, &dA);
-    free_csr(ctx, &dB);
-    free_csr(ctx, &pA);
-    free_csr(ctx, &pB);
+    info->input_tiles_A_before = estimate_input_tiles(A, nullptr, nullptr);
+    info->input_tiles_A_after = estimate_input_tiles(A, &info->row_perm, &info->inner_perm);
+    if (kind == REORDER_PROBLEM_AA)
+    {
+        info->input_tiles_B_before = info->input_tiles_A_before;
+        info->input_tiles_B_after = info->input_tiles_A_after;
+        info->estimated_c_tiles_before = estimate_c_tiles(A, A, nullptr, nullptr, nullptr, true);
+        info->estimated_c_tiles_after =
+            estimate_c_tiles(A, A, &info->row_perm, &info->inner_perm, &info->col_perm, true);
+    }
+    else
+    {
+        info->input_tiles_B_before = estimate_input_tiles(B, nullptr, nullptr);
+        info->input_tiles_B_after = estimate_input_tiles(B, &info->inner_perm, &info->col_perm);
+        info->estimated_c_tiles_before = estimate_c_tiles(A, B, nullptr, nullptr, nullptr, false);
+        info->estimated_c_tiles_after =
+            estimate_c_tiles(A, B, &info->row_perm, &info->inner_perm, &info->col_perm, false);
+    }
     const double ra = safe_ratio(info->input_tiles_A_after, info->input_tiles_A_before);
     const double rb = safe_ratio(info->input_tiles_B_after, info->input_tiles_B_before);
     info->risk_input_tile_ratio = ra > rb ? ra : rb;
     info->risk_c_tile_ratio = safe_ratio(info->estimated_c_tiles_after, info->estimated_c_tiles_before);
-    TSG_CUDA(cudaStreamSynchronize(ctx->stream));
+}
+
+extern "C" int tsg_reorder_estimates(ReorderProblemKind kind, const SMatrix *matrixA, const SMatrix *matrixB,
+                                     ReorderInfo *info)
+{
+    if (!matrixA || !info || (kind != REORDER_PROBLEM_AA && !matrixB) || !info->row_perm.old_id ||
+        !info->inner_perm.old_id || !info->col_perm.old_id)
+        return tsg_set_error(TSG_ERR_INVALID, "tsg_reorder_estimates: matrices and the plan's three permutations");
+    fill_estimates(kind, matrixA, kind == REORDER_PROBLEM_AA ? matrixA : matrixB, info);
     return TSG_OK;
 }
 
@@ -832,9 +937,7 @@ extern "C" int build_original_reorder_plan(ReorderProblemKind kind, const SMatri
     info->structural_conservative = 0;
     set_text(info->mode, sizeof(info->mode), "original");
     set_text(info->risk_reason, sizeof(info->risk_reason), "original_order");
-    tsg_context *ctx = tsg_dropin_context();
-    if (fill_estimates(ctx, matrixA, kind == REORDER_PROBLEM_AA ? matrixA : matrixB, info) != TSG_OK)
-        return -30;
+    fill_estimates(kind, matrixA, kind == REORDER_PROBLEM_AA ? matrixA : matrixB, info);
     return 0;
 }
 
@@ -952,8 +1055,7 @@ extern "C" int build_external_reorder_plan(ReorderProblemKind kind, const char *
     info->structural_conservative = 0;
     set_text(info->mode, sizeof(info->mode), algorithm);
     set_text(info->risk_reason, sizeof(info->risk_reason), "external_order");
-    if (fill_estimates(ctx, matrixA, kind == REORDER_PROBLEM_AA ? matrixA : matrixB, info) != TSG_OK)
-        return -30;
+    fill_estimates(kind, matrixA, kind == REORDER_PROBLEM_AA ? matrixA : matrixB, info);
     return 0;
 }
 

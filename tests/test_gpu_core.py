@@ -343,3 +343,32 @@ def test_row_blocks_of_a_give_the_whole_product(tsg, ctx, gen):
     np.testing.assert_array_equal(rp_all, whole[0])
     np.testing.assert_array_equal(np.concatenate([p[1] for p in parts]), whole[1])
     assert np.array_equal(np.concatenate([p[2] for p in parts]).view(np.uint64), whole[2].view(np.uint64))
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_intersection_bitmaps_match_the_drivers(tsg, oracle, name):
+    """tile_intersection_bitmaps equals the reference driver's loops
+    (src/main.cu:430-465) on the golden fixtures' tiles, and on a product
+    whose tile counts are not multiples of 32."""
+    z, mat = CASES[name]
+    if mat[0] != mat[1]:
+        pytest.skip("rectangular: A*A is not defined")
+    A = {k: z[f"{name}/A/{k}"] for k in TILE_KEYS}
+    B = {k: z[f"{name}/B/{k}"] for k in TILE_KEYS + ["csc_tile_ptr", "csc_tile_rowidx"]}
+    for d in (A, B):
+        d.update(m=mat[0], n=mat[1], nnz=mat[3].size, tilem=(mat[0] + 15) // 16, tilen=(mat[1] + 15) // 16,
+                 numtile=d["tile_columnidx"].size)
+    got = tsg.tile_intersection_bitmaps(A, B)
+    want = oracle.intersection_bitmaps(A, B)
+    for g, w in zip(got, want):
+        np.testing.assert_array_equal(g, w)
+
+
+def test_intersection_bitmaps_rectangular(tsg, oracle, gen):
+    a, b = gen.random_poisson(900, 1000, 4.0, seed=61), gen.random_poisson(1000, 777, 5.0, seed=62)
+    A, B = tsg.csr2tile_row_major(a), tsg.csr2tile_col_major(b)
+    got = tsg.tile_intersection_bitmaps(A, B)
+    want = oracle.intersection_bitmaps(A, B)
+    assert got[0].shape == (A["tilem"], (A["tilen"] + 31) // 32) and got[1].shape == (B["tilen"], (A["tilen"] + 31) // 32)
+    for g, w in zip(got, want):
+        np.testing.assert_array_equal(g, w)
