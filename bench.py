@@ -393,6 +393,7 @@ def _served_stream(srv, jobs, rate, rng):
     server's statistics and the wall time of the stream."""
     srv.done.clear()
     srv.batches = 0
+    srv.host_s = dict.fromkeys(srv.host_s, 0.0)
     gaps = rng.exponential(1.0 / rate, len(jobs))
     futs = []
     t0 = time.perf_counter()
@@ -439,6 +440,7 @@ def run_served(args, tsg, gen, device, deliver="device", n_jobs=None, half_capac
            "p99_ms": round(st["p99_ms"], 3), "gflops": round(2.0 * prods / wall / 1e9, 2),
            "batches": st["batches"], "mean_batch": round(st["mean_batch"], 2), "rejected": st["rejected"],
            "operand_cache": st["operand_cache"], "mem_cap_gb": 40, "deliver": deliver,
+           "dispatcher_s": dict(st["dispatcher_s"], wall=round(wall, 3)),
            "schedule": st["tuned"] if args.served_schedule == "auto" else "-".join(map(str, args.served_schedule))}
     if not half_capacity:
         srv.close()

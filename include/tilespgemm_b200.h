@@ -86,16 +86,6 @@ void csr2tile_row_major(SMatrix *matrix);
  * Replaces csr2tile_col_major, src/csr2tile.h:261-478. */
 void csr2tile_col_major(SMatrix *matrix);
 
-/* Tiled SpGEMM C = A*B.  A from csr2tile_row_major, B from
- * csr2tile_col_major.  Replaces tilespgemm, src/tilespgemm-cuda.h:2610-2624.
- * The intersection bitmaps (tile_intersection_bitmaps below) and the
- * densities are accepted for ABI compatibility and IGNORED: this
- * implementation's steps read A's and B's tile columns, masks and column
- * view directly instead of intersecting bitmaps.  Runs the product REPEAT (5) times,
- * reports the minimum time of the reference's window (C allocation through
- * the numeric step), and fills matrixC's host tile arrays (tile_ptr,
- * tile_columnidx, tile_rowidx, tile_nnz, tile_csr_Ptr, tile_csr_Col,
- * tile_csr_Value, mask, numtile, nnz, m, n, tilem, tilen). */
 /* The reference driver's intersection bitmaps (src/main.cu:430-465), built on
  * the GPU: len = ceil(A->tilen / 32); A's tile row i sets bit (31 - j % 32) of
  * word i * len + j / 32 for each of its tile columns j (tile_ptr,
@@ -106,6 +96,16 @@ void csr2tile_col_major(SMatrix *matrix);
 int tile_intersection_bitmaps(const SMatrix *A, const SMatrix *B, unsigned int **bitmask_A,
                               unsigned int **bitmask_B, int *bitmask_len);
 
+/* Tiled SpGEMM C = A*B.  A from csr2tile_row_major, B from
+ * csr2tile_col_major.  Replaces tilespgemm, src/tilespgemm-cuda.h:2610-2624.
+ * The intersection bitmaps (tile_intersection_bitmaps above) and the
+ * densities are accepted for ABI compatibility and IGNORED: this
+ * implementation's steps read A's and B's tile columns, masks and column
+ * view directly instead of intersecting bitmaps.  Runs the product REPEAT (5) times,
+ * reports the minimum time of the reference's window (C allocation through
+ * the numeric step), and fills matrixC's host tile arrays (tile_ptr,
+ * tile_columnidx, tile_rowidx, tile_nnz, tile_csr_Ptr, tile_csr_Col,
+ * tile_csr_Value, mask, numtile, nnz, m, n, tilem, tilen). */
 void tilespgemm(SMatrix *matrixA,
                 SMatrix *matrixB,
                 SMatrix *matrixC,
@@ -518,6 +518,11 @@ int tsg_tiled_to_csr_host(tsg_context *ctx, const tsg_tiled *C, int flags,
  * products (= nnzCub >= nnz(C)) and matched tile pairs (>= C tiles). */
 int tsg_product_bounds(tsg_context *ctx, const tsg_tiled *A, const tsg_tiled *B,
                        long long *products, long long *tile_pairs);
+/* The same for count products A[p]*B[p] with one synchronisation; c_tiles
+ * (may be NULL) receives each product's exact number of C tiles (step 1's
+ * count pass). */
+int tsg_product_bounds_many(tsg_context *ctx, int count, const tsg_tiled *A, const tsg_tiled *B,
+                            long long *products, long long *tile_pairs, long long *c_tiles);
 
 /* ------------------------------------------------------------------------ */
 /* Batched products: many independent C_p = A_p * B_p of uneven size run in  */
@@ -541,6 +546,14 @@ typedef struct tsg_batch tsg_batch;
  * params NULL = row schedule (16, 1024) with a graph. */
 int tsg_batch_create(tsg_context *ctx, int count, const tsg_tiled *A, const tsg_tiled *B,
                      const tsg_batch_params *params, tsg_batch **out);
+/* tsg_batch_create with the bounds already known (products and c_tiles of
+ * tsg_product_bounds_many, one entry per product): plans without running a
+ * kernel or waiting for the device, so a caller can form the next batch
+ * while another stream's batch holds the GPU.  Smaller bounds than the true
+ * ones make the run fail with TSG_ERR_OVERFLOW. */
+int tsg_batch_create_bounded(tsg_context *ctx, int count, const tsg_tiled *A, const tsg_tiled *B,
+                             const tsg_batch_params *params, const long long *products,
+                             const long long *c_tiles, tsg_batch **out);
 /* Queues one execution of the whole batch on the context's stream. */
 int tsg_batch_run(tsg_batch *b);
 /* Waits for the last run and reads per-product sizes; reports a device wait

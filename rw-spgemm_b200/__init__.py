@@ -699,6 +699,9 @@ def _declare_batch(L):
     vp, ip = ctypes.c_void_p, ctypes.c_int
     L.tsg_batch_create.argtypes = [vp, ip, ctypes.POINTER(TsgTiled), ctypes.POINTER(TsgTiled),
                                    ctypes.POINTER(BatchParams), ctypes.POINTER(vp)]
+    L.tsg_batch_create_bounded.argtypes = [vp, ip, ctypes.POINTER(TsgTiled), ctypes.POINTER(TsgTiled),
+                                           ctypes.POINTER(BatchParams), ctypes.POINTER(ctypes.c_longlong),
+                                           ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(vp)]
     L.tsg_batch_run.argtypes = [vp]
     L.tsg_batch_sync.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]
     L.tsg_batch_product.argtypes = [vp, ip, ctypes.POINTER(TsgTiled)]
@@ -709,6 +712,9 @@ def _declare_batch(L):
     L.tsg_batch_set_wait_limit.argtypes = [vp, ctypes.c_double]
     L.tsg_product_bounds.argtypes = [vp, ctypes.POINTER(TsgTiled), ctypes.POINTER(TsgTiled),
                                      ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]
+    L.tsg_product_bounds_many.argtypes = [vp, ip, ctypes.POINTER(TsgTiled), ctypes.POINTER(TsgTiled),
+                                          ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong),
+                                          ctypes.POINTER(ctypes.c_longlong)]
 
 
 _declare_prev = _declare
@@ -727,13 +733,31 @@ def product_bounds(ctx: Context, A: Tiled, B: Tiled):
     return pr.value, tp.value
 
 
+def product_bounds_many(ctx: Context, pairs, c_tiles: bool = False):
+    """product_bounds of every (A, B) in pairs with one synchronisation:
+    a list of (products, tile pairs), or of (products, tile pairs, C tiles)
+    with c_tiles (step 1's exact count)."""
+    n = len(pairs)
+    if n == 0:
+        return []
+    As = (TsgTiled * n)(*[a.s for a, _ in pairs])
+    Bs = (TsgTiled * n)(*[b.s for _, b in pairs])
+    pr, tp, ct = (ctypes.c_longlong * n)(), (ctypes.c_longlong * n)(), (ctypes.c_longlong * n)()
+    check(lib().tsg_product_bounds_many(ctx.handle, n, As, Bs, pr, tp, ct if c_tiles else None))
+    if c_tiles:
+        return [(pr[i], tp[i], ct[i]) for i in range(n)]
+    return [(pr[i], tp[i]) for i in range(n)]
+
+
 class Batch:
     """tsg_batch over device-resident (A, B) operand pairs."""
 
     def __init__(self, ctx: Context, pairs, schedule: str = "spa", seg_tiles: int = 8, acc_cap: int = 512,
-                 graph: bool = True, dense: int = 0):
+                 graph: bool = True, dense: int = 0, bounds=None):
         """dense: the 'spa' schedule's C values per tile from which a product
-        runs the tile kernel (0: the default 64)."""
+        runs the tile kernel (0: the default 64).  bounds: per pair its
+        (scalar products, C tiles) from product_bounds_many(c_tiles=True);
+        given, the batch is planned without waiting for the device."""
         self.ctx = ctx
         self.pairs = list(pairs)  # keep operands alive
         n = len(self.pairs)
@@ -741,7 +765,15 @@ class Batch:
         arrB = (TsgTiled * n)(*[b.s for _, b in self.pairs])
         prm = BatchParams(SCHEDULE_IDS[schedule], seg_tiles, acc_cap, 1 if graph else 0, int(dense))
         self.handle = ctypes.c_void_p()
-        check(lib().tsg_batch_create(ctx.handle, n, arrA, arrB, ctypes.byref(prm), ctypes.byref(self.handle)))
+        if bounds is None:
+            check(lib().tsg_batch_create(ctx.handle, n, arrA, arrB, ctypes.byref(prm), ctypes.byref(self.handle)))
+        else:
+            if len(bounds) != n:
+                raise ValueError("one (products, C tiles) bound per pair")
+            pr = (ctypes.c_longlong * n)(*[int(b[0]) for b in bounds])
+            ct = (ctypes.c_longlong * n)(*[int(b[1]) for b in bounds])
+            check(lib().tsg_batch_create_bounded(ctx.handle, n, arrA, arrB, ctypes.byref(prm), pr, ct,
+                                                 ctypes.byref(self.handle)))
         self.count = n
         self.params = dict(schedule=schedule, seg_tiles=seg_tiles, acc_cap=acc_cap, dense=dense)
 

@@ -26,7 +26,7 @@
 
 #include "tsg_device.cuh"
 
-int tsg_count_c_tiles(tsg_context *ctx, const tsg_tiled *A, const tsg_tiled *B, long long *numC);
+int tsg_count_c_tiles_async(tsg_context *ctx, const tsg_tiled *A, const tsg_tiled *B, unsigned long long *total);
 
 struct BatchProd
 {
@@ -63,6 +63,7 @@ struct tsg_batch
     std::vector<int> m, n, tilen; // per product C dimensions
     long long launches;
     unsigned long long wait_ns; // the grid barrier's wait limit
+    unsigned bar_init[8];       // host image of d_bar at creation (zeros, the wait limit at [4])
     int dense;                  // SPA schedule: values per C tile from which a product takes the tile kernel
 };
 
@@ -693,36 +694,66 @@ __global__ void k_bounds(int T, const int *__restrict__ A_col, const unsigned sh
     }
 }
 
+extern "C" int tsg_product_bounds_many(tsg_context *ctx, int count, const tsg_tiled *A, const tsg_tiled *B,
+                                       long long *products, long long *tile_pairs, long long *c_tiles)
+{
+    if (!ctx || count < 0 || (count && (!A || !B || !products || !tile_pairs)))
+        return tsg_set_error(TSG_ERR_INVALID, "null argument");
+    if (count == 0)
+        return TSG_OK;
+    int maxm = 0;
+    for (int p = 0; p < count; p++)
+        maxm = B[p].m > maxm ? B[p].m : maxm;
+    int *rowlen;
+    unsigned long long *d;
+    TSG_TRY(tsg_alloc(ctx, &rowlen, (size_t)maxm + 1));
+    TSG_TRY(tsg_alloc(ctx, &d, (size_t)count * 3));
+    TSG_CUDA(cudaMemsetAsync(d, 0, (size_t)count * 3 * sizeof(unsigned long long), ctx->stream));
+    int st = TSG_OK;
+    for (int p = 0; p < count && st == TSG_OK; p++)
+    {
+        // k_brow_len writes every row of B below m: the buffer is reused in
+        // stream order without clearing
+        if (B[p].tilem > 0)
+        {
+            k_brow_len<<<tsg_blocks((long long)B[p].tilem * 16, 256), 256, 0, ctx->stream>>>(
+                B[p].tilem, B[p].m, B[p].tile_ptr, B[p].mask, rowlen);
+            TSG_LAUNCH_CHECK();
+        }
+        if (A[p].numtile > 0)
+        {
+            k_bounds<<<tsg_blocks((long long)A[p].numtile * 16, 256), 256, 0, ctx->stream>>>(
+                A[p].numtile, A[p].tile_columnidx, A[p].mask, B[p].tile_ptr, rowlen, B[p].m, d + 3 * p);
+            TSG_LAUNCH_CHECK();
+        }
+        if (c_tiles)
+            st = tsg_count_c_tiles_async(ctx, &A[p], &B[p], d + 3 * p + 2);
+    }
+    if (st == TSG_OK)
+    {
+        std::vector<unsigned long long> h((size_t)count * 3);
+        TSG_CUDA(cudaMemcpyAsync(h.data(), d, h.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                                 ctx->stream));
+        TSG_CUDA(cudaStreamSynchronize(ctx->stream));
+        for (int p = 0; p < count; p++)
+        {
+            products[p] = (long long)h[3 * p];
+            tile_pairs[p] = (long long)h[3 * p + 1];
+            if (c_tiles)
+                c_tiles[p] = (long long)h[3 * p + 2];
+        }
+    }
+    tsg_release(ctx, rowlen);
+    tsg_release(ctx, d);
+    return st;
+}
+
 extern "C" int tsg_product_bounds(tsg_context *ctx, const tsg_tiled *A, const tsg_tiled *B, long long *products,
                                   long long *tile_pairs)
 {
     if (!ctx || !A || !B || !products || !tile_pairs)
         return tsg_set_error(TSG_ERR_INVALID, "null argument");
-    int *rowlen;
-    unsigned long long *d;
-    TSG_TRY(tsg_alloc(ctx, &rowlen, (size_t)B->m + 1));
-    TSG_TRY(tsg_alloc(ctx, &d, 2));
-    TSG_CUDA(cudaMemsetAsync(d, 0, 2 * sizeof(unsigned long long), ctx->stream));
-    TSG_CUDA(cudaMemsetAsync(rowlen, 0, ((size_t)B->m + 1) * sizeof(int), ctx->stream));
-    if (B->tilem > 0)
-    {
-        k_brow_len<<<tsg_blocks((long long)B->tilem * 16, 256), 256, 0, ctx->stream>>>(B->tilem, B->m, B->tile_ptr,
-                                                                                       B->mask, rowlen);
-        TSG_LAUNCH_CHECK();
-    }
-    if (A->numtile > 0)
-    {
-        k_bounds<<<tsg_blocks((long long)A->numtile * 16, 256), 256, 0, ctx->stream>>>(
-            A->numtile, A->tile_columnidx, A->mask, B->tile_ptr, rowlen, B->m, d);
-        TSG_LAUNCH_CHECK();
-    }
-    TSG_CUDA(cudaMemcpyAsync(ctx->h_pinned, d, 2 * sizeof(long long), cudaMemcpyDeviceToHost, ctx->stream));
-    TSG_CUDA(cudaStreamSynchronize(ctx->stream));
-    *products = ctx->h_pinned[0];
-    *tile_pairs = ctx->h_pinned[1];
-    tsg_release(ctx, rowlen);
-    tsg_release(ctx, d);
-    return TSG_OK;
+    return tsg_product_bounds_many(ctx, 1, A, B, products, tile_pairs, nullptr);
 }
 
 // ---------------------------------------------------------------------------
@@ -807,8 +838,11 @@ static int record_run(tsg_batch *b, cudaStream_t st)
     return TSG_OK;
 }
 
-extern "C" int tsg_batch_create(tsg_context *ctx, int count, const tsg_tiled *A, const tsg_tiled *B,
-                                const tsg_batch_params *params, tsg_batch **out)
+// products / c_tiles: the bounds of every product when the caller has them
+// (tsg_product_bounds_many), else null and computed here
+static int batch_create(tsg_context *ctx, int count, const tsg_tiled *A, const tsg_tiled *B,
+                        const tsg_batch_params *params, const long long *products, const long long *c_tiles,
+                        tsg_batch **out)
 {
     if (!ctx || !out || count <= 0 || !A || !B)
         return tsg_set_error(TSG_ERR_INVALID, "bad batch arguments");
@@ -856,24 +890,32 @@ extern "C" int tsg_batch_create(tsg_context *ctx, int count, const tsg_tiled *A,
     size_t bytes = 0;
     std::vector<size_t> off(count);
     long long run = 0, chunk_cap = 0, total_prods = 0;
+    // scalar products and the exact C tile count (step 1's count pass) of
+    // every product, one synchronisation for the whole batch
+    std::vector<long long> v_prods(count), v_pairs(count), v_tiles(count);
+    if (products && c_tiles)
+        for (int p = 0; p < count; p++)
+        {
+            if (products[p] < 0 || c_tiles[p] < 0)
+            {
+                delete b;
+                return tsg_set_error(TSG_ERR_INVALID, "product %d: negative bound", p);
+            }
+            v_prods[p] = products[p];
+            v_tiles[p] = c_tiles[p];
+        }
+    else
+    {
+        int st = tsg_product_bounds_many(ctx, count, A, B, v_prods.data(), v_pairs.data(), v_tiles.data());
+        if (st != TSG_OK)
+        {
+            delete b;
+            return st;
+        }
+    }
     for (int p = 0; p < count; p++)
     {
-        long long prods = 0, pairs = 0;
-        int st = tsg_product_bounds(ctx, &A[p], &B[p], &prods, &pairs);
-        if (st != TSG_OK)
-        {
-            delete b;
-            return st;
-        }
-        // exact C tile count (step 1's count pass) bounds both arrays tightly
-        long long capT = 0;
-        st = tsg_count_c_tiles(ctx, &A[p], &B[p], &capT);
-        if (st != TSG_OK)
-        {
-            delete b;
-            return st;
-        }
-        (void)pairs;
+        const long long prods = v_prods[p], capT = v_tiles[p];
         total_prods += prods;
         long long capN = prods < 256 * capT ? prods : 256 * capT;
         if (capN > 2147483647LL || capT > 2147483647LL / 16)
@@ -964,12 +1006,15 @@ extern "C" int tsg_batch_create(tsg_context *ctx, int count, const tsg_tiled *A,
     // an in-kernel error (a numeric accumulator overflow) goes to the batch's error word
     for (BatchProd &h : b->host)
         h.P.status = b->d_err;
+    // copies only (no memset kernels): creating a batch never waits for SMs
+    // held by another stream's persistent kernel
+    b->wait_ns = BATCH_WAIT_FLOOR_NS + BATCH_WAIT_NS_PER_PRODUCT * (unsigned long long)total_prods;
+    memset(b->bar_init, 0, sizeof(b->bar_init));
+    memcpy(&b->bar_init[4], &b->wait_ns, sizeof(unsigned long long));
     cudaMemcpyAsync(b->d_prod, b->host.data(), sizeof(BatchProd) * count, cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(b->d_rowoff, b->rowoff.data(), sizeof(long long) * (count + 1), cudaMemcpyHostToDevice, s);
-    cudaMemsetAsync(b->d_bar, 0, 8 * sizeof(unsigned), s);
-    cudaMemsetAsync(b->d_err, 0, sizeof(int), s);
-    b->wait_ns = BATCH_WAIT_FLOOR_NS + BATCH_WAIT_NS_PER_PRODUCT * (unsigned long long)total_prods;
-    cudaMemcpyAsync(b->d_bar + 4, &b->wait_ns, sizeof(unsigned long long), cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(b->d_bar, b->bar_init, sizeof(b->bar_init), cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(b->d_err, &b->bar_init[0], sizeof(int), cudaMemcpyHostToDevice, s);
     // co-resident grid
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
     {
@@ -1029,6 +1074,21 @@ extern "C" int tsg_batch_create(tsg_context *ctx, int count, const tsg_tiled *A,
     TSG_CUDA(cudaStreamSynchronize(s));
     *out = b;
     return TSG_OK;
+}
+
+extern "C" int tsg_batch_create(tsg_context *ctx, int count, const tsg_tiled *A, const tsg_tiled *B,
+                                const tsg_batch_params *params, tsg_batch **out)
+{
+    return batch_create(ctx, count, A, B, params, nullptr, nullptr, out);
+}
+
+extern "C" int tsg_batch_create_bounded(tsg_context *ctx, int count, const tsg_tiled *A, const tsg_tiled *B,
+                                        const tsg_batch_params *params, const long long *products,
+                                        const long long *c_tiles, tsg_batch **out)
+{
+    if (!products || !c_tiles)
+        return tsg_set_error(TSG_ERR_INVALID, "null bounds");
+    return batch_create(ctx, count, A, B, params, products, c_tiles, out);
 }
 
 extern "C" int tsg_batch_run(tsg_batch *b)

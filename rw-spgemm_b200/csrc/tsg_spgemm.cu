@@ -31,6 +31,27 @@ __global__ void __launch_bounds__(S1_WARPS * 32) k_step1(ProdView P, int *__rest
         C_cnt[i] = cnt;
 }
 
+// step 1's count pass summed over the block into one device word
+__global__ void __launch_bounds__(S1_WARPS * 32) k_step1_total(ProdView P, unsigned long long *__restrict__ total)
+{
+    __shared__ unsigned int s_bm[S1_WARPS][S1_WORDS];
+    __shared__ int s_cnt[S1_WARPS];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int i = blockIdx.x * S1_WARPS + warp;
+    const int cnt = i < P.tilemA ? step1_row<false>(P, i, s_bm[warp], lane, nullptr) : 0;
+    if (lane == 0)
+        s_cnt[warp] = cnt;
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        unsigned long long sum = 0;
+        for (int w = 0; w < S1_WARPS; w++)
+            sum += (unsigned long long)s_cnt[w];
+        if (sum)
+            atomicAdd(total, sum);
+    }
+}
+
 // fused step-1 emit + step 2 (warp per A tile row); wide rows are emitted by
 // step1_row and flagged for the wide-row step 2 (1, or 2 when hypersparse)
 __global__ void __launch_bounds__(256) k_step12(ProdView P, int *__restrict__ wide, int *__restrict__ bins)
@@ -775,21 +796,16 @@ int tsg_spgemm_to_host(tsg_context *ctx, const tsg_tiled *A, const tsg_tiled *B,
     return status;
 }
 
-// Number of C tiles of A*B (step 1's count pass only); A and B need their
-// row-major tile structure.
-int tsg_count_c_tiles(tsg_context *ctx, const tsg_tiled *A, const tsg_tiled *B, long long *numC)
+// Number of C tiles of A*B (step 1's count pass only) added to the device
+// word *total, without synchronising; A and B need their row-major tile
+// structure.
+int tsg_count_c_tiles_async(tsg_context *ctx, const tsg_tiled *A, const tsg_tiled *B, unsigned long long *total)
 {
-    *numC = 0;
     if (A->tilem == 0)
         return TSG_OK;
-    int *cnt;
-    TSG_TRY(tsg_alloc(ctx, &cnt, (size_t)A->tilem + 1));
     tsg_tiled Cdummy;
     memset(&Cdummy, 0, sizeof(Cdummy));
-    k_step1<false><<<tsg_blocks(A->tilem, S1_WARPS), S1_WARPS * 32, 0, ctx->stream>>>(make_view(A, B, &Cdummy), cnt,
-                                                                                       nullptr);
+    k_step1_total<<<tsg_blocks(A->tilem, S1_WARPS), S1_WARPS * 32, 0, ctx->stream>>>(make_view(A, B, &Cdummy), total);
     TSG_LAUNCH_CHECK();
-    TSG_TRY(tsg_scan_counts(ctx, cnt, cnt, A->tilem, numC));
-    tsg_release(ctx, cnt);
     return TSG_OK;
 }

@@ -25,6 +25,7 @@ from __future__ import annotations
 
 import collections
 import ctypes
+import itertools
 import math
 import threading
 import time
@@ -32,22 +33,34 @@ from concurrent.futures import Future
 
 import numpy as np
 
-from . import TSG_TILED_CSC_VIEW, Batch, Context, check, csr_host_to_tiled, lib, product_bounds
+from . import (TSG_TILED_CSC_VIEW, Batch, Context, check, csr_host_to_tiled, lib, product_bounds,
+               product_bounds_many)
 
 
 class Job:
-    __slots__ = ("jid", "kind", "a_key", "b_key", "t_submit", "t_done", "future", "pred_bytes", "pred_prods",
-                 "pred_tiles", "result_nnz")
+    __slots__ = ("jid", "kind", "a_key", "b_key", "cls", "t_submit", "t_done", "future", "pred_bytes",
+                 "pred_prods", "pred_tiles", "result_nnz")
 
-    def __init__(self, jid, kind, a_key, b_key):
-        self.jid, self.kind, self.a_key, self.b_key = jid, kind, a_key, b_key
+    def __init__(self, jid, kind, a_key, b_key, cls=0):
+        self.jid, self.kind, self.a_key, self.b_key, self.cls = jid, kind, a_key, b_key, cls
         self.t_submit = time.perf_counter()
         self.t_done = None
         self.future = Future()
         self.pred_bytes = 0
-        self.pred_prods = 0
+        self.pred_prods = -1  # not predicted yet
         self.pred_tiles = 0
         self.result_nnz = 0
+
+
+def skew_class(mat):
+    """floor(log2(longest row / mean row)) of a host CSR (0 when empty):
+    products whose A rows are this uneven take about as long to finish
+    their heaviest rows, so batches of one class overlap their tails."""
+    m, n, rp, ci, v = mat
+    d = np.diff(np.asarray(rp, dtype=np.int64))
+    if m == 0 or d.sum() == 0:
+        return 0
+    return int(math.log2(max(1.0, float(d.max()) / float(d.mean()))))
 
 
 def _transpose(mat):
@@ -90,6 +103,13 @@ class OperandCache:
         """Device bytes of a resident operand."""
         return self.tiled_bytes(self.tiles[key])
 
+    def drop(self, keys):
+        for key in keys:
+            t = self.tiles.pop(key, None)
+            if t is not None:
+                self.bytes -= self.tiled_bytes(t)
+                t.free()
+
     def evict_until(self, limit, pinned_keys):
         for key in list(self.tiles.keys()):
             if self.bytes <= limit:
@@ -105,9 +125,14 @@ class _Slot:
     """One in-flight batch position with its own stream."""
 
     def __init__(self, device):
-        self.ctx = Context(device, own_stream=True)
+        import torch
+        # a torch stream (non-blocking), so that torch copies of the results
+        # queue behind the library's work on it
+        self.stream = torch.cuda.Stream(device)
+        self.ctx = Context(device, stream=self.stream.cuda_stream)
         self.staging = None  # page-locked result staging, grown on demand
         self.batch = None
+        self.pending = None  # conversions queued, results not yet handed over
         self.jobs = []
         self.arena = 0
         self.t_launch = 0.0
@@ -126,6 +151,11 @@ class SpGEMMServer:
               bounds): a batch closes once it holds this much work, so a few
               large jobs do not hold many small ones back (a single job
               above it still runs, alone)
+    A batch takes the first queued job and the later jobs of the same skew
+    class (skew_class of the A operand) among the next 4 * max_batch queued,
+    in arrival order; jobs of other classes keep their places.  Products of
+    one class finish their heaviest rows at about the same time, so a batch
+    does not wait on one skewed product's tail while the GPU idles.
     schedule  (schedule, seg_tiles, acc_cap[, dense]) of the batched kernel,
               or "auto": the autotuner (`tuner`, a fresh one if None)
               times its candidates on the first batch of each density class
@@ -136,7 +166,7 @@ class SpGEMMServer:
     """
 
     def __init__(self, device=0, mem_cap=40 << 30, slots=2, max_batch=64, schedule=("spa", 8, 512),
-                 batch_products=2e8, deliver="host", tuner=None):
+                 batch_products=5e8, deliver="host", tuner=None):
         if deliver not in ("host", "device"):
             raise ValueError(deliver)
         self.deliver = deliver
@@ -162,10 +192,30 @@ class SpGEMMServer:
         self.done = []
         self.batches = 0
         self.rejected = 0
+        self.preds = {}  # (a_key, b_key) -> (arena bytes, scalar products, C tiles)
+        self.classes = {}  # operand key -> skew_class of the matrix
+        self.lookahead = 4 * max_batch  # queued jobs a batch may look through for its class
+        # dispatcher time by activity ("form" includes tune, predict, create
+        # and run); "gpu": the batches' kernel time, from their device timer
+        # stamps
+        self.host_s = {"form": 0.0, "tune": 0.0, "predict": 0.0, "create": 0.0, "run": 0.0, "finish": 0.0,
+                       "deliver": 0.0, "gpu": 0.0}
 
     # -- registration / submission -------------------------------------------
     def register(self, key, mat):
+        """Registers operand `key`.  Replacing one drops what was derived from
+        the old matrix (its transpose, bounds and resident tiles); an operand
+        of a queued or running job cannot be replaced."""
+        if key in self.matrices and self.matrices[key] is not mat:
+            keys = {key, (key, "T")}
+            busy = [j for j in self.queue] + [j for sl in self.slots for j in sl.jobs]
+            if any(j.a_key in keys or j.b_key in keys for j in busy):
+                raise RuntimeError(f"operand {key!r} is in use by a queued or running job")
+            self.matrices.pop((key, "T"), None)
+            self.preds = {k: v for k, v in self.preds.items() if not (set(k) & keys)}
+            self.cache.drop(keys)
         self.matrices[key] = mat
+        self.classes[key] = skew_class(mat)
 
     def submit(self, kind, a_key, b_key=None) -> Future:
         if kind not in ("AB", "AAT"):
@@ -176,7 +226,7 @@ class SpGEMMServer:
                 self.matrices[tkey] = _transpose(self.matrices[a_key])
             b_key = tkey
         with self.lock:
-            job = Job(self.next_id, kind, a_key, b_key)
+            job = Job(self.next_id, kind, a_key, b_key, self.classes.get(a_key, 0))
             self.next_id += 1
             self.queue.append(job)
             self.lock.notify()
@@ -220,15 +270,52 @@ class SpGEMMServer:
     def _in_use(self):
         return self.cache.bytes + sum(s.arena for s in self.slots if s.batch is not None)
 
+    @staticmethod
+    def _arena_of(A, prods, ctiles):
+        """Device bytes of a product's share of the batch arena, laid out as
+        tsg_batch_create does (row offsets and flags per A tile row, C's tile
+        arrays for ctiles tiles, min(products, 256 ctiles) values; every
+        array 256-byte aligned)."""
+        def al(x):
+            return (x + 255) & ~255
+        tm = A.s.tilem
+        vals = min(prods, 256 * ctiles)
+        return (al((tm + 1) * 4) + al(tm * 4) + 2 * al(ctiles * 4) + al((ctiles + 1) * 4) + al(ctiles * 32) +
+                al(ctiles * 16) + al(vals) + al(vals * 8))
+
+    def _predict_many(self, ops):
+        """(arena bytes, scalar products, C tiles) of each (A, B), with one
+        synchronisation (step 1's exact C-tile count)."""
+        return [(self._arena_of(A, prods, ctiles), prods, ctiles)
+                for (A, B), (prods, _, ctiles) in zip(ops, product_bounds_many(self.cache.ctx, ops, c_tiles=True))]
+
     def _predict(self, A, B):
-        """(device bytes of the result arena, scalar products, C-tile bound)
-        from the step-1 bounds; the arena's per-array 256-byte alignment
-        and per-tile-row flags included."""
-        prods, pairs = product_bounds(self.cache.ctx, A, B)
-        tiles = min(pairs, A.s.tilem * B.s.tilen)
-        vals = min(prods, 256 * tiles)
-        return (tiles * (4 * 3 + 4 + 32 + 16) + vals * 9 + (A.s.tilem + 1) * 4 + A.s.tilem * 4 + 8 * 256,
-                prods, tiles)
+        return self._predict_many([(A, B)])[0]
+
+    def _predict_jobs(self, jobs, ops):
+        """Fills the jobs' predictions: from the cache of earlier jobs on the
+        same operand pair, the others with one call."""
+        need = {}
+        for j, op in zip(jobs, ops):
+            if (j.a_key, j.b_key) not in self.preds:
+                need.setdefault((j.a_key, j.b_key), op)
+        if need:
+            keys = list(need)
+            preds = ([self._predict(*need[keys[0]])] if len(keys) == 1 else
+                     self._predict_many([need[k] for k in keys]))
+            self.preds.update(zip(keys, preds))
+        for j in jobs:
+            j.pred_bytes, j.pred_prods, j.pred_tiles = self.preds[(j.a_key, j.b_key)]
+
+    def _predict_queue(self):
+        """Predicts the queued jobs of the first job's class within the
+        lookahead (as many as a batch holds) whose operands are resident,
+        with at most one synchronisation."""
+        cls = self.queue[0].cls if self.queue else 0
+        todo = [j for j in itertools.islice(self.queue, self.lookahead) if j.cls == cls and j.pred_prods < 0 and
+                j.a_key in self.cache.tiles and j.b_key in self.cache.tiles][:self.max_batch]
+        if todo:
+            self._predict_jobs(todo, [(self.cache.tiles[j.a_key], self.cache.tiles[j.b_key]) for j in todo])
 
     def _schedule_for(self, slot, pairs, jobs):
         """The batch's (schedule, seg_tiles, acc_cap, dense)."""
@@ -239,18 +326,32 @@ class SpGEMMServer:
         tiles = max(1, sum(j.pred_tiles for j in jobs))
         key = int(math.log2(prods / tiles + 1))
         if key not in self.tuned:
+            t0 = time.perf_counter()
             self.tuned[key] = self.tuner.tune_batch(slot.ctx, pairs, reps=1, use_cache=False)
+            self.host_s["tune"] += time.perf_counter() - t0
         return self.tuned[key]
 
     def _form_batch(self, slot):
         jobs, pairs, pred, work = [], [], 0, 0
         # operands of batches still running must stay resident
         pinned = {k for s in self.slots if s.batch is not None for j in s.jobs for k in (j.a_key, j.b_key)}
-        while self.queue and len(jobs) < self.max_batch:
+        t0 = time.perf_counter()
+        self._predict_queue()
+        self.host_s["predict"] += time.perf_counter() - t0
+        # the batch takes the queue's first job and then, in arrival order,
+        # the later jobs of its class within the lookahead (the others keep
+        # their places)
+        cls = self.queue[0].cls if self.queue else 0
+        passed = []
+        while self.queue and len(jobs) < self.max_batch and len(passed) < self.lookahead:
             job = self.queue[0]
+            if job.cls != cls:
+                passed.append(self.queue.popleft())
+                continue
             A = self.cache.get(job.a_key, self.matrices[job.a_key])
             B = self.cache.get(job.b_key, self.matrices[job.b_key])
-            job.pred_bytes, job.pred_prods, job.pred_tiles = self._predict(A, B)
+            if job.pred_prods < 0:
+                self._predict_jobs([job], [(A, B)])
             if jobs and work + job.pred_prods > self.batch_products:
                 break  # the batch holds its share of work; this job opens the next
             # its operands stay resident while it runs: a job needing more
@@ -276,26 +377,33 @@ class SpGEMMServer:
             pairs.append((A, B))
             pred += job.pred_bytes
             work += job.pred_prods
+        self.queue.extendleft(reversed(passed))
         if not jobs:
             return False
         sch, seg, cap, dense = self._schedule_for(slot, pairs, jobs)
-        slot.batch = Batch(slot.ctx, pairs, sch, seg, cap, graph=False, dense=dense)
+        # planned from the predictions (exact C-tile counts): no device wait
+        # while the other slot's batch holds the GPU
+        t0 = time.perf_counter()
+        slot.batch = Batch(slot.ctx, pairs, sch, seg, cap, graph=False, dense=dense,
+                           bounds=[(j.pred_prods, j.pred_tiles) for j in jobs])
         slot.arena = slot.batch.info()["arena_bytes"]
         slot.jobs = jobs
-        slot.t_launch = time.perf_counter()
+        t1 = slot.t_launch = time.perf_counter()
         slot.batch.run()
+        self.host_s["create"] += t1 - t0
+        self.host_s["run"] += time.perf_counter() - t1
         self.batches += 1
         return True
 
     def _finish(self, slot):
-        """Converts every product of the finished batch to CSR on the device
-        (all conversions queued on the slot's stream, one synchronisation).
-        deliver="device": each job gets its device tensors.  deliver="host":
-        the batch's results go through the slot's reusable page-locked
-        staging buffer (one copy; pinning fresh memory per batch costs more)
-        into numpy arrays of each job."""
+        """Stage 1, once the batch's stream is idle: reads the products'
+        sizes and queues every conversion to CSR on the slot's stream, into
+        one device buffer (and, deliver="host", its copy into the slot's
+        reusable page-locked staging buffer), without waiting: the work runs
+        when the GPU is free and _deliver hands the results over."""
         import torch
         slot.batch.sync()
+        self.host_s["gpu"] += sum(slot.batch.phase_ms().values()) * 1e-3
         dev = torch.device("cuda", self.device)
         layout, total = [], 0
         for p, job in enumerate(slot.jobs):
@@ -306,26 +414,36 @@ class SpGEMMServer:
             ci_off = rp_off + 4 * (m + 1)
             total = (ci_off + 4 * nnz + 7) & ~7
             layout.append((job, C, m, C.s.n, nnz, v_off, rp_off, ci_off))
-        dbuf = torch.empty(max(total, 8), dtype=torch.uint8, device=dev)
+        with torch.cuda.stream(slot.stream):
+            dbuf = torch.empty(max(total, 8), dtype=torch.uint8, device=dev)
         base = dbuf.data_ptr()
         for job, C, m, n, nnz, v_off, rp_off, ci_off in layout:
             check(lib().tsg_tiled_to_csr(slot.ctx.handle, ctypes.byref(C.s), ctypes.c_void_p(base + rp_off),
                                          ctypes.c_void_p(base + ci_off), ctypes.c_void_p(base + v_off)))
-        slot.ctx.synchronize()
+        if self.deliver == "host":
+            if slot.staging is None or slot.staging.numel() < total:
+                slot.staging = torch.empty(max(total, 1 << 20), dtype=torch.uint8, pin_memory=True)
+            with torch.cuda.stream(slot.stream):
+                slot.staging[:max(total, 8)].copy_(dbuf, non_blocking=True)
+        slot.pending = (layout, dbuf)
+
+    def _deliver(self, slot):
+        """Stage 2, once the conversions (and copies) have run: hands each
+        job its result and releases the batch."""
+        import torch
+        layout, dbuf = slot.pending
         if self.deliver == "device":
             for job, C, m, n, nnz, v_off, rp_off, ci_off in layout:
                 res = (m, n, dbuf[rp_off:rp_off + 4 * (m + 1)].view(torch.int32),
                        dbuf[ci_off:ci_off + 4 * nnz].view(torch.int32), dbuf[v_off:v_off + 8 * nnz].view(torch.float64))
                 self._complete(job, nnz, res)
         else:
-            if slot.staging is None or slot.staging.numel() < total:
-                slot.staging = torch.empty(max(total, 1 << 20), dtype=torch.uint8, pin_memory=True)
-            slot.staging[:max(total, 8)].copy_(dbuf)
             raw = slot.staging.numpy()
             for job, C, m, n, nnz, v_off, rp_off, ci_off in layout:
                 res = (m, n, raw[rp_off:rp_off + 4 * (m + 1)].view(np.int32).copy(),
                        raw[ci_off:ci_off + 4 * nnz].view(np.int32).copy(), raw[v_off:v_off + 8 * nnz].view(np.float64).copy())
                 self._complete(job, nnz, res)
+        slot.pending = None
         self._release(slot)
 
     def _complete(self, job, nnz, res):
@@ -346,11 +464,16 @@ class SpGEMMServer:
             progressed = False
             for slot in self.slots:
                 if slot.batch is not None and slot.idle_stream():
-                    self._finish(slot)
+                    t0 = time.perf_counter()
+                    stage = "finish" if slot.pending is None else "deliver"
+                    (self._finish if slot.pending is None else self._deliver)(slot)
+                    self.host_s[stage] += time.perf_counter() - t0
                     progressed = True
             for slot in self.slots:
                 if slot.batch is None and self.queue:
+                    t0 = time.perf_counter()
                     progressed |= self._form_batch(slot)
+                    self.host_s["form"] += time.perf_counter() - t0
             if not progressed:
                 with self.lock:
                     if not self.queue and all(s.batch is None for s in self.slots):
@@ -372,4 +495,5 @@ class SpGEMMServer:
             "rejected": self.rejected,
             "operand_cache": {"hits": self.cache.hits, "misses": self.cache.misses, "bytes": self.cache.bytes},
             "tuned": {f"d{k}": "-".join(str(x) for x in v) for k, v in sorted(self.tuned.items())},
+            "dispatcher_s": {k: round(v, 4) for k, v in self.host_s.items()},
         }

@@ -86,6 +86,53 @@ def test_product_bounds_bound_the_result(tsg, ctx, oracle, gen):
         assert info["nnz_C"] <= prods and info["numtile_C"] <= pairs
 
 
+def test_product_bounds_of_many_products_in_one_call(tsg, ctx, oracle, gen):
+    mats = _pairs(gen)
+    pairs = [(_tiled(tsg, ctx, a, 1), _tiled(tsg, ctx, b, 2)) for a, b in mats]
+    many = tsg.product_bounds_many(ctx, pairs, c_tiles=True)
+    assert [m[:2] for m in many] == tsg.product_bounds_many(ctx, pairs)
+    for (a, b), (A, B), (prods, tpairs, ctiles) in zip(mats, pairs, many):
+        assert (prods, tpairs) == tsg.product_bounds(ctx, A, B)
+        assert prods == oracle.count_products(a, b)
+        C, info = tsg.spgemm(ctx, A, B)
+        assert ctiles == info["numtile_C"]      # step 1's count is exact
+    assert tsg.product_bounds_many(ctx, []) == []
+
+
+def test_batch_planned_from_given_bounds(tsg, ctx, gen):
+    """tsg_batch_create_bounded with tsg_product_bounds_many's bounds gives
+    the same bits and arena as the self-bounding create; a C-tile bound
+    below the true count makes the batch report TSG_ERR_OVERFLOW (the
+    kernel's own capacity check skips that product)."""
+    mats = _pairs(gen)
+    pairs = [(_tiled(tsg, ctx, a, tsg.TSG_TILED_PACKED_COL), _tiled(tsg, ctx, b, tsg.TSG_TILED_CSC_VIEW))
+             for a, b in mats]
+    bounds = [(pr, ct) for pr, _, ct in tsg.product_bounds_many(ctx, pairs, c_tiles=True)]
+    ref = tsg.Batch(ctx, pairs, "spa", 8, 512, graph=False)
+    ref.run()
+    ref.sync()
+    got = tsg.Batch(ctx, pairs, "spa", 8, 512, graph=False, bounds=bounds)
+    assert got.info()["arena_bytes"] == ref.info()["arena_bytes"]
+    got.run()
+    got.sync()
+    for p in range(len(mats)):
+        a, b = ref.product(p).download(), got.product(p).download()
+        for k in C_KEYS:
+            np.testing.assert_array_equal(np.asarray(b[k]).view(np.uint8), np.asarray(a[k]).view(np.uint8))
+    got.close()
+    p_big = max(range(len(bounds)), key=lambda i: bounds[i][1])
+    short = list(bounds)
+    short[p_big] = (bounds[p_big][0], bounds[p_big][1] - 1)
+    bad = tsg.Batch(ctx, pairs, "spa", 8, 512, graph=False, bounds=short)
+    bad.run()
+    with pytest.raises(tsg.TsgError, match="exceeded its bound"):
+        bad.sync()
+    bad.close()
+    ref.close()
+    with pytest.raises(ValueError):
+        tsg.Batch(ctx, pairs, bounds=bounds[:-1])
+
+
 def test_batch_phase_times(tsg, ctx, gen):
     mats = _pairs(gen)[:6]
     pairs = [(_tiled(tsg, ctx, a, 1), _tiled(tsg, ctx, b, 2)) for a, b in mats]

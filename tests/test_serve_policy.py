@@ -47,8 +47,9 @@ class FakeCache:
 
 
 class FakeBatch:
-    def __init__(self, ctx, pairs, *sched, graph=False, dense=0):
+    def __init__(self, ctx, pairs, *sched, graph=False, dense=0, bounds=None):
         self.pairs = list(pairs)
+        self.bounds = bounds
         self.sched = tuple(sched) + (dense,)
 
     def info(self):
@@ -62,6 +63,7 @@ class FakeSlot:
     def __init__(self):
         self.ctx = None
         self.batch = None
+        self.pending = None
         self.jobs = []
         self.arena = 0
         self.t_launch = 0.0
@@ -80,7 +82,11 @@ def make_server(serve_mod, monkeypatch, mem_cap, budget, sizes, predict):
     srv.lock = threading.Condition()
     srv.running, srv.thread, srv.next_id = False, None, 0
     srv.done, srv.batches, srv.rejected = [], 0, 0
+    srv.host_s = collections.defaultdict(float)
+    srv.preds = {}
+    srv.classes, srv.lookahead = {}, 256
     srv._predict = lambda A, B: tuple(predict[(A, B)]) + (1,) * (3 - len(predict[(A, B)]))
+    srv._predict_many = lambda ops: [srv._predict(A, B) for A, B in ops]
     return srv
 
 
@@ -155,3 +161,90 @@ def test_operand_bytes_are_the_librarys_allocation(serve_mod):
     class T:
         device_bytes = 12345
     assert serve_mod.OperandCache.tiled_bytes(T()) == 12345
+
+
+def test_queue_head_with_resident_operands_is_predicted_in_one_call(serve_mod, monkeypatch):
+    predict = {("a", "b"): (10, 5), ("c", "d"): (10, 5), ("a", "d"): (10, 5), ("e", "f"): (10, 5)}
+    srv = make_server(serve_mod, monkeypatch, 10_000, 1e9, {k: 1 for k in "abcdef"}, predict)
+    calls = {"many": [], "one": 0}
+    one = srv._predict
+
+    def many(ops):
+        calls["many"].append(list(ops))
+        return [one(A, B) for A, B in ops]
+
+    def single(A, B):
+        calls["one"] += 1
+        return one(A, B)
+    srv._predict_many, srv._predict = many, single
+    for k in "abcd":
+        srv.cache.get(k, None)
+    for a, b in [("a", "b"), ("c", "d"), ("a", "d"), ("e", "f")]:
+        srv.submit("AB", a, b)
+    assert srv._form_batch(srv.slots[0]) and batch_jobs(srv.slots[0]) == [0, 1, 2, 3]
+    # the three jobs on resident operands in one call, the one that uploads alone
+    assert calls["many"] == [[("a", "b"), ("c", "d"), ("a", "d")]] and calls["one"] == 1
+
+
+def test_batches_are_planned_from_cached_predictions(serve_mod, monkeypatch):
+    predict = {("a", "b"): (10, 7, 3), ("c", "d"): (10, 9, 4)}
+    srv = make_server(serve_mod, monkeypatch, 10_000, 1e9, {k: 1 for k in "abcd"}, predict)
+    n = {"one": 0}
+    one = srv._predict
+
+    def counted(A, B):
+        n["one"] += 1
+        return one(A, B)
+    srv._predict = counted
+    for a, b in [("a", "b"), ("c", "d"), ("a", "b")]:
+        srv.submit("AB", a, b)
+    s0, s1 = srv.slots
+    assert srv._form_batch(s0) and batch_jobs(s0) == [0, 1, 2]
+    # (products, C tiles) per job go to the batch; the repeated pair was predicted once
+    assert s0.batch.bounds == [(7, 3), (9, 4), (7, 3)] and n["one"] == 2
+    srv.submit("AB", "c", "d")
+    assert srv._form_batch(s1) and n["one"] == 2
+
+
+def test_replacing_an_operand_drops_what_came_from_it(serve_mod, monkeypatch):
+    predict = {("a", "b"): (10, 7, 3), ("a", ("a", "T")): (10, 7, 3)}
+    srv = make_server(serve_mod, monkeypatch, 10_000, 1e9, {"a": 1, "b": 1, ("a", "T"): 1}, predict)
+    srv.matrices = {"a": (1, 1, [0, 0], [], []), "b": None}
+    srv.preds = {("a", "b"): (1, 2, 3), ("b", "b"): (4, 5, 6)}
+    srv.matrices[("a", "T")] = "old transpose"
+    srv.cache.drop = lambda keys: srv.cache.evicted.extend(sorted(map(str, keys)))
+    srv.submit("AB", "b", "b")
+    srv.register("a", (2, 2, [0, 0, 0], [], []))
+    assert ("a", "T") not in srv.matrices and srv.preds == {("b", "b"): (4, 5, 6)}
+    assert srv.cache.evicted == ["('a', 'T')", "a"]
+    with pytest.raises(RuntimeError):
+        srv.register("b", "another")
+
+
+def test_batches_hold_one_skew_class_and_others_keep_their_places(serve_mod, monkeypatch):
+    predict = {(a, a): (10, 40) for a in "abcde"}
+    srv = make_server(serve_mod, monkeypatch, 10_000, 100, {k: 1 for k in "abcde"}, predict)
+    srv.classes = {"a": 0, "b": 3, "c": 0, "d": 3, "e": 0}
+    for a in "abcde":
+        srv.submit("AB", a, a)
+    s0, s1 = srv.slots
+    assert srv._form_batch(s0) and batch_jobs(s0) == [0, 2]        # class 0; 40 + 40 + 40 > 100: e waits
+    assert [j.jid for j in srv.queue] == [1, 3, 4]
+    assert srv._form_batch(s1) and batch_jobs(s1) == [1, 3]        # class 3
+    s0.batch = None
+    assert srv._form_batch(s0) and batch_jobs(s0) == [4] and not srv.queue
+    srv.lookahead = 1
+    for a in "bab":
+        srv.submit("AB", a, a)
+    s0.batch = None
+    assert srv._form_batch(s0) and batch_jobs(s0) == [5]            # looks past one job only
+    assert [j.jid for j in srv.queue] == [6, 7]
+
+
+def test_skew_class_of_a_matrix(serve_mod):
+    import numpy as np
+    serve = serve_mod
+    flat = (4, 4, np.array([0, 2, 4, 6, 8]), np.zeros(8, np.int32), np.ones(8))
+    hub = (4, 4, np.array([0, 13, 14, 15, 16]), np.zeros(16, np.int32), np.ones(16))
+    empty = (3, 3, np.zeros(4, np.int64), np.zeros(0, np.int32), np.zeros(0))
+    assert serve.skew_class(flat) == 0 and serve.skew_class(hub) == 1 and serve.skew_class(empty) == 0
