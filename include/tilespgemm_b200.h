@@ -176,8 +176,28 @@ typedef enum
     REORDER_PROBLEM_AB = 2
 } ReorderProblemKind;
 
+/* src/reorder.h:72-77 (field order kept). */
+typedef struct
+{
+    ReorderProblemKind kind;
+    const SMatrix *matrixA;
+    const SMatrix *matrixB; /* AA: may be matrixA or NULL; AAT: A's transpose */
+} ReorderProblem;
+
 void reorder_info_init(ReorderInfo *info);
 void reorder_info_destroy(ReorderInfo *info);
+
+/* The tile-aware planner (TASA, the CLI's default -reorder_algo); replaces
+ * build_reorder_plan, src/reorder.h:2407-2428, with the same plans, modes,
+ * risk guard and return codes (0, or -1 bad problem / non-square AA, -2.. on
+ * failure).  A*A of a symmetric matrix (isSymmetric): identity for n <=
+ * 50,000 with < 32 tiles per tile row, reverse Cuthill-McKee refined in
+ * windows of 32 for other n <= 50,000, windowed packing into 16-row groups
+ * above; general A*A, A*B and A*A^T: every axis sorted by tile signatures
+ * (computed on the GPU).  Environment: TASA_FORCE_ACTIVE=1 accepts any plan,
+ * TASA_AB_SHARED_SYM=1 lets A*B of two symmetric matrices use the symmetric
+ * plan. */
+int build_reorder_plan(const ReorderProblem *problem, ReorderInfo *info);
 
 /* Identity plan; replaces build_original_reorder_plan,
  * src/external_reorder.h:173-202.  Returns 0 or a negative code. */

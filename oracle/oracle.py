@@ -365,6 +365,8 @@ def rrlib():
         _rr.ref_fill_reorder_estimates.argtypes = [ctypes.c_int, vp, vp, vp]
         _rr.ref_build_original_reorder_plan.argtypes = [ctypes.c_int, vp, vp, vp]
         _rr.ref_reorder_info_init.argtypes = [vp]
+        _rr.ref_reorder_info_destroy.argtypes = [vp]
+        _rr.ref_build_reorder_plan.argtypes = [ctypes.c_int, vp, vp, vp]
     return _rr
 
 
@@ -474,3 +476,33 @@ def reorder_estimates(kind, matA, matB, row_old, inner_old, col_old):
     return dict(input_tiles_A_before=a0, input_tiles_A_after=a1, input_tiles_B_before=b0, input_tiles_B_after=b1,
                 estimated_c_tiles_before=c0, estimated_c_tiles_after=c1,
                 risk_input_tile_ratio=max(ratio(a1, a0), ratio(b1, b0)), risk_c_tile_ratio=ratio(c1, c0))
+
+
+PLAN_FIELDS = ("enabled", "n", "input_tiles_A_before", "input_tiles_A_after", "input_tiles_B_before",
+               "input_tiles_B_after", "estimated_c_tiles_before", "estimated_c_tiles_after", "risk_input_tile_ratio",
+               "risk_c_tile_ratio", "local_refine_window", "proxy_sample_rows", "guard_degraded_to_identity",
+               "structural_conservative", "shared_symmetric_csr")
+
+
+def ref_build_reorder_plan(kind, matA, matB=None, symmetric=False):
+    """The reference's tile-aware planner build_reorder_plan
+    (src/reorder.h:2407-2428) compiled from its sources: (status, plan dict
+    with the three new -> old permutations, PLAN_FIELDS, mode, risk_reason).
+    Symmetric A*A plans run on the host; the others need a GPU."""
+    R = rrlib()
+    hA = _CSRHold(matA)
+    hB = _CSRHold(matB) if matB is not None else hA
+    hA.om.isSymmetric = hB.om.isSymmetric = 1 if symmetric else 0
+    info = OReorderInfo()
+    R.ref_reorder_info_init(ctypes.byref(info))
+    st = R.ref_build_reorder_plan({"AA": 0, "AAT": 1, "AB": 2}[kind], ctypes.byref(hA.om), ctypes.byref(hB.om),
+                                  ctypes.byref(info))
+    out = {f: getattr(info, f) for f in PLAN_FIELDS}
+    out["mode"] = info.mode.decode()
+    out["risk_reason"] = info.risk_reason.decode()
+    for ax in ("row_perm", "inner_perm", "col_perm"):
+        p = getattr(info, ax)
+        out[ax] = np.ctypeslib.as_array(p.old_id, shape=(p.n,)).copy() if p.n > 0 and p.old_id else \
+            np.zeros(0, np.int32)
+    R.ref_reorder_info_destroy(ctypes.byref(info))
+    return st, out

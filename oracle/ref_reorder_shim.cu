@@ -6,7 +6,9 @@
  * (they need nvcc for their thrust kernels) and their host functions wrapped
  * in extern "C" entry points for ctypes: the sampled input-tile and C-tile
  * estimates (src/reorder.h:785-975), the plan's estimate fill
- * (src/external_reorder.h:143-171) and the original-order plan (:173-202).
+ * (src/external_reorder.h:143-171), the original-order plan (:173-202) and
+ * the tile-aware planner build_reorder_plan (src/reorder.h:2407-2428; its
+ * general-matrix plans run thrust kernels, so they need a GPU).
  */
 #include "common.h"
 #include "reorder.h"
@@ -39,6 +41,15 @@ void ref_fill_reorder_estimates(int kind, const SMatrix *a, const SMatrix *b, Re
 int ref_build_original_reorder_plan(int kind, const SMatrix *a, const SMatrix *b, ReorderInfo *info)
 {
     return build_original_reorder_plan((ReorderProblemKind)kind, a, b, info);
+}
+
+int ref_build_reorder_plan(int kind, const SMatrix *a, const SMatrix *b, ReorderInfo *info)
+{
+    ReorderProblem problem;
+    problem.kind = (ReorderProblemKind)kind;
+    problem.matrixA = a;
+    problem.matrixB = b;
+    return build_reorder_plan(&problem, info);
 }
 
 void ref_reorder_info_init(ReorderInfo *info) { reorder_info_init(info); }

@@ -536,6 +536,11 @@ class ReorderInfo(ctypes.Structure):
     ]
 
 
+class ReorderProblem(ctypes.Structure):
+    """src/reorder.h:72-77."""
+    _fields_ = [("kind", ctypes.c_int), ("matrixA", ctypes.POINTER(SMatrix)), ("matrixB", ctypes.POINTER(SMatrix))]
+
+
 def _declare_reorder(L):
     vp, ip = ctypes.c_void_p, ctypes.c_int
     L.tsg_order.argtypes = [vp, ip, ip, ip, ip, vp, vp, ctypes.c_ulonglong, vp]
@@ -550,6 +555,7 @@ def _declare_reorder(L):
     L.build_external_reorder_plan.argtypes = [ip, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
                                               ctypes.POINTER(SMatrix), ctypes.POINTER(SMatrix),
                                               ctypes.POINTER(ReorderInfo), ctypes.POINTER(ctypes.c_double)]
+    L.build_reorder_plan.argtypes = [ctypes.POINTER(ReorderProblem), ctypes.POINTER(ReorderInfo)]
     L.apply_bipermutation_csr.argtypes = [ctypes.POINTER(SMatrix), ctypes.POINTER(AxisPermutation),
                                           ctypes.POINTER(AxisPermutation), ctypes.POINTER(SMatrix)]
     L.restore_bipermutation_csr.argtypes = [ctypes.POINTER(SMatrix), ctypes.POINTER(AxisPermutation),
@@ -658,17 +664,27 @@ def restore_bipermutation_csr(mat, row_old, col_old):
 REORDER_PROBLEM = {"AA": 0, "AAT": 1, "AB": 2}
 
 
-def build_reorder_plan(kind: str, algorithm: str, matA, matB=None) -> dict:
+def build_reorder_plan(kind: str, algorithm: str, matA, matB=None, symmetric: bool = False) -> dict:
     """build_original_reorder_plan / build_external_reorder_plan
-    (src/external_reorder.h:173-321) with the ordering computed on the GPU."""
+    (src/external_reorder.h:173-321) with the ordering computed on the GPU;
+    algorithm "tasa": the tile-aware planner build_reorder_plan
+    (src/reorder.h:2407), whose A*A plan depends on `symmetric` (the
+    matrices' isSymmetric flag, as a symmetric Matrix Market file sets it)."""
     L = lib()
     hA = HostCSR(matA)
     hB = HostCSR(matB) if matB is not None else None
+    for h in (hA, hB):
+        if h is not None:
+            h.sm.isSymmetric = 1 if symmetric else 0
     info = ReorderInfo()
     L.reorder_info_init(ctypes.byref(info))
     ms = ctypes.c_double(0.0)
     pB = ctypes.byref(hB.sm) if hB else None
-    if algorithm == "original":
+    if algorithm == "tasa":
+        prob = ReorderProblem(REORDER_PROBLEM[kind], ctypes.pointer(hA.sm),
+                              ctypes.pointer(hB.sm) if hB else ctypes.pointer(hA.sm))
+        st = L.build_reorder_plan(ctypes.byref(prob), ctypes.byref(info))
+    elif algorithm == "original":
         st = L.build_original_reorder_plan(REORDER_PROBLEM[kind], ctypes.byref(hA.sm), pB, ctypes.byref(info))
     else:
         st = L.build_external_reorder_plan(REORDER_PROBLEM[kind], algorithm.encode(), b"", b"", ctypes.byref(hA.sm),

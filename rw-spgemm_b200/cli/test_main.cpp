@@ -1,6 +1,6 @@
 // Drop-in replacement of the reference CLI (src/main.cu:15-638):
 //
-//   ./test -d <dev> -aat <0|1> A.mtx [-b B.mtx] [-reorder 1] [-reorder_algo original|rcm|degree|gray|random]
+//   ./test -d <dev> -aat <0|1> A.mtx [-b B.mtx] [-reorder 1] [-reorder_algo tasa|original|rcm|degree|gray|random]
 //          [-o C.mtx]
 //
 // Same flags, same value overwrite (value[i] = i % 10, src/main.cu:191-197,
@@ -17,8 +17,8 @@
 // pointers, columns and values (relative 1e-12) -- where the reference ran
 // cuSPARSE with FP32 descriptors on FP64 data and compared structure only
 // (src/external/cusparse/spgemm_cusparse.h:162-173, :282).
-// The TASA planner (-reorder_algo tasa, src/reorder.h:785-2405) is not part
-// of this library; asking for it exits with the reference's failure message.
+// -reorder_algo tasa (the default, as in the reference) runs the library's
+// tile-aware planner build_reorder_plan (src/reorder.h:2407).
 #include <cuda_runtime.h>
 #include <cusparse.h>
 #include <math.h>
@@ -392,8 +392,16 @@ int main(int argc, char **argv)
         int st;
         if (!strcmp(reorder_algo, "tasa"))
         {
-            printf("reorder failed, status = %d. Exit.\n", -2);
-            return 0;
+            ReorderProblem problem;
+            problem.kind = kind;
+            problem.matrixA = &A0;
+            problem.matrixB = kind == REORDER_PROBLEM_AA ? &A0 : &B0;
+            st = build_reorder_plan(&problem, &info);
+            if (st)
+            {
+                printf("reorder failed, status = %d. Exit.\n", st);
+                return 0;
+            }
         }
         else if (!strcmp(reorder_algo, "original"))
         {

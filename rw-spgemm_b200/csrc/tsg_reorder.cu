@@ -633,6 +633,8 @@ extern "C" int tsg_permute_csr(tsg_context *ctx, int m, int n, int nnz, const in
 // ---------------------------------------------------------------------------
 // Drop-in reorder entry points on host SMatrix CSR.
 // ---------------------------------------------------------------------------
+#define PLAN_SAMPLE_ROWS 24 // tile rows the plan estimators sample
+
 static void axis_init(AxisPermutation *p)
 {
     p->n = 0;
@@ -647,7 +649,7 @@ static void axis_destroy(AxisPermutation *p)
     axis_init(p);
 }
 
-static int axis_alloc(AxisPermutation *p, int n)
+int tsg_axis_alloc(AxisPermutation *p, int n)
 {
     axis_destroy(p);
     p->n = n;
@@ -656,9 +658,9 @@ static int axis_alloc(AxisPermutation *p, int n)
     return (p->old_id && p->new_id) ? 0 : -1;
 }
 
-static int axis_from_order(AxisPermutation *p, const int *order, int n)
+int tsg_axis_from_order(AxisPermutation *p, const int *order, int n)
 {
-    if (axis_alloc(p, n) != 0)
+    if (tsg_axis_alloc(p, n) != 0)
         return -1;
     for (int i = 0; i < n; i++)
     {
@@ -668,16 +670,16 @@ static int axis_from_order(AxisPermutation *p, const int *order, int n)
     return 0;
 }
 
-static int axis_copy(AxisPermutation *dst, const AxisPermutation *src)
+int tsg_axis_copy(AxisPermutation *dst, const AxisPermutation *src)
 {
-    if (axis_alloc(dst, src->n) != 0)
+    if (tsg_axis_alloc(dst, src->n) != 0)
         return -1;
     memcpy(dst->old_id, src->old_id, (size_t)src->n * sizeof(int));
     memcpy(dst->new_id, src->new_id, (size_t)src->n * sizeof(int));
     return 0;
 }
 
-static void set_text(char *dst, size_t size, const char *src)
+void tsg_info_text(char *dst, size_t size, const char *src)
 {
     strncpy(dst, src ? src : "", size - 1);
     dst[size - 1] = '\0';
@@ -691,9 +693,9 @@ extern "C" void reorder_info_init(ReorderInfo *info)
     axis_init(&info->col_perm);
     info->risk_input_tile_ratio = 1.0;
     info->risk_c_tile_ratio = 1.0;
-    info->proxy_sample_rows = 0;
-    set_text(info->mode, sizeof(info->mode), "unset");
-    set_text(info->risk_reason, sizeof(info->risk_reason), "none");
+    info->proxy_sample_rows = PLAN_SAMPLE_ROWS;
+    tsg_info_text(info->mode, sizeof(info->mode), "unset");
+    tsg_info_text(info->risk_reason, sizeof(info->risk_reason), "none");
 }
 
 extern "C" void reorder_info_destroy(ReorderInfo *info)
@@ -769,7 +771,6 @@ static int permute_dev(tsg_context *ctx, const DevCSR *in, const int *h_row_old,
 // (total * tile rows / samples in double, truncated).  Host code, like the
 // reference's: 24 tile rows and their B tile rows, no device work.
 // ---------------------------------------------------------------------------
-#define PLAN_SAMPLE_ROWS 24
 
 static int perm_old(const AxisPermutation *p, int id) { return p ? p->old_id[id] : id; }
 static int perm_new(const AxisPermutation *p, int id) { return p ? p->new_id[id] : id; }
@@ -800,7 +801,7 @@ static void plan_samples(int tiles, int *count, int *stride)
 }
 
 // tile count of M under (row, col): distinct tile columns per sampled tile row
-static long long estimate_input_tiles(const SMatrix *M, const AxisPermutation *row, const AxisPermutation *col)
+long long tsg_estimate_input_tiles(const SMatrix *M, const AxisPermutation *row, const AxisPermutation *col)
 {
     const int tilem = (M->m + TSG_BS - 1) / TSG_BS, tilen = (M->n + TSG_BS - 1) / TSG_BS;
     int count, stride, used = 0;
@@ -828,8 +829,8 @@ static long long estimate_input_tiles(const SMatrix *M, const AxisPermutation *r
 // the distinct tile columns of the B tile rows its tile columns name.  one:
 // the reference's one-matrix form for A*A (every axis counted in A's tile
 // rows, B = A).
-static long long estimate_c_tiles(const SMatrix *A, const SMatrix *B, const AxisPermutation *row,
-                                  const AxisPermutation *inner, const AxisPermutation *col, bool one)
+long long tsg_estimate_c_tiles(const SMatrix *A, const SMatrix *B, const AxisPermutation *row,
+                               const AxisPermutation *inner, const AxisPermutation *col, bool one)
 {
     const int rows = (A->m + TSG_BS - 1) / TSG_BS;
     const int inner_tiles = one ? rows : (A->n + TSG_BS - 1) / TSG_BS;
@@ -878,23 +879,23 @@ static double safe_ratio(long long after, long long before)
 // before/after tile counts of a plan (src/external_reorder.h:143-171)
 static void fill_estimates(ReorderProblemKind kind, const SMatrix *A, const SMatrix *B, ReorderInfo *info)
 {
-    info->input_tiles_A_before = estimate_input_tiles(A, nullptr, nullptr);
-    info->input_tiles_A_after = estimate_input_tiles(A, &info->row_perm, &info->inner_perm);
+    info->input_tiles_A_before = tsg_estimate_input_tiles(A, nullptr, nullptr);
+    info->input_tiles_A_after = tsg_estimate_input_tiles(A, &info->row_perm, &info->inner_perm);
     if (kind == REORDER_PROBLEM_AA)
     {
         info->input_tiles_B_before = info->input_tiles_A_before;
         info->input_tiles_B_after = info->input_tiles_A_after;
-        info->estimated_c_tiles_before = estimate_c_tiles(A, A, nullptr, nullptr, nullptr, true);
+        info->estimated_c_tiles_before = tsg_estimate_c_tiles(A, A, nullptr, nullptr, nullptr, true);
         info->estimated_c_tiles_after =
-            estimate_c_tiles(A, A, &info->row_perm, &info->inner_perm, &info->col_perm, true);
+            tsg_estimate_c_tiles(A, A, &info->row_perm, &info->inner_perm, &info->col_perm, true);
     }
     else
     {
-        info->input_tiles_B_before = estimate_input_tiles(B, nullptr, nullptr);
-        info->input_tiles_B_after = estimate_input_tiles(B, &info->inner_perm, &info->col_perm);
-        info->estimated_c_tiles_before = estimate_c_tiles(A, B, nullptr, nullptr, nullptr, false);
+        info->input_tiles_B_before = tsg_estimate_input_tiles(B, nullptr, nullptr);
+        info->input_tiles_B_after = tsg_estimate_input_tiles(B, &info->inner_perm, &info->col_perm);
+        info->estimated_c_tiles_before = tsg_estimate_c_tiles(A, B, nullptr, nullptr, nullptr, false);
         info->estimated_c_tiles_after =
-            estimate_c_tiles(A, B, &info->row_perm, &info->inner_perm, &info->col_perm, false);
+            tsg_estimate_c_tiles(A, B, &info->row_perm, &info->inner_perm, &info->col_perm, false);
     }
     const double ra = safe_ratio(info->input_tiles_A_after, info->input_tiles_A_before);
     const double rb = safe_ratio(info->input_tiles_B_after, info->input_tiles_B_before);
@@ -921,8 +922,8 @@ extern "C" int build_original_reorder_plan(ReorderProblemKind kind, const SMatri
         return -2;
     reorder_info_destroy(info);
     const int ncol = kind == REORDER_PROBLEM_AA ? matrixA->n : matrixB->n;
-    if (axis_alloc(&info->row_perm, matrixA->m) || axis_alloc(&info->inner_perm, matrixA->n) ||
-        axis_alloc(&info->col_perm, ncol))
+    if (tsg_axis_alloc(&info->row_perm, matrixA->m) || tsg_axis_alloc(&info->inner_perm, matrixA->n) ||
+        tsg_axis_alloc(&info->col_perm, ncol))
         return -1;
     for (int i = 0; i < matrixA->m; i++)
         info->row_perm.old_id[i] = info->row_perm.new_id[i] = i;
@@ -935,8 +936,8 @@ extern "C" int build_original_reorder_plan(ReorderProblemKind kind, const SMatri
     info->shared_symmetric_csr = (kind == REORDER_PROBLEM_AA);
     info->guard_degraded_to_identity = 1;
     info->structural_conservative = 0;
-    set_text(info->mode, sizeof(info->mode), "original");
-    set_text(info->risk_reason, sizeof(info->risk_reason), "original_order");
+    tsg_info_text(info->mode, sizeof(info->mode), "original");
+    tsg_info_text(info->risk_reason, sizeof(info->risk_reason), "original_order");
     fill_estimates(kind, matrixA, kind == REORDER_PROBLEM_AA ? matrixA : matrixB, info);
     return 0;
 }
@@ -966,7 +967,7 @@ static int order_host(tsg_context *ctx, int kind, const SMatrix *M, AxisPermutat
     float e = 0.f;
     cudaEventElapsedTime(&e, ctx->ev[6], ctx->ev[7]);
     *ms += e;
-    int st = axis_from_order(perm, h, M->m) == 0 ? TSG_OK : TSG_ERR_OOM;
+    int st = tsg_axis_from_order(perm, h, M->m) == 0 ? TSG_OK : TSG_ERR_OOM;
     free(h);
     tsg_release(ctx, d_order);
     free_csr(ctx, &d);
@@ -1007,7 +1008,7 @@ extern "C" int build_external_reorder_plan(ReorderProblemKind kind, const char *
             return -4;
         }
         st = order_host(ctx, okind, matrixA, &info->row_perm, ordergen_ms);
-        if (st == TSG_OK && (axis_copy(&info->inner_perm, &info->row_perm) || axis_copy(&info->col_perm, &info->row_perm)))
+        if (st == TSG_OK && (tsg_axis_copy(&info->inner_perm, &info->row_perm) || tsg_axis_copy(&info->col_perm, &info->row_perm)))
             st = TSG_ERR_OOM;
         info->shared_symmetric_csr = 1;
     }
@@ -1019,7 +1020,7 @@ extern "C" int build_external_reorder_plan(ReorderProblemKind kind, const char *
             return -5;
         }
         st = order_host(ctx, okind, matrixA, &info->row_perm, ordergen_ms);
-        if (st == TSG_OK && (axis_copy(&info->inner_perm, &info->row_perm) || axis_copy(&info->col_perm, &info->row_perm)))
+        if (st == TSG_OK && (tsg_axis_copy(&info->inner_perm, &info->row_perm) || tsg_axis_copy(&info->col_perm, &info->row_perm)))
             st = TSG_ERR_OOM;
         info->shared_symmetric_csr = 0;
     }
@@ -1036,7 +1037,7 @@ extern "C" int build_external_reorder_plan(ReorderProblemKind kind, const char *
             return -7;
         }
         st = order_host(ctx, okind, matrixA, &info->row_perm, ordergen_ms);
-        if (st == TSG_OK && axis_copy(&info->inner_perm, &info->row_perm))
+        if (st == TSG_OK && tsg_axis_copy(&info->inner_perm, &info->row_perm))
             st = TSG_ERR_OOM;
         if (st == TSG_OK)
             st = order_host(ctx, okind, matrixB, &info->col_perm, ordergen_ms);
@@ -1053,8 +1054,8 @@ extern "C" int build_external_reorder_plan(ReorderProblemKind kind, const char *
     info->n = matrixA->n;
     info->guard_degraded_to_identity = 0;
     info->structural_conservative = 0;
-    set_text(info->mode, sizeof(info->mode), algorithm);
-    set_text(info->risk_reason, sizeof(info->risk_reason), "external_order");
+    tsg_info_text(info->mode, sizeof(info->mode), algorithm);
+    tsg_info_text(info->risk_reason, sizeof(info->risk_reason), "external_order");
     fill_estimates(kind, matrixA, kind == REORDER_PROBLEM_AA ? matrixA : matrixB, info);
     return 0;
 }

@@ -168,8 +168,24 @@ def test_cli_values_in_file_order_with_duplicates(tmp_path, oracle, mode):
     np.testing.assert_array_equal(v, G[4])                   # small integers: exact
 
 
-def test_cli_usage_and_tasa(tmp_path, gen):
+def test_cli_usage_and_tasa(tmp_path, gen, oracle):
     assert "Run the code by" in run(["-d", "0"])
     p = tmp_path / "x.mtx"
-    write_mtx(p, gen.laplacian_2d(6), symmetric_lower=True)
-    assert "reorder failed" in run(["-d", "0", "-aat", "0", str(p), "-reorder", "1"])
+    lap = gen.laplacian_2d(6)
+    write_mtx(p, lap, symmetric_lower=True)
+    txt = run(["-d", "0", "-aat", "0", str(p), "-reorder", "1"])        # tasa: the reference's default
+    assert "reorder algorithm = tasa" in txt and "reorder strategy = TASA-Fast-Unified" in txt
+    assert "reorder mode = identity_narrow_tiles" in txt and "reorder uses conservative identity" in txt
+    expect_passed(txt, oracle.gustavson(lap, lap)[3].size)
+    # a general (unsymmetric) file: the signature plan on the GPU, A*A and A*B
+    g = gen.random_poisson(700, 700, 6.0, seed=2)
+    b = gen.random_poisson(700, 500, 4.0, seed=3)
+    pg, pb = tmp_path / "g.mtx", tmp_path / "b.mtx"
+    write_mtx(pg, g)
+    write_mtx(pb, b)
+    txt = run(["-d", "0", "-aat", "0", str(pg), "-reorder", "1", "-reorder_algo", "tasa"])
+    assert re.search(r"reorder mode = (active_general|conservative_identity)\n", txt)
+    expect_passed(txt, oracle.gustavson(g, g)[3].size)
+    txt = run(["-d", "0", "-aat", "0", str(pg), "-b", str(pb), "-reorder", "1"])
+    assert re.search(r"reorder mode = (active_ab|conservative_identity)\n", txt)
+    expect_passed(txt, oracle.gustavson(g, b)[3].size)
