@@ -782,7 +782,21 @@ struct SpaStage
 {
     int2 bl[SPA_STAGE]; // B row: first entry, length
     double a[SPA_STAGE];
-    int tpre[32];       // FLAT staging: first entry of each lane's A tile
+};
+
+// The FLAT form stages A's entries with the whole CTA, SPA_CO_CHUNK at a
+// time (spa_coop_apply).
+#define SPA_CO_CHUNK 768
+#define SPA_CO_SLOTS (SPA_CO_CHUNK / 32)
+
+struct SpaCoop
+{
+    int2 bl[SPA_CO_CHUNK];        // B row (first entry, length) of each staged A entry, grouped by row
+    double a[SPA_CO_CHUNK];
+    int tile0[SPA_CO_CHUNK + 1];  // value offset of each A tile the chunk can touch
+    int wc[SPA_CO_SLOTS][TSG_BS]; // staged entries per (32-entry slot, row), then their offsets in the row
+    int rbeg[TSG_BS + 1];         // first staged entry of each row
+    int ptile;                    // the chunk's first A tile
 };
 
 struct SpaSmem
@@ -791,7 +805,11 @@ struct SpaSmem
     unsigned cm[TSG_BS * SPA_CMS];  // [row][tile]: (entries of the row in earlier tiles << 16) | C row mask
     int rstart[TSG_BS];             // first accumulator slot of each row's private, column-sorted run
     unsigned short map[SPA_WIN];    // tile column - J0 -> segment tile, 0xFFFF none
-    SpaStage stage[SPA_WARPS];
+    union
+    {
+        SpaStage stage[SPA_WARPS]; // per-row form
+        SpaCoop co;                // FLAT form
+    };
 };
 
 // accumulator slot of column col in the row (cmr, rs), -1 outside the segment
@@ -832,6 +850,261 @@ __device__ __forceinline__ void spa_add(SpaSmem &S, const unsigned *cmr, int rs,
 __host__ __device__ __forceinline__ bool spa_wants_flat(int browB, long long numC, long long nnzC, int tilem)
 {
     return browB < SPA_FLAT || numC > (long long)SPA_SEGT * tilem || nnzC > (long long)SPA_CAP * tilem;
+}
+
+// Applies ne (<= SPA_STAGE) staged entries A(r, k) of row r -- B row bounds
+// bl (cut to the segment) and values a, in k order -- to the row's
+// accumulator run.  FLATTEN: when their B rows hold fewer than SPA_FLAT
+// entries on average, the products are flattened, 32 per batch in k order;
+// lanes of a batch meeting the same slot are folded by the lowest of them in
+// lane order and batches follow one another behind warp barriers, so every
+// slot still sums its products in k order.  Otherwise (or !FLATTEN) a warp
+// pass per entry streams its B row, the next row's first 32 entries
+// prefetched.  bl is overwritten.
+template <bool FLATTEN>
+__device__ __forceinline__ void spa_apply_stage(const ProdView &P, SpaSmem &S, const unsigned *cmr, int rs, int J0,
+                                                int J1, bool full, int2 *bl, const double *a, int ne, int lane)
+{
+    if (FLATTEN)
+    {
+        const int l0 = lane < ne ? bl[lane].y : 0;
+        const int l1 = lane + 32 < ne ? bl[lane + 32].y : 0;
+        int i0 = l0, i1 = l1;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1)
+        {
+            const int o0 = __shfl_up_sync(TSG_FULL_MASK, i0, d);
+            const int o1 = __shfl_up_sync(TSG_FULL_MASK, i1, d);
+            if (lane >= d)
+            {
+                i0 += o0;
+                i1 += o1;
+            }
+        }
+        const int h0 = __shfl_sync(TSG_FULL_MASK, i0, 31);
+        const int ni = h0 + __shfl_sync(TSG_FULL_MASK, i1, 31);
+        if (ni < SPA_FLAT * ne)
+        {
+            // entry e becomes (its first B index - its first item, its first item)
+            if (lane < ne)
+                bl[lane] = make_int2(bl[lane].x - (i0 - l0), i0 - l0);
+            if (lane + 32 < ne)
+                bl[lane + 32] = make_int2(bl[lane + 32].x - (h0 + i1 - l1), h0 + i1 - l1);
+            __syncwarp();
+            int ent = 0;
+            for (int ib = 0; ib < ni; ib += 32)
+            {
+                const int item = ib + lane;
+                int pos = -1 - lane; // distinct keys for lanes without a slot
+                double prod = 0.0;
+                if (item < ni)
+                {
+                    while (ent + 1 < ne && bl[ent + 1].y <= item)
+                        ent++;
+                    const int bi = bl[ent].x + item;
+                    const int p = spa_slot(S, cmr, rs, J0, J1, full, P.B_rcol[bi]);
+                    if (p >= 0)
+                    {
+                        pos = p;
+                        prod = __dmul_rn(a[ent], P.B_rval[bi]);
+                    }
+                }
+                const unsigned grp = __match_any_sync(TSG_FULL_MASK, pos);
+                const bool lead = pos >= 0 && lane == __ffs(grp) - 1;
+                const int rounds = __reduce_max_sync(TSG_FULL_MASK, pos >= 0 ? __popc(grp) : 0);
+                double acc = lead ? S.acc[pos] : 0.0;
+                unsigned gl = grp;
+                for (int q = 0; q < rounds; q++)
+                {
+                    const double v = __shfl_sync(TSG_FULL_MASK, prod, gl ? __ffs(gl) - 1 : lane);
+                    if (gl)
+                    {
+                        acc = __dadd_rn(acc, v);
+                        gl &= gl - 1;
+                    }
+                }
+                if (lead)
+                    S.acc[pos] = acc;
+                __syncwarp();
+            }
+            return;
+        }
+    }
+    int2 nb = bl[0];
+    int c_cur = -1;
+    double v_cur = 0.0;
+    if (lane < nb.y)
+    {
+        c_cur = P.B_rcol[nb.x + lane];
+        v_cur = P.B_rval[nb.x + lane];
+    }
+    for (int i = 0; i < ne; i++)
+    {
+        const int2 cb = nb;
+        int c_nxt = -1;
+        double v_nxt = 0.0;
+        if (i + 1 < ne)
+        {
+            nb = bl[i + 1];
+            if (lane < nb.y)
+            {
+                c_nxt = P.B_rcol[nb.x + lane];
+                v_nxt = P.B_rval[nb.x + lane];
+            }
+        }
+        const double av = a[i];
+        if (c_cur >= 0)
+            spa_add(S, cmr, rs, J0, J1, full, c_cur, av, v_cur);
+        if (cb.y > 32) // B rows longer than a warp
+            for (int e = cb.x + 32 + lane; e < cb.x + cb.y; e += 32)
+                spa_add(S, cmr, rs, J0, J1, full, P.B_rcol[e], av, P.B_rval[e]);
+        __syncwarp();
+        c_cur = c_nxt;
+        v_cur = v_nxt;
+    }
+}
+
+// FLAT form of a segment's apply phase, with A's entries staged by the
+// whole CTA.  A's tile row I keeps its values contiguous, tile after tile
+// in column order, each tile row-major, so every row meets its own entries
+// in that order in k order.  The CTA takes them SPA_CO_CHUNK at a time:
+// every thread stages entries -- the row from the tile's row offsets, the
+// column from the entry's byte, B's row bounds cut to the segment's
+// columns -- entries whose B row holds nothing there are dropped and the
+// rest are grouped by row, keeping their order; then warp r applies its
+// row's staged entries in order (spa_apply_stage).  A row with many A
+// entries (R-MAT's hub rows) thus no longer stages them alone -- a binary
+// search of B's row per entry -- while the segment's other warps wait.
+__device__ __forceinline__ void spa_coop_apply(const ProdView &P, SpaSmem &S, int pa_beg, int pa_end, int J0, int J1,
+                                               bool full, int r, int lane, int tid, const unsigned *cmr, int rs)
+{
+    SpaCoop &C = S.co;
+    const bool ptr16 = (reinterpret_cast<unsigned long long>(P.A_Ptr) & 15ULL) == 0;
+    const int v_beg = P.A_tnnz[pa_beg], v_end = P.A_tnnz[pa_end];
+    for (int c0 = v_beg; c0 < v_end; c0 += SPA_CO_CHUNK)
+    {
+        const int ne = min(SPA_CO_CHUNK, v_end - c0);
+        if (tid == 0)
+        {
+            // the last tile of the row starting at or before c0
+            int lo = pa_beg, hi = pa_end - 1;
+            while (lo < hi)
+            {
+                const int mid = (lo + hi + 1) >> 1;
+                if (P.A_tnnz[mid] <= c0)
+                    lo = mid;
+                else
+                    hi = mid - 1;
+            }
+            C.ptile = lo;
+        }
+        for (int q = tid; q < SPA_CO_SLOTS * TSG_BS; q += SPA_THREADS)
+            C.wc[q / TSG_BS][q % TSG_BS] = 0;
+        __syncthreads();
+        const int p0 = C.ptile;
+        const int nt = min(ne, pa_end - p0); // tiles that can hold the chunk's entries
+        for (int q = tid; q <= nt; q += SPA_THREADS)
+            C.tile0[q] = P.A_tnnz[p0 + q];
+        __syncthreads();
+        int er[2], eb[2], el[2], ek[2];
+        double ea[2];
+#pragma unroll
+        for (int h = 0; h < 2; h++)
+        {
+            const int j = tid + h * SPA_THREADS;
+            int row = TSG_BS, b0 = 0, len = 0;
+            double av = 0.0;
+            if (j < ne)
+            {
+                const int v = c0 + j;
+                int lo = 0, hi = nt - 1;
+                while (lo < hi)
+                {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (C.tile0[mid] <= v)
+                        lo = mid;
+                    else
+                        hi = mid - 1;
+                }
+                const int p = p0 + lo, o = v - C.tile0[lo];
+                // the entry's row: the tile's row offsets 1..15 at or below o
+                const unsigned char *rp = P.A_Ptr + (long long)p * TSG_BS;
+                uint4 w;
+                if (ptr16)
+                    w = *reinterpret_cast<const uint4 *>(rp);
+                else
+                {
+                    unsigned u[4];
+                    for (int q = 0; q < 4; q++)
+                        u[q] = rp[4 * q] | (rp[4 * q + 1] << 8) | (rp[4 * q + 2] << 16) | ((unsigned)rp[4 * q + 3] << 24);
+                    w = make_uint4(u[0], u[1], u[2], u[3]);
+                }
+                const unsigned ob = (unsigned)o * 0x01010101u;
+                row = (__popc(__vcmpleu4(w.x, ob)) + __popc(__vcmpleu4(w.y, ob)) + __popc(__vcmpleu4(w.z, ob)) +
+                       __popc(__vcmpleu4(w.w, ob))) / 8 - 1;
+                const int k = P.A_col[p] * TSG_BS + (P.A_Colb[v] & 15);
+                av = P.A_Val[v];
+                b0 = P.B_rptr[k];
+                int b1 = P.B_rptr[k + 1];
+                if (!full)
+                {
+                    b0 += lower_bound_int(P.B_rcol + b0, b1 - b0, J0 * TSG_BS);
+                    b1 = b0 + lower_bound_int(P.B_rcol + b0, b1 - b0, J1 * TSG_BS);
+                }
+                len = b1 - b0;
+                if (len == 0)
+                    row = TSG_BS; // adds nothing to this segment
+            }
+            const unsigned peers = __match_any_sync(TSG_FULL_MASK, row);
+            er[h] = row;
+            eb[h] = b0;
+            el[h] = len;
+            ea[h] = av;
+            ek[h] = __popc(peers & ((1u << lane) - 1u));
+            if (row < TSG_BS && ek[h] == 0)
+                C.wc[j >> 5][row] = __popc(peers);
+        }
+        __syncthreads();
+        // warp 0: each row's entries before every slot, and the rows' starts
+        if (tid < 32)
+        {
+            int run = 0;
+            if (lane < TSG_BS)
+                for (int q = 0; q < SPA_CO_SLOTS; q++)
+                {
+                    const int t = C.wc[q][lane];
+                    C.wc[q][lane] = run;
+                    run += t;
+                }
+            int incl = run;
+#pragma unroll
+            for (int d = 1; d < TSG_BS; d <<= 1)
+            {
+                const int o = __shfl_up_sync(TSG_FULL_MASK, incl, d);
+                if (lane >= d)
+                    incl += o;
+            }
+            if (lane < TSG_BS)
+                C.rbeg[lane] = incl - run;
+            if (lane == TSG_BS - 1)
+                C.rbeg[TSG_BS] = incl;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int h = 0; h < 2; h++)
+            if (er[h] < TSG_BS)
+            {
+                const int j = tid + h * SPA_THREADS;
+                const int pos = C.rbeg[er[h]] + C.wc[j >> 5][er[h]] + ek[h];
+                C.bl[pos] = make_int2(eb[h], el[h]);
+                C.a[pos] = ea[h];
+            }
+        __syncthreads();
+        const int e1 = C.rbeg[r + 1];
+        for (int base = C.rbeg[r]; base < e1; base += SPA_STAGE)
+            spa_apply_stage<true>(P, S, cmr, rs, J0, J1, full, C.bl + base, C.a + base, min(SPA_STAGE, e1 - base), lane);
+        __syncthreads();
+    }
 }
 
 // The CTA computes C tiles [t0, t1) (one tile row, limits as above).  FLAT:
@@ -910,66 +1183,41 @@ __device__ __forceinline__ void step3_spa_segment(const ProdView &P, SpaSmem &S,
     __syncthreads();
     const int rs = S.rstart[r];
     const unsigned *cmr = S.cm + r * SPA_CMS;
-    SpaStage &G = S.stage[r];
     const int pa_beg = P.A_ptr[I], pa_end = P.A_ptr[I + 1];
-    for (int g = pa_beg; g < pa_end; g += 32)
+    if (FLAT)
     {
-        const int pa = g + lane;
-        unsigned mr = 0;
-        int st = 0, kb = 0;
-        if (pa < pa_end)
+        spa_coop_apply(P, S, pa_beg, pa_end, J0, J1, full, r, lane, tid, cmr, rs);
+    }
+    else
+    {
+        // warp r walks A's row r by itself, 32 A tiles at a time
+        SpaStage &G = S.stage[r];
+        for (int g = pa_beg; g < pa_end; g += 32)
         {
-            mr = P.A_mask[(long long)pa * TSG_BS + r];
-            st = P.A_tnnz[pa] + P.A_Ptr[(long long)pa * TSG_BS + r];
-            kb = P.A_col[pa] * TSG_BS;
-        }
-        const int cnt = __popc(mr);
-        int incl = cnt;
-#pragma unroll
-        for (int d = 1; d < 32; d <<= 1)
-        {
-            const int o = __shfl_up_sync(TSG_FULL_MASK, incl, d);
-            if (lane >= d)
-                incl += o;
-        }
-        const int total = __shfl_sync(TSG_FULL_MASK, incl, 31);
-        if (FLAT)
-        {
-            __syncwarp();
-            G.tpre[lane] = incl - cnt;
-        }
-        for (int base = 0; base < total; base += SPA_STAGE)
-        {
-            __syncwarp();
-            // stage A(r, k) entries [base, base + SPA_STAGE) of this group in
-            // column order: B row bounds and the A value
-            if (FLAT)
+            const int pa = g + lane;
+            unsigned mr = 0;
+            int st = 0, kb = 0;
+            if (pa < pa_end)
             {
-                // a lane per entry (A tiles holding many entries of the row
-                // would otherwise stage them one by one on a few lanes): the
-                // entry's tile is the last lane whose first entry is at or
-                // before it, its column the x-th set column of that tile's row
-                for (int h = 0; h < SPA_STAGE; h += 32)
-                {
-                    const int e = base + h + lane;
-                    int t, x;
-                    const int k = stage_entry(G.tpre, mr, kb, e, total, t, x);
-                    const int tst = __shfl_sync(TSG_FULL_MASK, st, t);
-                    if (e < total)
-                    {
-                        int b0 = P.B_rptr[k], b1 = P.B_rptr[k + 1];
-                        if (!full)
-                        {
-                            b0 += lower_bound_int(P.B_rcol + b0, b1 - b0, J0 * TSG_BS);
-                            b1 = b0 + lower_bound_int(P.B_rcol + b0, b1 - b0, J1 * TSG_BS);
-                        }
-                        G.bl[h + lane] = make_int2(b0, b1 - b0);
-                        G.a[h + lane] = P.A_Val[tst + x];
-                    }
-                }
+                mr = P.A_mask[(long long)pa * TSG_BS + r];
+                st = P.A_tnnz[pa] + P.A_Ptr[(long long)pa * TSG_BS + r];
+                kb = P.A_col[pa] * TSG_BS;
             }
-            else
+            const int cnt = __popc(mr);
+            int incl = cnt;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1)
             {
+                const int o = __shfl_up_sync(TSG_FULL_MASK, incl, d);
+                if (lane >= d)
+                    incl += o;
+            }
+            const int total = __shfl_sync(TSG_FULL_MASK, incl, 31);
+            for (int base = 0; base < total; base += SPA_STAGE)
+            {
+                __syncwarp();
+                // stage A(r, k) entries [base, base + SPA_STAGE) of this group in
+                // column order: B row bounds and the A value
                 unsigned bits = mr;
                 for (int x = 0; x < cnt; x++)
                 {
@@ -990,105 +1238,8 @@ __device__ __forceinline__ void step3_spa_segment(const ProdView &P, SpaSmem &S,
                         G.a[e] = P.A_Val[st + x];
                     }
                 }
-            }
-            __syncwarp();
-            const int ne = min(SPA_STAGE, total - base);
-            if (FLAT)
-            {
-                const int l0 = lane < ne ? G.bl[lane].y : 0;
-                const int l1 = lane + 32 < ne ? G.bl[lane + 32].y : 0;
-                int i0 = l0, i1 = l1;
-#pragma unroll
-                for (int d = 1; d < 32; d <<= 1)
-                {
-                    const int o0 = __shfl_up_sync(TSG_FULL_MASK, i0, d);
-                    const int o1 = __shfl_up_sync(TSG_FULL_MASK, i1, d);
-                    if (lane >= d)
-                    {
-                        i0 += o0;
-                        i1 += o1;
-                    }
-                }
-                const int h0 = __shfl_sync(TSG_FULL_MASK, i0, 31);
-                const int ni = h0 + __shfl_sync(TSG_FULL_MASK, i1, 31);
-                if (ni < SPA_FLAT * ne)
-                {
-                    // entry e becomes (its first B index - its first item, its first item)
-                    if (lane < ne)
-                        G.bl[lane] = make_int2(G.bl[lane].x - (i0 - l0), i0 - l0);
-                    if (lane + 32 < ne)
-                        G.bl[lane + 32] = make_int2(G.bl[lane + 32].x - (h0 + i1 - l1), h0 + i1 - l1);
-                    __syncwarp();
-                    int ent = 0;
-                    for (int ib = 0; ib < ni; ib += 32)
-                    {
-                        const int item = ib + lane;
-                        int pos = -1 - lane; // distinct keys for lanes without a slot
-                        double prod = 0.0;
-                        if (item < ni)
-                        {
-                            while (ent + 1 < ne && G.bl[ent + 1].y <= item)
-                                ent++;
-                            const int bi = G.bl[ent].x + item;
-                            const int p = spa_slot(S, cmr, rs, J0, J1, full, P.B_rcol[bi]);
-                            if (p >= 0)
-                            {
-                                pos = p;
-                                prod = __dmul_rn(G.a[ent], P.B_rval[bi]);
-                            }
-                        }
-                        const unsigned grp = __match_any_sync(TSG_FULL_MASK, pos);
-                        const bool lead = pos >= 0 && lane == __ffs(grp) - 1;
-                        const int rounds = __reduce_max_sync(TSG_FULL_MASK, pos >= 0 ? __popc(grp) : 0);
-                        double acc = lead ? S.acc[pos] : 0.0;
-                        unsigned gl = grp;
-                        for (int q = 0; q < rounds; q++)
-                        {
-                            const double v = __shfl_sync(TSG_FULL_MASK, prod, gl ? __ffs(gl) - 1 : lane);
-                            if (gl)
-                            {
-                                acc = __dadd_rn(acc, v);
-                                gl &= gl - 1;
-                            }
-                        }
-                        if (lead)
-                            S.acc[pos] = acc;
-                        __syncwarp();
-                    }
-                    continue;
-                }
-            }
-            int2 nb = G.bl[0];
-            int c_cur = -1;
-            double v_cur = 0.0;
-            if (lane < nb.y)
-            {
-                c_cur = P.B_rcol[nb.x + lane];
-                v_cur = P.B_rval[nb.x + lane];
-            }
-            for (int i = 0; i < ne; i++)
-            {
-                const int2 cb = nb;
-                int c_nxt = -1;
-                double v_nxt = 0.0;
-                if (i + 1 < ne)
-                {
-                    nb = G.bl[i + 1];
-                    if (lane < nb.y)
-                    {
-                        c_nxt = P.B_rcol[nb.x + lane];
-                        v_nxt = P.B_rval[nb.x + lane];
-                    }
-                }
-                const double a = G.a[i];
-                if (c_cur >= 0)
-                    spa_add(S, cmr, rs, J0, J1, full, c_cur, a, v_cur);
-                if (cb.y > 32) // B rows longer than a warp
-                    for (int e = cb.x + 32 + lane; e < cb.x + cb.y; e += 32)
-                        spa_add(S, cmr, rs, J0, J1, full, P.B_rcol[e], a, P.B_rval[e]);
                 __syncwarp();
-                c_cur = c_nxt;
-                v_cur = v_nxt;
+                spa_apply_stage<false>(P, S, cmr, rs, J0, J1, full, G.bl, G.a, min(SPA_STAGE, total - base), lane);
             }
         }
     }
