@@ -755,27 +755,53 @@ __device__ __forceinline__ void step3_rows_item(const ProdView &P, long long ite
 #define SPA_DENSE TSG_SPA_DENSE_DEFAULT
 #define SPA_FLAT 16  // B rows averaging fewer entries (inside a segment) have their products flattened
 
-// Staging a lane per A entry.  A warp's row entries are numbered across its
-// lanes' A tiles (lane order, then column order inside a tile); tpre[l] is
-// the first entry of lane l's tile, mr / kb that tile's row mask and first
-// column.  For entry e: the tile's lane t (the last lane whose first entry is
-// at or before e), the entry's index x inside the tile and its A column.
-// Every lane calls it (shuffles); lanes at or past total (the row's entries)
-// get t's values but must not use them.
-__device__ __forceinline__ int stage_entry(const int *tpre, unsigned mr, int kb, int e, int total, int &t, int &x)
+// entry of A value v in a chunk of an A tile row: its tile p (the last of tile0[0..nt)
+// starting at or before v, plus p0), its row (from the tile's row offsets)
+// and its column k
+__device__ __forceinline__ void a_entry(const ProdView &P, const int *tile0, int nt, int p0, bool ptr16, int v,
+                                        int &row, int &k)
 {
-    t = 0;
-#pragma unroll
-    for (int sz = 16; sz > 0; sz >>= 1)
-        if (t + sz < 32 && tpre[t + sz] <= e)
-            t += sz;
-    const unsigned tm = __shfl_sync(TSG_FULL_MASK, mr, t);
-    const int tkb = __shfl_sync(TSG_FULL_MASK, kb, t);
-    x = e - tpre[t];
-    unsigned cols = __brev(tm) >> 16; // bit c: column c of the tile's row
-    for (int q = e < total ? x : 0; q > 0; q--)
-        cols &= cols - 1;
-    return tkb + __ffs(cols) - 1;
+    int lo = 0, hi = nt - 1;
+    while (lo < hi)
+    {
+        const int mid = (lo + hi + 1) >> 1;
+        if (tile0[mid] <= v)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    const int p = p0 + lo, o = v - tile0[lo];
+    // the row: how many of the tile's row offsets 1..15 are at or below o
+    const unsigned char *rp = P.A_Ptr + (long long)p * TSG_BS;
+    uint4 w;
+    if (ptr16)
+        w = *reinterpret_cast<const uint4 *>(rp);
+    else
+    {
+        unsigned u[4];
+        for (int q = 0; q < 4; q++)
+            u[q] = rp[4 * q] | (rp[4 * q + 1] << 8) | (rp[4 * q + 2] << 16) | ((unsigned)rp[4 * q + 3] << 24);
+        w = make_uint4(u[0], u[1], u[2], u[3]);
+    }
+    const unsigned ob = (unsigned)o * 0x01010101u;
+    row = (__popc(__vcmpleu4(w.x, ob)) + __popc(__vcmpleu4(w.y, ob)) + __popc(__vcmpleu4(w.z, ob)) +
+           __popc(__vcmpleu4(w.w, ob))) / 8 - 1;
+    k = P.A_col[p] * TSG_BS + (P.A_Colb[v] & 15);
+}
+
+// the first A tile of tile row [pa_beg, pa_end) holding value offset c0
+__device__ __forceinline__ int a_tile_of(const ProdView &P, int pa_beg, int pa_end, int c0)
+{
+    int lo = pa_beg, hi = pa_end - 1;
+    while (lo < hi)
+    {
+        const int mid = (lo + hi + 1) >> 1;
+        if (P.A_tnnz[mid] <= c0)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
 }
 
 struct SpaStage
@@ -985,19 +1011,7 @@ __device__ __forceinline__ void spa_coop_apply(const ProdView &P, SpaSmem &S, in
     {
         const int ne = min(SPA_CO_CHUNK, v_end - c0);
         if (tid == 0)
-        {
-            // the last tile of the row starting at or before c0
-            int lo = pa_beg, hi = pa_end - 1;
-            while (lo < hi)
-            {
-                const int mid = (lo + hi + 1) >> 1;
-                if (P.A_tnnz[mid] <= c0)
-                    lo = mid;
-                else
-                    hi = mid - 1;
-            }
-            C.ptile = lo;
-        }
+            C.ptile = a_tile_of(P, pa_beg, pa_end, c0);
         for (int q = tid; q < SPA_CO_SLOTS * TSG_BS; q += SPA_THREADS)
             C.wc[q / TSG_BS][q % TSG_BS] = 0;
         __syncthreads();
@@ -1017,32 +1031,8 @@ __device__ __forceinline__ void spa_coop_apply(const ProdView &P, SpaSmem &S, in
             if (j < ne)
             {
                 const int v = c0 + j;
-                int lo = 0, hi = nt - 1;
-                while (lo < hi)
-                {
-                    const int mid = (lo + hi + 1) >> 1;
-                    if (C.tile0[mid] <= v)
-                        lo = mid;
-                    else
-                        hi = mid - 1;
-                }
-                const int p = p0 + lo, o = v - C.tile0[lo];
-                // the entry's row: the tile's row offsets 1..15 at or below o
-                const unsigned char *rp = P.A_Ptr + (long long)p * TSG_BS;
-                uint4 w;
-                if (ptr16)
-                    w = *reinterpret_cast<const uint4 *>(rp);
-                else
-                {
-                    unsigned u[4];
-                    for (int q = 0; q < 4; q++)
-                        u[q] = rp[4 * q] | (rp[4 * q + 1] << 8) | (rp[4 * q + 2] << 16) | ((unsigned)rp[4 * q + 3] << 24);
-                    w = make_uint4(u[0], u[1], u[2], u[3]);
-                }
-                const unsigned ob = (unsigned)o * 0x01010101u;
-                row = (__popc(__vcmpleu4(w.x, ob)) + __popc(__vcmpleu4(w.y, ob)) + __popc(__vcmpleu4(w.z, ob)) +
-                       __popc(__vcmpleu4(w.w, ob))) / 8 - 1;
-                const int k = P.A_col[p] * TSG_BS + (P.A_Colb[v] & 15);
+                int k;
+                a_entry(P, C.tile0, nt, p0, ptr16, v, row, k);
                 av = P.A_Val[v];
                 b0 = P.B_rptr[k];
                 int b1 = P.B_rptr[k + 1];
@@ -1289,19 +1279,54 @@ __device__ __forceinline__ void step3_spa_segment(const ProdView &P, SpaSmem &S,
 #define SP2_MS (SP2_SEGT + 1) // row stride of the [row][tile] mask words (a tile's rows in distinct banks)
 #define SP2_WIN 4096
 
-struct Spa2Stage
+#define SP2_CO_CHUNK 1024 // A entries the CTA stages per pass
+
+struct Spa2Coop
 {
-    int bs[SPA_STAGE];
-    int off[SPA_STAGE + 1];
-    int tpre[32]; // first entry of each lane's A tile
+    int bs[SP2_CO_CHUNK];          // B row start (cut to the segment) of each staged A entry
+    int off[SP2_CO_CHUNK + 1];     // its first item (B entry) in the chunk; off[n] = items
+    unsigned char row[SP2_CO_CHUNK];
+    int tile0[SP2_CO_CHUNK + 1];   // value offset of each A tile the chunk can touch
+    int wsum[SPA_WARPS];
+    int ptile;                     // the chunk's first A tile
 };
 
 struct Spa2Smem
 {
     unsigned m[TSG_BS * SP2_MS]; // [row][tile] mask words
     unsigned short map[SP2_WIN];
-    Spa2Stage stage[SPA_WARPS];
+    Spa2Coop co;
 };
+
+// exclusive prefix of v over the CTA's SPA_THREADS threads (thread order)
+// and the total; wsum holds SPA_WARPS ints
+__device__ __forceinline__ int block_excl_scan(int v, int *wsum, int *total, int tid, int lane)
+{
+    int incl = v;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1)
+    {
+        const int o = __shfl_up_sync(TSG_FULL_MASK, incl, d);
+        if (lane >= d)
+            incl += o;
+    }
+    const int warp = tid >> 5;
+    if (lane == 31)
+        wsum[warp] = incl;
+    __syncthreads();
+    int base = 0, tot = 0;
+#pragma unroll
+    for (int w = 0; w < SPA_WARPS; w++)
+    {
+        const int x = wsum[w];
+        base += w < warp ? x : 0;
+        tot += x;
+    }
+    __syncthreads();
+    *total = tot;
+    return base + incl - v;
+}
+
 
 // The CTA (SPA_THREADS threads) computes the masks of C tiles [t0, t1).
 __device__ __forceinline__ void step2_spa_segment(const ProdView &P, Spa2Smem &S, int t0, int t1, int *s_bins)
@@ -1325,96 +1350,87 @@ __device__ __forceinline__ void step2_spa_segment(const ProdView &P, Spa2Smem &S
             S.map[w] = (unsigned short)jl;
     }
     __syncthreads();
-    Spa2Stage &G = S.stage[r];
+    // A's entries of the tile row, SP2_CO_CHUNK at a time: every thread
+    // stages entries (row, B's row cut to the segment's columns), then the
+    // chunk's B entries are split evenly over the warps, each setting its
+    // entry's column bit in the row's mask word (an OR: any order)
+    Spa2Coop &C = S.co;
+    const bool ptr16 = (reinterpret_cast<unsigned long long>(P.A_Ptr) & 15ULL) == 0;
     const int pa_beg = P.A_ptr[I], pa_end = P.A_ptr[I + 1];
-    for (int g = pa_beg; g < pa_end; g += 32)
+    const int v_beg = P.A_tnnz[pa_beg], v_end = P.A_tnnz[pa_end];
+    for (int c0 = v_beg; c0 < v_end; c0 += SP2_CO_CHUNK)
     {
-        const int pa = g + lane;
-        unsigned mr = 0;
-        int kb = 0;
-        if (pa < pa_end)
-        {
-            mr = P.A_mask[(long long)pa * TSG_BS + r];
-            kb = P.A_col[pa] * TSG_BS;
-        }
-        const int cnt = __popc(mr);
-        int incl = cnt;
+        const int ne = min(SP2_CO_CHUNK, v_end - c0);
+        if (tid == 0)
+            C.ptile = a_tile_of(P, pa_beg, pa_end, c0);
+        __syncthreads();
+        const int p0 = C.ptile;
+        const int ntl = min(ne, pa_end - p0); // tiles that can hold the chunk's entries
+        for (int q = tid; q <= ntl; q += SPA_THREADS)
+            C.tile0[q] = P.A_tnnz[p0 + q];
+        __syncthreads();
+        int len[2];
 #pragma unroll
-        for (int d = 1; d < 32; d <<= 1)
+        for (int h = 0; h < 2; h++)
         {
-            const int o = __shfl_up_sync(TSG_FULL_MASK, incl, d);
-            if (lane >= d)
-                incl += o;
+            const int j = tid + h * SPA_THREADS;
+            len[h] = 0;
+            if (j < ne)
+            {
+                int row, k;
+                a_entry(P, C.tile0, ntl, p0, ptr16, c0 + j, row, k);
+                int b0 = P.B_rptr[k], b1 = P.B_rptr[k + 1];
+                if (!full)
+                {
+                    b0 += lower_bound_int(P.B_rcol + b0, b1 - b0, J0 * TSG_BS);
+                    b1 = b0 + lower_bound_int(P.B_rcol + b0, b1 - b0, J1 * TSG_BS);
+                }
+                C.bs[j] = b0;
+                C.row[j] = (unsigned char)row;
+                len[h] = b1 - b0;
+            }
         }
-        const int total = __shfl_sync(TSG_FULL_MASK, incl, 31);
-        __syncwarp();
-        G.tpre[lane] = incl - cnt;
-        for (int base = 0; base < total; base += SPA_STAGE)
+        int tot0, tot1;
+        const int x0 = block_excl_scan(len[0], C.wsum, &tot0, tid, lane);
+        const int x1 = block_excl_scan(len[1], C.wsum, &tot1, tid, lane);
+        if (tid < ne)
+            C.off[tid] = x0;
+        if (tid + SPA_THREADS < ne)
+            C.off[tid + SPA_THREADS] = tot0 + x1;
+        if (tid == 0)
+            C.off[ne] = tot0 + tot1;
+        __syncthreads();
+        const int items = tot0 + tot1;
+        const int per = (items + SPA_WARPS - 1) / SPA_WARPS;
+        const int w0 = r * per, w1 = min(items, w0 + per);
+        if (w0 + lane < w1)
         {
-            __syncwarp();
-            // a lane per entry: the entry's tile is the last lane whose first
-            // entry is at or before it, its column the x-th set column of that
-            // tile's row (A tiles holding many entries of the row would
-            // otherwise stage them one by one on a few lanes)
-            for (int h = 0; h < SPA_STAGE; h += 32)
+            // the entry of this lane's first item: the last entry starting at or before it
+            const int first = w0 + lane;
+            int lo = 0, hi = ne - 1;
+            while (lo < hi)
             {
-                const int e = base + h + lane;
-                int t, x;
-                const int k = stage_entry(G.tpre, mr, kb, e, total, t, x);
-                if (e < total)
-                {
-                    int b0 = P.B_rptr[k], b1 = P.B_rptr[k + 1];
-                    if (!full)
-                    {
-                        b0 += lower_bound_int(P.B_rcol + b0, b1 - b0, J0 * TSG_BS);
-                        b1 = b0 + lower_bound_int(P.B_rcol + b0, b1 - b0, J1 * TSG_BS);
-                    }
-                    G.bs[h + lane] = b0;
-                    G.off[h + lane] = b1 - b0;
-                }
+                const int mid = (lo + hi + 1) >> 1;
+                if (C.off[mid] <= first)
+                    lo = mid;
+                else
+                    hi = mid - 1;
             }
-            __syncwarp();
-            const int ne = min(SPA_STAGE, total - base);
+            int ent = lo;
+            for (int item = first; item < w1; item += 32)
             {
-                const int l0 = lane < ne ? G.off[lane] : 0;
-                const int l1 = lane + 32 < ne ? G.off[lane + 32] : 0;
-                int i0 = l0, i1 = l1;
-#pragma unroll
-                for (int d = 1; d < 32; d <<= 1)
-                {
-                    const int o0 = __shfl_up_sync(TSG_FULL_MASK, i0, d);
-                    const int o1 = __shfl_up_sync(TSG_FULL_MASK, i1, d);
-                    if (lane >= d)
-                    {
-                        i0 += o0;
-                        i1 += o1;
-                    }
-                }
-                const int t0s = __shfl_sync(TSG_FULL_MASK, i0, 31);
-                __syncwarp();
-                if (lane < ne)
-                    G.off[lane] = i0 - l0;
-                if (lane + 32 < ne)
-                    G.off[lane + 32] = t0s + i1 - l1;
-                if (lane == 31)
-                    G.off[ne] = t0s + i1;
-                __syncwarp();
-            }
-            const int ni = G.off[ne];
-            int ent = 0;
-            for (int item = lane; item < ni; item += 32)
-            {
-                while (G.off[ent + 1] <= item)
+                while (C.off[ent + 1] <= item)
                     ent++;
-                const int col = P.B_rcol[G.bs[ent] + (item - G.off[ent])];
+                const int col = P.B_rcol[C.bs[ent] + (item - C.off[ent])];
                 const int J = col >> 4;
                 if (J < J0 || J - J0 >= win)
                     continue;
                 const int slot = S.map[J - J0];
                 if (slot < nt)
-                    atomicOr(&S.m[r * SP2_MS + slot], 1u << (15 - (col & 15)));
+                    atomicOr(&S.m[C.row[ent] * SP2_MS + slot], 1u << (15 - (col & 15)));
             }
         }
+        __syncthreads();
     }
     __syncthreads();
     // half-warp per C tile: row offsets, masks, tile count, bin
