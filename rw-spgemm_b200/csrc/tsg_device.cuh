@@ -92,15 +92,66 @@ __device__ __forceinline__ int step1_row(const ProdView &P, int i, unsigned int 
             for (int w = lane; w < nw; w += 32)
                 bm[w] = 0;
             __syncwarp();
-            for (int pa = a0; pa < a1; pa++)
+            // A's tiles 32 at a time, a lane each; their B tile rows' tiles
+            // are either flattened over the lanes (short rows) or walked one
+            // A tile after another, a lane per B tile
+            for (int g = a0; g < a1; g += 32)
             {
-                const int k = P.A_col[pa];
-                const int b0 = P.B_ptr[k], b1 = P.B_ptr[k + 1];
-                for (int pb = b0 + lane; pb < b1; pb += 32)
+                const int cnt = min(32, a1 - g);
+                int b0 = 0, len = 0;
+                if (lane < cnt)
                 {
-                    const int j = P.B_col[pb];
-                    if (j >= c0 && j < c1)
-                        atomicOr(&bm[(j - c0) >> 5], 1u << ((j - c0) & 31));
+                    const int k = P.A_col[g + lane];
+                    b0 = P.B_ptr[k];
+                    len = P.B_ptr[k + 1] - b0;
+                }
+                int incl = len;
+#pragma unroll
+                for (int d = 1; d < 32; d <<= 1)
+                {
+                    const int o = __shfl_up_sync(TSG_FULL_MASK, incl, d);
+                    if (lane >= d)
+                        incl += o;
+                }
+                const int total = __shfl_sync(TSG_FULL_MASK, incl, 31);
+                const int pre = incl - len;
+                if (total < 16 * cnt)
+                {
+                    for (int base = 0; base < total; base += 32)
+                    {
+                        const int item = base + lane;
+                        // the A tile of this pair: the last one whose first pair is at or before it
+                        int t = 0;
+#pragma unroll
+                        for (int sz = 16; sz > 0; sz >>= 1)
+                        {
+                            const int pc = __shfl_sync(TSG_FULL_MASK, pre, t + sz);
+                            if (t + sz < cnt && pc <= item)
+                                t += sz;
+                        }
+                        const int ob = __shfl_sync(TSG_FULL_MASK, b0, t);
+                        const int op = __shfl_sync(TSG_FULL_MASK, pre, t);
+                        if (item < total)
+                        {
+                            const int j = P.B_col[ob + item - op];
+                            if (j >= c0 && j < c1)
+                                atomicOr(&bm[(j - c0) >> 5], 1u << ((j - c0) & 31));
+                        }
+                    }
+                }
+                else
+                {
+                    for (int t = 0; t < cnt; t++)
+                    {
+                        const int tb = __shfl_sync(TSG_FULL_MASK, b0, t);
+                        const int tl = __shfl_sync(TSG_FULL_MASK, len, t);
+                        for (int pb = tb + lane; pb < tb + tl; pb += 32)
+                        {
+                            const int j = P.B_col[pb];
+                            if (j >= c0 && j < c1)
+                                atomicOr(&bm[(j - c0) >> 5], 1u << ((j - c0) & 31));
+                        }
+                    }
                 }
             }
             __syncwarp();

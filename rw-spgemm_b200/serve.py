@@ -27,6 +27,7 @@ import collections
 import ctypes
 import itertools
 import math
+import os
 import threading
 import time
 from concurrent.futures import Future
@@ -259,6 +260,9 @@ class SpGEMMServer:
 
     def close(self):
         self.stop()
+        if getattr(self, "_pool", None) is not None:
+            self._pool.shutdown()
+            self._pool = None
         for t in self.cache.tiles.values():
             t.free()
         self.cache.tiles.clear()
@@ -438,13 +442,31 @@ class SpGEMMServer:
                        dbuf[ci_off:ci_off + 4 * nnz].view(torch.int32), dbuf[v_off:v_off + 8 * nnz].view(torch.float64))
                 self._complete(job, nnz, res)
         else:
+            # the results leave the reusable staging buffer for arrays of
+            # their own; the copies (and the first touch of the new pages)
+            # run on the host pool's threads, in pieces of at most 16 MB
             raw = slot.staging.numpy()
+            outs, pieces = [], []
             for job, C, m, n, nnz, v_off, rp_off, ci_off in layout:
-                res = (m, n, raw[rp_off:rp_off + 4 * (m + 1)].view(np.int32).copy(),
-                       raw[ci_off:ci_off + 4 * nnz].view(np.int32).copy(), raw[v_off:v_off + 8 * nnz].view(np.float64).copy())
+                arrs = []
+                for off, count, dt in ((rp_off, m + 1, np.int32), (ci_off, nnz, np.int32), (v_off, nnz, np.float64)):
+                    src = raw[off:off + count * np.dtype(dt).itemsize].view(dt)
+                    dst = np.empty(count, dt)
+                    step = max(1, (16 << 20) // np.dtype(dt).itemsize)
+                    pieces += [(dst, src, q, min(count, q + step)) for q in range(0, count, step)]
+                    arrs.append(dst)
+                outs.append((job, nnz, (m, n, *arrs)))
+            list(self._host_pool().map(lambda t: np.copyto(t[0][t[2]:t[3]], t[1][t[2]:t[3]]), pieces))
+            for job, nnz, res in outs:
                 self._complete(job, nnz, res)
         slot.pending = None
         self._release(slot)
+
+    def _host_pool(self):
+        if getattr(self, "_pool", None) is None:
+            from concurrent.futures import ThreadPoolExecutor
+            self._pool = ThreadPoolExecutor(max_workers=max(1, min(16, (os.cpu_count() or 2) // 2)))
+        return self._pool
 
     def _complete(self, job, nnz, res):
         job.t_done = time.perf_counter()
