@@ -1865,6 +1865,11 @@ __device__ __forceinline__ void step3_hyper_row(const ProdView &P, HypSmem &S, i
 // further into segments within the SPA limits.  A hypersparse row belongs
 // whole to the block holding its first tile.
 #define SPA_BLK 256
+// the numeric step's block for products whose C tiles average at least
+// SPA_BLK_NARROW_VALUES values (wide rows of skewed products such as R-MAT):
+// twice the blocks, so a hub row's segments spread over more CTAs
+#define SPA_BLK_NARROW 128
+#define SPA_BLK_NARROW_VALUES 4
 
 // calls piece(I, t0, t1) for the pieces [t0, t1) owned by block [tb, te),
 // rows longer than CH tiles being cut into CH-tile chunks.  [tb, te) may be a
@@ -1902,6 +1907,7 @@ __device__ __forceinline__ void spa_block_pieces(const ProdView &P, int tb, int 
 // owns has no work, nor have the row's following blocks before the one
 // holding the row's end: the claiming thread raises the block counter ctr
 // (blocks of this product numbered from base) past them.
+template <int BLK = SPA_BLK>
 __device__ __forceinline__ void spa_skip_hyper(const ProdView &P, const int *__restrict__ kind, int tb,
                                                unsigned *ctr, long long base)
 {
@@ -1910,8 +1916,8 @@ __device__ __forceinline__ void spa_skip_hyper(const ProdView &P, const int *__r
     const int I = P.C_row[tb];
     if (kind[I] != 2 || P.C_ptr[I] >= tb)
         return;
-    const long long next = base + P.C_ptr[I + 1] / SPA_BLK;
-    if (next > base + tb / SPA_BLK + 1)
+    const long long next = base + P.C_ptr[I + 1] / BLK;
+    if (next > base + tb / BLK + 1)
         atomicMax(ctr, (unsigned)next);
 }
 
@@ -1921,11 +1927,11 @@ static_assert(sizeof(HypSmem) <= sizeof(SpaSmem) && sizeof(HypSmem) <= sizeof(Sp
 
 // only (may be null): only the tile rows I with only[I] != 0 (the rows the
 // staged numeric step left).
-template <bool FLAT>
+template <bool FLAT, int BLK = SPA_BLK>
 __device__ __forceinline__ void step3_spa_block(const ProdView &P, SpaSmem &S, int tb, int te,
                                                 const int *__restrict__ kind, const int *__restrict__ only = nullptr)
 {
-    spa_block_pieces<SPA_BLK>(P, tb, te, [&](int I, int ps, int pe) {
+    spa_block_pieces<BLK>(P, tb, te, [&](int I, int ps, int pe) {
         if (only && !only[I])
             return;
         if (kind && kind[I] == 2)

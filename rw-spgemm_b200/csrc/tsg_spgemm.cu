@@ -209,7 +209,7 @@ __global__ void __launch_bounds__(128) k_step3_rows(ProdView P)
 // the tile rows [row0, row1) are done -- the blocks holding their tiles, each
 // clamped to those tiles (a separate instantiation keeps the whole-product
 // form's registers).
-template <bool FLAT, bool RANGED>
+template <bool FLAT, bool RANGED, int BLK>
 __global__ void __launch_bounds__(SPA_THREADS, 3) k_step3_spa(ProdView P, const int *__restrict__ kind, int row0,
                                                               int row1, unsigned *__restrict__ ctr)
 {
@@ -220,7 +220,7 @@ __global__ void __launch_bounds__(SPA_THREADS, 3) k_step3_spa(ProdView P, const 
     if (threadIdx.x == 0)
         nxt = atomicAdd(ctr, 1u);
     const int t_beg = RANGED ? P.C_ptr[row0] : 0, t_end = RANGED ? P.C_ptr[row1] : P.numC;
-    const long long blk0 = t_beg / SPA_BLK;
+    const long long blk0 = t_beg / BLK;
     for (;;)
     {
         __syncthreads();
@@ -230,13 +230,13 @@ __global__ void __launch_bounds__(SPA_THREADS, 3) k_step3_spa(ProdView P, const 
             nxt = atomicAdd(ctr, 1u);
         }
         __syncthreads();
-        const long long tb = (blk0 + s_blk) * SPA_BLK;
+        const long long tb = (blk0 + s_blk) * BLK;
         if (tb >= t_end)
             break;
         if (threadIdx.x == 0)
-            spa_skip_hyper(P, kind, (int)tb, ctr, -blk0);
+            spa_skip_hyper<BLK>(P, kind, (int)tb, ctr, -blk0);
         // the block, clamped to the tiles of rows [row0, row1)
-        step3_spa_block<FLAT>(P, S, max((int)tb, t_beg), (int)min((long long)t_end, tb + SPA_BLK), kind);
+        step3_spa_block<FLAT, BLK>(P, S, max((int)tb, t_beg), (int)min((long long)t_end, tb + BLK), kind);
     }
 }
 
@@ -408,17 +408,17 @@ static int launch_step2_spa(tsg_context *ctx, const ProdView &P, const int *d_wi
     return TSG_OK;
 }
 
-template <bool FLAT, bool RANGED>
+template <bool FLAT, bool RANGED, int BLK = SPA_BLK>
 static int launch_step3_spa(tsg_context *ctx, const ProdView &P0, const int *d_kind, int row0, int row1)
 {
     ProdView P = P0;
     P.status = ctx->d_status;
     unsigned *ctr = nullptr, grid = 0;
     const int smem = (int)sizeof(SpaSmem);
-    TSG_TRY(spa_grid(ctx, k_step3_spa<FLAT, RANGED>, smem, &grid));
+    TSG_TRY(spa_grid(ctx, k_step3_spa<FLAT, RANGED, BLK>, smem, &grid));
     TSG_TRY(tsg_alloc(ctx, &ctr, 1));
     TSG_CUDA(cudaMemsetAsync(ctr, 0, sizeof(unsigned), ctx->stream));
-    k_step3_spa<FLAT, RANGED><<<grid, SPA_THREADS, smem, ctx->stream>>>(P, d_kind, row0, row1, ctr);
+    k_step3_spa<FLAT, RANGED, BLK><<<grid, SPA_THREADS, smem, ctx->stream>>>(P, d_kind, row0, row1, ctr);
     TSG_LAUNCH_CHECK();
     tsg_release(ctx, ctr);
     return TSG_OK;
@@ -471,6 +471,9 @@ static int launch_step3_spa_rows(tsg_context *ctx, const ProdView &P, long long 
     const bool flat = spa_wants_flat(P.browB, P.numC, nnzC, P.tilemA);
     const bool whole = row0 == 0 && row1 == P.tilemA;
     ctx->last_step3 = flat ? TSG_STEP3_FLAT : P.padded ? TSG_STEP3_STAGED : TSG_STEP3_SPA;
+    if (flat && nnzC >= (long long)SPA_BLK_NARROW_VALUES * P.numC)
+        return whole ? launch_step3_spa<true, false, SPA_BLK_NARROW>(ctx, P, d_kind, 0, 0)
+                     : launch_step3_spa<true, true, SPA_BLK_NARROW>(ctx, P, d_kind, row0, row1);
     if (flat)
         return whole ? launch_step3_spa<true, false>(ctx, P, d_kind, 0, 0)
                      : launch_step3_spa<true, true>(ctx, P, d_kind, row0, row1);
