@@ -1,5 +1,5 @@
 """The selector's host logic: the model's pick when the matrix lies inside
-the training range, the exhaustive search (also the judge of the model's
+the training range, the exhaustive search (also the yardstick of the model's
 regret) when there is no model or the features fall outside it; regret is
 the relative slowdown against the best configuration.  Features, timings and
 the network's forward pass are stand-ins here; the GPU tests run them."""
