@@ -248,3 +248,49 @@ def test_skew_class_of_a_matrix(serve_mod):
     hub = (4, 4, np.array([0, 13, 14, 15, 16]), np.zeros(16, np.int32), np.ones(16))
     empty = (3, 3, np.zeros(4, np.int64), np.zeros(0, np.int32), np.zeros(0))
     assert serve.skew_class(flat) == 0 and serve.skew_class(hub) == 1 and serve.skew_class(empty) == 0
+
+
+def test_host_delivery_copies_every_result_out_of_the_staging_buffer(serve_mod, monkeypatch):
+    """Host delivery hands each job numpy arrays of its own, copied out of
+    the slot's reusable staging buffer in pieces on the host pool's threads
+    (pieces of at most 16 MB: the values of the second job span several)."""
+    import torch
+    import numpy as np
+    srv = make_server(serve_mod, monkeypatch, 10_000, 1e9, {}, {})
+    srv.deliver = "host"
+    rng = np.random.default_rng(4)
+    shapes = [(5, 3, 7), (1000, 900, 5_000_000), (0, 4, 0)]     # (m, n, nnz)
+    layout, total, want = [], 0, []
+    jobs = []
+    for jid, (m, n, nnz) in enumerate(shapes):
+        job = serve_mod.Job(jid, "AB", "a", "b")
+        jobs.append(job)
+        v_off = total
+        rp_off = v_off + 8 * nnz
+        ci_off = rp_off + 4 * (m + 1)
+        total = (ci_off + 4 * nnz + 7) & ~7
+        layout.append((job, None, m, n, nnz, v_off, rp_off, ci_off))
+        want.append((np.arange(m + 1, dtype=np.int32) * 3, rng.integers(0, 1 << 30, nnz).astype(np.int32),
+                     rng.standard_normal(nnz)))
+    staging = torch.zeros(total + 8, dtype=torch.uint8)
+    raw = staging.numpy()
+    for (job, _, m, n, nnz, v_off, rp_off, ci_off), (rp, ci, v) in zip(layout, want):
+        raw[rp_off:rp_off + rp.nbytes] = rp.view(np.uint8)
+        raw[ci_off:ci_off + ci.nbytes] = ci.view(np.uint8)
+        raw[v_off:v_off + v.nbytes] = v.view(np.uint8)
+
+    class Closing:
+        def close(self):
+            pass
+    slot = FakeSlot()
+    slot.staging, slot.pending, slot.batch, slot.jobs = staging, (layout, None), Closing(), jobs
+    srv._deliver(slot)
+    raw[:] = 0                                              # the staging buffer is reused by the next batch
+    for job, (m, n, nnz), (rp, ci, v) in zip(jobs, shapes, want):
+        got = job.future.result(timeout=0)
+        assert got[0] == m and got[1] == n and job.result_nnz == nnz
+        np.testing.assert_array_equal(got[2], rp)
+        np.testing.assert_array_equal(got[3], ci)
+        assert np.array_equal(got[4].view(np.uint64), v.view(np.uint64))
+    assert slot.pending is None and slot.batch is None
+    srv._pool.shutdown()
