@@ -58,6 +58,8 @@ CASES = {
     "stencil27_40_permuted": ("active_symmetric", lambda g: g.permute_symmetric(
         g.stencil_27pt_3d(40), g.random_symmetric_permutation(64000, seed=7))),
     "poisson_60000": ("active_symmetric", lambda g: _sym(g.random_poisson(60000, 60000, 4.0, seed=5))),
+    # the guard: a band the reverse Cuthill-McKee order does not improve
+    "banded_8000_no_gain": ("conservative_identity", lambda g: g.banded(8000, 300, seed=1)),
 }
 
 
@@ -73,6 +75,9 @@ def test_symmetric_plan_equals_the_references(ref, gen, name):
     n = M[0]
     window = 0 if mode == "identity_narrow_tiles" else (32 if n <= 50000 else 64)
     assert got["local_refine_window"] == window
+    if mode == "conservative_identity":
+        assert got["risk_reason"] == "small_no_tile_gain" and got["guard_degraded_to_identity"] == 1
+        np.testing.assert_array_equal(got["row_perm"], np.arange(n))
     for ax in ("row_perm", "inner_perm", "col_perm"):
         assert sorted(got[ax].tolist()) == list(range(n))
     np.testing.assert_array_equal(got["row_perm"], got["col_perm"])     # one order on every axis
